@@ -1,0 +1,91 @@
+"""Loads libalgebra_linear_gpu.so and declares the C ABI of
+include/algebra_linear_gpu.h for ctypes.
+
+The library is the product; there is no CPU fallback. If the shared object is
+missing, every import of this module raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "libalgebra_linear_gpu.so"
+
+# status codes (include/algebra_linear_gpu.h)
+OK = 0
+SINGULAR = 1
+BAD_SHAPE = 2
+CONVERGENCE = 3
+NOT_IMPLEMENTED = 4
+SP_BAD_SHAPE = 100
+SP_INVALID_STRUCTURE = 101
+SP_UNSORTED_ROWS = 102
+SP_DUPLICATE_ENTRY = 103
+SP_SINGULAR = 104
+SP_INDEX_OVERFLOW = 105
+SP_STRUCTURE_MISMATCH = 106
+SP_NOT_FINITE = 107
+SP_NOT_FACTORIZED = 108
+CUDA_ERROR = 200
+OUT_OF_DEVICE_MEMORY = 201
+TIMEOUT = 202
+INVALID_ARGUMENT = 203
+NO_DEVICE = 204
+
+UPDATE_EXACT = 0
+UPDATE_FMA = 1
+
+_P = C.c_void_p
+_SZ = C.c_size_t
+_I = C.c_int
+_D = C.POINTER(C.c_double)
+_SZP = C.POINTER(C.c_size_t)
+
+# (name, restype, argtypes) for every declared entry point
+SIGNATURES = [
+    ("alg_status_string", C.c_char_p, [_I]),
+    ("alg_version", C.c_char_p, []),
+    ("alg_kernel_launch_count", C.c_ulonglong, []),
+    ("alg_dgetrf", _I, [_P, _SZ, _P, _P]),
+    ("alg_dgetrf_rect", _I, [_P, _SZ, _SZ, _P]),
+    ("alg_dgesv", _I, [_P, _P, _SZ]),
+    ("alg_dgesv_nrhs", _I, [_P, _P, _SZ, _SZ]),
+    ("alg_dgesv_ex", _I, [_I, _P, _P, _SZ, _SZ, _P]),
+    ("alg_ctx_create", _I, [_P, C.POINTER(_P)]),
+    ("alg_ctx_destroy", None, [_P]),
+    ("alg_ctx_set_stream", _I, [_P, _P]),
+    ("alg_dgetrf_dev", _I, [_P, _I, _P, _I, _I, _P, _P]),
+    ("alg_dgetrs_dev", _I, [_P, _P, _I, _I, _P, _P, _I, _I]),
+    ("alg_dgesv_dev", _I, [_P, _I, _P, _I, _I, _P, _I, _I, _P]),
+]
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Returns the loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH.name} is missing: build it with `python -m algebra_linear_b200.build`"
+            )
+        lib = C.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def status_string(code: int) -> str:
+    return load().alg_status_string(code).decode()
+
+
+def ptr(arr) -> int:
+    """Address of a numpy array's data or a torch tensor's storage."""
+    if hasattr(arr, "data_ptr"):
+        return arr.data_ptr()
+    return arr.ctypes.data

@@ -1,0 +1,63 @@
+// The library context: device, stream, status block and a growable
+// workspace arena. One context is used by one thread at a time.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+struct alg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 0;
+  alg::DevStatus* d_status = nullptr;   // device status block
+  alg::DevStatus* h_status = nullptr;   // pinned host mirror
+  // Arena of named device buffers, grown on demand and reused across calls.
+  struct Buf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+  };
+  std::vector<Buf> bufs;
+  std::mutex mu;  // serialises the shared per-device contexts of the drop-ins
+};
+
+namespace alg {
+
+// Named workspace slots of the arena.
+enum WsSlot : int {
+  WS_A = 0,       // matrix copy (host drop-ins)
+  WS_B,           // right-hand sides (host drop-ins)
+  WS_X,           // solve scratch
+  WS_IPIV,
+  WS_PERM,
+  WS_LAB,
+  WS_PERM_TMP,
+  WS_A32,         // low-precision working matrix (mixed form)
+  WS_R,           // residual (mixed form)
+  WS_KRYLOV,      // GMRES basis (mixed form)
+  WS_PARTIAL,     // reduction partials
+  WS_MISC,
+  WS_COUNT
+};
+
+// Returns a device buffer of at least `bytes` for `slot`, growing it if needed.
+int ws_get(alg_ctx* ctx, int slot, size_t bytes, void** out);
+
+// Shared per-device context used by the host-pointer drop-ins (created on first
+// use; lives until process exit). Locks ctx->mu; the caller unlocks via guard.
+int default_ctx(alg_ctx** out);
+
+// Clears the status block (singular_col = INT_MAX, flags = 0) on the stream.
+int status_reset(alg_ctx* ctx);
+// Copies the status block to the host mirror and synchronises the stream.
+int status_fetch(alg_ctx* ctx);
+
+int ctx_init(alg_ctx* ctx, cudaStream_t stream);
+void ctx_release(alg_ctx* ctx);
+
+}  // namespace alg

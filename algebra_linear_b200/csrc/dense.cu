@@ -1,0 +1,390 @@
+// Host-side schedule of the blocked right-looking LU (sm_100a) and the
+// dense C entry points.
+//
+// Schedule for an m x nc matrix (m >= nc), block-panel width nb, leaf nbl:
+//   for each block-panel [k0, k0+kb):
+//     for each leaf [c0, c0+w) inside it:
+//       K1 panel_cluster_kernel   : factor rows [c0, m) of the leaf columns,
+//                                   swap the block-panel's other columns
+//       K3 trsm (w rows)          : U of the leaf's rows, block-panel columns right of it
+//       K4 gemm (k = w)           : rows below, block-panel columns right of the leaf
+//     K2 laswp_outside            : the block-panel's interchanges, all other columns
+//     K3 trsm (kb rows)           : U12 = L11^{-1} A12
+//     K4 gemm (k = kb)            : A22 -= L21 U12
+// Every entry sees its rank-1 terms in increasing pivot order, so with the
+// EXACT arithmetic the result equals the reference's kij loop
+// (src/lapack/mod.rs:112-163) bit for bit.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "dense.cuh"
+#include "dense_kernels.cuh"
+
+namespace alg {
+
+LuPlan default_plan(int n, int elem_bytes) {
+  LuPlan p;
+  p.nb = 64;
+  p.nbl = elem_bytes == 8 ? 16 : 32;
+  (void)n;
+  return p;
+}
+
+namespace {
+
+template <typename T, bool EXACT>
+int launch_panel(alg_ctx* ctx, const PanelArgs<T>& args) {
+  const int m = args.n - args.c0;
+  constexpr size_t kMaxSmem = 220 * 1024;
+  int C = 1;
+  size_t smem = 0;
+  for (C = 1; C <= 16; C *= 2) {
+    const int R = (m + C - 1) / C;
+    smem = panel_smem_bytes<T>(R, args.w);
+    if (smem <= kMaxSmem) break;
+  }
+  if (C > 16) return ALG_BAD_SHAPE;  // panel too tall for one cluster
+  static bool configured = false;
+  if (!configured) {
+    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, EXACT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem + 1024));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, EXACT>,
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    configured = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(kPanelThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ALG_CUDA_TRY(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<T, EXACT>, args));
+  count_launches();
+  return ALG_OK;
+}
+
+template <typename T, bool EXACT>
+int launch_trsm(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
+  if (ce <= cb || kb <= 1) return ALG_OK;
+  const size_t smem = sizeof(T) * ((size_t)kb * kb + (size_t)kb * kTrsmCols);
+  static bool configured = false;
+  if (!configured) {
+    ALG_CUDA_TRY(cudaFuncSetAttribute(trsm_lower_unit_kernel<T, EXACT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    configured = true;
+  }
+  const int grid = (ce - cb + kTrsmCols - 1) / kTrsmCols;
+  trsm_lower_unit_kernel<T, EXACT><<<grid, kTrsmThreads, smem, ctx->stream>>>(a, lda, r0, kb, cb, ce);
+    count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
+}  // namespace
+
+template <typename T, bool EXACT>
+int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T* B, int ldb,
+                 T* C, int ldc) {
+  if (M <= 0 || N <= 0 || K <= 0) return ALG_OK;
+  dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + kGemmBN - 1) / kGemmBN);
+  gemm_sub_kernel<T, EXACT><<<grid, kGemmThreads, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
+template <typename T, bool EXACT>
+int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* perm,
+                  const LuPlan& plan) {
+  if (m < nc || nc < 0 || lda < std::max(1, m)) return ALG_BAD_SHAPE;
+  if (nc == 0) return ALG_OK;
+  int* lab = nullptr;
+  int* perm_tmp = nullptr;
+  ALG_TRY(ws_get(ctx, WS_LAB, sizeof(int) * (size_t)m, reinterpret_cast<void**>(&lab)));
+  ALG_TRY(ws_get(ctx, WS_PERM_TMP, sizeof(int) * kSwapMaxMoves, reinterpret_cast<void**>(&perm_tmp)));
+  if (perm != nullptr) {
+    iota_kernel<<<std::min(1024, (m + 255) / 256), 256, 0, ctx->stream>>>(perm, m);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  const int nb = std::max(1, plan.nb);
+  const int nbl = std::max(1, std::min(plan.nbl, kPanelMaxW));
+  for (int k0 = 0; k0 < nc; k0 += nb) {
+    const int kb = std::min(nb, nc - k0);
+    for (int c0 = k0; c0 < k0 + kb; c0 += nbl) {
+      const int w = std::min(nbl, k0 + kb - c0);
+      PanelArgs<T> pa;
+      pa.a = a;
+      pa.lda = lda;
+      pa.n = m;
+      pa.c0 = c0;
+      pa.w = w;
+      pa.kb0 = k0;
+      pa.kb1 = k0 + kb;
+      pa.ipiv = ipiv;
+      pa.lab = lab;
+      pa.first_leaf = (c0 == k0) ? 1 : 0;
+      pa.status = ctx->d_status;
+      ALG_TRY((launch_panel<T, EXACT>(ctx, pa)));
+      const int cr = c0 + w;  // first column right of the leaf
+      if (cr < k0 + kb) {
+        ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, c0, w, cr, k0 + kb)));
+        ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - cr, k0 + kb - cr, w, a + (size_t)cr + (size_t)c0 * lda, lda,
+                                        a + (size_t)c0 + (size_t)cr * lda, lda,
+                                        a + (size_t)cr + (size_t)cr * lda, lda)));
+      }
+    }
+    // deferred interchanges of every other column (and of perm)
+    const int n_out = k0 + (nc - k0 - kb);
+    if (n_out > 0 || perm != nullptr) {
+      const int warps_needed = std::max(1, n_out);
+      const int grid = std::max(1, std::min(4 * ctx->sm_count, (warps_needed + 7) / 8));
+      laswp_outside_kernel<T><<<grid, kSwapThreads, 0, ctx->stream>>>(a, lda, m, nc, k0, kb, lab, perm,
+                                                                        perm_tmp);
+    count_launches();
+      ALG_CUDA_TRY(cudaGetLastError());
+    }
+    const int kr = k0 + kb;
+    if (kr < nc) {
+      ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, kr, nc)));
+    }
+    if (kr < nc || (kr < m && kr < nc)) {
+      ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - kr, nc - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+                                      a + (size_t)k0 + (size_t)kr * lda, lda,
+                                      a + (size_t)kr + (size_t)kr * lda, lda)));
+    }
+  }
+  return ALG_OK;
+}
+
+template <typename T, bool EXACT>
+int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs,
+                 int ldb) {
+  if (n == 0 || nrhs == 0) return ALG_OK;
+  if (nrhs > 65535) return ALG_BAD_SHAPE;
+  T* x = nullptr;
+  ALG_TRY(ws_get(ctx, WS_X, sizeof(T) * (size_t)n * nrhs, reinterpret_cast<void**>(&x)));
+  const int ldx = n;
+  {
+    dim3 grid(std::min(1024, (n + kSolveThreads - 1) / kSolveThreads), nrhs);
+    solve_gather_kernel<T><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, perm, b, ldb, x, ldx);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  const int B = kSolveB;
+  // forward (unit lower)
+  solve_fwd_kernel<T, EXACT><<<dim3(1, nrhs), kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, -B, B);
+    count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  for (int j0 = 0; j0 + B < n; j0 += B) {
+    const int j1 = j0 + B;
+    const int nb1 = std::min(B, n - j1);
+    const int rest = n - j1 - nb1;
+    dim3 grid(1 + (rest + kSolveThreads - 1) / kSolveThreads, nrhs);
+    solve_fwd_kernel<T, EXACT><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, j0, B);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  // backward (upper)
+  const int jl = ((n - 1) / B) * B;
+  solve_bwd_kernel<T, EXACT><<<dim3(1, nrhs), kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, n, 0,
+                                                                               n - jl);
+    count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  for (int j0 = jl; j0 > 0; j0 -= B) {
+    const int bs = std::min(B, n - j0);
+    const int jp = j0 - B;
+    dim3 grid(1 + (jp + kSolveThreads - 1) / kSolveThreads, nrhs);
+    solve_bwd_kernel<T, EXACT><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, j0, bs, B);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  ALG_CUDA_TRY(cudaMemcpy2DAsync(b, sizeof(T) * (size_t)ldb, x, sizeof(T) * (size_t)ldx,
+                                 sizeof(T) * (size_t)n, nrhs, cudaMemcpyDeviceToDevice, ctx->stream));
+  return ALG_OK;
+}
+
+// explicit instantiations
+#define ALG_INST(T, E)                                                                          \
+  template int lu_factor_dev<T, E>(alg_ctx*, T*, int, int, int, int*, int*, const LuPlan&);   \
+  template int lu_solve_dev<T, E>(alg_ctx*, const T*, int, int, const int*, T*, int, int);    \
+  template int gemm_sub_dev<T, E>(alg_ctx*, int, int, int, const T*, int, const T*, int, T*, int);
+ALG_INST(double, true)
+ALG_INST(double, false)
+ALG_INST(float, true)
+ALG_INST(float, false)
+#undef ALG_INST
+
+}  // namespace alg
+
+// ===========================================================================
+// C entry points (dense)
+// ===========================================================================
+namespace {
+
+using alg::LuPlan;
+
+int factor_any(alg_ctx* ctx, int update, double* d_a, int m, int nc, int lda, int* d_ipiv, int* d_perm) {
+  const LuPlan plan = alg::default_plan(nc, 8);
+  if (update == ALG_UPDATE_EXACT)
+    return alg::lu_factor_dev<double, true>(ctx, d_a, m, nc, lda, d_ipiv, d_perm, plan);
+  if (update == ALG_UPDATE_FMA)
+    return alg::lu_factor_dev<double, false>(ctx, d_a, m, nc, lda, d_ipiv, d_perm, plan);
+  return ALG_INVALID_ARGUMENT;
+}
+
+int solve_any(alg_ctx* ctx, int update, const double* d_lu, int n, int lda, const int* d_perm,
+              double* d_b, int nrhs, int ldb) {
+  if (update == ALG_UPDATE_EXACT)
+    return alg::lu_solve_dev<double, true>(ctx, d_lu, n, lda, d_perm, d_b, nrhs, ldb);
+  return alg::lu_solve_dev<double, false>(ctx, d_lu, n, lda, d_perm, d_b, nrhs, ldb);
+}
+
+// Sizes accepted by the int32-indexed kernels.
+bool size_ok(size_t n) { return n <= (size_t)INT_MAX / 2; }
+
+struct CtxLock {
+  alg_ctx* ctx = nullptr;
+  std::unique_lock<std::mutex> lk;
+  int rc = ALG_OK;
+  CtxLock() {
+    rc = alg::default_ctx(&ctx);
+    if (rc == ALG_OK) lk = std::unique_lock<std::mutex>(ctx->mu);
+  }
+};
+
+// Host drop-in core: copy a (and b) in, factor (and solve), copy back.
+int host_lu(int update, double* a, size_t m, size_t nc, size_t* ipiv, double* det, double* b,
+            size_t nrhs) {
+  if (!size_ok(m) || !size_ok(nc) || !size_ok(nrhs)) return ALG_BAD_SHAPE;
+  CtxLock L;
+  if (L.rc != ALG_OK) return L.rc;
+  alg_ctx* ctx = L.ctx;
+  const int M = (int)m, N = (int)nc, R = (int)nrhs;
+  double* d_a = nullptr;
+  double* d_b = nullptr;
+  int* d_ipiv = nullptr;
+  int* d_perm = nullptr;
+  ALG_TRY(alg::ws_get(ctx, alg::WS_A, sizeof(double) * m * nc, reinterpret_cast<void**>(&d_a)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_IPIV, sizeof(int) * nc, reinterpret_cast<void**>(&d_ipiv)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_PERM, sizeof(int) * m, reinterpret_cast<void**>(&d_perm)));
+  if (b != nullptr && R > 0)
+    ALG_TRY(alg::ws_get(ctx, alg::WS_B, sizeof(double) * m * nrhs, reinterpret_cast<void**>(&d_b)));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_a, a, sizeof(double) * m * nc, cudaMemcpyHostToDevice, ctx->stream));
+  if (d_b) ALG_CUDA_TRY(cudaMemcpyAsync(d_b, b, sizeof(double) * m * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_TRY(alg::status_reset(ctx));
+  ALG_TRY(factor_any(ctx, update, d_a, M, N, M, d_ipiv, d_perm));
+  ALG_TRY(alg::status_fetch(ctx));
+  const bool singular = ctx->h_status->singular_col != INT_MAX;
+  if (!singular && d_b) {
+    ALG_TRY(solve_any(ctx, update, d_a, M, M, d_perm, d_b, R, M));
+    ALG_CUDA_TRY(cudaMemcpyAsync(b, d_b, sizeof(double) * m * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ALG_CUDA_TRY(cudaMemcpyAsync(a, d_a, sizeof(double) * m * nc, cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<int> h_ipiv(nc);
+  ALG_CUDA_TRY(cudaMemcpyAsync(h_ipiv.data(), d_ipiv, sizeof(int) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (singular) return ALG_SINGULAR;
+  if (ipiv)
+    for (size_t k = 0; k < nc; ++k) ipiv[k] = (size_t)h_ipiv[k];
+  if (det) {
+    // mod.rs:120-150: sign flip per interchange, then times the pivot, in order
+    double d = 1.0;
+    for (size_t k = 0; k < nc; ++k) {
+      if ((size_t)h_ipiv[k] != k) d = -d;
+      d *= a[k + k * m];
+    }
+    *det = d;
+  }
+  return ALG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alg_dgetrf(double* a, size_t n, size_t* ipiv, double* det) {
+  if (n == 0) {
+    if (det) *det = 1.0;
+    return ALG_OK;
+  }
+  if (a == nullptr || ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  return host_lu(ALG_UPDATE_EXACT, a, n, n, ipiv, det, nullptr, 0);
+}
+
+int alg_dgetrf_rect(double* a, size_t nrows, size_t ncols, size_t* ipiv) {
+  if (nrows < ncols) return ALG_BAD_SHAPE;
+  if (ncols == 0) return ALG_OK;
+  if (a == nullptr || ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  return host_lu(ALG_UPDATE_EXACT, a, nrows, ncols, ipiv, nullptr, nullptr, 0);
+}
+
+int alg_dgesv(double* a, double* b, size_t n) {
+  if (n == 0) return ALG_OK;
+  if (a == nullptr || b == nullptr) return ALG_INVALID_ARGUMENT;
+  return host_lu(ALG_UPDATE_EXACT, a, n, n, nullptr, nullptr, b, 1);
+}
+
+int alg_dgesv_nrhs(double* a, double* b, size_t n, size_t nrhs) {
+  if (n == 0 || nrhs == 0) return ALG_OK;
+  if (a == nullptr || b == nullptr) return ALG_INVALID_ARGUMENT;
+  return host_lu(ALG_UPDATE_EXACT, a, n, n, nullptr, nullptr, b, nrhs);
+}
+
+int alg_dgesv_ex(int update, double* a, double* b, size_t n, size_t nrhs, size_t* ipiv) {
+  if (update != ALG_UPDATE_EXACT && update != ALG_UPDATE_FMA) return ALG_INVALID_ARGUMENT;
+  if (n == 0) return ALG_OK;
+  if (a == nullptr || (b == nullptr && nrhs > 0)) return ALG_INVALID_ARGUMENT;
+  return host_lu(update, a, n, n, ipiv, nullptr, b, nrhs);
+}
+
+int alg_dgetrf_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda, int32_t* d_ipiv,
+                   int32_t* d_perm) {
+  if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
+  if (n < 0 || lda < std::max(1, n)) return ALG_BAD_SHAPE;
+  if (n == 0) return ALG_OK;
+  int* ipiv = d_ipiv;
+  if (ipiv == nullptr) ALG_TRY(alg::ws_get(ctx, alg::WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&ipiv)));
+  ALG_TRY(alg::status_reset(ctx));
+  ALG_TRY(factor_any(ctx, update, d_a, n, n, lda, ipiv, d_perm));
+  ALG_TRY(alg::status_fetch(ctx));
+  return ctx->h_status->singular_col != INT_MAX ? ALG_SINGULAR : ALG_OK;
+}
+
+int alg_dgetrs_dev(alg_ctx* ctx, const double* d_lu, int n, int lda, const int32_t* d_perm,
+                   double* d_b, int nrhs, int ldb) {
+  if (ctx == nullptr || d_perm == nullptr) return ALG_INVALID_ARGUMENT;
+  if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n)) return ALG_BAD_SHAPE;
+  ALG_TRY(solve_any(ctx, ALG_UPDATE_EXACT, d_lu, n, lda, d_perm, d_b, nrhs, ldb));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return ALG_OK;
+}
+
+int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda, double* d_b, int nrhs,
+                  int ldb, int32_t* d_ipiv) {
+  if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
+  if (update != ALG_UPDATE_EXACT && update != ALG_UPDATE_FMA) return ALG_INVALID_ARGUMENT;
+  if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n)) return ALG_BAD_SHAPE;
+  if (n == 0) return ALG_OK;
+  int* ipiv = d_ipiv;
+  int* perm = nullptr;
+  if (ipiv == nullptr) ALG_TRY(alg::ws_get(ctx, alg::WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&ipiv)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_PERM, sizeof(int) * n, reinterpret_cast<void**>(&perm)));
+  ALG_TRY(alg::status_reset(ctx));
+  ALG_TRY(factor_any(ctx, update, d_a, n, n, lda, ipiv, perm));
+  ALG_TRY(alg::status_fetch(ctx));
+  if (ctx->h_status->singular_col != INT_MAX) return ALG_SINGULAR;
+  ALG_TRY(solve_any(ctx, update, d_a, n, lda, perm, d_b, nrhs, ldb));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return ALG_OK;
+}
+
+}  // extern "C"

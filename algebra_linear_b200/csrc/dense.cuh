@@ -1,0 +1,32 @@
+// Host-side drivers of the blocked dense LU and its solves.
+#pragma once
+
+#include "context.cuh"
+
+namespace alg {
+
+struct LuPlan {
+  int nb = 64;    // block-panel width (trailing-update depth)
+  int nbl = 16;   // leaf-panel width (one cluster kernel)
+};
+
+// In-place LU of the m x nc (m >= nc) device matrix a (leading dim lda).
+// ipiv: nc global interchanges; perm: m net permutation (may be null).
+// Status lands in ctx->d_status (singular_col). Stream-ordered, no sync.
+template <typename T, bool EXACT>
+int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* perm,
+                  const LuPlan& plan);
+
+// Solves with the packed factors: b (n x nrhs, ldb) becomes x. Stream-ordered.
+template <typename T, bool EXACT>
+int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs,
+                 int ldb);
+
+// C -= A B on the CUDA cores (column-major), stream-ordered.
+template <typename T, bool EXACT>
+int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T* B, int ldb,
+                 T* C, int ldc);
+
+LuPlan default_plan(int n, int elem_bytes);
+
+}  // namespace alg

@@ -1,0 +1,79 @@
+"""Device-resident entry points over torch tensors (the alg_*_dev C ABI).
+
+Matrices are 1-D (or any contiguous) float64 CUDA tensors holding
+column-major data, leading dimension n, as the host drop-ins take them. The
+context runs on torch's current CUDA stream.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from .lapack import LapackError, _KINDS
+
+
+def _check(rc: int) -> None:
+    if rc != _lib.OK:
+        raise LapackError(_KINDS.get(rc, _lib.status_string(rc)), rc)
+
+
+def _dev_f64(t: torch.Tensor, numel: int, name: str) -> torch.Tensor:
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() >= numel):
+        raise TypeError(f"{name} must be a contiguous float64 CUDA tensor with >= {numel} entries")
+    return t
+
+
+class Context:
+    """Owns an alg_ctx bound to torch's current stream."""
+
+    def __init__(self):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        stream = torch.cuda.current_stream().cuda_stream
+        _check(self._lib.alg_ctx_create(C.c_void_p(stream), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.alg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def sync_stream(self):
+        _check(self._lib.alg_ctx_set_stream(self.handle, C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    def dgetrf(self, a: torch.Tensor, n: int, update: int = _lib.UPDATE_EXACT):
+        """In-place LU; returns (ipiv, perm) int32 CUDA tensors."""
+        _dev_f64(a, n * n, "a")
+        ipiv = torch.empty(max(n, 1), dtype=torch.int32, device=a.device)
+        perm = torch.empty(max(n, 1), dtype=torch.int32, device=a.device)
+        _check(self._lib.alg_dgetrf_dev(self.handle, update, a.data_ptr(), n, n, ipiv.data_ptr(), perm.data_ptr()))
+        return ipiv[:n], perm[:n]
+
+    def dgetrs(self, lu: torch.Tensor, perm: torch.Tensor, b: torch.Tensor, n: int, nrhs: int = 1):
+        _dev_f64(lu, n * n, "lu")
+        _dev_f64(b, n * nrhs, "b")
+        _check(self._lib.alg_dgetrs_dev(self.handle, lu.data_ptr(), n, n, perm.data_ptr(), b.data_ptr(), nrhs, n))
+
+    def dgesv(self, a: torch.Tensor, b: torch.Tensor, n: int, nrhs: int = 1, update: int = _lib.UPDATE_EXACT):
+        """Solves in place (a -> LU, b -> x); returns ipiv (int32 CUDA tensor)."""
+        _dev_f64(a, n * n, "a")
+        _dev_f64(b, n * nrhs, "b")
+        ipiv = torch.empty(max(n, 1), dtype=torch.int32, device=a.device)
+        _check(self._lib.alg_dgesv_dev(self.handle, update, a.data_ptr(), n, n, b.data_ptr(), nrhs, n,
+                                       ipiv.data_ptr()))
+        return ipiv[:n]

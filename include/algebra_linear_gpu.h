@@ -1,0 +1,134 @@
+/*
+ * algebra_linear_gpu — B200 (sm_100a) LU solver behind the API of the
+ * cpmech/algebra_linear 4.0.0 crate's dense and sparse LU path.
+ *
+ * C ABI: plain pointers and sizes, column-major storage (a[i + j*n]),
+ * 0-based indices. Every entry point returns an int status (ALG_OK = 0).
+ * The host-pointer entry points are drop-ins for the Rust functions they cite:
+ * they copy the caller's arrays to the GPU, compute there, and copy results
+ * back into the same arrays. There is no CPU fallback: without a usable CUDA
+ * device every compute entry point returns ALG_NO_DEVICE.
+ *
+ * Threading: the host-pointer drop-ins share one library context per device,
+ * guarded by a mutex (calls serialise). An alg_ctx is owned by one thread at a
+ * time, like a `&mut` borrow in the reference.
+ */
+#ifndef ALGEBRA_LINEAR_GPU_H
+#define ALGEBRA_LINEAR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------
+ * 1..4 mirror lapack::LapackError (src/lapack/mod.rs:76-96).
+ * 100..108 mirror sparse::faer::Error in declaration order
+ * (src/sparse/faer/error.rs:5-24).
+ * 200.. are conditions only a GPU implementation has. */
+#define ALG_OK 0
+#define ALG_SINGULAR 1
+#define ALG_BAD_SHAPE 2
+#define ALG_CONVERGENCE 3
+#define ALG_NOT_IMPLEMENTED 4
+
+#define ALG_SP_BAD_SHAPE 100
+#define ALG_SP_INVALID_STRUCTURE 101
+#define ALG_SP_UNSORTED_ROWS 102
+#define ALG_SP_DUPLICATE_ENTRY 103
+#define ALG_SP_SINGULAR 104
+#define ALG_SP_INDEX_OVERFLOW 105
+#define ALG_SP_STRUCTURE_MISMATCH 106
+#define ALG_SP_NOT_FINITE 107
+#define ALG_SP_NOT_FACTORIZED 108
+
+#define ALG_CUDA_ERROR 200
+#define ALG_OUT_OF_DEVICE_MEMORY 201
+#define ALG_TIMEOUT 202
+#define ALG_INVALID_ARGUMENT 203
+#define ALG_NO_DEVICE 204
+
+/* Message for a status code (static storage). The sparse messages are the
+ * reference's Display strings (src/sparse/faer/error.rs:27-41). */
+const char* alg_status_string(int status);
+
+/* Library version string. */
+const char* alg_version(void);
+
+/* Number of CUDA kernels this library has launched in this process (all
+ * contexts). Lets a caller count the device work inside a timed region. */
+unsigned long long alg_kernel_launch_count(void);
+
+/* ---- dense drop-ins (host pointers) -------------------------------------- */
+
+/* Arithmetic of the trailing updates in the FP64 form.
+ * ALG_UPDATE_EXACT: every entry is updated as the reference's scalar loop does
+ *   (rounded product, rounded difference, in pivot order), so the factors,
+ *   pivots and determinant are bit-identical to lapack::dgetrf.
+ * ALG_UPDATE_FMA: fused multiply-adds (twice the FP64 rate); pivots agree with
+ *   the reference unless two candidates tie to within rounding. */
+#define ALG_UPDATE_EXACT 0
+#define ALG_UPDATE_FMA 1
+
+/* Replaces `pub fn dgetrf(a: &mut [f64], n: usize)
+ *   -> Result<(Vec<usize>, f64), LapackError>` (src/lapack/mod.rs:181-185).
+ * a: n*n column-major, overwritten with packed unit-lower L and U.
+ * ipiv: n entries, 0-based sequential row interchanges. det: ±prod(u_kk).
+ * n = 0: *det = 1, ALG_OK. On ALG_SINGULAR the contents of a and ipiv are
+ * unspecified (the reference leaves a partly factored). */
+int alg_dgetrf(double* a, size_t n, size_t* ipiv, double* det);
+
+/* Replaces `pub fn dgetrf_rect(a: &mut [f64], nrows: usize, ncols: usize,
+ *   ipiv: &mut [usize]) -> Result<(), LapackError>` (src/lapack/mod.rs:202-238).
+ * ALG_BAD_SHAPE if nrows < ncols; ncols = 0 is ALG_OK. */
+int alg_dgetrf_rect(double* a, size_t nrows, size_t ncols, size_t* ipiv);
+
+/* Replaces `pub fn dgesv(a: &mut [f64], b: &mut [f64])
+ *   -> Result<(), LapackError>` (src/lapack/mod.rs:309-323), n = b.len().
+ * a is destroyed (holds the LU factors); b becomes x. */
+int alg_dgesv(double* a, double* b, size_t n);
+
+/* dgesv with nrhs right-hand sides, b n x nrhs column-major: the reference's
+ * dgetrf followed by its dgetrs (src/lapack/mod.rs:330-354) per column. */
+int alg_dgesv_nrhs(double* a, double* b, size_t n, size_t nrhs);
+
+/* alg_dgesv_nrhs with a chosen update arithmetic (ALG_UPDATE_*); ipiv may be
+ * NULL, else receives the n interchanges. */
+int alg_dgesv_ex(int update, double* a, double* b, size_t n, size_t nrhs, size_t* ipiv);
+
+/* ---- device-resident API -------------------------------------------------
+ * An alg_ctx holds a CUDA stream (the caller's, or its own) and the device
+ * workspace; device pointers are the caller's. Calls are stream-ordered and
+ * return once the status is known (they synchronise the stream). */
+typedef struct alg_ctx alg_ctx;
+
+/* Context on the current CUDA device; stream = NULL means the context makes
+ * and owns a non-blocking stream. */
+int alg_ctx_create(void* cuda_stream, alg_ctx** out);
+void alg_ctx_destroy(alg_ctx* ctx);
+/* Rebinds the stream (e.g. to the caller framework's current stream). */
+int alg_ctx_set_stream(alg_ctx* ctx, void* cuda_stream);
+
+/* In-place LU of the n x n device matrix d_a (leading dimension lda >= n).
+ * d_ipiv: n int32, LAPACK-style sequential interchanges (0-based).
+ * d_perm: n int32, the net row permutation (row i of P*A is row perm[i] of A);
+ * either may be NULL. */
+int alg_dgetrf_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
+                   int32_t* d_ipiv, int32_t* d_perm);
+
+/* Solves with factors from alg_dgetrf_dev: d_b is n x nrhs (leading dim ldb),
+ * overwritten with x. */
+int alg_dgetrs_dev(alg_ctx* ctx, const double* d_lu, int n, int lda,
+                   const int32_t* d_perm, double* d_b, int nrhs, int ldb);
+
+/* alg_dgetrf_dev + alg_dgetrs_dev; d_ipiv may be NULL. */
+int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
+                  double* d_b, int nrhs, int ldb, int32_t* d_ipiv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALGEBRA_LINEAR_GPU_H */

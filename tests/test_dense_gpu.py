@@ -1,0 +1,250 @@
+"""GPU parity of the dense LU path against the oracle, through the C ABI.
+
+Tolerances (the spec's FP64 bar): identical pivot sequence and x within
+1e-12 relative. The exact-update form is held to more: the packed LU factors,
+pivots and determinant must be bit-identical to the reference's kij loop.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12
+SEEDY = [1988, 1989, 1990, 1991]
+
+
+def rel_err(x, ref):
+    return float(np.max(np.abs(x - ref)) / max(np.max(np.abs(ref)), 1e-300))
+
+
+def same_bits(x, y):
+    return np.array_equal(x.view(np.uint64), y.view(np.uint64))
+
+
+# ---- the reference's own unit tests, through the GPU drop-ins ---------------
+
+def test_reference_unit_cases_on_gpu(gpu, oracle):
+    from algebra_linear_b200.lapack import LapackError, dgesv, dgetrf, dgetrf_rect
+
+    from tests.test_oracle_kat import cofactor_det4, reconstruct_panel, sample4
+
+    a = sample4()
+    ipiv, det = dgetrf(a, 4)
+    assert abs(det - cofactor_det4()) < 1e-12  # mod.rs:483-495
+    ref = sample4()
+    _, ripiv, rdet, _ = oracle.dgetrf(ref, 4)
+    assert ipiv == ripiv and det == rdet and same_bits(a, ref)
+
+    with pytest.raises(LapackError) as e:  # mod.rs:497-502
+        dgetrf(np.array([1.0, 2.0, 3.0, 2.0, 4.0, 6.0, 1.0, 1.0, 1.0]), 3)
+    assert e.value.kind == "Singular"
+
+    a = sample4()  # mod.rs:537-551
+    x_true = np.array([1.0, -2.0, 3.0, 5.0])
+    b = oracle.dgemv(a, x_true, 4, 4)
+    dgesv(a, b)
+    assert np.all(np.abs(b - x_true) < 1e-12)
+
+    with pytest.raises(LapackError) as e:  # mod.rs:553-558
+        dgesv(np.array([1.0, 2.0, 3.0, 2.0, 4.0, 6.0, 1.0, 1.0, 1.0]), np.ones(3))
+    assert e.value.kind == "Singular"
+
+    a = np.array([1e-16, 0.0, 0.0, 1.0])  # mod.rs:670-683
+    ipiv, det = dgetrf(a, 2)
+    assert len(ipiv) == 2 and abs(det) < 1e-15
+    with pytest.raises(LapackError) as e:
+        dgetrf(np.array([1.0, 2.0, 2.0, 4.0]), 2)
+    assert e.value.kind == "Singular"
+
+    nrows, ncols = 5, 3  # mod.rs:723-733
+    a0 = np.array([1.0, 5.0, 2.0, 3.0, 4.0, 2.0, -1.0, 6.0, 0.0, 1.0, 3.0, 2.0, 1.0, 7.0, -2.0])
+    a = a0.copy()
+    piv = [0] * ncols
+    dgetrf_rect(a, nrows, ncols, piv)
+    pa, lu = reconstruct_panel(nrows, ncols, a0, a, piv)
+    assert np.all(np.abs(pa - lu) < 1e-12) and piv[0] == 1
+
+    with pytest.raises(LapackError) as e:  # mod.rs:743-744
+        dgetrf_rect(np.array([0.0, 0.0, 2.0, 3.0]), 2, 2, [0, 0])
+    assert e.value.kind == "Singular"
+
+
+# ---- bit-exact factors on the larnv workload --------------------------------
+
+SIZES = [1, 2, 3, 5, 15, 16, 17, 31, 33, 63, 64, 65, 100, 127, 129, 200, 257, 513, 1024]
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_dgetrf_is_bit_identical_to_the_reference(gpu, oracle, n):
+    from algebra_linear_b200.lapack import dgetrf
+
+    a0, _ = oracle.larnv("Symmetric", [11, 23, 37, 2 * n + 1], n * n)
+    a = a0.copy()
+    ipiv, det = dgetrf(a, n)
+    ref = a0.copy()
+    rc, ripiv, rdet, _ = oracle.dgetrf(ref, n)
+    assert rc == 0
+    assert ipiv == ripiv
+    assert same_bits(a, ref), f"max diff {np.max(np.abs(a - ref))}"
+    assert same_bits(np.array([det]), np.array([rdet]))
+
+
+def test_dgetrf_two_cluster_panel_bit_identical(gpu, oracle):
+    """n = 2048 makes the leaf panel span a 2-CTA cluster (rows > one CTA's
+    shared memory)."""
+    from algebra_linear_b200.lapack import dgetrf
+
+    n = 2048
+    a0, _ = oracle.larnv("Symmetric", SEEDY, n * n)
+    a = a0.copy()
+    ipiv, _ = dgetrf(a, n)
+    ref = a0.copy()
+    rc, ripiv, _, _ = oracle.dgetrf(ref, n)
+    assert rc == 0 and ipiv == ripiv and same_bits(a, ref)
+
+
+@pytest.mark.parametrize("shape", [(5, 3), (7, 7), (40, 17), (100, 64), (300, 129), (1000, 33), (513, 200)])
+def test_dgetrf_rect_is_bit_identical(gpu, oracle, shape):
+    from algebra_linear_b200.lapack import dgetrf_rect
+
+    nrows, ncols = shape
+    a0, _ = oracle.larnv("Symmetric", [5, 6, 7, 2 * ncols + 1], nrows * ncols)
+    a = a0.copy()
+    piv = [0] * ncols
+    dgetrf_rect(a, nrows, ncols, piv)
+    ref = a0.copy()
+    rc, rpiv = oracle.dgetrf_rect(ref, nrows, ncols)
+    assert rc == 0 and piv == rpiv and same_bits(a, ref)
+
+
+# ---- the C1 configuration: n = 1024, one RHS ---------------------------------
+
+@pytest.mark.parametrize("update", [0, 1], ids=["exact", "fma"])
+def test_c1_dgesv_parity(gpu, oracle, update):
+    from algebra_linear_b200.lapack import dgesv_nrhs
+
+    n = 1024
+    a, x_true, b = oracle.c1_system(n)
+    ra, rb = a.copy(), b.copy()
+    rc, ripiv = oracle.dgesv(ra, rb, n)
+    assert rc == 0
+    ga, gb = a.copy(), b.copy()
+    ipiv = dgesv_nrhs(ga, gb, n, 1, update=update)
+    assert ipiv == ripiv  # identical pivot sequence
+    assert rel_err(gb, rb) <= REL_TOL
+    if update == 0:
+        assert same_bits(ga, ra)  # bit-identical factors
+    assert oracle.backward_error(a, gb, b, n) < 10 * n * 2.0**-53
+
+
+def test_dgesv_64_rhs_matches_dgetrs_per_column(gpu, oracle):
+    from algebra_linear_b200.lapack import dgesv_nrhs
+
+    n, nrhs = 300, 64
+    a0, s = oracle.larnv("Symmetric", SEEDY, n * n)
+    b0, _ = oracle.larnv("Symmetric", s, n * nrhs)
+    ra, rb = a0.copy(), b0.copy()
+    rc, ripiv = oracle.dgesv(ra, rb, n, nrhs)
+    assert rc == 0
+    ga, gb = a0.copy(), b0.copy()
+    ipiv = dgesv_nrhs(ga, gb, n, nrhs)
+    assert ipiv == ripiv
+    assert rel_err(gb, rb) <= REL_TOL
+
+
+def test_forward_sweep_is_exact_and_solution_close(gpu, oracle):
+    """Odd sizes across several solve blocks (64 rows each)."""
+    from algebra_linear_b200.lapack import dgesv
+
+    for n in [1, 7, 64, 65, 130, 777]:
+        a, _, b = oracle.c1_system(n, seed=[3, 1, 4, 2 * n + 1])
+        ra, rb = a.copy(), b.copy()
+        oracle.dgesv(ra, rb, n)
+        ga, gb = a.copy(), b.copy()
+        dgesv(ga, gb)
+        assert rel_err(gb, rb) <= REL_TOL, n
+
+
+# ---- edge cases ---------------------------------------------------------------
+
+def test_nan_and_inf_follow_the_reference_pivot_rule(gpu, oracle):
+    """A NaN below the diagonal is never chosen; a NaN on the diagonal keeps
+    the pivot in place (strict '>' scan seeded with |a_kk|, mod.rs:123-134)."""
+    from algebra_linear_b200.lapack import dgetrf
+
+    n = 40
+    for case in range(4):
+        a0, _ = oracle.larnv("Symmetric", [9, 9, 9, 2 * case + 1], n * n)
+        if case == 0:
+            a0[5 + 3 * n] = np.nan          # below the diagonal in column 3
+        elif case == 1:
+            a0[3 + 3 * n] = np.nan          # on the diagonal
+        elif case == 2:
+            a0[17 + 0 * n] = np.inf         # an infinite candidate
+        else:
+            a0[0:n] = 0.0
+            a0[n - 1] = np.nan              # column 0 all zero but one NaN
+        a = a0.copy()
+        try:
+            ipiv, _ = dgetrf(a, n)
+            grc = 0
+        except Exception as e:  # noqa: BLE001
+            grc, ipiv = getattr(e, "code", -1), None
+        ref = a0.copy()
+        rc, ripiv, _, _ = oracle.dgetrf(ref, n)
+        assert grc == rc, case
+        if rc == 0:
+            assert ipiv == ripiv, case
+            assert np.array_equal(np.isnan(a), np.isnan(ref)), case
+            fin = ~np.isnan(ref)
+            assert same_bits(a[fin], ref[fin]), case
+
+
+def test_exactly_singular_large_matrix(gpu, oracle):
+    """A repeated column makes the reference's pivot exactly zero somewhere;
+    the GPU reports Singular in the same case (and not otherwise)."""
+    from algebra_linear_b200.lapack import LapackError, dgetrf
+
+    n = 96
+    a0, _ = oracle.larnv("Symmetric", SEEDY, n * n)
+    a0[70 * n:71 * n] = 2.0 * a0[10 * n:11 * n]
+    ref = a0.copy()
+    rc, *_ = oracle.dgetrf(ref, n)
+    a = a0.copy()
+    if rc == 1:
+        with pytest.raises(LapackError):
+            dgetrf(a, n)
+    else:
+        ipiv, _ = dgetrf(a, n)
+        assert same_bits(a, ref)
+
+
+def test_repeat_runs_are_bitwise_deterministic(gpu, oracle):
+    from algebra_linear_b200.lapack import dgesv_nrhs
+
+    n = 700
+    a, _, b = oracle.c1_system(n)
+    outs = []
+    for _ in range(2):
+        ga, gb = a.copy(), b.copy()
+        dgesv_nrhs(ga, gb, n, 1, update=1)
+        outs.append((ga, gb))
+    assert same_bits(outs[0][0], outs[1][0]) and same_bits(outs[0][1], outs[1][1])
+
+
+def test_device_api_matches_host_api(gpu, oracle):
+    import torch
+
+    from algebra_linear_b200 import device
+
+    n = 333
+    a, _, b = oracle.c1_system(n)
+    ra, rb = a.copy(), b.copy()
+    oracle.dgesv(ra, rb, n)
+    with device.Context() as ctx:
+        da = torch.from_numpy(a.copy()).cuda()  # column-major n*n
+        db = torch.from_numpy(b.copy()).cuda()
+        ipiv = ctx.dgesv(da, db, n)
+        assert ipiv.tolist() == oracle.dgesv(a.copy(), b.copy(), n)[1]
+        assert rel_err(db.cpu().numpy(), rb) <= REL_TOL
