@@ -33,6 +33,9 @@ TIMEOUT = 202
 INVALID_ARGUMENT = 203
 NO_DEVICE = 204
 
+KERNEL_CLASSES = ["panel", "laswp", "trsm", "gemm", "gemm_tc", "solve", "resid", "cast", "batch",
+                  "sparse", "misc"]
+
 UPDATE_EXACT = 0
 UPDATE_FMA = 1
 
@@ -56,8 +59,13 @@ SIGNATURES = [
     ("alg_ctx_destroy", None, [_P]),
     ("alg_ctx_set_stream", _I, [_P, _P]),
     ("alg_dgetrf_dev", _I, [_P, _I, _P, _I, _I, _P, _P]),
+    ("alg_dgetrf_rect_dev", _I, [_P, _I, _P, _I, _I, _I, _P]),
     ("alg_dgetrs_dev", _I, [_P, _P, _I, _I, _P, _P, _I, _I]),
     ("alg_dgesv_dev", _I, [_P, _I, _P, _I, _I, _P, _I, _I, _P]),
+    ("alg_ctx_set_profiling", _I, [_P, _I]),
+    ("alg_ctx_profile_reset", _I, [_P]),
+    ("alg_ctx_profile_get", _I, [_P, _I, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 ]
 
 _lib = None

@@ -49,8 +49,61 @@ int ctx_init(alg_ctx* ctx, cudaStream_t stream) {
   return ALG_OK;
 }
 
+static cudaEvent_t prof_event(alg_ctx* ctx) {
+  if (!ctx->prof_pool.empty()) {
+    cudaEvent_t e = ctx->prof_pool.back();
+    ctx->prof_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+int prof_begin(alg_ctx* ctx, int cls) {
+  if (!ctx->prof_on) return -1;
+  alg_ctx::ProfPending pp;
+  pp.cls = cls;
+  pp.e0 = prof_event(ctx);
+  pp.e1 = prof_event(ctx);
+  pp.flops = pp.bytes = 0;
+  cudaEventRecord(pp.e0, ctx->stream);
+  ctx->prof_pending.push_back(pp);
+  return (int)ctx->prof_pending.size() - 1;
+}
+
+void prof_end(alg_ctx* ctx, int token, double flops, double bytes) {
+  if (token < 0 || !ctx->prof_on) return;
+  auto& pp = ctx->prof_pending[token];
+  pp.flops = flops;
+  pp.bytes = bytes;
+  cudaEventRecord(pp.e1, ctx->stream);
+}
+
+void prof_collect(alg_ctx* ctx) {
+  if (ctx->prof_pending.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& pp : ctx->prof_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pp.e0, pp.e1) == cudaSuccess) {
+      auto& t = ctx->prof[pp.cls];
+      t.launches += 1;
+      t.ms += ms;
+      t.flops += pp.flops;
+      t.bytes += pp.bytes;
+    }
+    ctx->prof_pool.push_back(pp.e0);
+    ctx->prof_pool.push_back(pp.e1);
+  }
+  cudaGetLastError();
+  ctx->prof_pending.clear();
+}
+
 void ctx_release(alg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  prof_collect(ctx);
+  for (auto e : ctx->prof_pool) cudaEventDestroy(e);
+  ctx->prof_pool.clear();
   for (auto& b : ctx->bufs) {
     if (b.ptr) cudaFree(b.ptr);
     b = alg_ctx::Buf{};
@@ -112,6 +165,7 @@ int status_fetch(alg_ctx* ctx) {
   ALG_CUDA_TRY(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(DevStatus),
                                cudaMemcpyDeviceToHost, ctx->stream));
   ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
   if (ctx->h_status->timeout) return ALG_TIMEOUT;
   if (ctx->h_status->bad_input) return ALG_INVALID_ARGUMENT;
   return ALG_OK;
@@ -184,6 +238,32 @@ int alg_ctx_set_stream(alg_ctx* ctx, void* cuda_stream) {
     ALG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     ctx->own_stream = true;
   }
+  return ALG_OK;
+}
+
+int alg_ctx_set_profiling(alg_ctx* ctx, int on) {
+  if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
+  alg::prof_collect(ctx);
+  ctx->prof_on = on != 0;
+  return ALG_OK;
+}
+
+int alg_ctx_profile_reset(alg_ctx* ctx) {
+  if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
+  alg::prof_collect(ctx);
+  for (auto& t : ctx->prof) t = alg_ctx::ProfTotal{};
+  return ALG_OK;
+}
+
+int alg_ctx_profile_get(alg_ctx* ctx, int kernel_class, unsigned long long* launches,
+                        double* total_ms, double* flops, double* bytes) {
+  if (ctx == nullptr || kernel_class < 0 || kernel_class >= ALG_K_COUNT) return ALG_INVALID_ARGUMENT;
+  alg::prof_collect(ctx);
+  const auto& t = ctx->prof[kernel_class];
+  if (launches) *launches = t.launches;
+  if (total_ms) *total_ms = t.ms;
+  if (flops) *flops = t.flops;
+  if (bytes) *bytes = t.bytes;
   return ALG_OK;
 }
 

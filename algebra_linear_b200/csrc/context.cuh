@@ -10,6 +10,22 @@
 
 #include "common.cuh"
 
+// Kernel classes timed by the context's profiler (alg_ctx_set_profiling).
+enum AlgKernelClass : int {
+  ALG_K_PANEL = 0,   // leaf panel LU (cluster)
+  ALG_K_LASWP,       // deferred row interchanges
+  ALG_K_TRSM,        // U12 = L11^-1 A12
+  ALG_K_GEMM,        // trailing update on the CUDA cores
+  ALG_K_GEMM_TC,     // trailing update on the tensor cores (tcgen05)
+  ALG_K_SOLVE,       // triangular solves
+  ALG_K_RESID,       // FP64 residual / norms
+  ALG_K_CAST,        // precision conversion
+  ALG_K_BATCH,       // batched small systems
+  ALG_K_SPARSE,      // sparse factorization / solve
+  ALG_K_MISC,
+  ALG_K_COUNT
+};
+
 struct alg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -24,6 +40,20 @@ struct alg_ctx {
   };
   std::vector<Buf> bufs;
   std::mutex mu;  // serialises the shared per-device contexts of the drop-ins
+  // profiler: event pairs around launches of the timed classes
+  bool prof_on = false;
+  struct ProfPending {
+    int cls;
+    cudaEvent_t e0, e1;
+    double flops, bytes;
+  };
+  std::vector<ProfPending> prof_pending;
+  std::vector<cudaEvent_t> prof_pool;
+  struct ProfTotal {
+    unsigned long long launches = 0;
+    double ms = 0, flops = 0, bytes = 0;
+  };
+  ProfTotal prof[ALG_K_COUNT];
 };
 
 namespace alg {
@@ -58,6 +88,14 @@ int status_reset(alg_ctx* ctx);
 int status_fetch(alg_ctx* ctx);
 
 int ctx_init(alg_ctx* ctx, cudaStream_t stream);
+
+// Profiler hooks: prof_begin records a start event (if profiling is on) and
+// returns a token; prof_end records the stop event with the launch's
+// algorithmic flops/bytes. prof_collect (called after a stream sync) folds
+// finished pairs into the per-class totals.
+int prof_begin(alg_ctx* ctx, int cls);
+void prof_end(alg_ctx* ctx, int token, double flops, double bytes);
+void prof_collect(alg_ctx* ctx);
 void ctx_release(alg_ctx* ctx);
 
 }  // namespace alg

@@ -15,6 +15,7 @@
 // EXACT arithmetic the result equals the reference's kij loop
 // (src/lapack/mod.rs:112-163) bit for bit.
 #include <algorithm>
+#include <cstdlib>
 #include <climits>
 #include <cstring>
 #include <vector>
@@ -28,29 +29,42 @@ LuPlan default_plan(int n, int elem_bytes) {
   LuPlan p;
   p.nb = 64;
   p.nbl = elem_bytes == 8 ? 16 : 32;
+  if (const char* e = std::getenv("ALG_NB")) p.nb = std::max(16, std::atoi(e));
+  if (const char* e = std::getenv("ALG_NBL")) p.nbl = std::max(1, std::min(kPanelMaxW, std::atoi(e)));
   (void)n;
   return p;
 }
 
 namespace {
 
-template <typename T, bool EXACT>
-int launch_panel(alg_ctx* ctx, const PanelArgs<T>& args) {
+// Rows per CTA the cluster size aims for: fewer rows per CTA shorten each
+// column step, more CTAs lengthen the cluster barrier. ALG_PANEL_ROWS
+// overrides it (tuning).
+int panel_target_rows() {
+  static int v = [] {
+    const char* e = std::getenv("ALG_PANEL_ROWS");
+    return e ? std::max(16, std::atoi(e)) : 512;
+  }();
+  return v;
+}
+
+template <typename T, int W, bool EXACT>
+int launch_panel_w(alg_ctx* ctx, const PanelArgs<T>& args) {
   const int m = args.n - args.c0;
   constexpr size_t kMaxSmem = 220 * 1024;
   int C = 1;
-  size_t smem = 0;
-  for (C = 1; C <= 16; C *= 2) {
-    const int R = (m + C - 1) / C;
-    smem = panel_smem_bytes<T>(R, args.w);
-    if (smem <= kMaxSmem) break;
+  while (C < kPanelMaxC && (m + C - 1) / C > panel_target_rows()) C *= 2;
+  size_t smem = panel_smem_bytes<T, W>((m + C - 1) / C);
+  while (smem > kMaxSmem && C < kPanelMaxC) {
+    C *= 2;
+    smem = panel_smem_bytes<T, W>((m + C - 1) / C);
   }
-  if (C > 16) return ALG_BAD_SHAPE;  // panel too tall for one cluster
+  if (smem > kMaxSmem) return ALG_BAD_SHAPE;  // panel too tall for one cluster
   static bool configured = false;
   if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, EXACT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem + 1024));
-    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, EXACT>,
+    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, W, EXACT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, W, EXACT>,
                                       cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     configured = true;
   }
@@ -66,9 +80,74 @@ int launch_panel(alg_ctx* ctx, const PanelArgs<T>& args) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  ALG_CUDA_TRY(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<T, EXACT>, args));
+  double pflops = 0;
+  for (int j = 0; j < args.w; ++j) pflops += double(m - j - 1) * (1.0 + 2.0 * (args.w - j - 1));
+  const int tok = prof_begin(ctx, ALG_K_PANEL);
+  ALG_CUDA_TRY(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<T, W, EXACT>, args));
   count_launches();
+  prof_end(ctx, tok, pflops, 2.0 * sizeof(T) * m * args.w);
   return ALG_OK;
+}
+
+template <typename T, int W, int RPT, bool EXACT>
+int launch_panel_reg(alg_ctx* ctx, const PanelArgs<T>& args, int C) {
+  static bool configured = false;
+  if (!configured) {
+    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_reg_kernel<T, W, RPT, EXACT>,
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    configured = true;
+  }
+  const int m = args.n - args.c0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(kPanelRThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  double pflops = 0;
+  for (int j = 0; j < args.w; ++j) pflops += double(m - j - 1) * (1.0 + 2.0 * (args.w - j - 1));
+  const int tok = prof_begin(ctx, ALG_K_PANEL);
+  ALG_CUDA_TRY(cudaLaunchKernelEx(&cfg, panel_reg_kernel<T, W, RPT, EXACT>, args));
+  count_launches();
+  prof_end(ctx, tok, pflops, 2.0 * sizeof(T) * m * args.w);
+  return ALG_OK;
+}
+
+// Register-resident rows when a 16-CTA cluster can hold the panel's rows at
+// up to four rows per thread (two for 32 double columns); the shared-memory
+// slab kernel otherwise.
+template <typename T, bool EXACT>
+int launch_panel(alg_ctx* ctx, const PanelArgs<T>& args) {
+  const int m = args.n - args.c0;
+  const int max_rpt = (args.w > 16 && sizeof(T) == 8) ? 2 : 4;
+  const int target = std::max(1, panel_target_rows());
+  if (m <= kPanelMaxC * kPanelRThreads * max_rpt && !std::getenv("ALG_PANEL_SMEM")) {
+    int C = 1;
+    while (C < kPanelMaxC && (m + C - 1) / C > std::min(target, max_rpt * kPanelRThreads)) C *= 2;
+    while (C < kPanelMaxC && (m + C - 1) / C > max_rpt * kPanelRThreads) C *= 2;
+    const int R = (m + C - 1) / C;
+    const int rpt = R <= kPanelRThreads ? 1 : (R <= 2 * kPanelRThreads ? 2 : 4);
+    if (args.w <= 16) {
+      if (rpt == 1) return launch_panel_reg<T, 16, 1, EXACT>(ctx, args, C);
+      if (rpt == 2) return launch_panel_reg<T, 16, 2, EXACT>(ctx, args, C);
+      return launch_panel_reg<T, 16, 4, EXACT>(ctx, args, C);
+    }
+    if (rpt == 1) return launch_panel_reg<T, 32, 1, EXACT>(ctx, args, C);
+    if constexpr (sizeof(T) == 8) {
+      return launch_panel_reg<T, 32, 2, EXACT>(ctx, args, C);
+    } else {
+      if (rpt == 2) return launch_panel_reg<T, 32, 2, EXACT>(ctx, args, C);
+      return launch_panel_reg<T, 32, 4, EXACT>(ctx, args, C);
+    }
+  }
+  if (args.w <= 16) return launch_panel_w<T, 16, EXACT>(ctx, args);
+  return launch_panel_w<T, 32, EXACT>(ctx, args);
 }
 
 template <typename T, bool EXACT>
@@ -82,8 +161,10 @@ int launch_trsm(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
     configured = true;
   }
   const int grid = (ce - cb + kTrsmCols - 1) / kTrsmCols;
+  const int tok = prof_begin(ctx, ALG_K_TRSM);
   trsm_lower_unit_kernel<T, EXACT><<<grid, kTrsmThreads, smem, ctx->stream>>>(a, lda, r0, kb, cb, ce);
-    count_launches();
+  count_launches();
+  prof_end(ctx, tok, double(kb) * (kb - 1) * (ce - cb), sizeof(T) * (double(kb) * kb / 2 + 2.0 * kb * (ce - cb)));
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
 }
@@ -95,8 +176,10 @@ int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T
                  T* C, int ldc) {
   if (M <= 0 || N <= 0 || K <= 0) return ALG_OK;
   dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + kGemmBN - 1) / kGemmBN);
+  const int tok = prof_begin(ctx, ALG_K_GEMM);
   gemm_sub_kernel<T, EXACT><<<grid, kGemmThreads, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
-    count_launches();
+  count_launches();
+  prof_end(ctx, tok, 2.0 * M * N * K, sizeof(T) * (2.0 * M * N + double(M) * K + double(K) * N));
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
 }
@@ -147,9 +230,11 @@ int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* pe
     if (n_out > 0 || perm != nullptr) {
       const int warps_needed = std::max(1, n_out);
       const int grid = std::max(1, std::min(4 * ctx->sm_count, (warps_needed + 7) / 8));
+      const int tok = prof_begin(ctx, ALG_K_LASWP);
       laswp_outside_kernel<T><<<grid, kSwapThreads, 0, ctx->stream>>>(a, lda, m, nc, k0, kb, lab, perm,
                                                                         perm_tmp);
-    count_launches();
+      count_launches();
+      prof_end(ctx, tok, 0.0, 0.0);
       ALG_CUDA_TRY(cudaGetLastError());
     }
     const int kr = k0 + kb;
@@ -173,6 +258,7 @@ int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* 
   T* x = nullptr;
   ALG_TRY(ws_get(ctx, WS_X, sizeof(T) * (size_t)n * nrhs, reinterpret_cast<void**>(&x)));
   const int ldx = n;
+  const int tok = prof_begin(ctx, ALG_K_SOLVE);
   {
     dim3 grid(std::min(1024, (n + kSolveThreads - 1) / kSolveThreads), nrhs);
     solve_gather_kernel<T><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, perm, b, ldb, x, ldx);
@@ -209,6 +295,7 @@ int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* 
   }
   ALG_CUDA_TRY(cudaMemcpy2DAsync(b, sizeof(T) * (size_t)ldb, x, sizeof(T) * (size_t)ldx,
                                  sizeof(T) * (size_t)n, nrhs, cudaMemcpyDeviceToDevice, ctx->stream));
+  prof_end(ctx, tok, 2.0 * n * n * nrhs, sizeof(T) * (double(n) * n + 4.0 * n * nrhs));
   return ALG_OK;
 }
 
@@ -355,6 +442,17 @@ int alg_dgetrf_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda, int32_
   if (ipiv == nullptr) ALG_TRY(alg::ws_get(ctx, alg::WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&ipiv)));
   ALG_TRY(alg::status_reset(ctx));
   ALG_TRY(factor_any(ctx, update, d_a, n, n, lda, ipiv, d_perm));
+  ALG_TRY(alg::status_fetch(ctx));
+  return ctx->h_status->singular_col != INT_MAX ? ALG_SINGULAR : ALG_OK;
+}
+
+int alg_dgetrf_rect_dev(alg_ctx* ctx, int update, double* d_a, int nrows, int ncols, int lda,
+                        int32_t* d_ipiv) {
+  if (ctx == nullptr || d_ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  if (nrows < ncols || ncols < 0 || lda < std::max(1, nrows)) return ALG_BAD_SHAPE;
+  if (ncols == 0) return ALG_OK;
+  ALG_TRY(alg::status_reset(ctx));
+  ALG_TRY(factor_any(ctx, update, d_a, nrows, ncols, lda, d_ipiv, nullptr));
   ALG_TRY(alg::status_fetch(ctx));
   return ctx->h_status->singular_col != INT_MAX ? ALG_SINGULAR : ALG_OK;
 }

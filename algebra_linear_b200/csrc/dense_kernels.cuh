@@ -23,22 +23,29 @@ namespace cg = cooperative_groups;
 // ---------------------------------------------------------------------------
 // K1: leaf panel LU on one thread-block cluster.
 //
-// Factors the n_rows x w leaf panel whose top-left entry is (c0, c0). The
-// rows are split into C contiguous slabs, one per CTA of the cluster, each
-// held in shared memory for the whole panel. Per column j:
-//   1. every CTA finds its slab's candidate (first index of max |a_ij|; the
-//      row-j entry counts a NaN as the maximum, other rows never pick a NaN —
-//      the exact semantics of the strict '>' scan seeded with |a_jj|,
-//      mod.rs:123-134) and publishes it with a copy of the row;
-//   2. one cluster barrier;
-//   3. every CTA reads the C candidates over DSMEM, takes the same winner,
-//      swaps rows j and p inside the slabs that own them, and applies the
-//      rank-1 update to its own rows (mod.rs:141-159).
-// Publication buffers are double-buffered by column parity, so a column costs
-// one barrier. Rows carry two labels through the swaps: the original row
-// index within the current block-panel (for the deferred interchange of the
+// Factors the (m - c0) x w leaf panel whose top-left entry is (c0, c0). Its
+// rows are split into C contiguous slabs, one per CTA of the cluster, held in
+// shared memory for the whole panel (W = 16 or 32 columns, padded stride).
+// Thread (g, c) of a CTA owns column c of the slab rows g, g+G, g+2G, ...
+//
+// Pivot exchange without cluster barriers: for column j every CTA sends a
+// record — its candidate (first index of max |a_ij| with the reference's NaN
+// rule, mod.rs:123-134), a copy of that row and its labels — into the
+// mailbox of every CTA of the cluster with st.async DSMEM stores that count
+// their bytes on the receiver's mbarrier; the owner of row j also sends a
+// copy of row j. A CTA waits on its own mbarrier only, and every warp reduces
+// the C records redundantly to the same winner. Mailboxes and mbarriers are
+// double-buffered by column parity; a sender can only reach column j+2 after
+// every CTA has consumed column j (it needs their column j+1 records), so a
+// buffer is never overwritten while it is read.
+//
+// Per column j, after the exchange: swap rows j and p (mod.rs:141-146),
+// divide the rows below by the pivot (true division, mod.rs:153-155), apply
+// the rank-1 update (mod.rs:156-158) and scan column j+1 for the next
+// candidate. Rows carry two labels through the swaps: the original row within
+// the enclosing block-panel (for the deferred interchange of the matrix's
 // other columns) and within this leaf (for the block-panel's other columns,
-// which this kernel swaps itself at the end).
+// which this kernel swaps itself before it exits).
 // ---------------------------------------------------------------------------
 template <typename T>
 struct PanelArgs {
@@ -46,7 +53,7 @@ struct PanelArgs {
   int lda;
   int n;           // rows of the matrix
   int c0;          // first row and column of the leaf
-  int w;           // leaf width
+  int w;           // leaf width (<= W)
   int kb0, kb1;    // columns of the enclosing block-panel
   int* ipiv;       // global interchanges (0-based global rows)
   int* lab;        // cumulative source labels of rows [kb0, n)
@@ -54,25 +61,45 @@ struct PanelArgs {
   DevStatus* status;
 };
 
-constexpr int kPanelThreads = 256;
+constexpr int kPanelThreads = 512;
+constexpr int kPanelWarps = kPanelThreads / 32;
 constexpr int kPanelMaxW = 32;
+constexpr int kPanelMaxC = 16;
+constexpr int kSideCols = 16;  // block-panel columns swapped per pass at exit
 
-template <typename T>
-__host__ __device__ inline size_t panel_smem_bytes(int rows_per_cta, int w) {
-  size_t b = 0;
-  b += sizeof(T) * (size_t)rows_per_cta * (w + 1);   // tile
-  b += sizeof(T) * 6 * (size_t)kPanelMaxW;            // pub_row[2], pub_diag[2], u_s, spare
-  b += sizeof(int) * 2 * (size_t)rows_per_cta;        // cumulative + leaf labels
-  b += 64 * sizeof(double);                           // keys, indices, labels, reductions
-  b += 2 * kPanelMaxW * (kPanelMaxW + 2) * sizeof(T); // gathered rows for the side swap
-  b += 4 * kPanelMaxW * sizeof(int);                  // side-swap bookkeeping
-  return (b + 255) & ~size_t(255);
-}
-
-struct KeyIdx {
-  double key;
-  int idx;
+// One mailbox record, in 8-byte words: key, (row, cumulative label),
+// (leaf label, unused), then the row's W entries.
+template <typename T, int W>
+struct PanelRec {
+  static constexpr int kRowWords = (W * (int)sizeof(T)) / 8;
+  static constexpr int kWords = (3 + kRowWords + 1) & ~1;     // padded to 16 bytes
+  static constexpr int kBytes = 8 * kWords;
+  static constexpr int kDiagWords = (1 + kRowWords + 1) & ~1;  // (cumulative, leaf label), row
+  static constexpr int kDiagBytes = 8 * kDiagWords;
 };
+
+template <typename T, int W>
+struct PanelSmem {
+  unsigned long long mbar[2];
+  alignas(16) unsigned long long rec[2][kPanelMaxC][PanelRec<T, W>::kWords];
+  alignas(16) unsigned long long diag[2][PanelRec<T, W>::kDiagWords];
+  alignas(16) unsigned long long outbox[2][PanelRec<T, W>::kWords];
+  alignas(16) unsigned long long doutbox[2][PanelRec<T, W>::kDiagWords];
+  double cand_key[kPanelWarps];
+  int cand_idx[kPanelWarps];
+  T side_vals[4 * kPanelMaxW][kSideCols];
+  int side_rows[4 * kPanelMaxW];
+  int side_cnt;
+};
+
+template <typename T, int W>
+__host__ __device__ inline size_t panel_smem_bytes(int rows_per_cta) {
+  size_t b = sizeof(PanelSmem<T, W>);
+  b = (b + 15) & ~size_t(15);
+  b += sizeof(T) * (size_t)rows_per_cta * (W + 1);  // slab
+  b += sizeof(int) * 2 * (size_t)rows_per_cta;     // labels
+  return (b + 127) & ~size_t(127);
+}
 
 __device__ __forceinline__ void keyidx_combine(double& k, int& i, double ok, int oi) {
   if (ok > k || (ok == k && oi < i)) {
@@ -81,8 +108,408 @@ __device__ __forceinline__ void keyidx_combine(double& k, int& i, double ok, int
   }
 }
 
-template <typename T, bool EXACT>
+__device__ __forceinline__ double pivot_key(double v, bool is_diag) {
+  const double a = fabs(v);
+  if (isnan(a)) return is_diag ? CUDART_INF : -CUDART_INF;
+  return a;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_async_b64(uint32_t remote, unsigned long long v, uint32_t remote_bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
+               :: "r"(remote), "l"(v), "r"(remote_bar) : "memory");
+}
+// One bulk copy (async proxy) of `bytes` from this CTA's shared memory into
+// the shared memory of a CTA of the cluster, completing on that CTA's mbarrier.
+// Addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_to_cta(uint32_t remote_dst, uint32_t local_src, int bytes, uint32_t remote_bar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :: "r"(remote_dst), "r"(local_src), "r"(bytes), "r"(remote_bar) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arm(uint32_t bar, int bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+// Waits for the phase of the given parity; gives up after kWaitLimitNs and
+// returns false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, int parity) {
+  uint32_t done = 0;
+  uint64_t t0 = 0;
+  for (int it = 0;; ++it) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+    if (done) return true;
+    if ((it & 63) == 0) {
+      const uint64_t t = global_timer_ns();
+      if (it == 0) t0 = t;
+      else if (t - t0 > kWaitLimitNs) return false;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ unsigned long long pack2(T a, T b);
+template <>
+__device__ __forceinline__ unsigned long long pack2<float>(float a, float b) {
+  return (unsigned long long)__float_as_uint(a) | ((unsigned long long)__float_as_uint(b) << 32);
+}
+__device__ __forceinline__ unsigned long long pack_ii(int a, int b) {
+  return (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32);
+}
+
+// Word k of a slab row, as the record stores it.
+template <typename T, int W>
+__device__ __forceinline__ unsigned long long row_word(const T* row, int k) {
+  if constexpr (sizeof(T) == 8) {
+    return (unsigned long long)__double_as_longlong(static_cast<double>(row[k]));
+  } else {
+    return pack2<float>(static_cast<float>(row[2 * k]), static_cast<float>(row[2 * k + 1]));
+  }
+}
+template <typename T>
+__device__ __forceinline__ T rec_entry(const unsigned long long* words, int c) {
+  if constexpr (sizeof(T) == 8) {
+    return static_cast<T>(__longlong_as_double((long long)words[c]));
+  } else {
+    const unsigned long long wv = words[c >> 1];
+    return static_cast<T>(__uint_as_float((unsigned)(c & 1 ? (wv >> 32) : wv)));
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ bool div_fast_ok(T x) {
+  const double ax = fabs(static_cast<double>(x));
+  if constexpr (sizeof(T) == 8) {
+    return ax >= 0x1p-500 && ax <= 0x1p500;
+  } else {
+    return ax >= 0x1p-60f && ax <= 0x1p60f;
+  }
+}
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// a / d correctly rounded; y = RN(1/d), fast = d passed div_fast_ok.
+template <typename T>
+__device__ __forceinline__ T quotient(T a, T d, T y, bool fast) {
+  if (fast && div_fast_ok(a)) {
+    const T q = mul_rn(a, y);
+    const T r = fma_rn(-q, d, a);
+    return fma_rn(r, y, q);
+  }
+  return div_rn(a, d);
+}
+
+template <typename T, int W, bool EXACT>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelArgs<T> p) {
+  using Rec = PanelRec<T, W>;
+  constexpr int G = kPanelThreads / W;  // row groups
+  constexpr int LD = W + 1;
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks();
+  const int q = (int)cl.block_rank();
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int c = tid % W;   // column owned by this thread
+  const int g = tid / W;   // row group
+  const int m = p.n - p.c0;
+  const int R = (m + C - 1) / C;
+  const int rb = q * R;
+  const int re = min(m, rb + R);
+  const int nr = max(0, re - rb);
+  const int w = p.w;
+  const int step_bytes = C * Rec::kBytes + Rec::kDiagBytes;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PanelSmem<T, W>& S = *reinterpret_cast<PanelSmem<T, W>*>(smem_raw);
+  T* tile = reinterpret_cast<T*>(smem_raw + ((sizeof(PanelSmem<T, W>) + 15) & ~size_t(15)));
+  int* lab_s = reinterpret_cast<int*>(tile + (size_t)R * LD);
+  int* loc_s = lab_s + R;
+
+  // ---- load the slab, set up the mailboxes ----------------------------------
+  for (int cc = 0; cc < W; ++cc) {
+    const T* col = p.a + (size_t)(p.c0 + cc) * p.lda + (p.c0 + rb);
+    for (int r = tid; r < nr; r += kPanelThreads) tile[r * LD + cc] = cc < w ? col[r] : T(0);
+  }
+  for (int r = tid; r < nr; r += kPanelThreads) {
+    const int gr = p.c0 + rb + r;
+    lab_s[r] = p.first_leaf ? gr : p.lab[gr];
+    loc_s[r] = gr;
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&S.mbar[0]), 1);
+    mbar_init(smem_u32(&S.mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_arm(smem_u32(&S.mbar[0]), step_bytes);
+    if (w > 1) mbar_arm(smem_u32(&S.mbar[1]), step_bytes);
+  }
+  cl.sync();  // mbarriers live in every CTA before anyone sends
+
+  // first candidate (column 0)
+  {
+    double bk = -CUDART_INF;
+    int bi = INT_MAX;
+    if (c == 0) {
+      for (int r = g; r < nr; r += G) {
+        const double key = pivot_key((double)tile[r * LD], rb + r == 0);
+        if (key > bk) { bk = key; bi = rb + r; }
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ok = __shfl_down_sync(0xffffffffu, bk, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      keyidx_combine(bk, bi, ok, oi);
+    }
+    if (lane == 0) { S.cand_key[warp] = bk; S.cand_idx[warp] = bi; }
+  }
+  __syncthreads();
+
+  const uint32_t rec_base = smem_u32(&S.rec[0][0][0]);
+  const uint32_t diag_base = smem_u32(&S.diag[0][0]);
+  const uint32_t bar_base = smem_u32(&S.mbar[0]);
+  bool ok_wait = true;
+
+  for (int j = 0; j < w; ++j) {
+    const int par = j & 1;
+    // ---- send: CTA candidate record (+ row j) to every mailbox -------------
+    if (warp == 0) {
+      double bk = -CUDART_INF;
+      int bi = INT_MAX;
+      if (lane < kPanelWarps) { bk = S.cand_key[lane]; bi = S.cand_idx[lane]; }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ok = __shfl_down_sync(0xffffffffu, bk, off);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        keyidx_combine(bk, bi, ok, oi);
+      }
+      bk = __shfl_sync(0xffffffffu, bk, 0);
+      bi = __shfl_sync(0xffffffffu, bi, 0);
+      const bool have = bi != INT_MAX;
+      const T* crow = have ? tile + (size_t)(bi - rb) * LD : tile;
+      const bool own_j = j >= rb && j < re;
+      const T* drow = own_j ? tile + (size_t)(j - rb) * LD : tile;
+      unsigned long long* ob = &S.outbox[par][0];
+      unsigned long long* dob = &S.doutbox[par][0];
+      for (int kw = lane; kw < Rec::kWords; kw += 32) {
+        unsigned long long val = 0;
+        if (kw == 0) val = (unsigned long long)__double_as_longlong(bk);
+        else if (kw == 1) val = pack_ii(bi, have ? lab_s[bi - rb] : 0);
+        else if (kw == 2) val = pack_ii(have ? loc_s[bi - rb] : 0, 0);
+        else if (kw < 3 + Rec::kRowWords) val = row_word<T, W>(crow, kw - 3);
+        ob[kw] = val;
+      }
+      if (own_j) {
+        for (int kw = lane; kw < Rec::kDiagWords; kw += 32) {
+          unsigned long long val = 0;
+          if (kw == 0) val = pack_ii(lab_s[j - rb], loc_s[j - rb]);
+          else if (kw < 1 + Rec::kRowWords) val = row_word<T, W>(drow, kw - 1);
+          dob[kw] = val;
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane < C) {
+        const uint32_t rbar = mapa_u32(bar_base + 8u * par, lane);
+        const uint32_t la = rec_base + 8u * (uint32_t)((par * kPanelMaxC + q) * Rec::kWords);
+        bulk_to_cta(mapa_u32(la, lane), smem_u32(ob), Rec::kBytes, rbar);
+        if (own_j) {
+          const uint32_t ld2 = diag_base + 8u * (uint32_t)(par * Rec::kDiagWords);
+          bulk_to_cta(mapa_u32(ld2, lane), smem_u32(dob), Rec::kDiagBytes, rbar);
+        }
+      }
+    }
+    // ---- receive: wait for this column's records ---------------------------
+    // a wait that ran out stays failed: the rest of the leaf runs through
+    // without waiting and the host reports ALG_TIMEOUT
+    if (ok_wait && !mbar_wait(bar_base + 8u * par, (j >> 1) & 1)) {
+      ok_wait = false;
+      atomicExch(&p.status->timeout, 1);
+    }
+    __syncwarp();
+    if (tid == 0 && j + 2 < w) mbar_arm(bar_base + 8u * par, step_bytes);
+    // every warp reduces the C records to the same winner
+    double wk = -CUDART_INF;
+    int wi = INT_MAX, ws = 0;
+    if (lane < C) {
+      wk = __longlong_as_double((long long)S.rec[par][lane][0]);
+      wi = (int)(unsigned)(S.rec[par][lane][1] & 0xffffffffu);
+      ws = lane;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ok = __shfl_down_sync(0xffffffffu, wk, off);
+      const int oi = __shfl_down_sync(0xffffffffu, wi, off);
+      const int os = __shfl_down_sync(0xffffffffu, ws, off);
+      if (ok > wk || (ok == wk && oi < wi)) { wk = ok; wi = oi; ws = os; }
+    }
+    const int pr = __shfl_sync(0xffffffffu, wi, 0);  // winning panel row (>= j)
+    const int ps = __shfl_sync(0xffffffffu, ws, 0);  // CTA that sent it
+    const unsigned long long* wrow = &S.rec[par][ps][3];
+    const T d = rec_entry<T>(wrow, j);
+    const T u = rec_entry<T>(wrow, c);
+    // swap rows j and pr where this thread owns them (same thread updates them later)
+    if (j >= rb && j < re && (j - rb) % G == g) {
+      tile[(j - rb) * LD + c] = u;
+      if (c == 0) {
+        lab_s[j - rb] = (int)(unsigned)(S.rec[par][ps][1] >> 32);
+        loc_s[j - rb] = (int)(unsigned)(S.rec[par][ps][2] & 0xffffffffu);
+      }
+    }
+    if (pr != j && pr >= rb && pr < re && (pr - rb) % G == g) {
+      tile[(pr - rb) * LD + c] = rec_entry<T>(&S.diag[par][1], c);
+      if (c == 0) {
+        lab_s[pr - rb] = (int)(unsigned)(S.diag[par][0] & 0xffffffffu);
+        loc_s[pr - rb] = (int)(unsigned)(S.diag[par][0] >> 32);
+      }
+    }
+    if (tid == 0 && q == 0) {
+      p.ipiv[p.c0 + j] = p.c0 + pr;
+      if (fabs((double)d) <= 0.0) atomicMin(&p.status->singular_col, p.c0 + j);
+    }
+    __syncwarp();
+    // multipliers (correctly rounded quotient, as K1r) for the group's rows
+    // below j, spread over its lanes
+    const int r_first = max(0, j + 1 - rb);
+    const int r0 = r_first + ((g - r_first % G) + G) % G;  // first row >= r_first of group g
+    {
+      const bool fast = div_fast_ok(d);
+      const T y = fast ? rcp_rn(d) : T(1);
+      int k = 0;
+      for (int r = r0 + c * G; r < nr; r += W * G, k += W) {
+        const T av = tile[r * LD + j];
+        tile[r * LD + j] = quotient<T>(av, d, y, fast);
+      }
+    }
+    __syncwarp();
+    // rank-1 update, 8 independent rows per batch; column j+1 yields the next candidate
+    double bk = -CUDART_INF;
+    int bi = INT_MAX;
+    if (c > j && c < w) {
+      constexpr int B = 8;
+      for (int rs = r0; rs < nr; rs += B * G) {
+        T av[B], lv[B];
+#pragma unroll
+        for (int t = 0; t < B; ++t) {
+          const int r = rs + t * G;
+          av[t] = r < nr ? tile[r * LD + c] : T(0);
+          lv[t] = r < nr ? tile[r * LD + j] : T(0);
+        }
+#pragma unroll
+        for (int t = 0; t < B; ++t) av[t] = msub<EXACT>(av[t], lv[t], u);
+#pragma unroll
+        for (int t = 0; t < B; ++t) {
+          const int r = rs + t * G;
+          if (r < nr) {
+            tile[r * LD + c] = av[t];
+            if (c == j + 1) {
+              const double key = pivot_key((double)av[t], rb + r == j + 1);
+              if (key > bk) { bk = key; bi = rb + r; }
+            }
+          }
+        }
+      }
+    }
+    if (j + 1 < w) {
+      // collect the candidates of the warp's row groups (lanes with c == j+1)
+      const int src0 = (lane / W) * W + (j + 1);  // own group's candidate lane
+      double k0 = __shfl_sync(0xffffffffu, bk, src0 & 31);
+      int i0 = __shfl_sync(0xffffffffu, bi, src0 & 31);
+      if constexpr (W == 16) {
+        const double k1 = __shfl_sync(0xffffffffu, bk, (j + 1 + 16 - (lane / W) * W) & 31);
+        const int i1 = __shfl_sync(0xffffffffu, bi, (j + 1 + 16 - (lane / W) * W) & 31);
+        keyidx_combine(k0, i0, k1, i1);
+      }
+      if (lane == 0) { S.cand_key[warp] = k0; S.cand_idx[warp] = i0; }
+    }
+    __syncthreads();
+  }
+  cl.sync();  // every record consumed; no DSMEM access outlives its owner
+
+  // ---- swap the block-panel's other columns by this leaf's interchanges -----
+  // Rows whose leaf label moved take the old content of the labelled row; all
+  // reads of a pass precede the cluster barrier, all writes follow it.
+  if (tid == 0) S.side_cnt = 0;
+  __syncthreads();
+  for (int r = tid; r < nr; r += kPanelThreads) {
+    if (loc_s[r] != p.c0 + rb + r) {
+      const int s = atomicAdd(&S.side_cnt, 1);
+      if (s < 4 * kPanelMaxW) S.side_rows[s] = r;
+    }
+  }
+  __syncthreads();
+  const int n_side = min(S.side_cnt, 4 * kPanelMaxW);
+  const int side_w = (p.kb1 - p.kb0) - w;
+  for (int cbase = 0; cbase < side_w; cbase += kSideCols) {
+    const int ncol = min(kSideCols, side_w - cbase);
+    for (int idx = tid; idx < n_side * kSideCols; idx += kPanelThreads) {
+      const int s = idx / kSideCols, cc = idx % kSideCols;
+      if (cc >= ncol) continue;
+      int col = p.kb0 + cbase + cc;
+      if (col >= p.c0) col += w;
+      S.side_vals[s][cc] = p.a[(size_t)loc_s[S.side_rows[s]] + (size_t)col * p.lda];
+    }
+    cl.sync();
+    for (int idx = tid; idx < n_side * kSideCols; idx += kPanelThreads) {
+      const int s = idx / kSideCols, cc = idx % kSideCols;
+      if (cc >= ncol) continue;
+      int col = p.kb0 + cbase + cc;
+      if (col >= p.c0) col += w;
+      p.a[(size_t)(p.c0 + rb + S.side_rows[s]) + (size_t)col * p.lda] = S.side_vals[s][cc];
+    }
+    cl.sync();
+  }
+
+  // ---- write the slab back ------------------------------------------------
+  for (int cc = 0; cc < w; ++cc) {
+    T* col = p.a + (size_t)(p.c0 + cc) * p.lda + (p.c0 + rb);
+    for (int r = tid; r < nr; r += kPanelThreads) col[r] = tile[r * LD + cc];
+  }
+  for (int r = tid; r < nr; r += kPanelThreads) p.lab[p.c0 + rb + r] = lab_s[r];
+}
+
+// ---------------------------------------------------------------------------
+// K1r: leaf panel LU with register-resident rows (m <= 16 * 256 * RPT).
+//
+// Same cluster decomposition and st.async pivot exchange as K1, but every
+// thread keeps RPT whole rows of the slab (W entries each) in registers for
+// the whole panel, so the per-column update is W independent multiply-
+// subtracts per row with no shared-memory round trips, and the column loop is
+// unrolled (register indices are static). Per column: candidate from
+// registers -> warp shuffle -> one CTA barrier -> warp 0 sends the CTA record
+// -> every thread waits on its CTA's mbarrier -> swap / divide / update.
+//
+// Division: the multiplier is the correctly rounded quotient a/d
+// (mod.rs:154). With y = RN(1/d) computed once per column, q = RN(a*y) is
+// within one ulp of a/d, the remainder a - q*d is exact under an FMA, and
+// RN(q + (a - q*d)*y) is the correctly rounded quotient (Markstein's
+// theorem), as long as nothing over- or underflows; entries and pivots outside
+// [2^-500, 2^500] in magnitude, zeros and non-finite values take the plain
+// IEEE division instead.
+// ---------------------------------------------------------------------------
+constexpr int kPanelRThreads = 256;
+
+template <typename T, int W, int RPT, bool EXACT>
+__global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<T> p) {
+  using Rec = PanelRec<T, W>;
+  constexpr int NT = kPanelRThreads;
+  constexpr int NW = NT / 32;
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks();
   const int q = (int)cl.block_rank();
@@ -94,188 +521,292 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
   const int re = min(m, rb + R);
   const int nr = max(0, re - rb);
   const int w = p.w;
-  const int ld = w + 1;
+  const int step_bytes = C * Rec::kBytes + Rec::kDiagBytes;
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* tile = reinterpret_cast<T*>(smem_raw);
-  T* pub_row = tile + (size_t)R * ld;        // [2][kPanelMaxW]
-  T* pub_diag = pub_row + 2 * kPanelMaxW;    // [2][kPanelMaxW]
-  T* u_s = pub_diag + 2 * kPanelMaxW;        // [kPanelMaxW]
-  int* lab_s = reinterpret_cast<int*>(u_s + 2 * kPanelMaxW);  // [R]
-  int* loc_s = lab_s + R;                                      // [R]
-  double* misc = reinterpret_cast<double*>(
-      (reinterpret_cast<uintptr_t>(loc_s + R) + 15) & ~uintptr_t(15));
-  double* pub_key = misc;                                  // [2]
-  double* red_key = misc + 2;                              // [8]
-  int* pub_idx = reinterpret_cast<int*>(misc + 10);        // [2]
-  int* pub_rlab = pub_idx + 2;                             // [2][2] candidate row labels
-  int* pub_dlab = pub_rlab + 4;                            // [2][2] diagonal row labels
-  int* red_idx = pub_dlab + 4;                             // [8]
-  int* win = red_idx + 8;                                  // [4]
-  T* side_vals = reinterpret_cast<T*>(misc + 64);          // [2*kPanelMaxW][kPanelMaxW+2]
-  int* side_rows = reinterpret_cast<int*>(side_vals + 2 * kPanelMaxW * (kPanelMaxW + 2));
-  int* side_cnt = side_rows + 2 * kPanelMaxW;
+  __shared__ unsigned long long mbar[2];
+  __shared__ __align__(16) unsigned long long rec[2][kPanelMaxC][Rec::kWords];
+  __shared__ __align__(16) unsigned long long diag[2][Rec::kDiagWords];
+  __shared__ __align__(16) unsigned long long outbox[2][Rec::kWords];
+  __shared__ __align__(16) unsigned long long doutbox[2][Rec::kDiagWords];
+  __shared__ double cand_key[2][NW];
+  __shared__ int cand_idx[2][NW];
+  __shared__ int cand_lab[2][NW][2];
+  __shared__ T stage[2][NW][W];
+  __shared__ T dstage[2][W];
+  __shared__ int dlab[2][2];
+  __shared__ T side_vals[4 * kPanelMaxW][kSideCols];
+  __shared__ int side_rows[4 * kPanelMaxW];
+  __shared__ int side_src[4 * kPanelMaxW];
+  __shared__ int side_cnt;
 
-  // ---- load the slab ------------------------------------------------------
-  for (int idx = tid; idx < nr * w; idx += kPanelThreads) {
-    const int r = idx % nr, c = idx / nr;
-    tile[r * ld + c] = p.a[(size_t)(p.c0 + rb + r) + (size_t)(p.c0 + c) * p.lda];
-  }
-  for (int r = tid; r < nr; r += kPanelThreads) {
-    const int g = p.c0 + rb + r;
-    lab_s[r] = p.first_leaf ? g : p.lab[g];
-    loc_s[r] = g;
-  }
-  __syncthreads();
-
-  for (int j = 0; j < w; ++j) {
-    const int par = j & 1;
-    // ---- 1. slab candidate -------------------------------------------------
-    double bk = -CUDART_INF;
-    int bi = INT_MAX;
-    for (int r = tid; r < nr; r += kPanelThreads) {
-      const int gr = rb + r;
-      if (gr < j) continue;
-      const double v = fabs(static_cast<double>(tile[r * ld + j]));
-      double key;
-      if (gr == j) key = isnan(v) ? CUDART_INF : v;
-      else key = isnan(v) ? -CUDART_INF : v;
-      if (key > bk) { bk = key; bi = gr; }
-    }
+  // ---- rows into registers ----------------------------------------------
+  T v[RPT][W];
+  int lab[RPT], loc[RPT];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ok = __shfl_down_sync(0xffffffffu, bk, off);
-      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-      keyidx_combine(bk, bi, ok, oi);
-    }
-    if (lane == 0) { red_key[warp] = bk; red_idx[warp] = bi; }
-    __syncthreads();
-    if (tid == 0) {
-      for (int w2 = 1; w2 < kPanelThreads / 32; ++w2) keyidx_combine(bk, bi, red_key[w2], red_idx[w2]);
-      pub_key[par] = bk;
-      pub_idx[par] = bi;
-      win[3] = bi;
-      if (bi != INT_MAX) {
-        pub_rlab[par * 2 + 0] = lab_s[bi - rb];
-        pub_rlab[par * 2 + 1] = loc_s[bi - rb];
-      }
-      if (j >= rb && j < re) {
-        pub_dlab[par * 2 + 0] = lab_s[j - rb];
-        pub_dlab[par * 2 + 1] = loc_s[j - rb];
-      }
-    }
-    __syncthreads();
+  for (int k = 0; k < RPT; ++k) {
+    const int r = tid + k * NT;  // local row
+    const bool in = r < nr;
+    const int gr = p.c0 + rb + r;
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc)
+      v[k][cc] = (in && cc < w) ? p.a[(size_t)gr + (size_t)(p.c0 + cc) * p.lda] : T(0);
+    lab[k] = in ? (p.first_leaf ? gr : p.lab[gr]) : 0;
+    loc[k] = gr;
+  }
+  if (tid == 0 && C > 1) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_arm(smem_u32(&mbar[0]), step_bytes);
+    if (w > 1) mbar_arm(smem_u32(&mbar[1]), step_bytes);
+  }
+  cl.sync();
+
+  const uint32_t rec_base = smem_u32(&rec[0][0][0]);
+  const uint32_t diag_base = smem_u32(&diag[0][0]);
+  const uint32_t bar_base = smem_u32(&mbar[0]);
+  bool ok_wait = true;
+
+  // The column loop stays rolled: one copy of its code serves every column
+  // (an unrolled loop does not fit the instruction cache). Register entries
+  // are addressed with static indices under the predicates c == j / c > j.
+#pragma unroll 1
+  for (int j = 0; j < w; ++j) {
     {
-      const int mine = win[3];
-      if (mine != INT_MAX && tid < w) pub_row[par * kPanelMaxW + tid] = tile[(mine - rb) * ld + tid];
-      if (j >= rb && j < re && tid >= 64 && tid < 64 + w)
-        pub_diag[par * kPanelMaxW + (tid - 64)] = tile[(j - rb) * ld + (tid - 64)];
-    }
-    // ---- 2. cluster barrier (release/acquire at cluster scope) -------------
-    cl.sync();
-    // ---- 3. winner, swap, update ------------------------------------------
-    if (warp == 0) {
-      double k = -CUDART_INF;
-      int i = INT_MAX;
+      const int par = j & 1;
+      // ---- 1. candidate for column j from the registers ---------------------
+      double bk = -CUDART_INF;
+      int bi = INT_MAX;
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * NT;
+        T vj = v[k][0];
+#pragma unroll
+        for (int cc = 1; cc < W; ++cc)
+          if (cc == j) vj = v[k][cc];
+        if (r < nr && rb + r >= j) {
+          const double key = pivot_key((double)vj, rb + r == j);
+          if (key > bk) { bk = key; bi = rb + r; }
+        }
+      }
+      // owner of row j stages it (and its labels) for the diagonal record
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        if (tid + k * NT < nr && rb + tid + k * NT == j) {
+#pragma unroll
+          for (int cc = 0; cc < W; ++cc) dstage[par][cc] = v[k][cc];
+          dlab[par][0] = lab[k];
+          dlab[par][1] = loc[k];
+        }
+      }
+      double wk = bk;
+      int wi = bi;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ok = __shfl_xor_sync(0xffffffffu, wk, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, wi, off);
+        keyidx_combine(wk, wi, ok, oi);
+      }
+      // the lane holding the warp's best row stages it
+      if (wi != INT_MAX) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+          if (tid + k * NT < nr && rb + tid + k * NT == wi) {
+            cand_key[par][warp] = wk;
+            cand_idx[par][warp] = wi;
+            cand_lab[par][warp][0] = lab[k];
+            cand_lab[par][warp][1] = loc[k];
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) stage[par][warp][cc] = v[k][cc];
+          }
+        }
+      } else if (lane == 0) {
+        cand_key[par][warp] = -CUDART_INF;
+        cand_idx[par][warp] = INT_MAX;
+      }
+      __syncthreads();
+      // ---- 2. warp 0 sends the CTA record (and row j) to every mailbox -------
+      if (warp == 0) {
+        double ck = -CUDART_INF;
+        int ci = INT_MAX, cw = 0;
+        if (lane < NW) { ck = cand_key[par][lane]; ci = cand_idx[par][lane]; cw = lane; }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ok = __shfl_xor_sync(0xffffffffu, ck, off);
+          const int oi = __shfl_xor_sync(0xffffffffu, ci, off);
+          const int ow = __shfl_xor_sync(0xffffffffu, cw, off);
+          if (ok > ck || (ok == ck && oi < ci)) { ck = ok; ci = oi; cw = ow; }
+        }
+        const bool have = ci != INT_MAX;
+        const T* crow = &stage[par][cw][0];
+        const bool own_j = j >= rb && j < re;
+        // C == 1: the record goes straight into the CTA's own mailbox
+        unsigned long long* ob = C > 1 ? &outbox[par][0] : &rec[par][0][0];
+        unsigned long long* dob = C > 1 ? &doutbox[par][0] : &diag[par][0];
+        for (int kw = lane; kw < Rec::kWords; kw += 32) {
+          unsigned long long val = 0;
+          if (kw == 0) val = (unsigned long long)__double_as_longlong(ck);
+          else if (kw == 1) val = pack_ii(ci, have ? cand_lab[par][cw][0] : 0);
+          else if (kw == 2) val = pack_ii(have ? cand_lab[par][cw][1] : 0, 0);
+          else if (kw < 3 + Rec::kRowWords) val = row_word<T, W>(crow, kw - 3);
+          ob[kw] = val;
+        }
+        if (own_j) {
+          for (int kw = lane; kw < Rec::kDiagWords; kw += 32) {
+            unsigned long long val = 0;
+            if (kw == 0) val = pack_ii(dlab[par][0], dlab[par][1]);
+            else if (kw < 1 + Rec::kRowWords) val = row_word<T, W>(&dstage[par][0], kw - 1);
+            dob[kw] = val;
+          }
+        }
+        if (C > 1) {
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane < C) {
+            const uint32_t rbar = mapa_u32(bar_base + 8u * par, lane);
+            const uint32_t la = rec_base + 8u * (uint32_t)((par * kPanelMaxC + q) * Rec::kWords);
+            bulk_to_cta(mapa_u32(la, lane), smem_u32(ob), Rec::kBytes, rbar);
+            if (own_j) {
+              const uint32_t ld = diag_base + 8u * (uint32_t)(par * Rec::kDiagWords);
+              bulk_to_cta(mapa_u32(ld, lane), smem_u32(dob), Rec::kDiagBytes, rbar);
+            }
+          }
+        }
+      }
+      // ---- 3. wait for this column's records; every warp picks the winner ---
+      if (C == 1) {
+        __syncthreads();
+      } else {
+        if (ok_wait && !mbar_wait(bar_base + 8u * par, (j >> 1) & 1)) {
+          ok_wait = false;
+          atomicExch(&p.status->timeout, 1);
+        }
+        if (tid == 0 && j + 2 < w) mbar_arm(bar_base + 8u * par, step_bytes);
+      }
+      double xk = -CUDART_INF;
+      int xi = INT_MAX, xs = 0;
       if (lane < C) {
-        k = *cl.map_shared_rank(&pub_key[par], lane);
-        i = *cl.map_shared_rank(&pub_idx[par], lane);
+        xk = __longlong_as_double((long long)rec[par][lane][0]);
+        xi = (int)(unsigned)(rec[par][lane][1] & 0xffffffffu);
+        xs = lane;
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
-        const double ok = __shfl_down_sync(0xffffffffu, k, off);
-        const int oi = __shfl_down_sync(0xffffffffu, i, off);
-        keyidx_combine(k, i, ok, oi);
+        const double ok = __shfl_xor_sync(0xffffffffu, xk, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, xi, off);
+        const int os = __shfl_xor_sync(0xffffffffu, xs, off);
+        if (ok > xk || (ok == xk && oi < xi)) { xk = ok; xi = oi; xs = os; }
       }
-      if (lane == 0) win[0] = i;
-    }
-    __syncthreads();
-    const int pr = win[0];          // winning panel row (>= j)
-    const int po = pr / R;          // its owner
-    const int jo = j / R;           // owner of row j
-    if (tid < w) u_s[tid] = *cl.map_shared_rank(&pub_row[par * kPanelMaxW + tid], po);
-    if (q == po && pr != j && tid >= 64 && tid < 64 + w) {
-      tile[(pr - rb) * ld + (tid - 64)] = *cl.map_shared_rank(&pub_diag[par * kPanelMaxW + (tid - 64)], jo);
-    }
-    if (tid == 128) {
-      if (q == jo) {
-        lab_s[j - rb] = *cl.map_shared_rank(&pub_rlab[par * 2 + 0], po);
-        loc_s[j - rb] = *cl.map_shared_rank(&pub_rlab[par * 2 + 1], po);
+      const int pr = xi;  // winning panel row (>= j)
+      const int ps = xs;  // CTA that sent it
+      T u[W];
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) u[cc] = rec_entry<T>(&rec[par][ps][3], cc);
+      const T d = rec_entry<T>(&rec[par][ps][3], j);
+      // ---- 4. swap rows j and pr (registers of their owners) ----------------
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * NT;
+        if (r < nr) {
+          if (rb + r == j) {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) v[k][cc] = u[cc];
+            lab[k] = (int)(unsigned)(rec[par][ps][1] >> 32);
+            loc[k] = (int)(unsigned)(rec[par][ps][2] & 0xffffffffu);
+          } else if (rb + r == pr) {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) v[k][cc] = rec_entry<T>(&diag[par][1], cc);
+            lab[k] = (int)(unsigned)(diag[par][0] & 0xffffffffu);
+            loc[k] = (int)(unsigned)(diag[par][0] >> 32);
+          }
+        }
       }
-      if (q == po && pr != j) {
-        lab_s[pr - rb] = *cl.map_shared_rank(&pub_dlab[par * 2 + 0], jo);
-        loc_s[pr - rb] = *cl.map_shared_rank(&pub_dlab[par * 2 + 1], jo);
+      if (tid == 0 && q == 0) {
+        p.ipiv[p.c0 + j] = p.c0 + pr;
+        if (fabs((double)d) <= 0.0) atomicMin(&p.status->singular_col, p.c0 + j);
+      }
+      // ---- 5. divide and update the rows below j -----------------------------
+      const bool fast = div_fast_ok(d);
+      const T y = fast ? rcp_rn(d) : T(1);
+      T l[RPT];
+      bool fix = false;
+      T av[RPT];
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        av[k] = v[k][0];
+#pragma unroll
+        for (int cc = 1; cc < W; ++cc)
+          if (cc == j) av[k] = v[k][cc];
+        const T qv = mul_rn(av[k], y);
+        l[k] = fma_rn(fma_rn(-qv, d, av[k]), y, qv);
+        fix |= !(fast && div_fast_ok(av[k])) && (tid + k * NT < nr) && (rb + tid + k * NT > j);
+      }
+      if (fix) {  // zeros, non-finite values, extreme exponents: plain IEEE division
+#pragma unroll
+        for (int k = 0; k < RPT; ++k)
+          if (!(fast && div_fast_ok(av[k]))) l[k] = div_rn(av[k], d);
+      }
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * NT;
+        if (r < nr && rb + r > j) {
+#pragma unroll
+          for (int cc = 0; cc < W; ++cc) {
+            if (cc == j) v[k][cc] = l[k];
+            else if (cc > j) v[k][cc] = msub<EXACT>(v[k][cc], l[k], u[cc]);
+          }
+        }
       }
     }
-    __syncthreads();
-    if (q == jo && tid < w) tile[(j - rb) * ld + tid] = u_s[tid];
-    const T d = u_s[j];
-    if (q == 0 && tid == 0) {
-      p.ipiv[p.c0 + j] = p.c0 + pr;
-      if (fabs(static_cast<double>(d)) <= 0.0) atomicMin(&p.status->singular_col, p.c0 + j);
-    }
-    __syncthreads();
-    // multipliers (true division, mod.rs:154)
-    for (int r = tid; r < nr; r += kPanelThreads) {
-      if (rb + r > j) tile[r * ld + j] = div_rn(tile[r * ld + j], d);
-    }
-    __syncthreads();
-    const int wr = w - j - 1;
-    if (wr > 0) {
-      const int r_first = max(0, j + 1 - rb);
-      const int cnt = (nr - r_first) * wr;
-      for (int idx = tid; idx < cnt; idx += kPanelThreads) {
-        const int r = r_first + idx / wr;
-        const int c = j + 1 + idx % wr;
-        tile[r * ld + c] = msub<EXACT>(tile[r * ld + c], tile[r * ld + j], u_s[c]);
-      }
-    }
-    __syncthreads();
   }
+  cl.sync();  // every record consumed; no DSMEM access outlives its owner
 
   // ---- swap the block-panel's other columns by this leaf's interchanges -----
-  // Rows whose leaf label moved receive the old content of the labelled row.
-  // All reads happen before the cluster barrier, all writes after it.
-  if (tid == 0) side_cnt[0] = 0;
+  if (tid == 0) side_cnt = 0;
   __syncthreads();
-  for (int r = tid; r < nr; r += kPanelThreads) {
-    if (loc_s[r] != p.c0 + rb + r) {
-      const int s = atomicAdd(side_cnt, 1);
-      if (s < 2 * kPanelMaxW) side_rows[s] = r;
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int r = tid + k * NT;
+    if (r < nr && loc[k] != p.c0 + rb + r) {
+      const int s = atomicAdd(&side_cnt, 1);
+      if (s < 4 * kPanelMaxW) { side_rows[s] = r; side_src[s] = loc[k]; }
     }
   }
   __syncthreads();
-  const int n_side = min(side_cnt[0], 2 * kPanelMaxW);
-  const int side_w = (p.kb1 - p.kb0) - w;  // other columns of the block-panel
-  const int sw = min(side_w, kPanelMaxW + 2);
-  // other columns are processed in chunks of (kPanelMaxW + 2) columns
-  for (int cbase = 0; cbase < side_w; cbase += sw) {
-    const int ncol = min(sw, side_w - cbase);
-    for (int idx = tid; idx < n_side * ncol; idx += kPanelThreads) {
-      const int s = idx / ncol, cc = idx % ncol;
-      int col = p.kb0 + cbase + cc;
-      if (col >= p.c0) col += w;  // skip the leaf's own columns
-      const int src = loc_s[side_rows[s]];
-      side_vals[s * (kPanelMaxW + 2) + cc] = p.a[(size_t)src + (size_t)col * p.lda];
-    }
-    cl.sync();
-    for (int idx = tid; idx < n_side * ncol; idx += kPanelThreads) {
-      const int s = idx / ncol, cc = idx % ncol;
+  const int n_side = min(side_cnt, 4 * kPanelMaxW);
+  const int side_w = (p.kb1 - p.kb0) - w;
+  for (int cbase = 0; cbase < side_w; cbase += kSideCols) {
+    const int ncol = min(kSideCols, side_w - cbase);
+    for (int idx = tid; idx < n_side * kSideCols; idx += NT) {
+      const int s = idx / kSideCols, cc = idx % kSideCols;
+      if (cc >= ncol) continue;
       int col = p.kb0 + cbase + cc;
       if (col >= p.c0) col += w;
-      const int dst = p.c0 + rb + side_rows[s];
-      p.a[(size_t)dst + (size_t)col * p.lda] = side_vals[s * (kPanelMaxW + 2) + cc];
+      side_vals[s][cc] = p.a[(size_t)side_src[s] + (size_t)col * p.lda];
+    }
+    cl.sync();
+    for (int idx = tid; idx < n_side * kSideCols; idx += NT) {
+      const int s = idx / kSideCols, cc = idx % kSideCols;
+      if (cc >= ncol) continue;
+      int col = p.kb0 + cbase + cc;
+      if (col >= p.c0) col += w;
+      p.a[(size_t)(p.c0 + rb + side_rows[s]) + (size_t)col * p.lda] = side_vals[s][cc];
     }
     cl.sync();
   }
-  if (side_w <= 0) cl.sync();  // no DSMEM reader may outlive an owner
 
-  // ---- write the slab back ------------------------------------------------
-  for (int idx = tid; idx < nr * w; idx += kPanelThreads) {
-    const int r = idx % nr, c = idx / nr;
-    p.a[(size_t)(p.c0 + rb + r) + (size_t)(p.c0 + c) * p.lda] = tile[r * ld + c];
+  // ---- registers back to the matrix -------------------------------------
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int r = tid + k * NT;
+    if (r < nr) {
+      const int gr = p.c0 + rb + r;
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc)
+        if (cc < w) p.a[(size_t)gr + (size_t)(p.c0 + cc) * p.lda] = v[k][cc];
+      p.lab[gr] = lab[k];
+    }
   }
-  for (int r = tid; r < nr; r += kPanelThreads) p.lab[p.c0 + rb + r] = lab_s[r];
 }
 
 // ---------------------------------------------------------------------------
@@ -501,32 +1032,47 @@ __global__ void __launch_bounds__(kSolveThreads) solve_gather_kernel(
   }
 }
 
+// The diagonal blocks are staged in shared memory (Ls, kSolveB x kSolveB)
+// before their sequential sweep, so the sweep never waits on global memory.
 template <typename T, bool EXACT>
-__device__ void solve_diag_block_lower(const T* lu, int lda, T* xc, int j0, int bs, T* xs) {
-  // unit lower triangle of rows/cols [j0, j0+bs); xs is shared scratch [bs]
+__device__ void solve_diag_block_lower(const T* lu, int lda, T* xc, int j0, int bs, T* xs, T* Ls) {
+  // unit lower triangle of rows/cols [j0, j0+bs)
+  for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
+    const int i = idx % bs, k = idx / bs;
+    Ls[i + k * kSolveB] = lu[(size_t)(j0 + i) + (size_t)(j0 + k) * lda];
+  }
   for (int i = threadIdx.x; i < bs; i += blockDim.x) xs[i] = xc[j0 + i];
   __syncthreads();
-  for (int k = 0; k + 1 < bs; ++k) {
-    const T u = xs[k];
-    for (int i = k + 1 + threadIdx.x; i < bs; i += blockDim.x)
-      xs[i] = msub<EXACT>(xs[i], lu[(size_t)(j0 + i) + (size_t)(j0 + k) * lda], u);
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    // one warp: lanes own rows i = lane, lane+32; step k broadcasts x_k
+    for (int k = 0; k + 1 < bs; ++k) {
+      const T u = xs[k];
+      for (int i = k + 1 + threadIdx.x; i < bs; i += 32) xs[i] = msub<EXACT>(xs[i], Ls[i + k * kSolveB], u);
+      __syncwarp();
+    }
   }
+  __syncthreads();
   for (int i = threadIdx.x; i < bs; i += blockDim.x) xc[j0 + i] = xs[i];
 }
 
 template <typename T, bool EXACT>
-__device__ void solve_diag_block_upper(const T* lu, int lda, T* xc, int j0, int bs, T* xs) {
+__device__ void solve_diag_block_upper(const T* lu, int lda, T* xc, int j0, int bs, T* xs, T* Ls) {
+  for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
+    const int i = idx % bs, k = idx / bs;
+    Ls[i + k * kSolveB] = lu[(size_t)(j0 + i) + (size_t)(j0 + k) * lda];
+  }
   for (int i = threadIdx.x; i < bs; i += blockDim.x) xs[i] = xc[j0 + i];
   __syncthreads();
-  for (int k = bs - 1; k >= 0; --k) {
-    if (threadIdx.x == 0) xs[k] = div_rn(xs[k], lu[(size_t)(j0 + k) + (size_t)(j0 + k) * lda]);
-    __syncthreads();
-    const T u = xs[k];
-    for (int i = threadIdx.x; i < k; i += blockDim.x)
-      xs[i] = msub<EXACT>(xs[i], lu[(size_t)(j0 + i) + (size_t)(j0 + k) * lda], u);
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int k = bs - 1; k >= 0; --k) {
+      if (threadIdx.x == 0) xs[k] = div_rn(xs[k], Ls[k + k * kSolveB]);
+      __syncwarp();
+      const T u = xs[k];
+      for (int i = threadIdx.x; i < k; i += 32) xs[i] = msub<EXACT>(xs[i], Ls[i + k * kSolveB], u);
+      __syncwarp();
+    }
   }
+  __syncthreads();
   for (int i = threadIdx.x; i < bs; i += blockDim.x) xc[j0 + i] = xs[i];
 }
 
@@ -537,6 +1083,7 @@ __global__ void __launch_bounds__(kSolveThreads) solve_fwd_kernel(
     const T* __restrict__ lu, int lda, int n, T* __restrict__ x, int ldx, int j0, int bs) {
   __shared__ T xb[kSolveB];
   __shared__ T xs[kSolveB];
+  __shared__ T Ls[kSolveB * kSolveB];
   const int rhs = blockIdx.y;
   T* xc = x + (size_t)rhs * ldx;
   const int j1 = j0 + bs;                // first row below the block
@@ -559,7 +1106,7 @@ __global__ void __launch_bounds__(kSolveThreads) solve_fwd_kernel(
   }
   if (blockIdx.x == 0 && nb1 > 0) {
     __syncthreads();
-    solve_diag_block_lower<T, EXACT>(lu, lda, xc, j1, nb1, xs);
+    solve_diag_block_lower<T, EXACT>(lu, lda, xc, j1, nb1, xs, Ls);
   }
 }
 
@@ -572,6 +1119,7 @@ __global__ void __launch_bounds__(kSolveThreads) solve_bwd_kernel(
     int bp) {
   __shared__ T xb[kSolveB];
   __shared__ T xs[kSolveB];
+  __shared__ T Ls[kSolveB * kSolveB];
   const int rhs = blockIdx.y;
   T* xc = x + (size_t)rhs * ldx;
   const int jp = j0 - bp;  // first row of the previous block
@@ -593,7 +1141,7 @@ __global__ void __launch_bounds__(kSolveThreads) solve_bwd_kernel(
   }
   if (blockIdx.x == 0 && bp > 0) {
     __syncthreads();
-    solve_diag_block_upper<T, EXACT>(lu, lda, xc, jp, bp, xs);
+    solve_diag_block_upper<T, EXACT>(lu, lda, xc, jp, bp, xs, Ls);
   }
 }
 

@@ -77,3 +77,29 @@ class Context:
         _check(self._lib.alg_dgesv_dev(self.handle, update, a.data_ptr(), n, n, b.data_ptr(), nrhs, n,
                                        ipiv.data_ptr()))
         return ipiv[:n]
+
+
+def _profile_methods():
+    def set_profiling(self, on: bool = True):
+        _check(self._lib.alg_ctx_set_profiling(self.handle, 1 if on else 0))
+
+    def profile_reset(self):
+        _check(self._lib.alg_ctx_profile_reset(self.handle))
+
+    def profile(self) -> dict:
+        """{class: {"launches", "ms", "flops", "bytes"}} for classes that ran."""
+        out = {}
+        for i, name in enumerate(_lib.KERNEL_CLASSES):
+            n = C.c_ulonglong()
+            ms, fl, by = C.c_double(), C.c_double(), C.c_double()
+            _check(self._lib.alg_ctx_profile_get(self.handle, i, C.byref(n), C.byref(ms), C.byref(fl), C.byref(by)))
+            if n.value:
+                out[name] = {"launches": n.value, "ms": ms.value, "flops": fl.value, "bytes": by.value}
+        return out
+
+    Context.set_profiling = set_profiling
+    Context.profile_reset = profile_reset
+    Context.profile = profile
+
+
+_profile_methods()

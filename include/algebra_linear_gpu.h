@@ -118,10 +118,26 @@ int alg_ctx_set_stream(alg_ctx* ctx, void* cuda_stream);
 int alg_dgetrf_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
                    int32_t* d_ipiv, int32_t* d_perm);
 
+/* Panel LU of the nrows x ncols device matrix (nrows >= ncols), the device
+ * form of dgetrf_rect (src/lapack/mod.rs:202-238): interchanges stay within the
+ * ncols columns; d_ipiv receives ncols entries. */
+int alg_dgetrf_rect_dev(alg_ctx* ctx, int update, double* d_a, int nrows, int ncols, int lda,
+                        int32_t* d_ipiv);
+
 /* Solves with factors from alg_dgetrf_dev: d_b is n x nrhs (leading dim ldb),
  * overwritten with x. */
 int alg_dgetrs_dev(alg_ctx* ctx, const double* d_lu, int n, int lda,
                    const int32_t* d_perm, double* d_b, int nrhs, int ldb);
+
+/* Per-kernel-class timing of a context's launches with CUDA events, for
+ * roofline reporting. Classes: 0 panel, 1 row interchange, 2 trsm,
+ * 3 CUDA-core update, 4 tensor-core update, 5 triangular solve, 6 FP64
+ * residual, 7 precision cast, 8 batched systems, 9 sparse, 10 other.
+ * flops/bytes are the algorithmic counts of the timed launches. */
+int alg_ctx_set_profiling(alg_ctx* ctx, int on);
+int alg_ctx_profile_reset(alg_ctx* ctx);
+int alg_ctx_profile_get(alg_ctx* ctx, int kernel_class, unsigned long long* launches,
+                        double* total_ms, double* flops, double* bytes);
 
 /* alg_dgetrf_dev + alg_dgetrs_dev; d_ipiv may be NULL. */
 int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
