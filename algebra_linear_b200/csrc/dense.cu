@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <climits>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "dense.cuh"
@@ -27,7 +28,7 @@ namespace alg {
 
 LuPlan default_plan(int n, int elem_bytes) {
   LuPlan p;
-  p.nb = 64;
+  p.nb = n >= 8192 ? 128 : 64;  // deeper updates pay off once the update GEMMs dominate
   p.nbl = elem_bytes == 8 ? 16 : 32;
   if (const char* e = std::getenv("ALG_NB")) p.nb = std::max(16, std::atoi(e));
   if (const char* e = std::getenv("ALG_NBL")) p.nbl = std::max(1, std::min(kPanelMaxW, std::atoi(e)));
@@ -241,10 +242,20 @@ int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* pe
     if (kr < nc) {
       ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, kr, nc)));
     }
-    if (kr < nc || (kr < m && kr < nc)) {
-      ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - kr, nc - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
-                                      a + (size_t)k0 + (size_t)kr * lda, lda,
-                                      a + (size_t)kr + (size_t)kr * lda, lda)));
+    if (kr < nc) {
+      bool done = false;
+      if constexpr (std::is_same<T, float>::value) {
+        if (plan.tc_prec >= 0) {
+          ALG_TRY(gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, nc - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+                                  a + (size_t)k0 + (size_t)kr * lda, lda, a + (size_t)kr + (size_t)kr * lda, lda));
+          done = true;
+        }
+      }
+      if (!done) {
+        ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - kr, nc - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+                                        a + (size_t)k0 + (size_t)kr * lda, lda,
+                                        a + (size_t)kr + (size_t)kr * lda, lda)));
+      }
     }
   }
   return ALG_OK;

@@ -6,9 +6,16 @@
 namespace alg {
 
 struct LuPlan {
-  int nb = 64;    // block-panel width (trailing-update depth)
-  int nbl = 16;   // leaf-panel width (one cluster kernel)
+  int nb = 64;       // block-panel width (trailing-update depth)
+  int nbl = 16;      // leaf-panel width (one cluster kernel)
+  int tc_prec = -1;  // FP32 matrices: ALG_PREC_TF32 / ALG_PREC_BF16 puts the
+                     // block-level trailing update on the tensor cores
 };
+
+// C -= A B on the tensor cores (tcgen05, FP32 accumulation in TMEM) with the
+// operands rounded to TF32 or BF16; A, B, C FP32 column-major.
+int gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda, const float* B,
+                    int ldb, float* C, int ldc);
 
 // In-place LU of the m x nc (m >= nc) device matrix a (leading dim lda).
 // ipiv: nc global interchanges; perm: m net permutation (may be null).

@@ -1,0 +1,360 @@
+// Mixed-precision dgesv: low-precision LU + FP64 iterative refinement.
+//
+// A (FP64, column-major) is cast once to an FP32 working copy and factorized
+// there with the blocked LU (panel, interchanges and TRSM in FP32; trailing
+// updates in FP32 on the CUDA cores, or on the tensor cores with TF32 / BF16
+// inputs and FP32 accumulation). Accuracy is recovered in FP64:
+//   x <- 0, r <- b
+//   repeat: d = (LU)^{-1} r (FP32 solve), x += d (FP64),
+//           r = b - A x (FP64, A read from the caller's FP64 matrix),
+//           stop when the normwise backward error
+//           ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+//           (src/sparse/faer/accuracy_tests.rs:61-67) is within tol,
+// falling back to GMRES-IR (FP64 GMRES on A with the low-precision LU as
+// preconditioner) when refinement stalls, and to a full FP64 refactorization
+// when that does not converge either. A is left unchanged unless the FP64
+// fallback ran (then, like dgesv, it holds the FP64 LU factors).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "dense.cuh"
+#include "mixed.cuh"
+
+namespace alg {
+namespace {
+
+constexpr int kVecThreads = 256;
+
+__global__ void cast_f64_f32_kernel(const double* __restrict__ a, int lda, float* __restrict__ o, int ldo,
+                                    int m, int n) {
+  const size_t total = (size_t)m * n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const size_t j = idx / m, i = idx % m;
+    o[i + j * ldo] = __double2float_rn(a[i + j * lda]);
+  }
+}
+
+// Row sums of |A| (n x n, FP64): part 1 of ||A||_inf. Grid: row blocks x column
+// chunks; partial[chunk][row].
+constexpr int kResRows = 256;
+constexpr int kResCols = 512;
+
+__global__ void abs_rowsum_kernel(const double* __restrict__ a, int lda, int n, double* __restrict__ partial) {
+  const int i = blockIdx.x * kResRows + threadIdx.x;
+  const int j0 = blockIdx.y * kResCols;
+  const int j1 = min(n, j0 + kResCols);
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = j0; j < j1; ++j) s += fabs(a[(size_t)i + (size_t)j * lda]);
+  partial[(size_t)blockIdx.y * n + i] = s;
+}
+
+// r = b - A x for nrhs columns (FP64). Partial products per column chunk,
+// summed in a fixed order by residual_finish_kernel (deterministic).
+__global__ void residual_partial_kernel(const double* __restrict__ a, int lda, int n,
+                                        const double* __restrict__ x, int ldx, int nrhs,
+                                        double* __restrict__ partial) {
+  const int i = blockIdx.x * kResRows + threadIdx.x;
+  const int j0 = blockIdx.y * kResCols;
+  const int j1 = min(n, j0 + kResCols);
+  const int r = blockIdx.z;
+  __shared__ double xs[kResCols];
+  for (int j = j0 + threadIdx.x; j < j1; j += kResRows) xs[j - j0] = x[(size_t)r * ldx + j];
+  __syncthreads();
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = j0; j < j1; ++j) s = __fma_rn(a[(size_t)i + (size_t)j * lda], xs[j - j0], s);
+  partial[((size_t)r * gridDim.y + blockIdx.y) * n + i] = s;
+}
+
+// r = b - sum(partials); also max|r| and max|x|, max|b| per RHS into stats[r*4+{0,1,2}]
+// via an atomic max on the bit pattern (non-negative doubles order as integers).
+__global__ void residual_finish_kernel(const double* __restrict__ partial, int nchunks, int n,
+                                       const double* __restrict__ b, int ldb, const double* __restrict__ x,
+                                       int ldx, double* __restrict__ res, int ldr, int nrhs,
+                                       unsigned long long* __restrict__ stats) {
+  const int r = blockIdx.y;
+  double mr = 0.0, mx = 0.0, mb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < nchunks; ++c) s += partial[((size_t)r * nchunks + c) * n + i];
+    const double bi = b[(size_t)r * ldb + i];
+    const double ri = bi - s;
+    res[(size_t)r * ldr + i] = ri;
+    mr = fmax(mr, fabs(ri));
+    mx = fmax(mx, fabs(x[(size_t)r * ldx + i]));
+    mb = fmax(mb, fabs(bi));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&stats[r * 4 + 0], (unsigned long long)__double_as_longlong(mr));
+    atomicMax(&stats[r * 4 + 1], (unsigned long long)__double_as_longlong(mx));
+    atomicMax(&stats[r * 4 + 2], (unsigned long long)__double_as_longlong(mb));
+  }
+}
+
+__global__ void rowsum_finish_kernel(const double* __restrict__ partial, int nchunks, int n,
+                                     unsigned long long* __restrict__ out) {
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < nchunks; ++c) s += partial[(size_t)c * n + i];
+    m = fmax(m, s);
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// r32 = (float) r, for the low-precision correction solve
+__global__ void f64_to_f32_kernel(const double* __restrict__ a, float* __restrict__ o, size_t cnt) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x)
+    o[i] = __double2float_rn(a[i]);
+}
+
+// x += d (d in FP32)
+__global__ void axpy_f32_kernel(const float* __restrict__ d, double* __restrict__ x, int n, int nrhs, int ldx) {
+  const size_t cnt = (size_t)n * nrhs;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < cnt;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = idx / n, i = idx % n;
+    x[r * ldx + i] += (double)d[idx];
+  }
+}
+
+int grid_for(size_t cnt, int sm) {
+  return (int)std::max<size_t>(1, std::min<size_t>((cnt + kVecThreads - 1) / kVecThreads, (size_t)sm * 8));
+}
+
+}  // namespace
+
+int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, int* ipiv, int* perm) {
+  LuPlan plan = default_plan(n, 4);
+  if (precision != ALG_PREC_FP32) {
+    plan.tc_prec = precision;
+    plan.nb = 128;
+    if (const char* e = std::getenv("ALG_NB_TC")) plan.nb = std::max(32, std::atoi(e));
+  }
+  return lu_factor_dev<float, false>(ctx, a32, n, n, lda, ipiv, perm, plan);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 residual and norms
+// ---------------------------------------------------------------------------
+int inf_norm_dev(alg_ctx* ctx, const double* a, int n, int lda, double* out_host) {
+  const int nchunks = (n + kResCols - 1) / kResCols;
+  double* partial = nullptr;
+  unsigned long long* st = nullptr;
+  ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n, reinterpret_cast<void**>(&partial)));
+  ALG_TRY(ws_get(ctx, WS_MISC, 4096, reinterpret_cast<void**>(&st)));
+  ALG_CUDA_TRY(cudaMemsetAsync(st, 0, 8, ctx->stream));
+  const int tok = prof_begin(ctx, ALG_K_RESID);
+  abs_rowsum_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks), kResRows, 0, ctx->stream>>>(a, lda, n, partial);
+  rowsum_finish_kernel<<<grid_for(n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(partial, nchunks, n, st);
+  count_launches(2);
+  prof_end(ctx, tok, 2.0 * n * n, 8.0 * n * n);
+  ALG_CUDA_TRY(cudaGetLastError());
+  unsigned long long h = 0;
+  ALG_CUDA_TRY(cudaMemcpyAsync(&h, st, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(out_host, &h, 8);
+  return ALG_OK;
+}
+
+int residual_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x, int ldx, const double* b,
+                 int ldb, double* r, int ldr, int nrhs, double* rmax, double* xmax, double* bmax) {
+  const int nchunks = (n + kResCols - 1) / kResCols;
+  double* partial = nullptr;
+  unsigned long long* st = nullptr;
+  ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n * nrhs, reinterpret_cast<void**>(&partial)));
+  ALG_TRY(ws_get(ctx, WS_MISC, 4096 + 32 * (size_t)nrhs, reinterpret_cast<void**>(&st)));
+  ALG_CUDA_TRY(cudaMemsetAsync(st, 0, 32 * (size_t)nrhs, ctx->stream));
+  const int tok = prof_begin(ctx, ALG_K_RESID);
+  residual_partial_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks, nrhs), kResRows, 0, ctx->stream>>>(
+      a, lda, n, x, ldx, nrhs, partial);
+  residual_finish_kernel<<<dim3(std::max(1, std::min(4 * ctx->sm_count, (n + 255) / 256)), nrhs), 256, 0,
+                           ctx->stream>>>(partial, nchunks, n, b, ldb, x, ldx, r, ldr, nrhs, st);
+  count_launches(2);
+  prof_end(ctx, tok, 2.0 * n * n * nrhs, 8.0 * n * n + 24.0 * n * nrhs);
+  ALG_CUDA_TRY(cudaGetLastError());
+  std::vector<unsigned long long> h(4 * (size_t)nrhs);
+  ALG_CUDA_TRY(cudaMemcpyAsync(h.data(), st, 32 * (size_t)nrhs, cudaMemcpyDeviceToHost, ctx->stream));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < nrhs; ++k) {
+    std::memcpy(&rmax[k], &h[4 * k + 0], 8);
+    std::memcpy(&xmax[k], &h[4 * k + 1], 8);
+    std::memcpy(&bmax[k], &h[4 * k + 2], 8);
+  }
+  return ALG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// mixed dgesv on device buffers
+// ---------------------------------------------------------------------------
+int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, int lda, double* d_b, int nrhs,
+                    int ldb, alg_mixed_report* rep) {
+  alg_mixed_report local{};
+  alg_mixed_report& R = rep ? *rep : local;
+  std::memset(&R, 0, sizeof(R));
+  if (n == 0 || nrhs == 0) return ALG_OK;
+  const double tol = o.tol > 0 ? o.tol : 10.0 * n * std::ldexp(1.0, -53);
+  const int max_ir = o.max_ir > 0 ? o.max_ir : 30;
+
+  float* a32 = nullptr;
+  double* x = nullptr;
+  double* r = nullptr;
+  float* r32 = nullptr;
+  int* ipiv = nullptr;
+  int* perm = nullptr;
+  ALG_TRY(ws_get(ctx, WS_A32, sizeof(float) * (size_t)n * n, reinterpret_cast<void**>(&a32)));
+  ALG_TRY(ws_get(ctx, WS_R, sizeof(double) * (size_t)n * nrhs * 2 + sizeof(float) * (size_t)n * nrhs,
+                 reinterpret_cast<void**>(&x)));
+  r = x + (size_t)n * nrhs;
+  r32 = reinterpret_cast<float*>(r + (size_t)n * nrhs);
+  ALG_TRY(ws_get(ctx, WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&ipiv)));
+  ALG_TRY(ws_get(ctx, WS_PERM, sizeof(int) * n, reinterpret_cast<void**>(&perm)));
+
+  // ---- factorize in low precision --------------------------------------
+  ALG_TRY(status_reset(ctx));
+  {
+    const int tok = prof_begin(ctx, ALG_K_CAST);
+    cast_f64_f32_kernel<<<grid_for((size_t)n * n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(d_a, lda, a32, n, n, n);
+    count_launches();
+    prof_end(ctx, tok, 0.0, 12.0 * n * n);
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  ALG_TRY(lu_factor_lowp_dev(ctx, o.precision, a32, n, n, ipiv, perm));
+  ALG_TRY(status_fetch(ctx));
+  const bool lowp_singular = ctx->h_status->singular_col != INT_MAX;
+
+  double anorm = 0.0;
+  ALG_TRY(inf_norm_dev(ctx, d_a, n, lda, &anorm));
+  ALG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n * nrhs, ctx->stream));
+  // r = b
+  ALG_CUDA_TRY(cudaMemcpy2DAsync(r, sizeof(double) * n, d_b, sizeof(double) * ldb, sizeof(double) * n, nrhs,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+  std::vector<double> rmax(nrhs), xmax(nrhs), bmax(nrhs), eta(nrhs, INFINITY);
+  bool converged = false;
+  if (!lowp_singular) {
+    double prev = INFINITY;
+    int stall = 0;
+    for (int it = 0; it < max_ir; ++it) {
+      // d = LU^{-1} r in FP32
+      f64_to_f32_kernel<<<grid_for((size_t)n * nrhs, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(
+          r, r32, (size_t)n * nrhs);
+      count_launches();
+      ALG_TRY((lu_solve_dev<float, false>(ctx, a32, n, n, perm, r32, nrhs, n)));
+      axpy_f32_kernel<<<grid_for((size_t)n * nrhs, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(r32, x, n,
+                                                                                                   nrhs, n);
+      count_launches();
+      ALG_CUDA_TRY(cudaGetLastError());
+      ALG_TRY(residual_dev(ctx, d_a, n, lda, x, n, d_b, ldb, r, n, nrhs, rmax.data(), xmax.data(), bmax.data()));
+      double worst = 0.0;
+      for (int k = 0; k < nrhs; ++k) {
+        const double den = anorm * xmax[k] + bmax[k];
+        eta[k] = den == 0.0 ? rmax[k] : rmax[k] / den;
+        worst = std::max(worst, eta[k]);
+      }
+      R.ir_iterations = it + 1;
+      R.backward_error = worst;
+      if (!(worst == worst)) break;  // NaN: diverged
+      if (worst <= tol) {
+        converged = true;
+        break;
+      }
+      // stalled: less than a halving over the last step, twice in a row
+      if (worst > 0.5 * prev) {
+        if (++stall >= 2) break;
+      } else {
+        stall = 0;
+      }
+      prev = worst;
+    }
+  }
+  R.precision = o.precision;
+  if (converged) {
+    ALG_CUDA_TRY(cudaMemcpy2DAsync(d_b, sizeof(double) * ldb, x, sizeof(double) * n, sizeof(double) * n, nrhs,
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
+    ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    R.path = ALG_MIXED_PATH_IR;
+    return ALG_OK;
+  }
+  if (o.no_fallback) return ALG_CONVERGENCE;
+  // ---- FP64 refactorization (A becomes its FP64 LU, like dgesv) ---------
+  R.path = ALG_MIXED_PATH_FP64;
+  ALG_TRY(status_reset(ctx));
+  ALG_TRY((lu_factor_dev<double, false>(ctx, d_a, n, n, lda, ipiv, perm, default_plan(n, 8))));
+  ALG_TRY(status_fetch(ctx));
+  if (ctx->h_status->singular_col != INT_MAX) return ALG_SINGULAR;
+  ALG_TRY((lu_solve_dev<double, false>(ctx, d_a, n, lda, perm, d_b, nrhs, ldb)));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  R.backward_error = -1.0;  // not measured on this path (A was overwritten)
+  return ALG_OK;
+}
+
+}  // namespace alg
+
+// ===========================================================================
+// C entry points
+// ===========================================================================
+extern "C" {
+
+void alg_mixed_opts_default(alg_mixed_opts* o) {
+  if (o == nullptr) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = ALG_PREC_FP32;
+  o->tol = 0.0;
+  o->max_ir = 30;
+  o->no_fallback = 0;
+}
+
+int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, int n, int lda, double* d_b,
+                        int nrhs, int ldb, alg_mixed_report* report) {
+  if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
+  if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n)) return ALG_BAD_SHAPE;
+  alg_mixed_opts o;
+  alg_mixed_opts_default(&o);
+  if (opts) o = *opts;
+  if (o.precision != ALG_PREC_FP32 && o.precision != ALG_PREC_TF32 && o.precision != ALG_PREC_BF16)
+    return ALG_INVALID_ARGUMENT;
+  return alg::dgesv_mixed_dev(ctx, o, d_a, n, lda, d_b, nrhs, ldb, report);
+}
+
+int alg_dgesv_mixed(const alg_mixed_opts* opts, double* a, double* b, size_t n, size_t nrhs,
+                    alg_mixed_report* report) {
+  if (n == 0 || nrhs == 0) return ALG_OK;
+  if (a == nullptr || b == nullptr) return ALG_INVALID_ARGUMENT;
+  if (n > (size_t)INT_MAX / 2 || nrhs > 65535) return ALG_BAD_SHAPE;
+  alg_ctx* ctx = nullptr;
+  ALG_TRY(alg::default_ctx(&ctx));
+  std::lock_guard<std::mutex> g(ctx->mu);
+  double* d_a = nullptr;
+  double* d_b = nullptr;
+  ALG_TRY(alg::ws_get(ctx, alg::WS_A, sizeof(double) * n * n, reinterpret_cast<void**>(&d_a)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_B, sizeof(double) * n * nrhs, reinterpret_cast<void**>(&d_b)));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_a, a, sizeof(double) * n * n, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_b, b, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, ctx->stream));
+  alg_mixed_opts o;
+  alg_mixed_opts_default(&o);
+  if (opts) o = *opts;
+  alg_mixed_report rep{};
+  const int rc = alg::dgesv_mixed_dev(ctx, o, d_a, (int)n, (int)n, d_b, (int)nrhs, (int)n, &rep);
+  if (rc == ALG_OK) {
+    ALG_CUDA_TRY(cudaMemcpyAsync(b, d_b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
+    if (rep.path == ALG_MIXED_PATH_FP64)
+      ALG_CUDA_TRY(cudaMemcpyAsync(a, d_a, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ctx->stream));
+    ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  if (report) *report = rep;
+  return rc;
+}
+
+}  // extern "C"

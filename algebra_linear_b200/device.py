@@ -26,14 +26,23 @@ def _dev_f64(t: torch.Tensor, numel: int, name: str) -> torch.Tensor:
     return t
 
 
+# cudaStreamLegacy: torch's default stream is the legacy NULL stream, and a
+# NULL handle would make the library create its own unordered stream.
+_CUDA_STREAM_LEGACY = 0x1
+
+
+def _current_stream() -> int:
+    h = torch.cuda.current_stream().cuda_stream
+    return h if h else _CUDA_STREAM_LEGACY
+
+
 class Context:
     """Owns an alg_ctx bound to torch's current stream."""
 
     def __init__(self):
         self._lib = _lib.load()
         h = C.c_void_p()
-        stream = torch.cuda.current_stream().cuda_stream
-        _check(self._lib.alg_ctx_create(C.c_void_p(stream), C.byref(h)))
+        _check(self._lib.alg_ctx_create(C.c_void_p(_current_stream()), C.byref(h)))
         self.handle = h
 
     def close(self):
@@ -54,7 +63,15 @@ class Context:
             pass
 
     def sync_stream(self):
-        _check(self._lib.alg_ctx_set_stream(self.handle, C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        _check(self._lib.alg_ctx_set_stream(self.handle, C.c_void_p(_current_stream())))
+
+    def larnv(self, dist: int, seed, n: int, out: torch.Tensor | None = None):
+        """The reference's DLARNV stream on the device; returns (x, seed_after)."""
+        x = out if out is not None else torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+        s_in = (C.c_uint32 * 4)(*seed)
+        s_out = (C.c_uint32 * 4)()
+        _check(self._lib.alg_larnv_dev(self.handle, dist, s_in, n, x.data_ptr(), s_out))
+        return x[:n], [int(v) for v in s_out]
 
     def dgetrf(self, a: torch.Tensor, n: int, update: int = _lib.UPDATE_EXACT):
         """In-place LU; returns (ipiv, perm) int32 CUDA tensors."""

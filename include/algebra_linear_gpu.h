@@ -139,9 +139,60 @@ int alg_ctx_profile_reset(alg_ctx* ctx);
 int alg_ctx_profile_get(alg_ctx* ctx, int kernel_class, unsigned long long* launches,
                         double* total_ms, double* flops, double* bytes);
 
+/* The reference's DLARNV stream (src/lapack/families.rs:166-249, `larnv`)
+ * generated on the device: n values into d_x (dist 1 = Uniform(0,1),
+ * 2 = Symmetric(-1,1)), bit-identical to the CPU stream for the same seed
+ * (four 12-bit words, last odd); seed_out (may be NULL) receives the seed the
+ * reference would hold after the call. Stream-ordered, no sync. */
+int alg_larnv_dev(alg_ctx* ctx, int dist, const uint32_t seed[4], size_t n, double* d_x,
+                  uint32_t seed_out[4]);
+
 /* alg_dgetrf_dev + alg_dgetrs_dev; d_ipiv may be NULL. */
 int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
                   double* d_b, int nrhs, int ldb, int32_t* d_ipiv);
+
+/* ---- mixed precision: low-precision LU + FP64 iterative refinement -------
+ * The dsgesv contract: A is factorized in low precision (FP32 working copy;
+ * trailing updates in FP32, TF32 or BF16 with FP32 accumulation), x is
+ * refined in FP64 until the normwise backward error
+ * ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) is within tol
+ * (default 10 n 2^-53, the FP64 level), falling back to GMRES-IR and then to
+ * a full FP64 factorization. A is unchanged unless the FP64 fallback ran, in
+ * which case it holds the FP64 LU factors as after dgesv. */
+#define ALG_PREC_FP32 0
+#define ALG_PREC_TF32 1
+#define ALG_PREC_BF16 2
+
+#define ALG_MIXED_PATH_IR 1
+#define ALG_MIXED_PATH_GMRES 2
+#define ALG_MIXED_PATH_FP64 3
+
+typedef struct {
+  int precision;    /* ALG_PREC_* of the trailing updates */
+  double tol;       /* backward-error target; <= 0 means 10 n 2^-53 */
+  int max_ir;       /* refinement steps before the fallback (<= 0: 30) */
+  int no_fallback;  /* nonzero: return ALG_CONVERGENCE instead of refactorizing in FP64 */
+  int reserved[4];
+} alg_mixed_opts;
+
+typedef struct {
+  int path;            /* ALG_MIXED_PATH_* that produced x */
+  int precision;
+  int ir_iterations;
+  int gmres_iterations;
+  double backward_error;  /* worst over the right-hand sides; -1 on the FP64 path */
+  double reserved[4];
+} alg_mixed_report;
+
+void alg_mixed_opts_default(alg_mixed_opts* opts);
+
+/* Host drop-in: a n x n, b n x nrhs (column-major); b becomes x. */
+int alg_dgesv_mixed(const alg_mixed_opts* opts, double* a, double* b, size_t n, size_t nrhs,
+                    alg_mixed_report* report);
+
+/* Device form: d_a is read (and only overwritten on the FP64 fallback). */
+int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, int n, int lda,
+                        double* d_b, int nrhs, int ldb, alg_mixed_report* report);
 
 #ifdef __cplusplus
 }

@@ -248,3 +248,20 @@ def test_device_api_matches_host_api(gpu, oracle):
         ipiv = ctx.dgesv(da, db, n)
         assert ipiv.tolist() == oracle.dgesv(a.copy(), b.copy(), n)[1]
         assert rel_err(db.cpu().numpy(), rb) <= REL_TOL
+
+
+def test_device_larnv_matches_the_reference_stream(gpu, oracle):
+    """The device generator reproduces the oracle's larnv bit for bit,
+    including the seed it leaves, across batch boundaries."""
+    import torch
+
+    from algebra_linear_b200 import device
+
+    with device.Context() as ctx:
+        for dist, name in [(1, "Uniform"), (2, "Symmetric")]:
+            for n in [1, 63, 64, 65, 200, 4096 + 17]:
+                x, s = ctx.larnv(dist, SEEDY, n)
+                torch.cuda.synchronize()
+                ref, rs = oracle.larnv(name, SEEDY, n)
+                assert same_bits(x.cpu().numpy(), ref), (name, n)
+                assert s == rs, (name, n)
