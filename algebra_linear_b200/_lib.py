@@ -66,6 +66,7 @@ SIGNATURES = [
     ("alg_mixed_opts_default", None, [_P]),
     ("alg_dgesv_mixed", _I, [_P, _P, _P, _SZ, _SZ, _P]),
     ("alg_dgesv_mixed_dev", _I, [_P, _P, _P, _I, _I, _P, _I, _I, _P]),
+    ("alg_gemm_tc_sub_dev", _I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
     ("alg_ctx_set_profiling", _I, [_P, _I]),
     ("alg_ctx_profile_reset", _I, [_P]),
     ("alg_ctx_profile_get", _I, [_P, _I, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double),

@@ -194,6 +194,14 @@ int alg_dgesv_mixed(const alg_mixed_opts* opts, double* a, double* b, size_t n, 
 int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, int n, int lda,
                         double* d_b, int nrhs, int ldb, alg_mixed_report* report);
 
+/* The tensor-core trailing update of the low-precision LU on device buffers:
+ * C (FP32, M x N) -= A (M x K) * B (K x N), all column-major, operands
+ * rounded to prec (ALG_PREC_TF32 or ALG_PREC_BF16), FP32 accumulation.
+ * K must be a multiple of 64 (BF16) or 32 (TF32). Synchronises. Exposed for
+ * tests and benchmarks of the kernel on its own. */
+int alg_gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda,
+                        const float* B, int ldb, float* C, int ldc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,93 @@
+"""GPU tests of the mixed-precision path: the tcgen05 trailing update against
+a torch FP32 reference of the same rounded operands, and the refined solve
+against the oracle's FP64 solution.
+
+Tolerances: the tensor-core update must match the reference product of the
+rounded operands to FP32 accumulation error (1e-4 relative to the largest
+|product|); the refined x must reach the FP64 backward-error level
+10 n 2^-53 and agree with the oracle's x to cond-scaled FP64 accuracy.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _round_bf16(t):
+    import torch
+
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def _round_tf32(t):
+    import torch
+
+    u = t.contiguous().view(torch.int32)
+    # round-to-nearest (ties away) to 10 mantissa bits, as cvt.rna.tf32.f32
+    r = (u + 0x1000) & ~0x1FFF
+    return r.view(torch.float32)
+
+
+@pytest.mark.parametrize("prec", ["bf16", "tf32"])
+@pytest.mark.parametrize("shape", [(128, 256, 64), (300, 500, 128), (1000, 700, 256), (4096, 4096, 128), (17, 9, 128)])
+def test_tensor_core_update_matches_reference(gpu, prec, shape):
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    M, N, K = shape
+    if prec == "tf32" and K % 32 or prec == "bf16" and K % 64:
+        pytest.skip("K must be whole slices")
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K)
+    A = torch.rand((K, M), generator=g, device="cuda") * 2 - 1      # storage of a column-major M x K
+    B = torch.rand((N, K), generator=g, device="cuda") * 2 - 1      # storage of a column-major K x N
+    C0 = torch.rand((N, M), generator=g, device="cuda") * 2 - 1     # storage of a column-major M x N
+    C = C0.clone()
+    with device.Context() as ctx:
+        rc = gpu.alg_gemm_tc_sub_dev(ctx.handle, mixed.PRECISIONS[prec], M, N, K, A.data_ptr(), M, B.data_ptr(),
+                                     K, C.data_ptr(), M)
+        assert rc == 0, rc
+    rnd = _round_bf16 if prec == "bf16" else _round_tf32
+    Am = rnd(A).t().double()      # M x K
+    Bm = rnd(B).t().double()      # K x N
+    ref = C0.t().double() - Am @ Bm
+    err = (C.t().double() - ref).abs().max().item()
+    scale = (Am.abs() @ Bm.abs()).max().item()
+    assert err <= 1e-4 * scale, (err, scale)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "tf32", "bf16"])
+def test_mixed_solve_reaches_fp64_backward_error(gpu, oracle, prec):
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    n = 1536
+    a, x_true, b = oracle.c1_system(n, seed=[7, 7, 7, 9])
+    ra, rb = a.copy(), b.copy()
+    rc, _ = oracle.dgesv(ra, rb, n)
+    assert rc == 0
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        B = torch.from_numpy(b.copy()).cuda()
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision=prec)
+        x = B.cpu().numpy()
+        assert np.array_equal(A.cpu().numpy(), a), "A must be unchanged on the refinement path"
+    assert rep["path"] in ("ir", "gmres"), rep
+    eta = oracle.backward_error(a, x, b, n)
+    assert eta <= 10 * n * 2.0**-53, (eta, rep)
+    # same solution as the FP64 reference to the accuracy the conditioning allows
+    assert np.max(np.abs(x - rb)) / np.max(np.abs(rb)) < 1e-9
+
+
+def test_mixed_host_api_keeps_a(gpu, oracle):
+    from algebra_linear_b200 import _lib, mixed
+
+    n = 700
+    a, _, b = oracle.c1_system(n, seed=[1, 2, 3, 5])
+    ha, hb = a.copy(), b.copy()
+    rc = mixed.dgesv_mixed_host(ha.ctypes.data, hb.ctypes.data, n, 1, precision="bf16")
+    assert rc == 0, _lib.status_string(rc)
+    assert np.array_equal(ha, a)
+    assert oracle.backward_error(a, hb, b, n) <= 10 * n * 2.0**-53
