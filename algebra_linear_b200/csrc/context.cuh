@@ -72,6 +72,10 @@ enum WsSlot : int {
   WS_KRYLOV,      // GMRES basis (mixed form)
   WS_PARTIAL,     // reduction partials
   WS_MISC,
+  WS_GMRES,       // GMRES basis and work vectors (mixed form)
+  WS_PRECOND,     // preconditioner scratch (mixed form)
+  WS_RBT,         // butterfly coefficients (mixed form)
+  WS_IDENT,       // identity permutation
   WS_COUNT
 };
 

@@ -264,50 +264,12 @@ int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* pe
 template <typename T, bool EXACT>
 int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs,
                  int ldb) {
-  if (n == 0 || nrhs == 0) return ALG_OK;
   if (nrhs > 65535) return ALG_BAD_SHAPE;
-  T* x = nullptr;
-  ALG_TRY(ws_get(ctx, WS_X, sizeof(T) * (size_t)n * nrhs, reinterpret_cast<void**>(&x)));
-  const int ldx = n;
-  const int tok = prof_begin(ctx, ALG_K_SOLVE);
-  {
-    dim3 grid(std::min(1024, (n + kSolveThreads - 1) / kSolveThreads), nrhs);
-    solve_gather_kernel<T><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, perm, b, ldb, x, ldx);
-    count_launches();
-    ALG_CUDA_TRY(cudaGetLastError());
-  }
-  const int B = kSolveB;
-  // forward (unit lower)
-  solve_fwd_kernel<T, EXACT><<<dim3(1, nrhs), kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, -B, B);
-    count_launches();
-  ALG_CUDA_TRY(cudaGetLastError());
-  for (int j0 = 0; j0 + B < n; j0 += B) {
-    const int j1 = j0 + B;
-    const int nb1 = std::min(B, n - j1);
-    const int rest = n - j1 - nb1;
-    dim3 grid(1 + (rest + kSolveThreads - 1) / kSolveThreads, nrhs);
-    solve_fwd_kernel<T, EXACT><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, j0, B);
-    count_launches();
-    ALG_CUDA_TRY(cudaGetLastError());
-  }
-  // backward (upper)
-  const int jl = ((n - 1) / B) * B;
-  solve_bwd_kernel<T, EXACT><<<dim3(1, nrhs), kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, n, 0,
-                                                                               n - jl);
-    count_launches();
-  ALG_CUDA_TRY(cudaGetLastError());
-  for (int j0 = jl; j0 > 0; j0 -= B) {
-    const int bs = std::min(B, n - j0);
-    const int jp = j0 - B;
-    dim3 grid(1 + (jp + kSolveThreads - 1) / kSolveThreads, nrhs);
-    solve_bwd_kernel<T, EXACT><<<grid, kSolveThreads, 0, ctx->stream>>>(lu, lda, n, x, ldx, j0, bs, B);
-    count_launches();
-    ALG_CUDA_TRY(cudaGetLastError());
-  }
-  ALG_CUDA_TRY(cudaMemcpy2DAsync(b, sizeof(T) * (size_t)ldb, x, sizeof(T) * (size_t)ldx,
-                                 sizeof(T) * (size_t)n, nrhs, cudaMemcpyDeviceToDevice, ctx->stream));
-  prof_end(ctx, tok, 2.0 * n * n * nrhs, sizeof(T) * (double(n) * n + 4.0 * n * nrhs));
-  return ALG_OK;
+  return lu_solve_dataflow_dev<T, EXACT>(ctx, lu, n, lda, perm, b, nrhs, ldb);
+}
+
+int trsm_lower_unit_f32(alg_ctx* ctx, float* a, int lda, int r0, int kb, int cb, int ce) {
+  return launch_trsm<float, false>(ctx, a, lda, r0, kb, cb, ce);
 }
 
 // explicit instantiations

@@ -29,6 +29,11 @@ template <typename T, bool EXACT>
 int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs,
                  int ldb);
 
+// Same contract as lu_solve_dev: gather by perm, then the forward and
+// backward sweeps as single dataflow launches (trsv.cu).
+template <typename T, bool EXACT>
+int lu_solve_dataflow_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs, int ldb);
+
 // C -= A B on the CUDA cores (column-major), stream-ordered.
 template <typename T, bool EXACT>
 int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T* B, int ldb,

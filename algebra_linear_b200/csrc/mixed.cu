@@ -22,7 +22,9 @@
 #include <vector>
 
 #include "dense.cuh"
+#include "gmres.cuh"
 #include "mixed.cuh"
+#include "rbt.cuh"
 
 namespace alg {
 namespace {
@@ -72,8 +74,12 @@ __global__ void residual_partial_kernel(const double* __restrict__ a, int lda, i
   partial[((size_t)r * gridDim.y + blockIdx.y) * n + i] = s;
 }
 
+// max that keeps a NaN (fmax would drop it and hide a diverged solve)
+__device__ __forceinline__ double nanmax(double m, double v) { return (v != v || v > m) ? v : m; }
+
 // r = b - sum(partials); also max|r| and max|x|, max|b| per RHS into stats[r*4+{0,1,2}]
-// via an atomic max on the bit pattern (non-negative doubles order as integers).
+// via an atomic max on the bit pattern (non-negative doubles order as integers,
+// and a NaN's pattern lies above every number's).
 __global__ void residual_finish_kernel(const double* __restrict__ partial, int nchunks, int n,
                                        const double* __restrict__ b, int ldb, const double* __restrict__ x,
                                        int ldx, double* __restrict__ res, int ldr, int nrhs,
@@ -86,14 +92,14 @@ __global__ void residual_finish_kernel(const double* __restrict__ partial, int n
     const double bi = b[(size_t)r * ldb + i];
     const double ri = bi - s;
     res[(size_t)r * ldr + i] = ri;
-    mr = fmax(mr, fabs(ri));
-    mx = fmax(mx, fabs(x[(size_t)r * ldx + i]));
-    mb = fmax(mb, fabs(bi));
+    mr = nanmax(mr, fabs(ri));
+    mx = nanmax(mx, fabs(x[(size_t)r * ldx + i]));
+    mb = nanmax(mb, fabs(bi));
   }
   for (int off = 16; off > 0; off >>= 1) {
-    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-    mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
+    mr = nanmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
+    mx = nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    mb = nanmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
   }
   if ((threadIdx.x & 31) == 0) {
     atomicMax(&stats[r * 4 + 0], (unsigned long long)__double_as_longlong(mr));
@@ -102,15 +108,28 @@ __global__ void residual_finish_kernel(const double* __restrict__ partial, int n
   }
 }
 
+__global__ void gemv_finish_kernel(const double* __restrict__ partial, int nchunks, int n, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < nchunks; ++c) s += partial[(size_t)c * n + i];
+    y[i] = s;
+  }
+}
+
+__global__ void f32_to_f64_kernel(const float* __restrict__ a, double* __restrict__ o, size_t cnt) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x)
+    o[i] = (double)a[i];
+}
+
 __global__ void rowsum_finish_kernel(const double* __restrict__ partial, int nchunks, int n,
                                      unsigned long long* __restrict__ out) {
   double m = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int c = 0; c < nchunks; ++c) s += partial[(size_t)c * n + i];
-    m = fmax(m, s);
+    m = nanmax(m, s);
   }
-  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  for (int off = 16; off > 0; off >>= 1) m = nanmax(m, __shfl_xor_sync(0xffffffffu, m, off));
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
@@ -169,6 +188,20 @@ int inf_norm_dev(alg_ctx* ctx, const double* a, int n, int lda, double* out_host
   return ALG_OK;
 }
 
+int gemv_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x, double* y) {
+  const int nchunks = (n + kResCols - 1) / kResCols;
+  double* partial = nullptr;
+  ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n, reinterpret_cast<void**>(&partial)));
+  const int tok = prof_begin(ctx, ALG_K_RESID);
+  residual_partial_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks, 1), kResRows, 0, ctx->stream>>>(
+      a, lda, n, x, n, 1, partial);
+  gemv_finish_kernel<<<grid_for(n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(partial, nchunks, n, y);
+  count_launches(2);
+  prof_end(ctx, tok, 2.0 * n * n, 8.0 * n * n + 16.0 * n);
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
 int residual_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x, int ldx, const double* b,
                  int ldb, double* r, int ldr, int nrhs, double* rmax, double* xmax, double* bmax) {
   const int nchunks = (n + kResCols - 1) / kResCols;
@@ -199,61 +232,137 @@ int residual_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x,
 // ---------------------------------------------------------------------------
 // mixed dgesv on device buffers
 // ---------------------------------------------------------------------------
+namespace {
+
+__global__ void iota_i32_kernel(int* v, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+// Low-precision factorization and its preconditioner M^{-1} on n x k blocks.
+struct LowpFactor {
+  alg_ctx* ctx = nullptr;
+  int n = 0;
+  float* a32 = nullptr;
+  int* perm = nullptr;  // row permutation (identity for the butterfly form)
+  bool rbt = false;
+  RbtState rs;
+  double* t64 = nullptr;  // n x kmax scratch
+  float* t32 = nullptr;   // n x kmax scratch
+  int kmax = 0;
+
+  // z = M^{-1} v for k columns (n x k, leading dimension n).
+  int apply(const double* v, double* z, int k) {
+    for (int k0 = 0; k0 < k; k0 += kmax) {
+      const int kk = std::min(kmax, k - k0);
+      const double* vk = v + (size_t)k0 * n;
+      double* zk = z + (size_t)k0 * n;
+      if (rbt) {
+        for (int c = 0; c < kk; ++c) ALG_TRY(rbt_vector(ctx, rs, true, vk + (size_t)c * n, t64 + (size_t)c * n));
+        vk = t64;
+      }
+      f64_to_f32_kernel<<<grid_for((size_t)n * kk, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(vk, t32,
+                                                                                                 (size_t)n * kk);
+      count_launches();
+      ALG_TRY((lu_solve_dev<float, false>(ctx, a32, n, n, perm, t32, kk, n)));
+      double* dst = rbt ? t64 : zk;
+      f32_to_f64_kernel<<<grid_for((size_t)n * kk, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(t32, dst,
+                                                                                                 (size_t)n * kk);
+      count_launches();
+      if (rbt)
+        for (int c = 0; c < kk; ++c) ALG_TRY(rbt_vector(ctx, rs, false, t64 + (size_t)c * n, zk + (size_t)c * n));
+      ALG_CUDA_TRY(cudaGetLastError());
+    }
+    return ALG_OK;
+  }
+};
+
+// x += d
+__global__ void axpy_f64_kernel(const double* __restrict__ d, double* __restrict__ x, size_t cnt) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x)
+    x[i] += d[i];
+}
+
+}  // namespace
+
 int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, int lda, double* d_b, int nrhs,
                     int ldb, alg_mixed_report* rep) {
   alg_mixed_report local{};
   alg_mixed_report& R = rep ? *rep : local;
   std::memset(&R, 0, sizeof(R));
+  R.precision = o.precision;
   if (n == 0 || nrhs == 0) return ALG_OK;
   const double tol = o.tol > 0 ? o.tol : 10.0 * n * std::ldexp(1.0, -53);
   const int max_ir = o.max_ir > 0 ? o.max_ir : 30;
+  const int kmax = std::min(nrhs, 8);
 
-  float* a32 = nullptr;
+  LowpFactor F;
+  F.ctx = ctx;
+  F.n = n;
+  F.kmax = kmax;
   double* x = nullptr;
-  double* r = nullptr;
-  float* r32 = nullptr;
   int* ipiv = nullptr;
-  int* perm = nullptr;
-  ALG_TRY(ws_get(ctx, WS_A32, sizeof(float) * (size_t)n * n, reinterpret_cast<void**>(&a32)));
-  ALG_TRY(ws_get(ctx, WS_R, sizeof(double) * (size_t)n * nrhs * 2 + sizeof(float) * (size_t)n * nrhs,
+  ALG_TRY(ws_get(ctx, WS_A32, sizeof(float) * (size_t)n * n, reinterpret_cast<void**>(&F.a32)));
+  ALG_TRY(ws_get(ctx, WS_R,
+                 sizeof(double) * (size_t)n * nrhs * 3 + sizeof(double) * (size_t)n * kmax +
+                     sizeof(float) * (size_t)n * kmax + 64,
                  reinterpret_cast<void**>(&x)));
-  r = x + (size_t)n * nrhs;
-  r32 = reinterpret_cast<float*>(r + (size_t)n * nrhs);
+  double* r = x + (size_t)n * nrhs;
+  double* dlt = r + (size_t)n * nrhs;
+  F.t64 = dlt + (size_t)n * nrhs;
+  F.t32 = reinterpret_cast<float*>(F.t64 + (size_t)n * kmax);
   ALG_TRY(ws_get(ctx, WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&ipiv)));
-  ALG_TRY(ws_get(ctx, WS_PERM, sizeof(int) * n, reinterpret_cast<void**>(&perm)));
 
   // ---- factorize in low precision --------------------------------------
-  ALG_TRY(status_reset(ctx));
-  {
-    const int tok = prof_begin(ctx, ALG_K_CAST);
-    cast_f64_f32_kernel<<<grid_for((size_t)n * n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(d_a, lda, a32, n, n, n);
+  // AUTO keeps partial pivoting: on matrices that are already random (the
+  // dense workloads here) LU without pivoting has large growth even after the
+  // butterflies, so the butterfly form is an explicit choice.
+  bool use_rbt = o.pivoting == ALG_PIVOT_RBT;
+  if (o.pivoting == ALG_PIVOT_RBT && n % 4 != 0) return ALG_BAD_SHAPE;
+  bool lowp_singular = false;
+  if (use_rbt) {
+    ALG_TRY(ws_get(ctx, WS_IDENT, sizeof(int) * n, reinterpret_cast<void**>(&F.perm)));
+    iota_i32_kernel<<<grid_for(n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(F.perm, n);
     count_launches();
-    prof_end(ctx, tok, 0.0, 12.0 * n * n);
-    ALG_CUDA_TRY(cudaGetLastError());
+    ALG_TRY(rbt_prepare(ctx, n, 0x5eed0f1eULL ^ (uint64_t)n, &F.rs));
+    ALG_TRY(status_reset(ctx));
+    ALG_TRY(rbt_transform(ctx, F.rs, d_a, lda, F.a32, n));
+    ALG_TRY(genp_factor(ctx, o.precision, F.a32, n, n, 128));
+    ALG_TRY(status_fetch(ctx));
+    if (ctx->h_status->singular_col != INT_MAX) use_rbt = false;  // a zero pivot: pivot after all
+    F.rbt = use_rbt;
+    R.reserved[0] = use_rbt ? 1.0 : 0.0;
   }
-  ALG_TRY(lu_factor_lowp_dev(ctx, o.precision, a32, n, n, ipiv, perm));
-  ALG_TRY(status_fetch(ctx));
-  const bool lowp_singular = ctx->h_status->singular_col != INT_MAX;
+  if (!use_rbt) {
+    ALG_TRY(ws_get(ctx, WS_PERM, sizeof(int) * n, reinterpret_cast<void**>(&F.perm)));
+    ALG_TRY(status_reset(ctx));
+    {
+      const int tok = prof_begin(ctx, ALG_K_CAST);
+      cast_f64_f32_kernel<<<grid_for((size_t)n * n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(d_a, lda, F.a32,
+                                                                                                   n, n, n);
+      count_launches();
+      prof_end(ctx, tok, 0.0, 12.0 * n * n);
+      ALG_CUDA_TRY(cudaGetLastError());
+    }
+    ALG_TRY(lu_factor_lowp_dev(ctx, o.precision, F.a32, n, n, ipiv, F.perm));
+    ALG_TRY(status_fetch(ctx));
+    lowp_singular = ctx->h_status->singular_col != INT_MAX;
+  }
 
   double anorm = 0.0;
   ALG_TRY(inf_norm_dev(ctx, d_a, n, lda, &anorm));
   ALG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n * nrhs, ctx->stream));
-  // r = b
   ALG_CUDA_TRY(cudaMemcpy2DAsync(r, sizeof(double) * n, d_b, sizeof(double) * ldb, sizeof(double) * n, nrhs,
                                  cudaMemcpyDeviceToDevice, ctx->stream));
   std::vector<double> rmax(nrhs), xmax(nrhs), bmax(nrhs), eta(nrhs, INFINITY);
   bool converged = false;
   if (!lowp_singular) {
+    // ---- plain refinement: x += M^{-1} r, r = b - A x -------------------
     double prev = INFINITY;
     int stall = 0;
     for (int it = 0; it < max_ir; ++it) {
-      // d = LU^{-1} r in FP32
-      f64_to_f32_kernel<<<grid_for((size_t)n * nrhs, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(
-          r, r32, (size_t)n * nrhs);
-      count_launches();
-      ALG_TRY((lu_solve_dev<float, false>(ctx, a32, n, n, perm, r32, nrhs, n)));
-      axpy_f32_kernel<<<grid_for((size_t)n * nrhs, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(r32, x, n,
-                                                                                                   nrhs, n);
+      ALG_TRY(F.apply(r, dlt, nrhs));
+      axpy_f64_kernel<<<grid_for((size_t)n * nrhs, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(
+          dlt, x, (size_t)n * nrhs);
       count_launches();
       ALG_CUDA_TRY(cudaGetLastError());
       ALG_TRY(residual_dev(ctx, d_a, n, lda, x, n, d_b, ldb, r, n, nrhs, rmax.data(), xmax.data(), bmax.data()));
@@ -265,31 +374,54 @@ int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, i
       }
       R.ir_iterations = it + 1;
       R.backward_error = worst;
-      if (!(worst == worst)) break;  // NaN: diverged
+      if (!(worst == worst) || std::isinf(worst)) break;  // diverged
       if (worst <= tol) {
         converged = true;
         break;
       }
-      // stalled: less than a halving over the last step, twice in a row
-      if (worst > 0.5 * prev) {
+      if (worst > 0.5 * prev) {  // stalled: less than a halving, twice in a row
         if (++stall >= 2) break;
       } else {
         stall = 0;
       }
       prev = worst;
     }
+    if (!converged && !o.no_gmres) {
+      // ---- GMRES-IR: FP64 GMRES preconditioned by the low-precision LU ----
+      Precond M = [&](alg_ctx*, const double* v, double* z) -> int { return F.apply(v, z, 1); };
+      GmresOpts go;
+      go.tol = tol;
+      if (o.gmres_restart > 0) go.restart = o.gmres_restart;
+      bool all = true;
+      double worst = 0.0;
+      for (int k = 0; k < nrhs && all; ++k) {
+        double* xk = x + (size_t)k * n;
+        if (!(eta[k] == eta[k]) || eta[k] > 1.0) ALG_CUDA_TRY(cudaMemsetAsync(xk, 0, sizeof(double) * n, ctx->stream));
+        GmresResult gr;
+        const int rc = gmres_ir_dev(ctx, d_a, n, lda, d_b + (size_t)k * ldb, xk, anorm, M, go, &gr);
+        R.gmres_iterations += gr.inner;
+        worst = std::max(worst, gr.backward_error);
+        if (rc != ALG_OK || !gr.converged) all = false;
+      }
+      if (all) {
+        converged = true;
+        R.backward_error = worst;
+        R.path = ALG_MIXED_PATH_GMRES;
+      }
+    }
   }
-  R.precision = o.precision;
   if (converged) {
     ALG_CUDA_TRY(cudaMemcpy2DAsync(d_b, sizeof(double) * ldb, x, sizeof(double) * n, sizeof(double) * n, nrhs,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
     ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    R.path = ALG_MIXED_PATH_IR;
+    if (R.path != ALG_MIXED_PATH_GMRES) R.path = ALG_MIXED_PATH_IR;
     return ALG_OK;
   }
   if (o.no_fallback) return ALG_CONVERGENCE;
   // ---- FP64 refactorization (A becomes its FP64 LU, like dgesv) ---------
   R.path = ALG_MIXED_PATH_FP64;
+  int* perm = nullptr;
+  ALG_TRY(ws_get(ctx, WS_PERM, sizeof(int) * n, reinterpret_cast<void**>(&perm)));
   ALG_TRY(status_reset(ctx));
   ALG_TRY((lu_factor_dev<double, false>(ctx, d_a, n, n, lda, ipiv, perm, default_plan(n, 8))));
   ALG_TRY(status_fetch(ctx));
@@ -314,6 +446,9 @@ void alg_mixed_opts_default(alg_mixed_opts* o) {
   o->tol = 0.0;
   o->max_ir = 30;
   o->no_fallback = 0;
+  o->no_gmres = 0;
+  o->gmres_restart = 30;
+  o->pivoting = ALG_PIVOT_AUTO;
 }
 
 int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, int n, int lda, double* d_b,

@@ -19,7 +19,7 @@ PATHS = {1: "ir", 2: "gmres", 3: "fp64"}
 
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_ir", C.c_int), ("no_fallback", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("no_gmres", C.c_int), ("gmres_restart", C.c_int), ("pivoting", C.c_int), ("reserved", C.c_int)]
 
 
 class Report(C.Structure):
@@ -28,13 +28,20 @@ class Report(C.Structure):
 
     def as_dict(self) -> dict:
         return {"path": PATHS.get(self.path, "none"), "ir_iterations": self.ir_iterations,
-                "gmres_iterations": self.gmres_iterations, "backward_error": self.backward_error}
+                "gmres_iterations": self.gmres_iterations, "backward_error": self.backward_error,
+                "butterfly": bool(self.reserved[0])}
 
 
-def opts(precision: str = "fp32", tol: float = 0.0, max_ir: int = 30, no_fallback: bool = False) -> Opts:
+PIVOTING = {"auto": 0, "partial": 1, "rbt": 2}
+
+
+def opts(precision: str = "fp32", tol: float = 0.0, max_ir: int = 30, no_fallback: bool = False,
+         pivoting: str = "auto", no_gmres: bool = False) -> Opts:
     o = Opts()
     _lib.load().alg_mixed_opts_default(C.byref(o))
     o.precision = PRECISIONS[precision]
+    o.pivoting = PIVOTING[pivoting]
+    o.no_gmres = 1 if no_gmres else 0
     o.tol = tol
     o.max_ir = max_ir
     o.no_fallback = 1 if no_fallback else 0

@@ -163,6 +163,16 @@ int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
 #define ALG_PREC_TF32 1
 #define ALG_PREC_BF16 2
 
+/* Stabilisation of the low-precision LU: partial pivoting (the reference's
+ * strategy, column-serial panel), or a random butterfly transformation of A
+ * followed by LU without pivoting (Baboulin, Dongarra, Herrmann, Tomov, ACM
+ * TOMS 2013; needs n divisible by 4; falls back to pivoting on a zero pivot).
+ * AUTO means partial pivoting: LU without pivoting keeps a large growth factor
+ * on matrices that are random to begin with, butterflies or not. */
+#define ALG_PIVOT_AUTO 0
+#define ALG_PIVOT_PARTIAL 1
+#define ALG_PIVOT_RBT 2
+
 #define ALG_MIXED_PATH_IR 1
 #define ALG_MIXED_PATH_GMRES 2
 #define ALG_MIXED_PATH_FP64 3
@@ -172,7 +182,10 @@ typedef struct {
   double tol;       /* backward-error target; <= 0 means 10 n 2^-53 */
   int max_ir;       /* refinement steps before the fallback (<= 0: 30) */
   int no_fallback;  /* nonzero: return ALG_CONVERGENCE instead of refactorizing in FP64 */
-  int reserved[4];
+  int no_gmres;     /* nonzero: skip GMRES-IR when plain refinement stalls */
+  int gmres_restart;/* Krylov dimension of GMRES-IR (<= 0: 30) */
+  int pivoting;     /* ALG_PIVOT_*: how the low-precision LU is kept stable */
+  int reserved;
 } alg_mixed_opts;
 
 typedef struct {

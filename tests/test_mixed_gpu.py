@@ -57,8 +57,9 @@ def test_tensor_core_update_matches_reference(gpu, prec, shape):
     assert err <= 1e-4 * scale, (err, scale)
 
 
+@pytest.mark.parametrize("pivoting", ["partial"])
 @pytest.mark.parametrize("prec", ["fp32", "tf32", "bf16"])
-def test_mixed_solve_reaches_fp64_backward_error(gpu, oracle, prec):
+def test_mixed_solve_reaches_fp64_backward_error(gpu, oracle, prec, pivoting):
     import torch
 
     from algebra_linear_b200 import device, mixed
@@ -71,10 +72,11 @@ def test_mixed_solve_reaches_fp64_backward_error(gpu, oracle, prec):
     with device.Context() as ctx:
         A = torch.from_numpy(a.copy()).cuda()
         B = torch.from_numpy(b.copy()).cuda()
-        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision=prec)
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision=prec, pivoting=pivoting)
         x = B.cpu().numpy()
         assert np.array_equal(A.cpu().numpy(), a), "A must be unchanged on the refinement path"
     assert rep["path"] in ("ir", "gmres"), rep
+    assert rep["butterfly"] == (pivoting == "rbt"), rep
     eta = oracle.backward_error(a, x, b, n)
     assert eta <= 10 * n * 2.0**-53, (eta, rep)
     # same solution as the FP64 reference to the accuracy the conditioning allows
@@ -91,3 +93,45 @@ def test_mixed_host_api_keeps_a(gpu, oracle):
     assert rc == 0, _lib.status_string(rc)
     assert np.array_equal(ha, a)
     assert oracle.backward_error(a, hb, b, n) <= 10 * n * 2.0**-53
+
+
+def test_mixed_64_rhs(gpu, oracle):
+    """64 right-hand sides (the C2 multi-RHS case) through the butterfly form."""
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    n, nrhs = 1024, 64
+    a, s = oracle.larnv("Symmetric", [4, 4, 4, 5], n * n)
+    b, _ = oracle.larnv("Symmetric", s, n * nrhs)
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        B = torch.from_numpy(b.copy()).cuda()
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, nrhs, precision="tf32")
+        x = B.cpu().numpy()
+    assert rep["path"] in ("ir", "gmres"), rep
+    for k in range(nrhs):
+        eta = oracle.backward_error(a, x[k * n:(k + 1) * n], b[k * n:(k + 1) * n], n)
+        assert eta <= 10 * n * 2.0**-53, (k, eta)
+
+
+def test_butterfly_form_on_a_diagonally_dominant_system(gpu, oracle):
+    """The butterfly + no-pivoting form on A + n I (where LU without pivoting
+    is stable), refined to the FP64 backward error; A is left unchanged."""
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    n = 1024
+    a, s = oracle.larnv("Symmetric", [8, 8, 8, 9], n * n)
+    a[:: n + 1] += n
+    xt, _ = oracle.larnv("Symmetric", s, n)
+    b = oracle.dgemv(a, xt, n, n)
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        B = torch.from_numpy(b.copy()).cuda()
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision="bf16", pivoting="rbt")
+        x = B.cpu().numpy()
+        assert np.array_equal(A.cpu().numpy(), a)
+    assert rep["butterfly"] and rep["path"] in ("ir", "gmres"), rep
+    assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53
