@@ -66,6 +66,14 @@ SIGNATURES = [
     ("alg_mixed_opts_default", None, [_P]),
     ("alg_dgesv_mixed", _I, [_P, _P, _P, _SZ, _SZ, _P]),
     ("alg_dgesv_mixed_dev", _I, [_P, _P, _P, _I, _I, _P, _I, _I, _P]),
+    ("alg_batch_create", _I, [_P, _I, _P, _I, C.POINTER(_P)]),
+    ("alg_batch_offsets", _I, [_P, _P, _P]),
+    ("alg_batch_solve", _I, [_P, _P, _P, _P]),
+    ("alg_batch_solve_graph", _I, [_P, _P, _P, _P]),
+    ("alg_batch_autotune", _I, [_P, _P, _P, _P, _P, _P, _P]),
+    ("alg_batch_info", _I, [_P, _P, _P, _P, _P, _P]),
+    ("alg_batch_eta", _I, [_P, _P]),
+    ("alg_batch_destroy", None, [_P]),
     ("alg_gemm_tc_sub_dev", _I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
     ("alg_ctx_set_profiling", _I, [_P, _I]),
     ("alg_ctx_profile_reset", _I, [_P]),

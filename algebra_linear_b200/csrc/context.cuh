@@ -76,6 +76,7 @@ enum WsSlot : int {
   WS_PRECOND,     // preconditioner scratch (mixed form)
   WS_RBT,         // butterfly coefficients (mixed form)
   WS_IDENT,       // identity permutation
+  WS_BATCH,       // batched-solve queues
   WS_COUNT
 };
 

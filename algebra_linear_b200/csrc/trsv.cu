@@ -27,7 +27,7 @@ constexpr int kTB = 64;         // block rows
 constexpr int kTThreads = 256;  // 64 rows x 4 column quarters
 constexpr int kMaxRhs = 4;      // right-hand sides handled per pass
 template <typename T>
-constexpr size_t kTSmem = 3 * kTB * kTB * sizeof(T);  // two factor tiles + the diagonal block
+constexpr size_t kTSmem = 4 * kTB * kTB * sizeof(T);  // two factor tiles, the diagonal block, its inverse
 
 __device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __res
   extern __shared__ __align__(16) unsigned char tsm[];
   T* tiles = reinterpret_cast<T*>(tsm);                 // [2][kTB*kTB] factor tiles, [col][row]
   T* dtile = tiles + 2 * kTB * kTB;                      // diagonal block, [col][row]
+  T* dinv = tiles + 3 * kTB * kTB;                       // its inverse (non-EXACT), [col][row]
   __shared__ T xs[kTB][kMaxRhs];       // x of the block being consumed
   __shared__ T part[4][kTB][kMaxRhs];  // partial sums of the four column quarters
   __shared__ T acc_s[kTB][kMaxRhs];
@@ -91,6 +92,33 @@ __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __res
       prefetch_tile<T>(tiles, lu, lda, i0, bj * kTB, rows, min(kTB, n - bj * kTB));
     }
     cp_async_commit();
+    if constexpr (!EXACT) {
+      // Invert the diagonal block now, while earlier blocks are still being
+      // solved: the critical path then only pays a matrix-vector product.
+      cp_async_wait<1>();  // the diagonal block (first group) has landed
+      __syncthreads();
+      if (threadIdx.x < rows) {
+        const int c = threadIdx.x;
+        T* xcol = dinv + c * kTB;
+        if constexpr (!UPPER) {  // unit lower: x = L^{-1} e_c
+          for (int rr = 0; rr < c; ++rr) xcol[rr] = T(0);
+          xcol[c] = T(1);
+          for (int rr = c + 1; rr < rows; ++rr) {
+            T acc = T(0);
+            for (int k = c; k < rr; ++k) acc = fma_rn(dtile[k * kTB + rr], xcol[k], acc);
+            xcol[rr] = -acc;
+          }
+        } else {  // upper: x = U^{-1} e_c
+          for (int rr = c + 1; rr < rows; ++rr) xcol[rr] = T(0);
+          xcol[c] = div_rn(T(1), dtile[c * kTB + c]);
+          for (int rr = c - 1; rr >= 0; --rr) {
+            T acc = T(0);
+            for (int k = rr + 1; k <= c; ++k) acc = fma_rn(dtile[k * kTB + rr], xcol[k], acc);
+            xcol[rr] = -div_rn(acc, dtile[rr * kTB + rr]);
+          }
+        }
+      }
+    }
     __syncthreads();
     for (int t = 0; t < s; ++t) {
       const int bj = UPPER ? nb - 1 - t : t;
@@ -164,7 +192,21 @@ __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __res
     }
     cp_async_wait<0>();
     __syncthreads();
-    if (threadIdx.x < 32) {
+    if constexpr (!EXACT) {
+      // x_i = inv(D_ii) y_i: four column quarters per row, fixed-order combine
+      if (r < rows) {
+        const int c0 = qt * (kTB / 4), c1 = min(rows, c0 + kTB / 4);
+        for (int k = 0; k < nrhs; ++k) {
+          T p = T(0);
+          for (int c = c0; c < c1; ++c) p = fma_rn(dinv[c * kTB + r], acc_s[c][k], p);
+          part[qt][r][k] = p;
+        }
+      }
+      __syncthreads();
+      if (qt == 0 && r < rows)
+        for (int k = 0; k < nrhs; ++k)
+          acc_s[r][k] = (part[0][r][k] + part[1][r][k]) + (part[2][r][k] + part[3][r][k]);
+    } else if (threadIdx.x < 32) {
       for (int k = 0; k < nrhs; ++k) {
         if constexpr (!UPPER) {
           for (int c = 0; c + 1 < rows; ++c) {
@@ -187,9 +229,11 @@ __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __res
     __syncthreads();
     if (qt == 0 && r < rows)
       for (int k = 0; k < nrhs; ++k) x[(size_t)k * ldx + i0 + r] = acc_s[r][k];
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) st_release(&flags[bi], 1);
+    if (threadIdx.x == 0) {
+      __threadfence();  // cumulative: the block's stores, ordered by the barrier, before the flag
+      st_release(&flags[bi], 1);
+    }
   }
 }
 

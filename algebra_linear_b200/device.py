@@ -45,7 +45,18 @@ class Context:
         _check(self._lib.alg_ctx_create(C.c_void_p(_current_stream()), C.byref(h)))
         self.handle = h
 
+    def adopt(self, child):
+        """Children (plans, sparse handles) are closed before the context."""
+        import weakref
+
+        self.__dict__.setdefault("_children", []).append(weakref.ref(child))
+        return child
+
     def close(self):
+        for ref in self.__dict__.get("_children", []):
+            child = ref()
+            if child is not None:
+                child.close()
         if self.handle:
             self._lib.alg_ctx_destroy(self.handle)
             self.handle = None

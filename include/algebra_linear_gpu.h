@@ -207,6 +207,35 @@ int alg_dgesv_mixed(const alg_mixed_opts* opts, double* a, double* b, size_t n, 
 int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, int n, int lda,
                         double* d_b, int nrhs, int ldb, alg_mixed_report* report);
 
+/* ---- batched dgesv: many independent systems of uneven order ------------
+ * Each system is the reference's dgesv (src/lapack/mod.rs:309-354) on its own
+ * n_i x n_i matrix (1 <= n_i <= 512). Matrices and right-hand sides live
+ * packed in two device buffers at the offsets alg_batch_offsets reports
+ * (column-major, leading dimension n_i). A plan sorts the systems into size
+ * buckets (largest first) and issues one persistent launch per bucket.
+ * mixed = 0: FP64 LU with partial pivoting (A becomes its LU, b becomes x).
+ * mixed = 1: FP32 LU + FP64 refinement to the backward error 10 n 2^-53
+ * (A is left unchanged; b becomes x; alg_batch_eta reports each system's
+ * backward error). d_info: per system 0, 1 + the first zero pivot's column,
+ * or -(iterations + 1) when refinement did not reach the target. */
+typedef struct alg_batch alg_batch;
+int alg_batch_create(alg_ctx* ctx, int count, const int* n_host, int mixed, alg_batch** out);
+int alg_batch_offsets(const alg_batch* batch, int64_t* a_off, int64_t* b_off);
+/* Stream-ordered; no synchronisation. */
+int alg_batch_solve(alg_batch* batch, double* d_a, double* d_b, int* d_info);
+/* The same launch sequence captured once in a CUDA graph (per buffer set) and
+ * replayed; the capturing call solves the batch too. */
+int alg_batch_solve_graph(alg_batch* batch, double* d_a, double* d_b, int* d_info);
+/* Autotuner: times 128/256/512 threads per CTA for every size bucket on this
+ * batch (restoring the inputs from d_a_src/d_b_src before each trial) and
+ * keeps the fastest; threads_out (may be NULL) receives one value per bucket. */
+int alg_batch_autotune(alg_batch* batch, double* d_a, double* d_b, int* d_info, const double* d_a_src,
+                       const double* d_b_src, int* threads_out);
+int alg_batch_info(const alg_batch* batch, int* n_buckets, int* caps, int* threads, int* counts,
+                   double* flops);
+int alg_batch_eta(const alg_batch* batch, double* eta_host);
+void alg_batch_destroy(alg_batch* batch);
+
 /* The tensor-core trailing update of the low-precision LU on device buffers:
  * C (FP32, M x N) -= A (M x K) * B (K x N), all column-major, operands
  * rounded to prec (ALG_PREC_TF32 or ALG_PREC_BF16), FP32 accumulation.
