@@ -39,11 +39,10 @@ import time
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "dgesv GFLOP/s, FP64 vs mixed-precision+IR at equal backward error; p99 latency"
-SEEDY = [1988, 1989, 1990, 1991]
-# dram bytes per algorithmic flop of the CUDA-core update kernel, from the ncu
-# capture summarised in profiles/gemm_sub_kernel_fp64.md (null until captured)
-GEMM_TRAFFIC_PER_FLOP = None
+# DRAM bytes per algorithmic flop of the CUDA-core trailing-update kernel, per
+# form, from ncu captures of its largest launch at n = 4096 (profiles/); a
+# form without a capture reports traffic null.
+GEMM_TRAFFIC_PER_FLOP = {}
 
 
 def flops_dgesv(n: int, nrhs: int) -> float:
@@ -238,24 +237,33 @@ def run_form(name, spec, ctx, A0, b0, xt, n, nrhs, steps, warmup, pg, sample_clo
     }
 
 
-def fp64_peak_tflops():
-    """cuBLAS DGEMM (torch.matmul float64, 8192^3), best of 3, measured here:
-    the FP64 ceiling for the CUDA-core update kernels."""
+def gemm_peaks_tflops():
+    """cuBLAS GEMM throughput at 8192^3 (torch.matmul), best of 4, measured in
+    this run: the ceilings of the update kernels — "f64" (DGEMM) for the FP64
+    forms, "f32" (SGEMM on CUDA cores, TF32 off) for the FP32 LU of the mixed
+    form, "tf32" for its tensor-core TF32 LU."""
     import torch
 
-    a = torch.rand(8192, 8192, dtype=torch.float64, device="cuda")
-    b = torch.rand(8192, 8192, dtype=torch.float64, device="cuda")
-    best = 1e9
-    for _ in range(4):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        best = min(best, e0.elapsed_time(e1))
-    del a, b
-    return 2 * 8192**3 / best / 1e9
+    out = {}
+    saved = torch.backends.cuda.matmul.allow_tf32
+    for key, dt, tf32 in (("f64", torch.float64, False), ("f32", torch.float32, False),
+                          ("tf32", torch.float32, True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.rand(8192, 8192, dtype=dt, device="cuda")
+        b = torch.rand(8192, 8192, dtype=dt, device="cuda")
+        best = 1e9
+        for _ in range(4):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        out[key] = 2 * 8192**3 / best / 1e9
+    torch.backends.cuda.matmul.allow_tf32 = saved
+    return out
 
 
 def measured_peaks():
@@ -268,7 +276,7 @@ def measured_peaks():
     return {}
 
 
-def roofline(res, form, peaks, fp64_peak):
+def roofline(res, form, peaks, gemm_peaks):
     prof = res["profile"]
     if not prof:
         return None
@@ -276,16 +284,19 @@ def roofline(res, form, peaks, fp64_peak):
     per_launch_ms = rec["ms"] / max(rec["launches"], 1)
     if cls in ("gemm", "gemm_tc", "panel", "trsm"):
         achieved = rec["flops"] / rec["ms"] / 1e9  # TFLOP/s
-        if cls == "gemm_tc":
+        if cls == "gemm_tc" and form == "mixed_bf16":
             peak = peaks.get("bf16_tflops")
             src = "MEASURED_PEAKS.json bf16_tflops (measured)" if peak else "fallback 1590"
             peak = peak or 1590.0
+        elif cls == "gemm_tc":
+            peak, src = gemm_peaks["tf32"], "cuBLAS TF32 GEMM measured in this run"
+        elif form.startswith("fp64"):
+            peak, src = gemm_peaks["f64"], "cuBLAS DGEMM measured in this run"
         else:
-            peak = fp64_peak
-            src = "cuBLAS DGEMM measured in this run"
+            peak, src = gemm_peaks["f32"], "cuBLAS SGEMM (CUDA cores, TF32 off) measured in this run"
         traffic = None
-        if cls == "gemm" and GEMM_TRAFFIC_PER_FLOP is not None:
-            traffic = GEMM_TRAFFIC_PER_FLOP * rec["flops"] / max(rec["launches"], 1)
+        if cls == "gemm" and GEMM_TRAFFIC_PER_FLOP.get(form) is not None:
+            traffic = GEMM_TRAFFIC_PER_FLOP[form] * rec["flops"] / max(rec["launches"], 1)
         return {"kernel": cls, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": src,
                 "launches": rec["launches"], "avg_launch_ms": per_launch_ms, "share_of_step":
@@ -392,7 +403,7 @@ def run_ours(args, world, rank, local, pg):
     n, nrhs = args.n, args.nrhs
     seed = [SEEDY[0], SEEDY[1], SEEDY[2], SEEDY[3] + 2 * rank]
     peaks = measured_peaks()
-    fp64_peak = fp64_peak_tflops()
+    gemm_peaks = gemm_peaks_tflops()
     ctx = device.Context()
     A0, s1 = ctx.larnv(2, seed, n * n)
     xt, _ = ctx.larnv(2, s1, n * nrhs)
@@ -400,7 +411,10 @@ def run_ours(args, world, rank, local, pg):
     torch.cuda.synchronize()
 
     reg = form_registry()
-    names = [f for f in (args.forms.split(",") if args.forms else reg.keys()) if f in reg]
+    # default forms: the FP64 pair and the mixed forms whose LU is a strong
+    # enough preconditioner at this order (BF16 falls back to FP64 past n ~ 4096)
+    default = [f for f in reg if f != "mixed_bf16" or n <= 4096]
+    names = [f for f in (args.forms.split(",") if args.forms else default) if f in reg]
     results = {}
     for name in names:
         results[name] = run_form(name, reg[name], ctx, A0, b0, xt, n, nrhs, args.steps, args.warmup, pg,
@@ -426,12 +440,14 @@ def run_ours(args, world, rank, local, pg):
         "config": {"workload": f"dense dgesv n={n}, {nrhs} RHS, A iid U(-1,1) no shift, b = A x_true",
                    "n": n, "nrhs": nrhs, "form": head, "parallelism": f"replicas x{world}",
                    "l2": "inputs (8 n^2 B) larger than L2; no flush"},
-        "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("profile",)} for k, v in results.items()},
+        "forms": {k: {**{kk: vv for kk, vv in v.items() if kk != "profile"},
+                      "kernel_ms_per_step": {c: r["ms"] / args.steps for c, r in (v["profile"] or {}).items()}}
+                  for k, v in results.items()},
         "backward_error_bound": tol,
         "gpu_launches": hr["gpu_launches"],
         "clocks": hr["clocks"],
-        "roofline": roofline(hr, head, peaks, fp64_peak),
-        "fp64_dgemm_peak_tflops": fp64_peak,
+        "roofline": roofline(hr, head, peaks, gemm_peaks),
+        "cublas_gemm_peaks_tflops": gemm_peaks,
     }
     if not args.no_e2e:
         line["e2e"] = e2e_run(head, A0, b0, n, nrhs, steps=max(2, min(args.steps, 3)))
