@@ -39,6 +39,8 @@ import time
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+METRIC = "dgesv GFLOP/s, FP64 vs mixed-precision+IR at equal backward error; p99 latency"
+SEEDY = [1988, 1989, 1990, 1991]
 # DRAM bytes per algorithmic flop of the CUDA-core trailing-update kernel, per
 # form, from ncu captures of its largest launch at n = 4096 (profiles/); a
 # form without a capture reports traffic null.
