@@ -75,6 +75,7 @@ SIGNATURES = [
     ("alg_batch_eta", _I, [_P, _P]),
     ("alg_batch_destroy", None, [_P]),
     ("alg_gemm_tc_sub_dev", _I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
+    ("alg_dgesv_mixed_noalloc", _I, [_P, _P, _P, _I, _P, _P, _P]),
     ("alg_ctx_set_profiling", _I, [_P, _I]),
     ("alg_ctx_profile_reset", _I, [_P]),
     ("alg_ctx_profile_get", _I, [_P, _I, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double),

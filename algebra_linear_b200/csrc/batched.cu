@@ -15,7 +15,10 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include <math_constants.h>
@@ -714,3 +717,148 @@ void alg_batch_destroy(alg_batch* b) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free solve of one small system (no counterpart in the reference)
+// ===========================================================================
+// Some callers cannot call cudaMalloc: code running inside another library's
+// memory pool that owns the device's free memory, serving loops where the
+// implicit device-wide synchronisation of cudaMalloc/cudaFree would stall
+// unrelated streams, and callers that must never fail with out-of-memory after
+// start-up. alg_dgesv_mixed_noalloc serves them: it runs the mixed form of the
+// batched kernel above (FP32 LU with partial pivoting, FP64 refinement) on
+// one system, and takes its working memory (the FP32 copy of A, the residual
+// vector, the work counter) from the file-scope array below instead of from
+// an allocation. Set-up per device (the array's address and the kernel's
+// shared-memory limit) is host-side work done by the first call on that
+// device. Every call on a device shares the one array, so calls that overlap
+// on the GPU (different streams, or different host threads) race on it;
+// calls on one stream are ordered and safe.
+namespace alg {
+namespace {
+
+constexpr int kNoAllocMaxN = 512;
+// Layout: FP32 copy of A (max order squared), residual (max order doubles),
+// pivots (max order ints), then a 256-byte header of per-call fields.
+constexpr size_t kNoAllocA32 = sizeof(float) * (size_t)kNoAllocMaxN * kNoAllocMaxN;
+constexpr size_t kNoAllocWork = sizeof(double) * kNoAllocMaxN;
+constexpr size_t kNoAllocIpiv = sizeof(int) * kNoAllocMaxN;
+constexpr size_t kNoAllocHeader = 256;
+constexpr size_t kNoAllocBytes = kNoAllocA32 + kNoAllocWork + kNoAllocIpiv + kNoAllocHeader;
+static_assert(kNoAllocBytes == 1054976, "scratch size is part of the C interface");
+
+struct NoAllocHeader {
+  long long a_off;  // offset of the system in A, b, pivots and the FP32 copy (always 0)
+  long long b_off;
+  int queue;        // work counter of the persistent kernel: must be 0 when it starts
+  int order;        // queue position -> system (always 0)
+  int n;            // the system's order
+  int info;         // spare slot (the caller's info pointer is required)
+  double eta;       // used when the caller passes no backward-error pointer
+};
+static_assert(sizeof(NoAllocHeader) <= kNoAllocHeader, "header fits its slot");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Writes the per-call header, in stream order before the solve kernel; this
+// is what resets the work counter to 0 for each call.
+__global__ void noalloc_header_kernel(NoAllocHeader* h, int n) {
+  h->a_off = 0;
+  h->b_off = 0;
+  h->queue = 0;
+  h->order = 0;
+  h->n = n;
+  h->info = 0;
+  h->eta = 0.0;
+}
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Per-device set-up (host side, not stream work), with `dev` current: the
+// scratch array's device address and the dynamic shared-memory limit of each
+// kernel instantiation used below.
+int noalloc_setup(int dev, unsigned char** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    ALG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    const size_t smem_max = std::max(kernel_smem(kMaxN, false), kernel_smem(kMaxN, true));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_max));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_max));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_max));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  return ALG_OK;
+}
+
+template <int NT>
+int noalloc_launch(cudaStream_t s, const BatchArgs& p) {
+  batched_gesv_kernel<NT><<<1, NT, kernel_smem(p.cap, true), s>>>(p);
+  count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
+}  // namespace
+}  // namespace alg
+
+extern "C" int alg_dgesv_mixed_noalloc(void* stream, const double* d_a, double* d_b, int n, int* d_ipiv,
+                                       int* d_info, double* d_eta) {
+  using namespace alg;
+  if (n < 0 || n > kNoAllocMaxN) {
+    if (std::getenv("ALG_VERBOSE"))
+      std::fprintf(stderr, "alg_dgesv_mixed_noalloc: order %d outside 0..%d (the size of its static scratch)\n", n,
+                   kNoAllocMaxN);
+    return ALG_BAD_SHAPE;
+  }
+  if (n == 0) return ALG_OK;
+  if (d_a == nullptr || d_b == nullptr || d_info == nullptr) return ALG_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return ALG_NO_DEVICE;
+  }
+  int dev = 0;
+  ALG_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return ALG_INVALID_ARGUMENT;
+  unsigned char* base = nullptr;
+  ALG_TRY(noalloc_setup(dev, &base));
+  auto* hdr = reinterpret_cast<NoAllocHeader*>(base + kNoAllocA32 + kNoAllocWork + kNoAllocIpiv);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the size bucket and CTA size a one-system plan of this order uses
+  int cap = 32;
+  while (cap < n) cap *= 2;
+  const int threads = cap >= 256 ? 512 : (cap >= 64 ? 256 : 128);
+  BatchArgs p;
+  p.count = 1;
+  p.order = &hdr->order;
+  p.n = &hdr->n;
+  p.a_off = &hdr->a_off;
+  p.b_off = &hdr->b_off;
+  p.a = const_cast<double*>(d_a);  // the mixed form only reads A
+  p.b = d_b;
+  p.a32 = reinterpret_cast<float*>(base);
+  p.ipiv = d_ipiv ? d_ipiv : reinterpret_cast<int*>(base + kNoAllocA32 + kNoAllocWork);
+  p.work = reinterpret_cast<double*>(base + kNoAllocA32);
+  p.info = d_info;
+  p.eta = d_eta ? d_eta : &hdr->eta;
+  p.queue = &hdr->queue;
+  p.cap = cap;
+  p.mixed = 1;
+  p.max_ir = 10;
+  p.tol_scale = 10.0;
+  noalloc_header_kernel<<<1, 1, 0, s>>>(hdr, n);
+  count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  switch (threads) {
+    case 128: return noalloc_launch<128>(s, p);
+    case 512: return noalloc_launch<512>(s, p);
+    default: return noalloc_launch<256>(s, p);
+  }
+}

@@ -244,6 +244,44 @@ void alg_batch_destroy(alg_batch* batch);
 int alg_gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda,
                         const float* B, int ldb, float* C, int ldc);
 
+/* ---- allocation-free solve of one small system ---------------------------
+ * No counterpart in the reference crate. For callers that cannot call
+ * cudaMalloc: code that runs inside another library's memory pool which owns
+ * the device's free memory, serving loops where the device-wide
+ * synchronisation of cudaMalloc/cudaFree would stall other streams, and
+ * callers that must not meet out-of-memory after start-up. This entry point
+ * allocates nothing, and needs no alg_ctx (creating one allocates).
+ *
+ * Solves A x = b for ONE system of order 1 <= n <= ALG_NOALLOC_MAX_N with the
+ * mixed form of the batched kernel (FP32 LU with partial pivoting, FP64
+ * refinement to the backward error 10 n 2^-53, at most 10 steps): the same
+ * kernel, CTA size and arithmetic as a one-system alg_batch plan with
+ * mixed = 1. d_a (n x n, column-major, leading dimension n) is only read;
+ * d_b (n) becomes x; *d_info receives 0, 1 + the first zero pivot's column,
+ * or -(iterations + 1) when refinement missed the target. d_ipiv (n ints,
+ * the FP32 LU's 0-based pivot rows) and d_eta (the backward error) may be
+ * NULL. All pointers are device pointers; the work is queued on `stream` (a
+ * cudaStream_t; NULL is the default stream) and the call returns without
+ * synchronising.
+ *
+ * Working memory: one static device array of ALG_NOALLOC_SCRATCH_BYTES,
+ * which every GPU that loads the library holds until exit (the FP32 copy of
+ * A, a residual vector, pivots, a work counter). n > ALG_NOALLOC_MAX_N (or
+ * n < 0) returns ALG_BAD_SHAPE and queues nothing; n = 0 returns ALG_OK.
+ * The array keeps the previous call's contents; the work counter must be 0
+ * when the kernel starts, and each call resets it itself, in stream order,
+ * so the caller clears nothing. All calls on one device share the array:
+ * calls that overlap on the GPU (on different streams, or from different
+ * host threads without ordering) race on it and give wrong results; calls
+ * queued on one stream are safe. The first call on each device does
+ * host-side set-up (looks up the array's device address and sets the
+ * kernel's shared-memory limit); make that first call before beginning any
+ * stream capture. */
+#define ALG_NOALLOC_MAX_N 512
+#define ALG_NOALLOC_SCRATCH_BYTES 1054976
+int alg_dgesv_mixed_noalloc(void* stream, const double* d_a, double* d_b, int n, int* d_ipiv, int* d_info,
+                            double* d_eta);
+
 #ifdef __cplusplus
 }
 #endif
