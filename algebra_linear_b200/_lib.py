@@ -76,6 +76,19 @@ SIGNATURES = [
     ("alg_batch_destroy", None, [_P]),
     ("alg_gemm_tc_sub_dev", _I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
     ("alg_dgesv_mixed_noalloc", _I, [_P, _P, _P, _I, _P, _P, _P]),
+    ("alg_splu_analyze", _I, [_P, _SZ, _P, _SZ, _I, C.c_double, _P]),
+    ("alg_splu_factorize", _I, [_P, _P, _SZ, _P, _SZ, _P, _SZ]),
+    ("alg_splu_solve", _I, [_P, _P, _SZ]),
+    ("alg_splu_effective_method", _I, [_P]),
+    ("alg_splu_flop_ratio", _I, [_P, _P]),
+    ("alg_splu_get_stats", _I, [_P, _P]),
+    ("alg_splu_free", None, [_P]),
+    ("alg_splu_symbolic", _I, [_P, _P, _P, _P, _P, _P]),
+    ("alg_splu_row_perm", _I, [_P, _P]),
+    ("alg_splu_plan_info", _I, [_P, _P]),
+    ("alg_splu_set_ctx", _I, [_P, _P]),
+    ("alg_splu_factorize_dev", _I, [_P, _P]),
+    ("alg_splu_solve_dev", _I, [_P, _P]),
     ("alg_ctx_set_profiling", _I, [_P, _I]),
     ("alg_ctx_profile_reset", _I, [_P]),
     ("alg_ctx_profile_get", _I, [_P, _I, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double),

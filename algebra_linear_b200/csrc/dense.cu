@@ -188,7 +188,13 @@ int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T
 template <typename T, bool EXACT>
 int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* perm,
                   const LuPlan& plan) {
-  if (m < nc || nc < 0 || lda < std::max(1, m)) return ALG_BAD_SHAPE;
+  return lu_factor_partial_dev<T, EXACT>(ctx, a, m, nc, nc, lda, ipiv, perm, plan);
+}
+
+template <typename T, bool EXACT>
+int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, int* ipiv, int* perm,
+                          const LuPlan& plan) {
+  if (m < nc || nc < 0 || ntot < nc || lda < std::max(1, m)) return ALG_BAD_SHAPE;
   if (nc == 0) return ALG_OK;
   int* lab = nullptr;
   int* perm_tmp = nullptr;
@@ -227,32 +233,32 @@ int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* pe
       }
     }
     // deferred interchanges of every other column (and of perm)
-    const int n_out = k0 + (nc - k0 - kb);
+    const int n_out = k0 + (ntot - k0 - kb);
     if (n_out > 0 || perm != nullptr) {
       const int warps_needed = std::max(1, n_out);
       const int grid = std::max(1, std::min(4 * ctx->sm_count, (warps_needed + 7) / 8));
       const int tok = prof_begin(ctx, ALG_K_LASWP);
-      laswp_outside_kernel<T><<<grid, kSwapThreads, 0, ctx->stream>>>(a, lda, m, nc, k0, kb, lab, perm,
+      laswp_outside_kernel<T><<<grid, kSwapThreads, 0, ctx->stream>>>(a, lda, m, ntot, k0, kb, lab, perm,
                                                                         perm_tmp);
       count_launches();
       prof_end(ctx, tok, 0.0, 0.0);
       ALG_CUDA_TRY(cudaGetLastError());
     }
     const int kr = k0 + kb;
-    if (kr < nc) {
-      ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, kr, nc)));
+    if (kr < ntot) {
+      ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, kr, ntot)));
     }
-    if (kr < nc) {
+    if (kr < ntot && kr < m) {
       bool done = false;
       if constexpr (std::is_same<T, float>::value) {
         if (plan.tc_prec >= 0) {
-          ALG_TRY(gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, nc - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+          ALG_TRY(gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ntot - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                   a + (size_t)k0 + (size_t)kr * lda, lda, a + (size_t)kr + (size_t)kr * lda, lda));
           done = true;
         }
       }
       if (!done) {
-        ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - kr, nc - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+        ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - kr, ntot - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                         a + (size_t)k0 + (size_t)kr * lda, lda,
                                         a + (size_t)kr + (size_t)kr * lda, lda)));
       }
@@ -275,6 +281,7 @@ int trsm_lower_unit_f32(alg_ctx* ctx, float* a, int lda, int r0, int kb, int cb,
 // explicit instantiations
 #define ALG_INST(T, E)                                                                          \
   template int lu_factor_dev<T, E>(alg_ctx*, T*, int, int, int, int*, int*, const LuPlan&);   \
+  template int lu_factor_partial_dev<T, E>(alg_ctx*, T*, int, int, int, int, int*, int*, const LuPlan&); \
   template int lu_solve_dev<T, E>(alg_ctx*, const T*, int, int, const int*, T*, int, int);    \
   template int gemm_sub_dev<T, E>(alg_ctx*, int, int, int, const T*, int, const T*, int, T*, int);
 ALG_INST(double, true)

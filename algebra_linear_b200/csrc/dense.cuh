@@ -24,6 +24,14 @@ template <typename T, bool EXACT>
 int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* perm,
                   const LuPlan& plan);
 
+// LU with partial pivoting of the first nc columns of the m x ntot device
+// matrix a (m >= nc): the row interchanges span all ntot columns, the block
+// row to the right becomes U12 and the trailing (m - nc) x (ntot - nc) block
+// becomes the Schur complement. ntot = nc is lu_factor_dev.
+template <typename T, bool EXACT>
+int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, int* ipiv, int* perm,
+                          const LuPlan& plan);
+
 // Solves with the packed factors: b (n x nrhs, ldb) becomes x. Stream-ordered.
 template <typename T, bool EXACT>
 int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs,

@@ -1,0 +1,266 @@
+// Host construction of the static front plan of the sparse LU (sparse.cuh).
+#include <algorithm>
+#include <numeric>
+
+#include "sparse.cuh"
+
+namespace alg {
+namespace sp {
+
+int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, FrontPlan* out) {
+  FrontPlan& F = *out;
+  F = FrontPlan();
+  const idx n = p.n, ns = S.n_supernodes(), nnz = p.nnz();
+  F.n = n;
+  F.nnz = nnz;
+  F.ns = ns;
+  F.col_perm.assign(S.col_perm.begin(), S.col_perm.end());
+  F.fronts.assign(ns, FrontDesc{});
+  if (n == 0) return SP_OK;
+  const std::vector<idx>& ptr = S.supernode_ptr;
+  std::vector<int32_t> owner(n);
+  for (idx s = 0; s < ns; ++s)
+    for (idx c = ptr[s]; c < ptr[s + 1]; ++c) owner[c] = (int32_t)s;
+
+  // rows of A in positions: each row's columns (new positions) and the CSC
+  // index of each entry
+  std::vector<int64_t> rp(n + 1, 0);
+  for (idx q = 0; q < nnz; ++q) rp[p.row_idx[q] + 1] += 1;
+  for (idx r = 0; r < n; ++r) rp[r + 1] += rp[r];
+  std::vector<int32_t> rpos((size_t)nnz);
+  std::vector<int64_t> rq((size_t)nnz);
+  {
+    std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+    for (idx c = 0; c < n; ++c)
+      for (size_t q = p.col_ptr[c]; q < p.col_ptr[c + 1]; ++q) {
+        const int64_t t = fill[p.row_idx[q]]++;
+        rpos[t] = (int32_t)S.col_perm_inv[c];
+        rq[t] = (int64_t)q;
+      }
+  }
+  // the front each row enters: the owner of its first column
+  std::vector<int32_t> leaf(n, -1);
+  for (idx r = 0; r < n; ++r) {
+    if (rp[r + 1] == rp[r]) {
+      F.structurally_singular = true;  // an empty row
+      continue;
+    }
+    int32_t lo = rpos[rp[r]];
+    for (int64_t t = rp[r]; t < rp[r + 1]; ++t) lo = std::min(lo, rpos[t]);
+    leaf[r] = owner[lo];
+  }
+  std::vector<int32_t> newptr(ns + 1, 0);
+  for (idx r = 0; r < n; ++r)
+    if (leaf[r] >= 0) newptr[leaf[r] + 1] += 1;
+  for (idx s = 0; s < ns; ++s) newptr[s + 1] += newptr[s];
+  F.new_rows.assign(newptr[ns], 0);
+  {
+    std::vector<int32_t> fill(newptr.begin(), newptr.end() - 1);
+    for (idx r = 0; r < n; ++r)
+      if (leaf[r] >= 0) F.new_rows[fill[leaf[r]]++] = (int32_t)r;  // increasing r within a front
+  }
+  // children in increasing order
+  std::vector<int32_t> kptr(ns + 1, 0);
+  for (idx s = 0; s < ns; ++s)
+    if (S.super_etree[s] >= 0) kptr[S.super_etree[s] + 1] += 1;
+  for (idx s = 0; s < ns; ++s) kptr[s + 1] += kptr[s];
+  F.child_idx.assign(kptr[ns], 0);
+  F.child_slot.assign(kptr[ns], 0);
+  {
+    std::vector<int32_t> fill(kptr.begin(), kptr.end() - 1);
+    for (idx s = 0; s < ns; ++s)
+      if (S.super_etree[s] >= 0) F.child_idx[fill[S.super_etree[s]]++] = (int32_t)s;
+  }
+
+  // fronts in postorder: slots, Struct(s), column maps
+  std::vector<int32_t> mark(n, -1);
+  std::vector<int32_t> sbeg(ns + 1, 0);
+  std::vector<int32_t> cand;
+  F.cb_colmap.clear();
+  for (idx s = 0; s < ns; ++s) {
+    FrontDesc& d = F.fronts[s];
+    const int32_t b = (int32_t)ptr[s], e = (int32_t)ptr[s + 1];
+    d.begin = b;
+    d.size = e - b;
+    d.child_begin = kptr[s];
+    d.child_end = kptr[s + 1];
+    d.new_begin = newptr[s];
+    d.new_end = newptr[s + 1];
+    int32_t slot = 0;
+    cand.clear();
+    for (int32_t k = d.child_begin; k < d.child_end; ++k) {
+      const int32_t c = F.child_idx[k];
+      const FrontDesc& dc = F.fronts[c];
+      F.child_slot[k] = slot;
+      slot += dc.rows - dc.size;
+      for (int32_t t = sbeg[c]; t < sbeg[c + 1]; ++t) {
+        const int32_t q = F.struct_cols[t];
+        if (q >= e && mark[q] != s) {
+          mark[q] = (int32_t)s;
+          cand.push_back(q);
+        }
+      }
+    }
+    for (int32_t k = d.new_begin; k < d.new_end; ++k) {
+      const int32_t r = F.new_rows[k];
+      for (int64_t t = rp[r]; t < rp[r + 1]; ++t) {
+        const int32_t q = rpos[t];
+        if (q >= e && mark[q] != s) {
+          mark[q] = (int32_t)s;
+          cand.push_back(q);
+        }
+      }
+    }
+    d.rows = slot + (d.new_end - d.new_begin);
+    if (d.rows < d.size) F.structurally_singular = true;
+    std::sort(cand.begin(), cand.end());
+    sbeg[s] = (int32_t)F.struct_cols.size();
+    d.struct_begin = sbeg[s];
+    F.struct_cols.insert(F.struct_cols.end(), cand.begin(), cand.end());
+    sbeg[s + 1] = (int32_t)F.struct_cols.size();
+    d.ncb = (int32_t)cand.size();
+    // the children's contribution columns in this front's local numbering
+    for (int32_t k = d.child_begin; k < d.child_end; ++k) {
+      const int32_t c = F.child_idx[k];
+      for (int32_t t = sbeg[c]; t < sbeg[c + 1]; ++t) {
+        const int32_t q = F.struct_cols[t];
+        int32_t loc;
+        if (q < e) {
+          loc = q - b;
+        } else {
+          loc = d.size + (int32_t)(std::lower_bound(cand.begin(), cand.end(), q) - cand.begin());
+        }
+        F.cb_colmap.resize(std::max<size_t>(F.cb_colmap.size(), (size_t)t + 1));
+        F.cb_colmap[t] = loc;
+      }
+    }
+  }
+  F.cb_colmap.resize(F.struct_cols.size());
+
+  // A values of the entering rows: slot and local column in their front
+  {
+    std::vector<int32_t> cnt(ns + 1, 0);
+    for (idx r = 0; r < n; ++r)
+      if (leaf[r] >= 0) cnt[leaf[r] + 1] += (int32_t)(rp[r + 1] - rp[r]);
+    for (idx s = 0; s < ns; ++s) cnt[s + 1] += cnt[s];
+    F.anew_q.assign(cnt[ns], 0);
+    F.anew_slot.assign(cnt[ns], 0);
+    F.anew_col.assign(cnt[ns], 0);
+    for (idx s = 0; s < ns; ++s) {
+      FrontDesc& d = F.fronts[s];
+      d.anew_begin = cnt[s];
+      d.anew_end = cnt[s + 1];
+      int32_t w = cnt[s];
+      const int32_t slot0 = d.rows - (d.new_end - d.new_begin);
+      const int32_t* st = F.struct_cols.data() + d.struct_begin;
+      for (int32_t k = d.new_begin; k < d.new_end; ++k) {
+        const int32_t r = F.new_rows[k];
+        for (int64_t t = rp[r]; t < rp[r + 1]; ++t) {
+          const int32_t q = rpos[t];
+          F.anew_q[w] = rq[t];
+          F.anew_slot[w] = slot0 + (k - d.new_begin);
+          F.anew_col[w] = q < d.begin + d.size
+                              ? q - d.begin
+                              : d.size + (int32_t)(std::lower_bound(st, st + d.ncb, q) - st);
+          ++w;
+        }
+      }
+    }
+  }
+
+  // small fronts: few rows, small block, every child small
+  std::vector<int32_t> height(ns, 0);
+  for (idx s = 0; s < ns; ++s) {
+    FrontDesc& d = F.fronts[s];
+    bool small = d.rows <= small_rows && (int64_t)d.rows * (d.size + d.ncb) <= (1 << 21);
+    int32_t h = 0;
+    for (int32_t k = d.child_begin; k < d.child_end; ++k) {
+      const int32_t c = F.child_idx[k];
+      small = small && F.fronts[c].small;
+      h = std::max(h, height[c] + 1);
+    }
+    d.small = small ? 1 : 0;
+    height[s] = h;
+  }
+  // offsets
+  int64_t lo = 0, uo = 0, ro = 0, bo = 0;
+  for (idx s = 0; s < ns; ++s) {
+    FrontDesc& d = F.fronts[s];
+    d.l_off = lo;
+    lo += (int64_t)d.rows * d.size;
+    d.u_off = uo;
+    uo += (int64_t)d.size * d.ncb;
+    d.rowid_off = ro;
+    ro += d.rows;
+    if (d.small) {
+      d.block_off = bo;
+      bo += (int64_t)d.rows * (d.size + d.ncb);
+      d.cb_off = d.block_off + d.size + (int64_t)d.size * d.rows;
+      d.cb_ld = d.rows;
+    } else {
+      d.block_off = -1;
+    }
+    const double m = d.rows, k = d.size, c = d.ncb;
+    F.flops += 2.0 * k * k * m - 2.0 / 3.0 * k * k * k + k * k * c + 2.0 * (m - k) * c * k;
+  }
+  F.l_total = lo;
+  F.u_total = uo;
+  F.rowid_total = ro;
+  F.block_total = bo;
+  // large fronts: postorder, contribution blocks on a stack
+  {
+    std::vector<std::pair<int64_t, int64_t>> stack;  // (offset, length)
+    int64_t top = 0, peak = 0, fbuf = 0;
+    for (idx s = 0; s < ns; ++s) {
+      FrontDesc& d = F.fronts[s];
+      if (d.small) continue;
+      F.big_order.push_back((int32_t)s);
+      fbuf = std::max(fbuf, (int64_t)d.rows * (d.size + d.ncb));
+      int nbig = 0;
+      for (int32_t k = d.child_begin; k < d.child_end; ++k) nbig += F.fronts[F.child_idx[k]].small ? 0 : 1;
+      for (int i = 0; i < nbig; ++i) {
+        top = stack.back().first;
+        stack.pop_back();
+      }
+      d.cb_off = top;
+      d.cb_ld = std::max(1, d.rows - d.size);
+      const int64_t len = (int64_t)(d.rows - d.size) * d.ncb;
+      stack.push_back({top, len});
+      top += len;
+      peak = std::max(peak, top);
+    }
+    F.stack_total = peak;
+    F.front_buf = fbuf;
+  }
+  // levels: small fronts (batched kernel) and all fronts (solve)
+  {
+    int32_t hmax = 0;
+    for (idx s = 0; s < ns; ++s) hmax = std::max(hmax, height[s]);
+    std::vector<int32_t> cs(hmax + 2, 0), ca(hmax + 2, 0);
+    for (idx s = 0; s < ns; ++s) {
+      if (F.fronts[s].small) cs[height[s] + 1] += 1;
+      ca[height[s] + 1] += 1;
+    }
+    for (int32_t h = 0; h <= hmax; ++h) {
+      cs[h + 1] += cs[h];
+      ca[h + 1] += ca[h];
+    }
+    F.small_level_ptr = cs;
+    F.solve_level_ptr = ca;
+    F.small_level_fronts.assign(cs[hmax + 1], 0);
+    F.solve_level_fronts.assign(ca[hmax + 1], 0);
+    std::vector<int32_t> fs(cs.begin(), cs.end() - 1), fa(ca.begin(), ca.end() - 1);
+    for (idx s = 0; s < ns; ++s) {
+      if (F.fronts[s].small) F.small_level_fronts[fs[height[s]]++] = (int32_t)s;
+      F.solve_level_fronts[fa[height[s]]++] = (int32_t)s;
+    }
+    // drop trailing empty small levels
+    while (F.small_level_ptr.size() > 1 &&
+           F.small_level_ptr[F.small_level_ptr.size() - 1] == F.small_level_ptr[F.small_level_ptr.size() - 2])
+      F.small_level_ptr.pop_back();
+  }
+  return SP_OK;
+}
+
+}  // namespace sp
+}  // namespace alg

@@ -244,6 +244,81 @@ void alg_batch_destroy(alg_batch* batch);
 int alg_gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda,
                         const float* B, int ldb, float* C, int ldc);
 
+/* ---- sparse LU (sparse::faer::SparseLu, src/sparse/faer/sparse_lu.rs) -----
+ * The handle owns the symbolic analysis (host) and the numeric factors (GPU).
+ * CSC arrays are borrowed per call and never retained: col_ptr (n + 1),
+ * row_idx (nnz, strictly increasing within a column), values (nnz). All
+ * indices 0-based. Status codes are ALG_SP_* (error.rs:5-24) plus the GPU
+ * codes 200..204. */
+#define ALG_SPLU_SIMPLICIAL 0 /* LuMethod::Simplicial (solver.rs:71-82) */
+#define ALG_SPLU_SUPERNODAL 1 /* LuMethod::Supernodal */
+#define ALG_SPLU_AUTO 2       /* LuMethod::Auto { flop_ratio_threshold } */
+
+typedef struct alg_splu alg_splu;
+
+/* SparseLuStats (src/sparse/faer/stats.rs:13-35); times in seconds. */
+typedef struct {
+  size_t n, nnz_a, nnz_l, nnz_u;
+  double fill_ratio;
+  size_t flops_estimate;
+  int method;          /* ALG_SPLU_SIMPLICIAL / ALG_SPLU_SUPERNODAL */
+  int has_flop_ratio;  /* Option<f64> */
+  double flop_ratio;
+  double ordering_time;
+  double factorization_time;
+} alg_splu_stats;
+
+/* SparseLu::analyze (sparse_lu.rs:64-78): n = col_ptr_len - 1; a row index
+ * >= n is ALG_SP_BAD_SHAPE, then the CSC validation of csc.rs:39-76; COLAMD,
+ * the supernodal symbolic analysis and the GPU front plan run on the host
+ * (no GPU needed). flop_ratio_threshold is used by ALG_SPLU_AUTO (the
+ * reference's default is 40.0). The numeric factorization runs on the GPU
+ * for every method: the reference's simplicial numeric path has no GPU
+ * counterpart here, so a handle whose effective method is Simplicial is
+ * factored by the supernodal GPU path (same pivots, values to rounding). */
+int alg_splu_analyze(const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx, size_t row_idx_len,
+                     int method, double flop_ratio_threshold, alg_splu** out);
+/* SparseLu::factorize (sparse_lu.rs:91-121): CSC view errors, then
+ * ALG_SP_STRUCTURE_MISMATCH (order, nnz and FNV-1a fingerprint),
+ * ALG_SP_NOT_FINITE, ALG_SP_SINGULAR. Synchronises. On failure the previous
+ * factors and statistics stay in place. */
+int alg_splu_factorize(alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx,
+                       size_t row_idx_len, const double* values, size_t values_len);
+/* SparseLu::solve (sparse_lu.rs:125-130): ALG_SP_NOT_FACTORIZED before a
+ * successful factorization, ALG_SP_BAD_SHAPE if b_len != n. b becomes x. */
+int alg_splu_solve(const alg_splu* lu, double* b, size_t b_len);
+/* effective_method (sparse_lu.rs:137-140): ALG_SPLU_SIMPLICIAL / _SUPERNODAL. */
+int alg_splu_effective_method(const alg_splu* lu);
+/* flop_ratio (sparse_lu.rs:146-149): returns 1 and sets *ratio when the
+ * supernodal symbolic analysis ran (method Supernodal or Auto), else 0. */
+int alg_splu_flop_ratio(const alg_splu* lu, double* ratio);
+/* stats (sparse_lu.rs:152-155): ALG_SP_NOT_FACTORIZED until a factorization
+ * has succeeded (the reference's None). */
+int alg_splu_get_stats(const alg_splu* lu, alg_splu_stats* out);
+void alg_splu_free(alg_splu* lu);
+
+/* Inspection (no reference counterpart; for tests and tools): the symbolic
+ * analysis (any pointer may be NULL; supernode_ptr holds n_supernodes + 1)
+ * and the row permutation of the current factors (position -> row). */
+int alg_splu_symbolic(const alg_splu* lu, size_t* col_perm, size_t* col_perm_inv, size_t* col_counts,
+                      size_t* supernode_ptr, size_t* n_supernodes);
+int alg_splu_row_perm(const alg_splu* lu, size_t* row_perm);
+typedef struct {
+  size_t n_fronts, n_small_fronts, small_levels, solve_levels, max_front_rows, max_front_cols;
+  size_t factor_bytes, work_bytes;
+  double plan_flops;
+  int structurally_singular;
+} alg_splu_plan;
+int alg_splu_plan_info(const alg_splu* lu, alg_splu_plan* out);
+
+/* Device-resident use: bind a context (its stream) before the first
+ * factorization; d_values (nnz, CSC order of the analyzed pattern) and d_b
+ * (n) are device pointers. factorize_dev synchronises (it reports the
+ * outcome); solve_dev is stream-ordered. */
+int alg_splu_set_ctx(alg_splu* lu, alg_ctx* ctx);
+int alg_splu_factorize_dev(alg_splu* lu, const double* d_values);
+int alg_splu_solve_dev(alg_splu* lu, double* d_b);
+
 /* ---- allocation-free solve of one small system ---------------------------
  * No counterpart in the reference crate. For callers that cannot call
  * cudaMalloc: code that runs inside another library's memory pool which owns
