@@ -67,5 +67,11 @@ struct FrontPlan {
 // all small go to the batched kernel.
 int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, FrontPlan* out);
 
+// A coarser partition for the GPU plan: chains of only-children merged into
+// their parents while the merged front's flops grow by at most tol.
+void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std::vector<idx>* ptr_out);
+// S with another supernode partition (same order, counts and column etree).
+void repartition(const Supernodal& S, const std::vector<idx>& ptr, Supernodal* out);
+
 }  // namespace sp
 }  // namespace alg

@@ -36,6 +36,7 @@ struct alg_splu {
 namespace {
 
 constexpr int kSmallFrontRows = 256;
+constexpr double kChainTolerance = 0.05;
 
 // CscView::new for an n x n matrix (csc.rs:39-76, 178-189).
 int check_view(const alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx,
@@ -142,8 +143,22 @@ int alg_splu_analyze(const size_t* col_ptr, size_t col_ptr_len, const size_t* ro
     lu->effective = lu->flop_ratio > flop_ratio_threshold ? ALG_SPLU_SUPERNODAL : ALG_SPLU_SIMPLICIAL;
   else
     lu->effective = ALG_SPLU_SIMPLICIAL;
-  rc = alg::sp::build_front_plan(p, lu->sym, kSmallFrontRows, &lu->plan);
-  if (rc != ALG_OK) return rc;
+  // GPU plan: the reference's partition with chains of only-children merged
+  {
+    alg::sp::FrontPlan first;
+    rc = alg::sp::build_front_plan(p, lu->sym, kSmallFrontRows, &first);
+    if (rc != ALG_OK) return rc;
+    std::vector<idx> ptr;
+    alg::sp::amalgamate_chains(first, lu->sym, kChainTolerance, &ptr);
+    if (ptr.size() == lu->sym.supernode_ptr.size()) {
+      lu->plan = std::move(first);
+    } else {
+      alg::sp::Supernodal coarse;
+      alg::sp::repartition(lu->sym, ptr, &coarse);
+      rc = alg::sp::build_front_plan(p, coarse, kSmallFrontRows, &lu->plan);
+      if (rc != ALG_OK) return rc;
+    }
+  }
   *out = lu.release();
   return ALG_OK;
 }

@@ -286,54 +286,110 @@ __global__ void scatter_cols_kernel(const double* x, const int32_t* col_perm, do
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) b[col_perm[j]] = x[j];
 }
 
-// Forward sweep of one level: unit-lower solve of each front's diagonal block
-// (column by column), then y[rows below] -= L21 y_s.
-__global__ void __launch_bounds__(kSolveThreads) forward_level_kernel(const FrontDesc* fronts,
-                                                                      const int32_t* level, const double* L,
-                                                                      const int32_t* rowid,
-                                                                      const int32_t* pos_of_row, double* y) {
+constexpr int kRowChunk = 256;   // rows of L21 / U12 per CTA
+constexpr int kColChunk = 1024;  // columns of U12 per CTA
+
+// Forward, diagonal block of each front of a level (one CTA per front):
+// unit-lower solve in 32-column blocks, a warp for the block, all threads
+// for the rows below it.
+__global__ void __launch_bounds__(kSolveThreads) fwd_diag_kernel(const FrontDesc* fronts, const int32_t* level,
+                                                                 const double* L, double* y) {
   const FrontDesc d = fronts[level[blockIdx.x]];
-  const int rows = d.rows, size = d.size;
+  const int rows = d.rows, m = d.size;
   const double* lp = L + d.l_off;
   double* ys = y + d.begin;
-  for (int k = 0; k < size; ++k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int kb = 0; kb < m; kb += 32) {
+    const int w = min(32, m - kb);
+    if (warp == 0) {
+      double v = lane < w ? ys[kb + lane] : 0.0;
+      for (int k = 0; k < w; ++k) {
+        const double yk = __shfl_sync(0xffffffffu, v, k);
+        if (lane > k && lane < w) v -= lp[(kb + lane) + (int64_t)(kb + k) * rows] * yk;
+      }
+      if (lane < w) ys[kb + lane] = v;
+    }
     __syncthreads();
-    const double yk = ys[k];
-    for (int i = k + 1 + threadIdx.x; i < size; i += kSolveThreads) ys[i] -= lp[i + (int64_t)k * rows] * yk;
-  }
-  __syncthreads();
-  for (int i = size + threadIdx.x; i < rows; i += kSolveThreads) {
-    double acc = 0.0;
-    for (int k = 0; k < size; ++k) acc = fma(lp[i + (int64_t)k * rows], ys[k], acc);
-    const int32_t pos = pos_of_row[rowid[d.rowid_off + i]];
-    y[pos] -= acc;
+    for (int i = kb + w + threadIdx.x; i < m; i += kSolveThreads) {
+      double acc = 0.0;
+      for (int k = 0; k < w; ++k) acc = fma(lp[i + (int64_t)(kb + k) * rows], ys[kb + k], acc);
+      ys[i] -= acc;
+    }
+    __syncthreads();
   }
 }
 
-// Backward sweep of one level: x_s -= U12 x[Struct(s)] (a thread per row of
-// the block), then the upper solve of the diagonal block, x_j times the
-// reciprocal of its diagonal, as in the reference's upper sweep.
-__global__ void __launch_bounds__(kSolveThreads) backward_level_kernel(const FrontDesc* fronts,
-                                                                       const int32_t* level, const double* L,
-                                                                       const double* U,
-                                                                       const int32_t* struct_cols, double* x) {
-  const FrontDesc d = fronts[level[blockIdx.x]];
-  const int rows = d.rows, size = d.size;
+// Forward, rows below the diagonal block: y[pos(row)] -= L21 y_s, a CTA per
+// chunk of rows (rows of different fronts of one level are distinct).
+__global__ void __launch_bounds__(kSolveThreads) fwd_l21_kernel(const FrontDesc* fronts, const SolveItem* items,
+                                                                const double* L, const int32_t* rowid,
+                                                                const int32_t* pos_of_row, double* y) {
+  const SolveItem it = items[blockIdx.x];
+  const FrontDesc d = fronts[it.front];
+  const int i = d.size + it.chunk * kRowChunk + threadIdx.x;
+  if (i >= d.rows) return;
   const double* lp = L + d.l_off;
+  const double* ys = y + d.begin;
+  double acc = 0.0;
+  for (int k = 0; k < d.size; ++k) acc = fma(lp[i + (int64_t)k * d.rows], ys[k], acc);
+  y[pos_of_row[rowid[d.rowid_off + i]]] -= acc;
+}
+
+// Backward, U12 x[Struct(s)] in partial sums over column chunks (summed in a
+// fixed order by the diagonal kernel, so a solve is deterministic).
+__global__ void __launch_bounds__(kSolveThreads) bwd_u12_kernel(const FrontDesc* fronts, const SolveItem* items,
+                                                                const double* U, const int32_t* struct_cols,
+                                                                const int64_t* part_off, const double* x,
+                                                                double* partial) {
+  const SolveItem it = items[blockIdx.x];
+  const FrontDesc d = fronts[it.front];
+  const int kk = it.chunk * kRowChunk + threadIdx.x;
+  if (kk >= d.size) return;
   const double* up = U + d.u_off;
-  double* xs = x + d.begin;
   const int32_t* st = struct_cols + d.struct_begin;
-  for (int kk = threadIdx.x; kk < size; kk += kSolveThreads) {
+  const int t0 = it.tchunk * kColChunk, t1 = min(d.ncb, t0 + kColChunk);
+  double acc = 0.0;
+  for (int t = t0; t < t1; ++t) acc = fma(up[kk + (int64_t)t * d.size], x[st[t]], acc);
+  partial[part_off[it.front] + (int64_t)it.tchunk * d.size + kk] = acc;
+}
+
+// Backward, diagonal block (one CTA per front): subtract the U12 partial sums,
+// then the upper solve in 32-column blocks from the last, x_j times the
+// reciprocal of its diagonal as in the reference's upper sweep.
+__global__ void __launch_bounds__(kSolveThreads) bwd_diag_kernel(const FrontDesc* fronts, const int32_t* level,
+                                                                 const double* L, const int64_t* part_off,
+                                                                 const double* partial, double* x) {
+  const int s = level[blockIdx.x];
+  const FrontDesc d = fronts[s];
+  const int rows = d.rows, m = d.size;
+  const double* lp = L + d.l_off;
+  double* xs = x + d.begin;
+  const int ntc = (d.ncb + kColChunk - 1) / kColChunk;
+  for (int kk = threadIdx.x; kk < m; kk += kSolveThreads) {
     double acc = 0.0;
-    for (int t = 0; t < d.ncb; ++t) acc = fma(up[kk + (int64_t)t * size], x[st[t]], acc);
+    for (int tc = 0; tc < ntc; ++tc) acc += partial[part_off[s] + (int64_t)tc * m + kk];
     xs[kk] -= acc;
   }
-  for (int j = size - 1; j >= 0; --j) {
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int jb = m; jb > 0; jb -= 32) {
+    const int j0 = max(0, jb - 32), w = jb - j0;
+    if (warp == 0) {
+      double v = lane < w ? xs[j0 + lane] : 0.0;
+      for (int j = w - 1; j >= 0; --j) {
+        if (lane == j) v = v * (1.0 / lp[(j0 + j) + (int64_t)(j0 + j) * rows]);
+        const double xj = __shfl_sync(0xffffffffu, v, j);
+        if (lane < j) v -= lp[(j0 + lane) + (int64_t)(j0 + j) * rows] * xj;
+      }
+      if (lane < w) xs[j0 + lane] = v;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) xs[j] = xs[j] * (1.0 / lp[j + (int64_t)j * rows]);
+    for (int i = threadIdx.x; i < j0; i += kSolveThreads) {
+      double acc = 0.0;
+      for (int l = 0; l < w; ++l) acc = fma(lp[i + (int64_t)(j0 + l) * rows], xs[j0 + l], acc);
+      xs[i] -= acc;
+    }
     __syncthreads();
-    const double xj = xs[j];
-    for (int i = threadIdx.x; i < j; i += kSolveThreads) xs[i] -= lp[i + (int64_t)j * rows] * xj;
   }
 }
 
@@ -386,6 +442,35 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
   ALG_TRY(dmalloc((void**)&d_flag, sizeof(int) * 4));
   ALG_TRY(dmalloc((void**)&d_y, sizeof(double) * n));
   ALG_TRY(dmalloc((void**)&d_rhs, sizeof(double) * n));
+  {
+    // solve work items per level and the U12 partial-sum offsets
+    std::vector<SolveItem> fwd, bwd;
+    std::vector<int64_t> poff(std::max<idx>(F.ns, 1), 0);
+    int64_t ptot = 0;
+    for (idx s = 0; s < F.ns; ++s) {
+      const FrontDesc& d = F.fronts[s];
+      poff[s] = ptot;
+      ptot += (int64_t)((d.ncb + kColChunk - 1) / kColChunk) * d.size;
+    }
+    const int nl = (int)F.solve_level_ptr.size() - 1;
+    fwd_item_ptr.assign(std::max(nl, 0) + 1, 0);
+    bwd_item_ptr.assign(std::max(nl, 0) + 1, 0);
+    for (int h = 0; h < nl; ++h) {
+      for (int t = F.solve_level_ptr[h]; t < F.solve_level_ptr[h + 1]; ++t) {
+        const int s = F.solve_level_fronts[t];
+        const FrontDesc& d = F.fronts[s];
+        for (int c = 0; c * kRowChunk < d.rows - d.size; ++c) fwd.push_back(SolveItem{s, c, 0, 0});
+        for (int c = 0; c * kRowChunk < d.size; ++c)
+          for (int tc = 0; tc * kColChunk < d.ncb; ++tc) bwd.push_back(SolveItem{s, c, tc, 0});
+      }
+      fwd_item_ptr[h + 1] = (int)fwd.size();
+      bwd_item_ptr[h + 1] = (int)bwd.size();
+    }
+    ALG_TRY(upload(fwd, &d_fwd_items));
+    ALG_TRY(upload(bwd, &d_bwd_items));
+    ALG_TRY(upload(poff, &d_part_off));
+    ALG_TRY(dmalloc((void**)&d_partial, sizeof(double) * std::max<int64_t>(ptot, 1)));
+  }
   for (int b = 0; b < 2; ++b) {
     ALG_TRY(dmalloc((void**)&fac[b].L, sizeof(double) * F.l_total));
     ALG_TRY(dmalloc((void**)&fac[b].U, sizeof(double) * F.u_total));
@@ -403,7 +488,8 @@ void DeviceLu::release() {
                   (void*)d_cb_colmap, (void*)d_anew_q, (void*)d_anew_slot, (void*)d_anew_col, (void*)d_new_rows,
                   (void*)d_small_levels, (void*)d_solve_levels, (void*)d_col_perm, (void*)d_values,
                   (void*)d_block, (void*)d_stack, (void*)d_front, (void*)d_ipiv, (void*)d_perm, (void*)d_rowtmp,
-                  (void*)d_flag, (void*)d_y, (void*)d_rhs})
+                  (void*)d_flag, (void*)d_y, (void*)d_rhs, (void*)d_fwd_items, (void*)d_bwd_items,
+                  (void*)d_part_off, (void*)d_partial})
     if (q) cudaFree(q);
   for (auto& f : fac)
     for (void* q : {(void*)f.L, (void*)f.U, (void*)f.rowid, (void*)f.pos_of_row, (void*)f.row_perm,
@@ -542,21 +628,32 @@ int DeviceLu::solve(int b) {
   for (int h = 0; h < nl; ++h) {
     const int cnt = F.solve_level_ptr[h + 1] - F.solve_level_ptr[h];
     if (cnt == 0) continue;
-    forward_level_kernel<<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_levels + F.solve_level_ptr[h], f.L,
-                                                         f.rowid, f.pos_of_row, d_y);
+    fwd_diag_kernel<<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_levels + F.solve_level_ptr[h], f.L, d_y);
     count_launches();
+    const int ni = fwd_item_ptr[h + 1] - fwd_item_ptr[h];
+    if (ni > 0) {
+      fwd_l21_kernel<<<ni, kSolveThreads, 0, st>>>(d_fronts, d_fwd_items + fwd_item_ptr[h], f.L, f.rowid,
+                                                   f.pos_of_row, d_y);
+      count_launches();
+    }
   }
   for (int h = nl - 1; h >= 0; --h) {
     const int cnt = F.solve_level_ptr[h + 1] - F.solve_level_ptr[h];
     if (cnt == 0) continue;
-    backward_level_kernel<<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_levels + F.solve_level_ptr[h], f.L,
-                                                          f.U, d_struct_cols, d_y);
+    const int ni = bwd_item_ptr[h + 1] - bwd_item_ptr[h];
+    if (ni > 0) {
+      bwd_u12_kernel<<<ni, kSolveThreads, 0, st>>>(d_fronts, d_bwd_items + bwd_item_ptr[h], f.U, d_struct_cols,
+                                                   d_part_off, d_y, d_partial);
+      count_launches();
+    }
+    bwd_diag_kernel<<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_levels + F.solve_level_ptr[h], f.L,
+                                                    d_part_off, d_partial, d_y);
     count_launches();
   }
   scatter_cols_kernel<<<grid_for(ctx, n, 256), 256, 0, st>>>(d_y, d_col_perm, d_rhs, n);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
-  prof_end(ctx, tok, 0.0, 0.0);
+  prof_end(ctx, tok, 4.0 * (double)(F.l_total + F.u_total), 8.0 * (double)(F.l_total + F.u_total));
   return ALG_OK;
 }
 

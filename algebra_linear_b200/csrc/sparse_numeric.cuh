@@ -4,11 +4,18 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 
 #include "sparse.cuh"
 
 namespace alg {
 namespace sp {
+
+// A work item of the multi-CTA solve kernels: a front and a chunk of its
+// rows (and of its U12 columns).
+struct SolveItem {
+  int32_t front, chunk, tchunk, pad;
+};
 
 struct Stats {
   uint64_t nnz_l = 0, nnz_u = 0, flops_estimate = 0;
@@ -30,6 +37,12 @@ struct DeviceLu {
   int32_t* d_rowtmp = nullptr;
   int* d_flag = nullptr;       // [0]: a small front met a zero pivot
   double *d_y = nullptr, *d_rhs = nullptr;
+  // solve: per-level work items of the multi-CTA kernels, U12 partial sums
+  SolveItem* d_fwd_items = nullptr;
+  SolveItem* d_bwd_items = nullptr;
+  std::vector<int> fwd_item_ptr, bwd_item_ptr;
+  int64_t* d_part_off = nullptr;
+  double* d_partial = nullptr;
   struct Factors {
     double* L = nullptr;
     double* U = nullptr;

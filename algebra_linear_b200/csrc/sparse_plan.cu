@@ -1,5 +1,6 @@
 // Host construction of the static front plan of the sparse LU (sparse.cuh).
 #include <algorithm>
+#include <iterator>
 #include <numeric>
 
 #include "sparse.cuh"
@@ -74,8 +75,10 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
 
   // fronts in postorder: slots, Struct(s), column maps
   std::vector<int32_t> mark(n, -1);
+  std::vector<int32_t> loc_of(n, -1);             // position -> local column in the current front
+  std::vector<int32_t> rloc((size_t)nnz, -1);     // local column of each row-form entry in its front
   std::vector<int32_t> sbeg(ns + 1, 0);
-  std::vector<int32_t> cand;
+  std::vector<int32_t> cand, merged, extra;
   F.cb_colmap.clear();
   for (idx s = 0; s < ns; ++s) {
     FrontDesc& d = F.fronts[s];
@@ -86,6 +89,8 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
     d.child_end = kptr[s + 1];
     d.new_begin = newptr[s];
     d.new_end = newptr[s + 1];
+    // Struct(s): sorted union of the children's Struct (each sorted) and of
+    // the entering rows' columns, restricted to columns after s
     int32_t slot = 0;
     cand.clear();
     for (int32_t k = d.child_begin; k < d.child_end; ++k) {
@@ -93,49 +98,54 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
       const FrontDesc& dc = F.fronts[c];
       F.child_slot[k] = slot;
       slot += dc.rows - dc.size;
-      for (int32_t t = sbeg[c]; t < sbeg[c + 1]; ++t) {
-        const int32_t q = F.struct_cols[t];
-        if (q >= e && mark[q] != s) {
-          mark[q] = (int32_t)s;
-          cand.push_back(q);
-        }
+      const int32_t* lo = std::lower_bound(F.struct_cols.data() + sbeg[c], F.struct_cols.data() + sbeg[c + 1], e);
+      const int32_t* hi = F.struct_cols.data() + sbeg[c + 1];
+      if (cand.empty()) {
+        cand.assign(lo, hi);
+      } else {
+        merged.clear();
+        std::set_union(cand.begin(), cand.end(), lo, hi, std::back_inserter(merged));
+        cand.swap(merged);
       }
     }
+    extra.clear();
     for (int32_t k = d.new_begin; k < d.new_end; ++k) {
       const int32_t r = F.new_rows[k];
       for (int64_t t = rp[r]; t < rp[r + 1]; ++t) {
         const int32_t q = rpos[t];
         if (q >= e && mark[q] != s) {
           mark[q] = (int32_t)s;
-          cand.push_back(q);
+          extra.push_back(q);
         }
       }
     }
+    if (!extra.empty()) {
+      std::sort(extra.begin(), extra.end());
+      merged.clear();
+      std::set_union(cand.begin(), cand.end(), extra.begin(), extra.end(), std::back_inserter(merged));
+      cand.swap(merged);
+    }
     d.rows = slot + (d.new_end - d.new_begin);
     if (d.rows < d.size) F.structurally_singular = true;
-    std::sort(cand.begin(), cand.end());
     sbeg[s] = (int32_t)F.struct_cols.size();
     d.struct_begin = sbeg[s];
     F.struct_cols.insert(F.struct_cols.end(), cand.begin(), cand.end());
     sbeg[s + 1] = (int32_t)F.struct_cols.size();
     d.ncb = (int32_t)cand.size();
     // the children's contribution columns in this front's local numbering
+    for (int32_t j = b; j < e; ++j) loc_of[j] = j - b;
+    for (int32_t t = 0; t < d.ncb; ++t) loc_of[cand[t]] = d.size + t;
+    F.cb_colmap.resize(F.struct_cols.size());
     for (int32_t k = d.child_begin; k < d.child_end; ++k) {
       const int32_t c = F.child_idx[k];
-      for (int32_t t = sbeg[c]; t < sbeg[c + 1]; ++t) {
-        const int32_t q = F.struct_cols[t];
-        int32_t loc;
-        if (q < e) {
-          loc = q - b;
-        } else {
-          loc = d.size + (int32_t)(std::lower_bound(cand.begin(), cand.end(), q) - cand.begin());
-        }
-        F.cb_colmap.resize(std::max<size_t>(F.cb_colmap.size(), (size_t)t + 1));
-        F.cb_colmap[t] = loc;
-      }
+      for (int32_t t = sbeg[c]; t < sbeg[c + 1]; ++t) F.cb_colmap[t] = loc_of[F.struct_cols[t]];
+    }
+    // local columns of the A entries of the rows entering here
+    for (int32_t k = d.new_begin; k < d.new_end; ++k) {
+      const int32_t r = F.new_rows[k];
+      for (int64_t t = rp[r]; t < rp[r + 1]; ++t) rloc[t] = loc_of[rpos[t]];
     }
   }
-  F.cb_colmap.resize(F.struct_cols.size());
 
   // A values of the entering rows: slot and local column in their front
   {
@@ -152,16 +162,12 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
       d.anew_end = cnt[s + 1];
       int32_t w = cnt[s];
       const int32_t slot0 = d.rows - (d.new_end - d.new_begin);
-      const int32_t* st = F.struct_cols.data() + d.struct_begin;
       for (int32_t k = d.new_begin; k < d.new_end; ++k) {
         const int32_t r = F.new_rows[k];
         for (int64_t t = rp[r]; t < rp[r + 1]; ++t) {
-          const int32_t q = rpos[t];
           F.anew_q[w] = rq[t];
           F.anew_slot[w] = slot0 + (k - d.new_begin);
-          F.anew_col[w] = q < d.begin + d.size
-                              ? q - d.begin
-                              : d.size + (int32_t)(std::lower_bound(st, st + d.ncb, q) - st);
+          F.anew_col[w] = rloc[t];
           ++w;
         }
       }
@@ -260,6 +266,58 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
       F.small_level_ptr.pop_back();
   }
   return SP_OK;
+}
+
+
+// Merges chains of only-children into their parents when the merged front's
+// flops stay within (1 + tol) of the two separate fronts': a chain step no
+// longer copies its whole contribution block into the next front. The merged
+// front of a child c and its parent s has size_c + size_s columns,
+// rows_s + size_c rows and the parent's Struct (c's Struct outside s's
+// columns is contained in s's). Pivots do not depend on the partition.
+void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std::vector<idx>* ptr_out) {
+  const idx ns = F.ns;
+  auto flops = [](double m, double k, double c) {
+    return 2.0 * k * k * m - 2.0 / 3.0 * k * k * k + k * k * c + 2.0 * (m - k) * c * k;
+  };
+  std::vector<int32_t> nkid(ns, 0);
+  for (idx s = 0; s < ns; ++s)
+    if (S.super_etree[s] >= 0) nkid[S.super_etree[s]] += 1;
+  std::vector<double> gm(ns), gk(ns), gc(ns);
+  std::vector<char> into_next(ns, 0);
+  for (idx s = 0; s < ns; ++s) {
+    const FrontDesc& d = F.fronts[s];
+    gm[s] = d.rows;
+    gk[s] = d.size;
+    gc[s] = d.ncb;
+    if (s > 0 && nkid[s] == 1 && S.super_etree[s - 1] == s) {
+      const double m2 = d.rows + gk[s - 1], k2 = d.size + gk[s - 1], c2 = d.ncb;
+      const double sep = flops(gm[s - 1], gk[s - 1], gc[s - 1]) + flops(d.rows, d.size, d.ncb);
+      if (flops(m2, k2, c2) <= (1.0 + tol) * sep) {
+        into_next[s - 1] = 1;
+        gm[s] = m2;
+        gk[s] = k2;
+        gc[s] = c2;
+      }
+    }
+  }
+  ptr_out->assign(1, 0);
+  for (idx s = 0; s < ns; ++s)
+    if (!into_next[s]) ptr_out->push_back(S.supernode_ptr[s + 1]);
+}
+
+void repartition(const Supernodal& S, const std::vector<idx>& ptr, Supernodal* out) {
+  *out = S;
+  out->supernode_ptr = ptr;
+  const idx ns = (idx)ptr.size() - 1;
+  std::vector<idx> owner(S.n);
+  for (idx s = 0; s < ns; ++s)
+    for (idx c = ptr[s]; c < ptr[s + 1]; ++c) owner[c] = s;
+  out->super_etree.assign(ns, -1);
+  for (idx s = 0; s < ns; ++s) {
+    const idx last = ptr[s + 1] - 1;
+    if (S.etree[last] >= 0) out->super_etree[s] = owner[S.etree[last]];
+  }
 }
 
 }  // namespace sp

@@ -10,6 +10,12 @@ Writes tests/golden/larnv_kat.json from the test
 whose values the reference captured from LAPACK 3.12.1's libtmglib (`dlarnv_`)
 for seed [1988, 1989, 1990, 1991], n = 200: x[0..12], x[198..200] and the seed
 after the call, for the Uniform, Symmetric and Normal distributions.
+
+Writes tests/golden/colamd_kat.json from the test `matches_faer_on_fixtures`
+in src/sparse/faer/colamd.rs:886-918 (permutations the reference captured from
+faer's colamd::order): each fixture's CSC pattern, built here from the
+fixture's definition in the same test module (colamd.rs:800-880), and the
+expected perm and perm_inv read from the test's text.
 """
 
 import json
@@ -46,11 +52,74 @@ def extract_larnv(src: str) -> dict:
     }
 
 
+def _from_cols(cols):
+    col_ptr, row_idx = [0], []
+    for c in cols:
+        c = sorted(set(c))
+        row_idx.extend(c)
+        col_ptr.append(len(row_idx))
+    return col_ptr, row_idx
+
+
+def colamd_fixtures():
+    """The fixture patterns of colamd.rs's tests (tridiag5, arrow8, grid4x5,
+    ring12, lcg30), in the test's order."""
+    out = {}
+    out["tridiag5"] = _from_cols([[0, 1], [0, 1, 2], [1, 2, 3], [2, 3, 4], [3, 4]])
+    out["arrow8"] = _from_cols([list(range(8)) if j == 0 else [0, j] for j in range(8)])
+    rows, cn = 4, 5
+    cols = []
+    for i in range(rows * cn):
+        r, c = divmod(i, cn)
+        v = [i]
+        if r > 0:
+            v.append((r - 1) * cn + c)
+        if r + 1 < rows:
+            v.append((r + 1) * cn + c)
+        if c > 0:
+            v.append(r * cn + c - 1)
+        if c + 1 < cn:
+            v.append(r * cn + c + 1)
+        cols.append(v)
+    out["grid4x5"] = _from_cols(cols)
+    out["ring12"] = _from_cols([[j, (j + 1) % 12, (j + 3) % 12, (j + 7) % 12] for j in range(12)])
+    state, m64, cols = 0x2545F4914F6CDD1D, (1 << 64) - 1, []
+    for j in range(30):
+        v = [j]
+        for _ in range(4):
+            state = (state * 6364136223846793005 + 1442695040888963407) & m64
+            v.append((state >> 33) % 30)
+        cols.append(v)
+    out["lcg30"] = _from_cols(cols)
+    return out
+
+
+def extract_colamd(src: str) -> dict:
+    start = src.index("fn matches_faer_on_fixtures")
+    body = src[start:src.index("fn returns_valid_permutations", start)]
+    vecs = [[int(x) for x in m.group(1).replace("\n", " ").split(",") if x.strip()]
+            for m in re.finditer(r"vec!\[([0-9,\s]+)\]", body)]
+    fx = colamd_fixtures()
+    names = list(fx)
+    assert len(vecs) == 2 * len(names), len(vecs)
+    cases = []
+    for i, name in enumerate(names):
+        cp, ri = fx[name]
+        perm, inv = vecs[2 * i], vecs[2 * i + 1]
+        assert len(perm) == len(cp) - 1 == len(inv), name
+        cases.append({"name": name, "col_ptr": cp, "row_idx": ri, "perm": perm, "perm_inv": inv})
+    return {"source": "src/sparse/faer/colamd.rs:886-918 (matches_faer_on_fixtures)", "cases": cases}
+
+
 def main() -> None:
     root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     fam = (root / "src/lapack/families.rs").read_text()
     out = HERE / "larnv_kat.json"
     out.write_text(json.dumps(extract_larnv(fam), indent=1) + "\n")
+    print("wrote", out)
+    col = (root / "src/sparse/faer/colamd.rs").read_text()
+    out = HERE / "colamd_kat.json"
+    out.write_text(json.dumps(extract_colamd(col)) + "\n")
     print("wrote", out)
 
 

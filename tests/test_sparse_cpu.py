@@ -1,0 +1,208 @@
+"""Sparse LU: the host-side analysis through the C ABI and the oracle against
+the reference's own tests. CPU only — analyze needs no GPU, and the
+factorize/solve checks here are the ones the reference makes before any
+numeric work.
+
+Pins: COLAMD permutations (colamd.rs:886-918, tests/golden/colamd_kat.json),
+column counts against dense symbolic elimination of (AQ)^T (AQ)
+(supernodal.rs:463-531), the supernode partition's invariants
+(supernodal.rs:533-560), shape and structure errors (sparse_lu.rs:318-351,
+csc.rs), the method choice and flop ratio (sparse_lu.rs:385-503), and the
+oracle's solutions of the reference's 2 x 2 examples (sparse_lu.rs:251-309)."""
+
+import json
+import pathlib
+
+import numpy as np
+import pytest
+
+from algebra_linear_b200.sparse import LuMethod, SparseError, SparseLu
+
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+
+COL_PTR = [0, 2, 4]
+ROW_IDX = [0, 1, 0, 1]
+VALUES = [4.0, 1.0, 1.0, 3.0]
+
+
+def colamd_cases():
+    return json.loads((GOLDEN / "colamd_kat.json").read_text())["cases"]
+
+
+@pytest.mark.parametrize("case", colamd_cases(), ids=lambda c: c["name"])
+def test_colamd_matches_the_reference_fixtures(case):
+    lu = SparseLu.analyze(case["col_ptr"], case["row_idx"], LuMethod.supernodal())
+    sym = lu.symbolic()
+    assert sym["col_perm"].tolist() == case["perm"]
+    assert sym["col_perm_inv"].tolist() == case["perm_inv"]
+
+
+def _dense_pattern(cp, ri, n):
+    a = np.zeros((n, n), bool)
+    for j in range(n):
+        a[ri[cp[j]:cp[j + 1]], j] = True
+    return a
+
+
+def brute_force_counts(cp, ri, perm):
+    """Symbolic Cholesky of (A Q)^T (A Q) by dense elimination."""
+    n = len(cp) - 1
+    a = _dense_pattern(cp, ri, n)[:, perm]
+    b = (a.T.astype(int) @ a.astype(int)) > 0
+    np.fill_diagonal(b, True)
+    counts = np.zeros(n, int)
+    for j in range(n):
+        col = [i for i in range(j, n) if b[i, j]]
+        counts[j] = len(col)
+        for i in col:
+            if i > j:
+                for k in col:
+                    if k >= i:
+                        b[k, i] = True
+    return counts
+
+
+@pytest.mark.parametrize("case", colamd_cases(), ids=lambda c: c["name"])
+def test_column_counts_match_dense_symbolic_elimination(case):
+    lu = SparseLu.analyze(case["col_ptr"], case["row_idx"], LuMethod.supernodal())
+    sym = lu.symbolic()
+    want = brute_force_counts(case["col_ptr"], case["row_idx"], sym["col_perm"])
+    assert sym["col_counts"].tolist() == want.tolist()
+    ptr = sym["supernode_ptr"]
+    n = len(case["col_ptr"]) - 1
+    assert ptr[0] == 0 and ptr[-1] == n and np.all(np.diff(ptr) > 0)
+
+
+def test_diagonal_matrix_has_singleton_supernodes():
+    n = 6
+    lu = SparseLu.analyze(list(range(n + 1)), list(range(n)), LuMethod.supernodal())
+    sym = lu.symbolic()
+    assert sym["supernode_ptr"].tolist() == list(range(n + 1))
+    assert sym["col_counts"].tolist() == [1] * n
+
+
+def _raises(code_name, fn, *args):
+    with pytest.raises(SparseError) as e:
+        fn(*args)
+    assert e.value.kind == code_name, e.value.kind
+    return e.value
+
+
+def test_rejects_non_square_and_malformed_input():
+    # sparse_lu.rs:340-351 and the CSC validation of csc.rs:39-76
+    _raises("BadShape", SparseLu.analyze, [0, 2, 3], [0, 1, 2])
+    _raises("BadShape", SparseLu.analyze, [], [])
+    _raises("UnsortedRows", SparseLu.analyze, [0, 2, 2], [1, 0])
+    _raises("DuplicateEntry", SparseLu.analyze, [0, 2, 2], [1, 1])
+    _raises("InvalidStructure", SparseLu.analyze, [1, 2, 2], [1])
+    _raises("InvalidStructure", SparseLu.analyze, [0, 2, 1, 2], [0, 1])
+    _raises("BadShape", SparseLu.analyze, [0, 2, 3], [0, 1])
+
+
+def test_factorize_checks_before_numeric_work():
+    lu = SparseLu.analyze(COL_PTR, ROW_IDX, LuMethod.auto())
+    b = np.array([1.0, 2.0])
+    assert _raises("NotFactorized", lu.solve, b)
+    # a changed pattern (sparse_lu.rs:301-314)
+    _raises("StructureMismatch", lu.factorize, [0, 2, 3], [0, 1, 1], [1.0, 1.0, 1.0])
+    for bad in (np.nan, np.inf, -np.inf):  # sparse_lu.rs:327-334
+        _raises("NotFinite", lu.factorize, COL_PTR, ROW_IDX, [4.0, 1.0, bad, 3.0])
+    _raises("BadShape", lu.factorize, COL_PTR, ROW_IDX, [4.0, 1.0, 1.0])
+    assert lu.stats() is None
+
+
+def _tridiag(n, dense=False):
+    cp, ri, v = [0], [], []
+    for j in range(n):
+        rng = range(n) if dense else range(max(j - 1, 0), min(j + 1, n - 1) + 1)
+        for i in rng:
+            ri.append(i)
+            v.append((2.0 * n if dense else 5.0) if i == j else 1.0)
+        cp.append(len(ri))
+    return cp, ri, v
+
+
+def test_effective_method_and_flop_ratio():
+    # sparse_lu.rs:430-484
+    cp, ri, _ = _tridiag(9)
+    lu = SparseLu.analyze(cp, ri, LuMethod.simplicial())
+    assert lu.effective_method() == "Simplicial" and lu.flop_ratio() is None
+    lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+    assert lu.effective_method() == "Supernodal" and lu.flop_ratio() > 0
+    lu = SparseLu.analyze(cp, ri, LuMethod.auto())
+    r = lu.flop_ratio()
+    assert lu.effective_method() == "Simplicial" and 0 < r <= 40
+    cp, ri, _ = _tridiag(12, dense=True)
+    lu = SparseLu.analyze(cp, ri, LuMethod.auto(1.0))
+    assert lu.effective_method() == "Supernodal" and lu.flop_ratio() > 1.0
+
+
+def test_empty_matrix_has_zero_fill_and_flops():
+    # sparse_lu.rs:486-503
+    lu = SparseLu.analyze([0], [], LuMethod.auto())
+    assert lu.effective_method() == "Simplicial"
+    assert lu.flop_ratio() == 0.0
+    lu.factorize([0], [], [])
+    s = lu.stats()
+    assert s["n"] == 0 and s["nnz_a"] == 0 and s["fill_ratio"] == 0.0 and s["flops_estimate"] == 0
+    assert s["nnz_l"] + s["nnz_u"] == 0 and s["method"] == "Simplicial" and s["flop_ratio"] == 0.0
+    lu.solve(np.zeros(0))
+
+
+def _oracle_factors(oracle_sparse, cp, ri, v, method=LuMethod.supernodal()):
+    lu = SparseLu.analyze(cp, ri, method)
+    sym = lu.symbolic()
+    return oracle_sparse.Factors(len(cp) - 1, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], sym["supernode_ptr"])
+
+
+@pytest.fixture(scope="module")
+def oracle_sparse(oracle):
+    from oracle import sparse
+
+    return sparse
+
+
+def test_oracle_solves_the_reference_examples(oracle_sparse):
+    # sparse_lu.rs:251-309: A = [4 1; 1 3]
+    f = _oracle_factors(oracle_sparse, COL_PTR, ROW_IDX, VALUES)
+    assert f.status == 0
+    np.testing.assert_allclose(f.solve([1.0, 2.0]), [1 / 11, 7 / 11], rtol=0, atol=1e-14 * 2)
+    np.testing.assert_allclose(f.solve([1.0, 1.0]), [2 / 11, 3 / 11], rtol=0, atol=1e-14 * 2)
+    f = _oracle_factors(oracle_sparse, COL_PTR, ROW_IDX, [5.0, 2.0, 2.0, 2.0])
+    np.testing.assert_allclose(f.solve([1.0, 1.0]), [0.0, 0.5], rtol=0, atol=1e-14 * 2)
+    assert f.nnz_l >= 3 and f.nnz_u >= 2
+
+
+def test_oracle_reconstructs_the_permuted_matrix(oracle_sparse):
+    # supernodal_lu.rs:707-741: P A Q = L U on the 4 x 5 grid
+    case = [c for c in colamd_cases() if c["name"] == "grid4x5"][0]
+    cp, ri = case["col_ptr"], case["row_idx"]
+    n = len(cp) - 1
+    v = np.array([5.0 if ri[k] == j else 1.0 for j in range(n) for k in range(cp[j], cp[j + 1])])
+    f = _oracle_factors(oracle_sparse, cp, ri, v)
+    assert f.status == 0
+    A = np.zeros((n, n))
+    for j in range(n):
+        A[ri[cp[j]:cp[j + 1]], j] = v[cp[j]:cp[j + 1]]
+    L = np.zeros((n, n))
+    U = np.zeros((n, n))
+    for j in range(n):
+        for k in range(int(f.l_col_ptr[j]), int(f.l_col_ptr[j + 1])):
+            L[int(f.l_row_idx[k]), j] = f.l_val[k]
+        for k in range(int(f.u_col_ptr[j]), int(f.u_col_ptr[j + 1])):
+            U[int(f.u_row_idx[k]), j] = f.u_val[k]
+    sym = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
+    PAQ = A[f.row_perm.astype(int)][:, sym["col_perm"]]
+    np.testing.assert_allclose(L @ U, PAQ, atol=1e-12)
+    assert np.all(np.diag(L) == 1.0)
+
+
+def test_grid_values_follow_the_stencil(oracle_sparse):
+    cp, ri, kind = oracle_sparse.grid_pattern(4, 3, 2)
+    v, _ = oracle_sparse.convection_diffusion_values(kind, [1, 2, 3, 5])
+    n = len(cp) - 1
+    diag = np.array([v[k] for j in range(n) for k in range(int(cp[j]), int(cp[j + 1])) if ri[k] == j])
+    assert np.all((diag >= 6.0) & (diag <= 6.1))
+    assert np.all(v[kind == 3] == -1.0)
+    assert np.all((v[kind == 2] >= -1.0) & (v[kind == 2] <= -0.7))
+    assert np.all((v[kind == 1] >= -1.3) & (v[kind == 1] <= -1.0))
