@@ -63,6 +63,11 @@ def parse_args():
     ap.add_argument("--cpu-n", type=int, default=1024, help="order of the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["dense", "sparse"], default="dense",
+                    help="dense: dgesv (the headline); sparse: supernodal LU refactorize+solve rounds")
+    ap.add_argument("--grid", type=int, default=48, help="sparse: grid points per side")
+    ap.add_argument("--grid-nz", type=int, default=0, help="sparse: points along z (0: = grid; 1: 2-D)")
+    ap.add_argument("--cpu-grid", type=int, default=16, help="sparse: grid side of the CPU-baseline sample")
     return ap.parse_args()
 
 
@@ -160,7 +165,7 @@ def form_registry():
     try:
         from algebra_linear_b200 import mixed  # noqa: F401
 
-        for prec in ("tf32", "bf16"):
+        for prec in ("fp32", "tf32", "bf16"):
             forms[f"mixed_{prec}"] = (False, (lambda p: lambda ctx, A, b, n, nrhs: mixed.dgesv_mixed_dev(
                 ctx, A, b, n, nrhs, precision=p))(prec))
     except ImportError:
@@ -365,6 +370,182 @@ def cpu_baseline(n_cpu: int, reps: int = 3):
                       f"({t:.2f} s each); the reference path is single-threaded"}
 
 
+
+# --------------------------------------------------------------------------- sparse
+def grid_csc(nx: int, ny: int, nz: int):
+    """CSC pattern of the 7-point (nz > 1) or 5-point (nz == 1) stencil, node
+    x + nx (y + ny z), rows sorted per column; kind per entry: 0 diagonal,
+    1 the row's west neighbour, 2 its east neighbour, 3 y/z neighbours."""
+    import numpy as np
+
+    n = nx * ny * nz
+    idx = np.arange(n, dtype=np.int64)
+    x, y = idx % nx, (idx // nx) % ny
+    z = idx // (nx * ny)
+    offs = [(-1, x > 0, 2), (1, x < nx - 1, 1), (-nx, y > 0, 3), (nx, y < ny - 1, 3)]
+    if nz > 1:
+        offs += [(-nx * ny, z > 0, 3), (nx * ny, z < nz - 1, 3)]
+    rows, cols, kinds = [idx], [idx], [np.zeros(n, np.int8)]
+    for off, ok, k in offs:
+        c = idx[ok]
+        rows.append(c + off)
+        cols.append(c)
+        kinds.append(np.full(c.size, k, np.int8))
+    r, c, k = np.concatenate(rows), np.concatenate(cols), np.concatenate(kinds)
+    order = np.lexsort((r, c))
+    r, c, k = r[order], c[order], k[order]
+    col_ptr = np.zeros(n + 1, np.uint64)
+    np.add.at(col_ptr, c + 1, 1)
+    return np.cumsum(col_ptr).astype(np.uint64), r.astype(np.uint64), k
+
+
+def sparse_cpu_baseline(side: int):
+    """The oracle (C++ restatement of the reference's supernodal LU,
+    supernodal_lu.rs) on one host core: one factorize + solve of the
+    side^3 grid, GFLOP/s on the reference's own flop estimate."""
+    import numpy as np
+
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+    from oracle import sparse as osp
+
+    cp, ri, kind = grid_csc(side, side, side)
+    v, _ = osp.convection_diffusion_values(kind, SEEDY)
+    sym = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
+    t0 = time.perf_counter()
+    f = osp.Factors(len(cp) - 1, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], sym["supernode_ptr"])
+    f.solve(np.ones(len(cp) - 1))
+    t = time.perf_counter() - t0
+    fl = 2.0 * f.flops_estimate() + 2.0 * (f.nnz_l + f.nnz_u)
+    return {"value": fl / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
+            "sample": f"one factorize+solve of the {side}^3 grid ({t:.1f} s); the reference path is single-threaded"}
+
+
+def run_sparse(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from algebra_linear_b200 import _lib, device
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+
+    torch.cuda.set_device(local)
+    lib = _lib.load()
+    nx = args.grid
+    nz = args.grid_nz if args.grid_nz > 0 else nx
+    cp, ri, kind = grid_csc(nx, nx, nz)
+    n, nnz = len(cp) - 1, len(ri)
+    seed = [SEEDY[0], SEEDY[1], SEEDY[2], SEEDY[3] + 2 * rank]
+    gemm_peaks = gemm_peaks_tflops()
+    ctx = device.Context()
+    u, s = ctx.larnv(1, seed, nnz)
+    kt = torch.from_numpy(kind.astype(np.int64)).cuda()
+    v0 = torch.where(kt == 0, 6.0 + 0.1 * u,
+                     torch.where(kt == 2, -1.0 + 0.3 * u, torch.where(kt == 1, -1.0 - 0.3 * u, -torch.ones_like(u))))
+    rounds = []
+    for _ in range(args.warmup + args.steps):  # every round's values: v0 (1 + 0.01 U(-1,1))
+        w, s = ctx.larnv(2, s, nnz)
+        rounds.append((v0 * (1.0 + 0.01 * w)).contiguous())
+    t0 = time.perf_counter()
+    lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+    analyze_s = time.perf_counter() - t0
+    lu.bind(ctx)
+    b0 = torch.ones(n, dtype=torch.float64, device="cuda")
+    b = b0.clone()
+    for k in range(args.warmup):
+        lu.factorize_dev(rounds[k])
+        b.copy_(b0)
+        lu.solve_dev(b)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    launches0 = lib.alg_kernel_launch_count()
+    sampler = ClockSampler(local)
+    sampler.__enter__()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for k in range(args.warmup, args.warmup + args.steps):
+        lu.factorize_dev(rounds[k])
+        b.copy_(b0)
+        lu.solve_dev(b)
+    e1.record()
+    torch.cuda.synchronize()
+    sampler.__exit__()
+    ms = e0.elapsed_time(e1)
+    launches = lib.alg_kernel_launch_count() - launches0
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    st = lu.stats()
+    plan = lu.plan()
+    # normwise backward error of the last round (host check)
+    import scipy.sparse as sps
+
+    vh = rounds[-1].cpu().numpy()
+    A = sps.csc_matrix((vh, ri.astype(np.int64), cp.astype(np.int64)), shape=(n, n))
+    x = b.cpu().numpy()
+    res = 1.0 - A @ x
+    eta = float(np.abs(res).max() / (abs(A).sum(axis=1).max() * np.abs(x).max() + 1.0))
+    fl_round = 2.0 * st["flops_estimate"] + 2.0 * (st["nnz_l"] + st["nnz_u"])
+    per_round = ms / args.steps
+    value = fl_round * world / per_round / 1e6
+    # roofline: the top kernel class of the timed rounds
+    cls, rec = max(((c, r) for c, r in prof.items() if c != "sparse"), key=lambda kv: kv[1]["ms"])
+    roof = None
+    if cls == "gemm":
+        ach = rec["flops"] / rec["ms"] / 1e9
+        roof = {"kernel": "gemm", "bound": "tensor", "achieved": ach, "peak": gemm_peaks["f64"], "unit": "TFLOP/s",
+                "frac": ach / gemm_peaks["f64"], "traffic": None,
+                "peak_source": "cuBLAS DGEMM measured in this run", "launches": rec["launches"],
+                "share_of_step": rec["ms"] / (prof["sparse"]["ms"] + prof.get("solve", {"ms": 0})["ms"])}
+    else:
+        ach = rec["flops"] / rec["ms"] / 1e9
+        roof = {"kernel": cls, "bound": "latency", "achieved": ach, "peak": gemm_peaks["f64"], "unit": "TFLOP/s",
+                "frac": ach / gemm_peaks["f64"], "traffic": None, "launches": rec["launches"]}
+    line = {
+        "metric": "sparse LU refactorize+solve GFLOP/s (reference flop estimate); rounds/s",
+        "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_round, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": f"synthetic: convection-diffusion stencil, U(0,1) from the DLARNV stream seed {seed}",
+        "config": {"workload": f"{nx}x{nx}x{nz} grid, {'7' if nz > 1 else '5'}-point convection-diffusion, "
+                               f"n={n}, nnz={nnz}; analyze once, then per round: values x (1 + 0.01 U(-1,1)), "
+                               "factorize, solve", "n": n, "nnz": nnz, "parallelism": f"replicas x{world}",
+                   "l2": "factors (GBs) larger than L2; no flush"},
+        "rounds_per_s": 1e3 / per_round, "analyze_s": analyze_s, "backward_error": eta,
+        "stats": {k: st[k] for k in ("nnz_l", "nnz_u", "fill_ratio", "flops_estimate")},
+        "plan": {k: plan[k] for k in ("n_fronts", "n_small_fronts", "max_front_rows", "max_front_cols",
+                                       "plan_flops", "factor_bytes", "work_bytes")},
+        "kernel_ms_per_step": {c: r["ms"] / args.steps for c, r in prof.items()},
+        "gpu_launches": int(launches), "clocks": sampler.summary(), "roofline": roof,
+        "cublas_gemm_peaks_tflops": gemm_peaks,
+    }
+    if not args.no_e2e and rank == 0:
+        lu_h = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+        hv = [r.cpu().numpy() for r in rounds[-3:]]
+        lu_h.factorize(cp, ri, hv[0])
+        ts = []
+        for vv in hv:
+            bh = np.ones(n)
+            t0 = time.perf_counter()
+            lu_h.factorize(cp, ri, vv)
+            lu_h.solve(bh)
+            ts.append(time.perf_counter() - t0)
+        t = statistics.median(ts)
+        line["e2e"] = {"value": fl_round / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * nnz + 8 * n,
+                       "d2h_bytes_per_step": 8 * n, "ms_per_step": 1e3 * t, "api": "alg_splu_factorize + alg_splu_solve"}
+        lu_h.close()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = sparse_cpu_baseline(args.cpu_grid)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    lu.close()
+    ctx.close()
+
 # --------------------------------------------------------------------------- arms
 def run_reference(args, world, rank, pg):
     if rank != 0:
@@ -466,6 +647,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, pg)
+        elif args.workload == "sparse":
+            run_sparse(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:
