@@ -75,6 +75,7 @@ SIGNATURES = [
     ("alg_batch_eta", _I, [_P, _P]),
     ("alg_batch_destroy", None, [_P]),
     ("alg_gemm_tc_sub_dev", _I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
+    ("alg_gemm_dmma_sub_dev", _I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
     ("alg_dgesv_mixed_noalloc", _I, [_P, _P, _P, _I, _P, _P, _P]),
     ("alg_splu_analyze", _I, [_P, _SZ, _P, _SZ, _I, C.c_double, _P]),
     ("alg_splu_factorize", _I, [_P, _P, _SZ, _P, _SZ, _P, _SZ]),
@@ -89,6 +90,15 @@ SIGNATURES = [
     ("alg_splu_set_ctx", _I, [_P, _P]),
     ("alg_splu_factorize_dev", _I, [_P, _P]),
     ("alg_splu_solve_dev", _I, [_P, _P]),
+    ("alg_splu_clone", _I, [_P, _P]),
+    ("alg_splu_factorize_values", _I, [_P, _P]),
+    ("alg_server_create", _I, [_I, _SZ, _SZ, _P]),
+    ("alg_server_submit", _I, [_P, _P]),
+    ("alg_server_wait", _I, [_P, _P]),
+    ("alg_server_drain", _I, [_P]),
+    ("alg_server_completed", C.c_ulonglong, [_P]),
+    ("alg_server_now_ns", C.c_int64, []),
+    ("alg_server_destroy", None, [_P]),
     ("alg_ctx_set_profiling", _I, [_P, _I]),
     ("alg_ctx_profile_reset", _I, [_P]),
     ("alg_ctx_profile_get", _I, [_P, _I, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double),

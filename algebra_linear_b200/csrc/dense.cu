@@ -172,10 +172,23 @@ int launch_trsm(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
 
 }  // namespace
 
+// ALG_NO_DMMA=1 keeps the fused FP64 updates on the CUDA cores (for comparison).
+bool dmma_disabled() {
+  static const bool off = [] {
+    const char* e = std::getenv("ALG_NO_DMMA");
+    return e != nullptr && e[0] == '1';
+  }();
+  return off;
+}
+
 template <typename T, bool EXACT>
 int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T* B, int ldb,
                  T* C, int ldc) {
   if (M <= 0 || N <= 0 || K <= 0) return ALG_OK;
+  if constexpr (std::is_same<T, double>::value && !EXACT) {
+    // the fused FP64 form runs on the FP64 tensor cores
+    if (!dmma_disabled()) return gemm_dmma_sub_dev(ctx, M, N, K, A, lda, B, ldb, C, ldc);
+  }
   dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + kGemmBN - 1) / kGemmBN);
   const int tok = prof_begin(ctx, ALG_K_GEMM);
   gemm_sub_kernel<T, EXACT><<<grid, kGemmThreads, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);

@@ -42,6 +42,11 @@ int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* 
 template <typename T, bool EXACT>
 int lu_solve_dataflow_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs, int ldb);
 
+// FP64 C -= A B on the FP64 tensor cores (mma.sync m8n8k4), fused arithmetic;
+// column-major, any leading dimensions, stream-ordered.
+int gemm_dmma_sub_dev(alg_ctx* ctx, int M, int N, int K, const double* A, int lda, const double* B, int ldb,
+                      double* C, int ldc);
+
 // C -= A B on the CUDA cores (column-major), stream-ordered.
 template <typename T, bool EXACT>
 int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T* B, int ldb,

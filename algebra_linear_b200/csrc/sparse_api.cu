@@ -310,6 +310,37 @@ int alg_splu_solve_dev(alg_splu* lu, double* d_b) {
   return ALG_OK;
 }
 
+int alg_splu_clone(const alg_splu* src, alg_splu** out) {
+  if (src == nullptr || out == nullptr) return ALG_INVALID_ARGUMENT;
+  auto lu = std::make_unique<alg_splu>();
+  lu->n = src->n;
+  lu->nnz = src->nnz;
+  lu->fingerprint = src->fingerprint;
+  lu->effective = src->effective;
+  lu->has_ratio = src->has_ratio;
+  lu->flop_ratio = src->flop_ratio;
+  lu->ordering_time = src->ordering_time;
+  lu->sym = src->sym;
+  lu->plan = src->plan;
+  *out = lu.release();
+  return ALG_OK;
+}
+
+int alg_splu_factorize_values(alg_splu* lu, const double* values) {
+  if (lu == nullptr || (lu->nnz > 0 && values == nullptr)) return ALG_INVALID_ARGUMENT;
+  for (size_t q = 0; q < lu->nnz; ++q)
+    if (!std::isfinite(values[q])) return ALG_SP_NOT_FINITE;
+  if (lu->n == 0) {
+    lu->cur = 0;
+    return ALG_OK;
+  }
+  if (lu->plan.structurally_singular) return ALG_SP_SINGULAR;
+  ALG_TRY(ensure_device(lu));
+  ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_values, values, sizeof(double) * lu->nnz, cudaMemcpyHostToDevice,
+                               lu->ctx->stream));
+  return factor_loaded(lu);
+}
+
 void alg_splu_free(alg_splu* lu) {
   if (lu == nullptr) return;
   if (lu->dev_ready) {

@@ -150,7 +150,8 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
     const double inv = 1.0 / pv;
     for (int i = k + 1 + tid; i < rows; i += kSmallThreads) f[i + (int64_t)k * rows] *= inv;
     __syncthreads();
-    const int mr = rows - k - 1, mc = cols - k - 1;
+    // rank-1 update of the front's own columns only
+    const int mr = rows - k - 1, mc = size - k - 1;
     const int64_t upd = (int64_t)mr * mc;
     for (int64_t e = tid; e < upd; e += kSmallThreads) {
       const int i = k + 1 + (int)(e % mr), j = k + 1 + (int)(e / mr);
@@ -158,6 +159,27 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
     }
     __syncthreads();
   }
+  // U12 = L11^-1 A12: forward substitution, a thread per column
+  for (int c = size + tid; c < cols; c += kSmallThreads) {
+    double* col = f + (int64_t)c * rows;
+    for (int k = 0; k < size; ++k) {
+      const double uk = col[k];
+      for (int i = k + 1; i < size; ++i) col[i] = fma(-f[i + (int64_t)k * rows], uk, col[i]);
+    }
+  }
+  __syncthreads();
+  // contribution block: CB -= L21 U12, one dot product per entry
+  {
+    const int mr = rows - size;
+    const int64_t upd = (int64_t)mr * d.ncb;
+    for (int64_t e = tid; e < upd; e += kSmallThreads) {
+      const int i = size + (int)(e % mr), c = size + (int)(e / mr);
+      double acc = 0.0;
+      for (int k = 0; k < size; ++k) acc = fma(f[i + (int64_t)k * rows], f[k + (int64_t)c * rows], acc);
+      f[i + (int64_t)c * rows] -= acc;
+    }
+  }
+  __syncthreads();
   double* lp = a.L + d.l_off;
   for (int64_t e = tid; e < (int64_t)rows * size; e += kSmallThreads) lp[e] = f[e];
   double* up = a.U + d.u_off;

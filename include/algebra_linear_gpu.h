@@ -244,6 +244,12 @@ void alg_batch_destroy(alg_batch* batch);
 int alg_gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda,
                         const float* B, int ldb, float* C, int ldc);
 
+/* FP64 C (M x N) -= A (M x K) * B (K x N) on the FP64 tensor cores (the
+ * update of the fused FP64 forms); column-major, synchronises. Exposed for
+ * tests and benchmarks of the kernel on its own. */
+int alg_gemm_dmma_sub_dev(alg_ctx* ctx, int M, int N, int K, const double* A, int lda, const double* B, int ldb,
+                          double* C, int ldc);
+
 /* ---- sparse LU (sparse::faer::SparseLu, src/sparse/faer/sparse_lu.rs) -----
  * The handle owns the symbolic analysis (host) and the numeric factors (GPU).
  * CSC arrays are borrowed per call and never retained: col_ptr (n + 1),
@@ -318,6 +324,61 @@ int alg_splu_plan_info(const alg_splu* lu, alg_splu_plan* out);
 int alg_splu_set_ctx(alg_splu* lu, alg_ctx* ctx);
 int alg_splu_factorize_dev(alg_splu* lu, const double* d_values);
 int alg_splu_solve_dev(alg_splu* lu, double* d_b);
+
+/* A handle sharing src's symbolic analysis and GPU plan (no new ordering),
+ * with its own numeric state: for several streams factoring the same
+ * pattern concurrently. */
+int alg_splu_clone(const alg_splu* src, alg_splu** out);
+/* factorize for the analyzed pattern itself: only the nnz values (host) are
+ * passed; ALG_SP_NOT_FINITE, ALG_SP_SINGULAR as alg_splu_factorize. */
+int alg_splu_factorize_values(alg_splu* lu, const double* values);
+
+/* ---- serving loop (no counterpart in the reference) -----------------------
+ * A device-resident request loop: requests are queued in arrival order and
+ * taken by worker threads (each with its own CUDA stream and workspace) as
+ * soon as a worker is idle and the request's device bytes fit in the HBM
+ * budget, so arriving requests are admitted while others run and their work
+ * overlaps on the GPU. Dense requests: dgesv of order n (A is not modified;
+ * x receives the solution; precision ALG_REQ_FP64 = FP64 LU with fused
+ * updates, ALG_REQ_MIXED = FP32 LU + FP64 refinement). Sparse requests:
+ * refactorize `pattern` (an analyzed handle, shared read-only) with `values`
+ * and solve; each worker keeps its own factors of each pattern on the
+ * device. A request's result depends only on its inputs (deterministic
+ * kernels, private workspaces), so it is the same alone and in a mix.
+ * Timestamps are steady-clock nanoseconds (alg_server_now_ns). */
+#define ALG_REQ_DENSE 0
+#define ALG_REQ_SPARSE 1
+#define ALG_REQ_FP64 0
+#define ALG_REQ_MIXED 1
+typedef struct {
+  int kind;
+  int precision;
+  size_t n;
+  const double* a;          /* dense: n x n column-major, host */
+  const double* values;     /* sparse: nnz values in the pattern's CSC order, host */
+  const alg_splu* pattern;  /* sparse: analyzed handle */
+  const double* b;          /* n, host */
+  double* x;                /* n, host: the solution */
+  /* filled by the server */
+  int status;
+  int worker;
+  double backward_error;    /* dense mixed: the refinement's final backward error; else -1 */
+  int64_t t_submit_ns, t_start_ns, t_done_ns;
+  volatile int done;
+} alg_request;
+typedef struct alg_server alg_server;
+/* max_dense_n: largest dense order (workspaces are sized and kernels set up
+ * at creation, before the workers start). */
+int alg_server_create(int n_workers, size_t hbm_budget_bytes, size_t max_dense_n, alg_server** out);
+/* Queues a request (it must stay alive until done); returns at once. */
+int alg_server_submit(alg_server* server, alg_request* request);
+/* Blocks until the request is done; returns its status. */
+int alg_server_wait(alg_server* server, alg_request* request);
+/* Blocks until the queue is empty and no request is running. */
+int alg_server_drain(alg_server* server);
+unsigned long long alg_server_completed(const alg_server* server);
+int64_t alg_server_now_ns(void);
+void alg_server_destroy(alg_server* server);
 
 /* ---- allocation-free solve of one small system ---------------------------
  * No counterpart in the reference crate. For callers that cannot call

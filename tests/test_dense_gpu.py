@@ -265,3 +265,31 @@ def test_device_larnv_matches_the_reference_stream(gpu, oracle):
                 ref, rs = oracle.larnv(name, SEEDY, n)
                 assert same_bits(x.cpu().numpy(), ref), (name, n)
                 assert s == rs, (name, n)
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 16), (300, 500, 64), (4032, 4032, 64), (17, 9, 5), (1000, 33, 130)])
+def test_fp64_tensor_core_update_matches_torch(gpu, shape):
+    """The fused FP64 update on the FP64 tensor cores (mma.sync m8n8k4):
+    C - A B against torch's FP64 product, to a few ulps of |A| |B|, with
+    leading dimensions larger than the rows (sub-blocks of a front)."""
+    import torch
+
+    from algebra_linear_b200 import device
+
+    M, N, K = shape
+    lda, ldb, ldc = M + 3, K + 1, M + 5
+    g = torch.Generator(device="cuda").manual_seed(M + 7 * N + 11 * K)
+    A = torch.rand((K, lda), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    B = torch.rand((N, ldb), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    C0 = torch.rand((N, ldc), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    C = C0.clone()
+    with device.Context() as ctx:
+        rc = gpu.alg_gemm_dmma_sub_dev(ctx.handle, M, N, K, A.data_ptr(), lda, B.data_ptr(), ldb, C.data_ptr(), ldc)
+        assert rc == 0, rc
+    Am, Bm = A[:, :M].t(), B[:, :K].t()
+    ref = C0[:, :M].t() - Am @ Bm
+    err = (C[:, :M].t() - ref).abs().max().item()
+    scale = (Am.abs() @ Bm.abs()).max().item()
+    assert err <= 4 * K * 2.0**-53 * scale, (err, scale)
+    # padding rows between the leading dimension and M are untouched
+    assert torch.equal(C[:, M:], C0[:, M:])
