@@ -545,6 +545,7 @@ int DeviceLu::factor(int b) {
   sa.U = out.U;
   sa.rowid = out.rowid;
   sa.singular = d_flag;
+  const int tok_small = prof_begin(ctx, ALG_K_BATCH);
   for (size_t h = 0; h + 1 < F.small_level_ptr.size(); ++h) {
     const int cnt = F.small_level_ptr[h + 1] - F.small_level_ptr[h];
     if (cnt == 0) continue;
@@ -553,6 +554,7 @@ int DeviceLu::factor(int b) {
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
+  prof_end(ctx, tok_small, 0.0, 0.0);
   // large fronts in postorder
   LuPlan lp;
   lp.nb = 64;

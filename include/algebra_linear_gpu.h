@@ -132,7 +132,8 @@ int alg_dgetrs_dev(alg_ctx* ctx, const double* d_lu, int n, int lda,
 /* Per-kernel-class timing of a context's launches with CUDA events, for
  * roofline reporting. Classes: 0 panel, 1 row interchange, 2 trsm,
  * 3 CUDA-core update, 4 tensor-core update, 5 triangular solve, 6 FP64
- * residual, 7 precision cast, 8 batched systems, 9 sparse, 10 other.
+ * residual, 7 precision cast, 8 batched systems (and the sparse small fronts),
+ * 9 sparse factorization (whole), 10 other.
  * flops/bytes are the algorithmic counts of the timed launches. */
 int alg_ctx_set_profiling(alg_ctx* ctx, int on);
 int alg_ctx_profile_reset(alg_ctx* ctx);
