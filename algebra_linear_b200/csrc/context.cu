@@ -99,8 +99,29 @@ void prof_collect(alg_ctx* ctx) {
   ctx->prof_pending.clear();
 }
 
+int ctx_lookahead_streams(alg_ctx* ctx) {
+  if (ctx->la_stream[0]) return ALG_OK;
+  int least = 0, greatest = 0;
+  ALG_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  ALG_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->la_stream[0], cudaStreamNonBlocking, greatest));
+  ALG_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->la_stream[1], cudaStreamNonBlocking, least));
+  for (auto& e : ctx->la_event) ALG_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return ALG_OK;
+}
+
 void ctx_release(alg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& s : ctx->la_stream)
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+      s = nullptr;
+    }
+  for (auto& e : ctx->la_event)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
   prof_collect(ctx);
   for (auto e : ctx->prof_pool) cudaEventDestroy(e);
   ctx->prof_pool.clear();

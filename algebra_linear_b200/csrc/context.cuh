@@ -54,6 +54,10 @@ struct alg_ctx {
     double ms = 0, flops = 0, bytes = 0;
   };
   ProfTotal prof[ALG_K_COUNT];
+  // look-ahead LU: a high-priority stream for the panel chain and a
+  // low-priority one for the rest of each trailing update (created on use)
+  cudaStream_t la_stream[2] = {nullptr, nullptr};
+  cudaEvent_t la_event[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace alg {
@@ -102,5 +106,7 @@ int prof_begin(alg_ctx* ctx, int cls);
 void prof_end(alg_ctx* ctx, int token, double flops, double bytes);
 void prof_collect(alg_ctx* ctx);
 void ctx_release(alg_ctx* ctx);
+// The look-ahead streams and events of ctx (created on first use).
+int ctx_lookahead_streams(alg_ctx* ctx);
 
 }  // namespace alg

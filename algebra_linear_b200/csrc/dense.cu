@@ -204,14 +204,23 @@ int lu_factor_dev(alg_ctx* ctx, T* a, int m, int nc, int lda, int* ipiv, int* pe
   return lu_factor_partial_dev<T, EXACT>(ctx, a, m, nc, nc, lda, ipiv, perm, plan);
 }
 
+// ALG_LOOKAHEAD=0 factors block after block on one stream (for comparison).
+bool lookahead_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("ALG_LOOKAHEAD");
+    return !(e != nullptr && e[0] == '0');
+  }();
+  return on;
+}
+
 template <typename T, bool EXACT>
 int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, int* ipiv, int* perm,
                           const LuPlan& plan) {
   if (m < nc || nc < 0 || ntot < nc || lda < std::max(1, m)) return ALG_BAD_SHAPE;
   if (nc == 0) return ALG_OK;
-  int* lab = nullptr;
+  int* lab = nullptr;  // two label buffers: block k's swaps are applied while block k + 1 is factored
   int* perm_tmp = nullptr;
-  ALG_TRY(ws_get(ctx, WS_LAB, sizeof(int) * (size_t)m, reinterpret_cast<void**>(&lab)));
+  ALG_TRY(ws_get(ctx, WS_LAB, 2 * sizeof(int) * (size_t)m, reinterpret_cast<void**>(&lab)));
   ALG_TRY(ws_get(ctx, WS_PERM_TMP, sizeof(int) * kSwapMaxMoves, reinterpret_cast<void**>(&perm_tmp)));
   if (perm != nullptr) {
     iota_kernel<<<std::min(1024, (m + 255) / 256), 256, 0, ctx->stream>>>(perm, m);
@@ -220,8 +229,9 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   }
   const int nb = std::max(1, plan.nb);
   const int nbl = std::max(1, std::min(plan.nbl, kPanelMaxW));
-  for (int k0 = 0; k0 < nc; k0 += nb) {
-    const int kb = std::min(nb, nc - k0);
+
+  // the leaf panels of block [k0, k0 + kb), with their in-block updates
+  auto factor_block = [&](int k0, int kb, int* lb) -> int {
     for (int c0 = k0; c0 < k0 + kb; c0 += nbl) {
       const int w = std::min(nbl, k0 + kb - c0);
       PanelArgs<T> pa;
@@ -233,7 +243,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
       pa.kb0 = k0;
       pa.kb1 = k0 + kb;
       pa.ipiv = ipiv;
-      pa.lab = lab;
+      pa.lab = lb;
       pa.first_leaf = (c0 == k0) ? 1 : 0;
       pa.status = ctx->d_status;
       ALG_TRY((launch_panel<T, EXACT>(ctx, pa)));
@@ -245,39 +255,89 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
                                         a + (size_t)cr + (size_t)cr * lda, lda)));
       }
     }
-    // deferred interchanges of every other column (and of perm)
-    const int n_out = k0 + (ntot - k0 - kb);
-    if (n_out > 0 || perm != nullptr) {
-      const int warps_needed = std::max(1, n_out);
-      const int grid = std::max(1, std::min(4 * ctx->sm_count, (warps_needed + 7) / 8));
-      const int tok = prof_begin(ctx, ALG_K_LASWP);
-      laswp_outside_kernel<T><<<grid, kSwapThreads, 0, ctx->stream>>>(a, lda, m, ntot, k0, kb, lab, perm,
-                                                                        perm_tmp);
-      count_launches();
-      prof_end(ctx, tok, 0.0, 0.0);
-      ALG_CUDA_TRY(cudaGetLastError());
-    }
+    return ALG_OK;
+  };
+  // block k's deferred interchanges on the columns of [cb, ce) outside the block
+  auto swaps = [&](int k0, int kb, const int* lb, int cb, int ce, int* pm) -> int {
+    const int n_out = std::max(0, std::min(ce, k0) - cb) + std::max(0, ce - std::max(cb, k0 + kb));
+    if (n_out <= 0 && pm == nullptr) return ALG_OK;
+    const int grid = std::max(1, std::min(4 * ctx->sm_count, (std::max(1, n_out) + 7) / 8));
+    const int tok = prof_begin(ctx, ALG_K_LASWP);
+    laswp_outside_kernel<T><<<grid, kSwapThreads, 0, ctx->stream>>>(a, lda, m, cb, ce, k0, kb, lb, pm, perm_tmp);
+    count_launches();
+    prof_end(ctx, tok, 0.0, 0.0);
+    ALG_CUDA_TRY(cudaGetLastError());
+    return ALG_OK;
+  };
+  // U12 and the trailing update of columns [cb, ce) by block [k0, k0 + kb)
+  auto update = [&](int k0, int kb, int cb, int ce) -> int {
+    if (ce <= cb) return ALG_OK;
     const int kr = k0 + kb;
-    if (kr < ntot) {
-      ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, kr, ntot)));
+    ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, cb, ce)));
+    if (kr >= m) return ALG_OK;
+    if constexpr (std::is_same<T, float>::value) {
+      if (plan.tc_prec >= 0)
+        return gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+                               a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
     }
-    if (kr < ntot && kr < m) {
-      bool done = false;
-      if constexpr (std::is_same<T, float>::value) {
-        if (plan.tc_prec >= 0) {
-          ALG_TRY(gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ntot - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
-                                  a + (size_t)k0 + (size_t)kr * lda, lda, a + (size_t)kr + (size_t)kr * lda, lda));
-          done = true;
-        }
-      }
-      if (!done) {
-        ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - kr, ntot - kr, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
-                                        a + (size_t)k0 + (size_t)kr * lda, lda,
-                                        a + (size_t)kr + (size_t)kr * lda, lda)));
-      }
+    return gemm_sub_dev<T, EXACT>(ctx, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
+                                  a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
+  };
+
+  // the tensor-core update shares one operand workspace, so it stays on one stream
+  const bool la = lookahead_enabled() && plan.tc_prec < 0 && nc > nb;
+  if (!la) {
+    for (int k0 = 0; k0 < nc; k0 += nb) {
+      const int kb = std::min(nb, nc - k0);
+      ALG_TRY(factor_block(k0, kb, lab));
+      ALG_TRY(swaps(k0, kb, lab, 0, ntot, perm));
+      ALG_TRY(update(k0, kb, k0 + kb, ntot));
     }
+    return ALG_OK;
   }
-  return ALG_OK;
+
+  // Look-ahead by one block: the high-priority stream runs the critical
+  // chain (block k's swaps, U12 and update restricted to block k + 1's
+  // columns, then block k + 1's panels) while the low-priority stream applies
+  // block k to everything else; the two meet once per block.
+  ALG_TRY(ctx_lookahead_streams(ctx));
+  cudaStream_t user = ctx->stream, sa = ctx->la_stream[0], sb = ctx->la_stream[1];
+  cudaEvent_t ev_a = ctx->la_event[0], ev_b = ctx->la_event[1], ev_in = ctx->la_event[2];
+  ALG_CUDA_TRY(cudaEventRecord(ev_in, user));
+  ALG_CUDA_TRY(cudaStreamWaitEvent(sa, ev_in, 0));
+  ALG_CUDA_TRY(cudaStreamWaitEvent(sb, ev_in, 0));
+  int rc = ALG_OK;
+  ctx->stream = sa;
+  rc = factor_block(0, std::min(nb, nc), lab);
+  for (int blk = 0, k0 = 0; rc == ALG_OK && k0 < nc; k0 += nb, ++blk) {
+    const int kb = std::min(nb, nc - k0), kr = k0 + kb;
+    const int kb1 = kr < nc ? std::min(nb, nc - kr) : 0;
+    int* lk = lab + (size_t)(blk & 1) * m;
+    int* ln = lab + (size_t)((blk + 1) & 1) * m;
+    // the rest of the update needs block k factored
+    if ((rc = cudaEventRecord(ev_a, sa) == cudaSuccess ? ALG_OK : ALG_CUDA_ERROR) != ALG_OK) break;
+    if ((rc = cudaStreamWaitEvent(sb, ev_a, 0) == cudaSuccess ? ALG_OK : ALG_CUDA_ERROR) != ALG_OK) break;
+    ctx->stream = sa;
+    if (kb1 > 0) {
+      if ((rc = swaps(k0, kb, lk, kr, kr + kb1, nullptr)) != ALG_OK) break;
+      if ((rc = update(k0, kb, kr, kr + kb1)) != ALG_OK) break;
+      if ((rc = factor_block(kr, kb1, ln)) != ALG_OK) break;
+    }
+    ctx->stream = sb;
+    if ((rc = swaps(k0, kb, lk, 0, k0, perm)) != ALG_OK) break;
+    if ((rc = swaps(k0, kb, lk, kr + kb1, ntot, nullptr)) != ALG_OK) break;
+    if ((rc = update(k0, kb, kr + kb1, ntot)) != ALG_OK) break;
+    // block k + 1's swaps touch these columns next
+    if ((rc = cudaEventRecord(ev_b, sb) == cudaSuccess ? ALG_OK : ALG_CUDA_ERROR) != ALG_OK) break;
+    if ((rc = cudaStreamWaitEvent(sa, ev_b, 0) == cudaSuccess ? ALG_OK : ALG_CUDA_ERROR) != ALG_OK) break;
+  }
+  ctx->stream = user;
+  // join both streams back into the caller's stream, also on an error path
+  cudaEventRecord(ev_b, sb);
+  cudaStreamWaitEvent(sa, ev_b, 0);
+  cudaEventRecord(ev_a, sa);
+  cudaStreamWaitEvent(user, ev_a, 0);
+  return rc;
 }
 
 template <typename T, bool EXACT>

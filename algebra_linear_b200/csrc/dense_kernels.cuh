@@ -821,7 +821,7 @@ constexpr int kSwapMaxMoves = 512;
 
 template <typename T>
 __global__ void __launch_bounds__(kSwapThreads) laswp_outside_kernel(
-    T* a, int lda, int n, int ncols, int k0, int kb, const int* lab, int* perm, int* perm_tmp) {
+    T* a, int lda, int n, int cb, int ce, int k0, int kb, const int* lab, int* perm, int* perm_tmp) {
   __shared__ int mv_dst[kSwapMaxMoves];
   __shared__ int mv_src[kSwapMaxMoves];
   __shared__ int mv_cnt;
@@ -839,10 +839,13 @@ __global__ void __launch_bounds__(kSwapThreads) laswp_outside_kernel(
   const int lane = threadIdx.x & 31;
   const int warps_total = gridDim.x * (kSwapThreads / 32);
   const int gwarp = blockIdx.x * (kSwapThreads / 32) + (threadIdx.x >> 5);
-  const int n_out = k0 + (ncols - k0 - kb);  // columns [0,k0) and [k0+kb, ncols)
+  // columns of the window [cb, ce) outside the block [k0, k0 + kb)
+  const int n_before = max(0, min(ce, k0) - cb);
+  const int after0 = max(cb, k0 + kb);
+  const int n_out = n_before + max(0, ce - after0);
   constexpr int kPer = kSwapMaxMoves / 32;
   for (int cidx = gwarp; cidx < n_out; cidx += warps_total) {
-    const int col = cidx < k0 ? cidx : cidx + kb;
+    const int col = cidx < n_before ? cb + cidx : after0 + (cidx - n_before);
     T* colp = a + (size_t)col * lda;
     T vals[kPer];
 #pragma unroll
