@@ -79,6 +79,52 @@ __device__ int block_first_max(double key, int idx, double* rk, int* ri) {
   return r;
 }
 
+// C (mr x nc) -= A (mr x kd) B (kd x nc), all inside one front (column-major,
+// leading dimension ld), by one CTA of kSmallThreads: 64 x 64 tiles, each
+// thread a 4 x 4 register block, K staged through shared memory 16 at a time.
+__device__ void cta_gemm_sub(double* C, const double* A, const double* B, int ld, int mr, int nc, int kd,
+                             double* As, double* Bs) {
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int i0 = 0; i0 < mr; i0 += 64)
+    for (int j0 = 0; j0 < nc; j0 += 64) {
+      double acc[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+      for (int k0 = 0; k0 < kd; k0 += 16) {
+        __syncthreads();
+        for (int e = tid; e < 64 * 16; e += kSmallThreads) {
+          const int r = e & 63, k = e >> 6;  // A tile, rows contiguous
+          As[k * 64 + r] = (i0 + r < mr && k0 + k < kd) ? A[(i0 + r) + (int64_t)(k0 + k) * ld] : 0.0;
+          const int kk = e & 15, c = e >> 4;  // B tile, k contiguous
+          Bs[kk * 64 + c] = (j0 + c < nc && k0 + kk < kd) ? B[(k0 + kk) + (int64_t)(j0 + c) * ld] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+          double av[4], bv[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) av[r] = As[k * 64 + tx * 4 + r];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) bv[c] = Bs[k * 64 + ty * 4 + c];
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int i = i0 + tx * 4 + r, j = j0 + ty * 4 + c;
+          if (i < mr && j < nc) C[i + (int64_t)j * ld] -= acc[r][c];
+        }
+    }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a) {
   __shared__ double rk[kSmallThreads / 32];
   __shared__ int ri[kSmallThreads / 32];
@@ -159,27 +205,26 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
     }
     __syncthreads();
   }
-  // U12 = L11^-1 A12: forward substitution, a thread per column
-  for (int c = size + tid; c < cols; c += kSmallThreads) {
-    double* col = f + (int64_t)c * rows;
-    for (int k = 0; k < size; ++k) {
-      const double uk = col[k];
-      for (int i = k + 1; i < size; ++i) col[i] = fma(-f[i + (int64_t)k * rows], uk, col[i]);
+  __shared__ double As[64 * 16], Bs[16 * 64];
+  // U12 = L11^-1 A12 in 16-row blocks: forward substitution within the block
+  // (a thread per column), then the rows below by the tiled update
+  for (int kb = 0; kb < size; kb += 16) {
+    const int ke = min(size, kb + 16);
+    for (int c = size + tid; c < cols; c += kSmallThreads) {
+      double* col = f + (int64_t)c * rows;
+      for (int k = kb; k < ke; ++k) {
+        const double uk = col[k];
+        for (int i = k + 1; i < ke; ++i) col[i] = fma(-f[i + (int64_t)k * rows], uk, col[i]);
+      }
     }
+    __syncthreads();
+    if (ke < size)
+      cta_gemm_sub(f + ke + (int64_t)size * rows, f + ke + (int64_t)kb * rows, f + kb + (int64_t)size * rows, rows,
+                   size - ke, d.ncb, ke - kb, As, Bs);
   }
-  __syncthreads();
-  // contribution block: CB -= L21 U12, one dot product per entry
-  {
-    const int mr = rows - size;
-    const int64_t upd = (int64_t)mr * d.ncb;
-    for (int64_t e = tid; e < upd; e += kSmallThreads) {
-      const int i = size + (int)(e % mr), c = size + (int)(e / mr);
-      double acc = 0.0;
-      for (int k = 0; k < size; ++k) acc = fma(f[i + (int64_t)k * rows], f[k + (int64_t)c * rows], acc);
-      f[i + (int64_t)c * rows] -= acc;
-    }
-  }
-  __syncthreads();
+  // contribution block: CB -= L21 U12 (register-tiled)
+  cta_gemm_sub(f + size + (int64_t)size * rows, f + size, f + (int64_t)size * rows, rows, rows - size, d.ncb, size,
+               As, Bs);
   double* lp = a.L + d.l_off;
   for (int64_t e = tid; e < (int64_t)rows * size; e += kSmallThreads) lp[e] = f[e];
   double* up = a.U + d.u_off;
