@@ -92,6 +92,8 @@ SIGNATURES = [
     ("alg_splu_solve_dev", _I, [_P, _P]),
     ("alg_splu_clone", _I, [_P, _P]),
     ("alg_splu_factorize_values", _I, [_P, _P]),
+    ("alg_splu_set_precision", _I, [_P, _I, C.c_double, _I]),
+    ("alg_splu_last_solve", _I, [_P, _P]),
     ("alg_server_create", _I, [_I, _SZ, _SZ, _P]),
     ("alg_server_submit", _I, [_P, _P]),
     ("alg_server_wait", _I, [_P, _P]),

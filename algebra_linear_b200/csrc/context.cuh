@@ -81,6 +81,7 @@ enum WsSlot : int {
   WS_RBT,         // butterfly coefficients (mixed form)
   WS_IDENT,       // identity permutation
   WS_BATCH,       // batched-solve queues
+  WS_TSLU,        // tournament-pivoting panel scratch
   WS_COUNT
 };
 

@@ -222,6 +222,11 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   int* perm_tmp = nullptr;
   ALG_TRY(ws_get(ctx, WS_LAB, 2 * sizeof(int) * (size_t)m, reinterpret_cast<void**>(&lab)));
   ALG_TRY(ws_get(ctx, WS_PERM_TMP, sizeof(int) * kSwapMaxMoves, reinterpret_cast<void**>(&perm_tmp)));
+  void* tslu_ws = nullptr;
+  if (std::is_same<T, float>::value && plan.tslu) {
+    ALG_TRY(ws_get(ctx, WS_TSLU, tslu_scratch_bytes(), &tslu_ws));
+    ALG_CUDA_TRY(cudaMemsetAsync(tslu_ws, 0, tslu_scratch_bytes(), ctx->stream));  // arrival counters
+  }
   if (perm != nullptr) {
     iota_kernel<<<std::min(1024, (m + 255) / 256), 256, 0, ctx->stream>>>(perm, m);
     count_launches();
@@ -246,7 +251,14 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
       pa.lab = lb;
       pa.first_leaf = (c0 == k0) ? 1 : 0;
       pa.status = ctx->d_status;
-      ALG_TRY((launch_panel<T, EXACT>(ctx, pa)));
+      int prc = ALG_NOT_IMPLEMENTED;
+      if constexpr (std::is_same<T, float>::value) {
+        if (tslu_ws)
+          prc = tslu_panel(ctx, TsluArgs{a, lda, m, c0, w, k0, k0 + kb, ipiv, lb, pa.first_leaf, ctx->d_status},
+                           tslu_ws);
+      }
+      if (prc == ALG_NOT_IMPLEMENTED) prc = launch_panel<T, EXACT>(ctx, pa);
+      ALG_TRY(prc);
       const int cr = c0 + w;  // first column right of the leaf
       if (cr < k0 + kb) {
         ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, c0, w, cr, k0 + kb)));
@@ -269,14 +281,17 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
     ALG_CUDA_TRY(cudaGetLastError());
     return ALG_OK;
   };
-  // U12 and the trailing update of columns [cb, ce) by block [k0, k0 + kb)
-  auto update = [&](int k0, int kb, int cb, int ce) -> int {
+  // U12 and the trailing update of columns [cb, ce) by block [k0, k0 + kb);
+  // tc: the tensor-core kernel may take it (one stream at a time uses its
+  // operand workspace: the wide update, never the look-ahead's narrow one)
+  auto update = [&](int k0, int kb, int cb, int ce, bool tc) -> int {
     if (ce <= cb) return ALG_OK;
     const int kr = k0 + kb;
     ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, cb, ce)));
     if (kr >= m) return ALG_OK;
     if constexpr (std::is_same<T, float>::value) {
-      if (plan.tc_prec >= 0)
+      // the tensor-core kernel takes whole 128-byte K slices; a ragged last block stays in FP32
+      if (tc && plan.tc_prec >= 0 && kb % (plan.tc_prec == ALG_PREC_BF16 ? 64 : 32) == 0)
         return gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
     }
@@ -284,14 +299,13 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
                                   a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
   };
 
-  // the tensor-core update shares one operand workspace, so it stays on one stream
-  const bool la = lookahead_enabled() && plan.tc_prec < 0 && nc > nb;
+  const bool la = lookahead_enabled() && nc > nb;
   if (!la) {
     for (int k0 = 0; k0 < nc; k0 += nb) {
       const int kb = std::min(nb, nc - k0);
       ALG_TRY(factor_block(k0, kb, lab));
       ALG_TRY(swaps(k0, kb, lab, 0, ntot, perm));
-      ALG_TRY(update(k0, kb, k0 + kb, ntot));
+      ALG_TRY(update(k0, kb, k0 + kb, ntot, true));
     }
     return ALG_OK;
   }
@@ -320,13 +334,13 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
     ctx->stream = sa;
     if (kb1 > 0) {
       if ((rc = swaps(k0, kb, lk, kr, kr + kb1, nullptr)) != ALG_OK) break;
-      if ((rc = update(k0, kb, kr, kr + kb1)) != ALG_OK) break;
+      if ((rc = update(k0, kb, kr, kr + kb1, false)) != ALG_OK) break;
       if ((rc = factor_block(kr, kb1, ln)) != ALG_OK) break;
     }
     ctx->stream = sb;
     if ((rc = swaps(k0, kb, lk, 0, k0, perm)) != ALG_OK) break;
     if ((rc = swaps(k0, kb, lk, kr + kb1, ntot, nullptr)) != ALG_OK) break;
-    if ((rc = update(k0, kb, kr + kb1, ntot)) != ALG_OK) break;
+    if ((rc = update(k0, kb, kr + kb1, ntot, true)) != ALG_OK) break;
     // block k + 1's swaps touch these columns next
     if ((rc = cudaEventRecord(ev_b, sb) == cudaSuccess ? ALG_OK : ALG_CUDA_ERROR) != ALG_OK) break;
     if ((rc = cudaStreamWaitEvent(sa, ev_b, 0) == cudaSuccess ? ALG_OK : ALG_CUDA_ERROR) != ALG_OK) break;

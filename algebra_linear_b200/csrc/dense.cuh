@@ -10,7 +10,27 @@ struct LuPlan {
   int nbl = 16;      // leaf-panel width (one cluster kernel)
   int tc_prec = -1;  // FP32 matrices: ALG_PREC_TF32 / ALG_PREC_BF16 puts the
                      // block-level trailing update on the tensor cores
+  int tslu = 0;      // FP32 matrices: tournament pivoting for the leaf panels
 };
+
+// Tournament-pivoting leaf panel of the FP32 LU (tslu.cu) and its scratch
+// size: columns [c0, c0 + w) of rows [c0, n), inside the block panel
+// [kb0, kb1); the same outputs as the partial-pivoting leaf kernel.
+struct TsluArgs {
+  float* a;
+  int lda, n, c0, w, kb0, kb1;
+  int* ipiv;
+  int* lab;
+  int first_leaf;
+  DevStatus* status;
+};
+// One multi-CTA triangular sweep over the leading n x n block of LU factors
+// (lda): unit-lower or upper; flags: n / 64 + 1 ints, abort_flag zero.
+template <typename T>
+int tri_solve_dev(alg_ctx* ctx, const T* lu, int lda, int n, T* x, bool upper, int* flags, int* abort_flag);
+
+size_t tslu_scratch_bytes();
+int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch);
 
 // C -= A B on the tensor cores (tcgen05, FP32 accumulation in TMEM) with the
 // operands rounded to TF32 or BF16; A, B, C FP32 column-major.

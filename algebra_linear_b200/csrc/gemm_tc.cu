@@ -235,7 +235,21 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ---- operand preparation ---------------------------------------------------------
-// A (M x K, column-major) -> At (M rows of K entries); through a 32 x 32 tile.
+// FMT 3 (TF32x3, the split-precision scheme of Ootomo and Yokota, "Recovering
+// single precision accuracy from Tensor Cores while surpassing the FP32
+// theoretical peak performance", IJHPCA 2022): every FP32 entry v becomes
+// hi = tf32(v) and lo = tf32(v - hi) (v - hi is exact in FP32), and the
+// operands are laid out along a tripled K as
+//   A row: [hi | hi | lo],  B row: [hi | lo | hi]
+// so one TF32 GEMM over 3K accumulates a_hi b_hi + a_hi b_lo + a_lo b_hi in
+// FP32; the dropped a_lo b_lo term is below FP32 rounding of the products.
+__device__ __forceinline__ void split_tf32(float v, uint32_t& hi, uint32_t& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(v));
+  const float r = v - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+// A (M x K, column-major) -> At (M rows of K entries, 3K for FMT 3); through a 32 x 32 tile.
 template <int FMT>
 __global__ void prep_a_kernel(const float* __restrict__ a, int lda, int M, int K, void* __restrict__ out) {
   __shared__ float t[32][33];
@@ -251,6 +265,13 @@ __global__ void prep_a_kernel(const float* __restrict__ a, int lda, int M, int K
       const float v = t[threadIdx.x][ii];
       if constexpr (FMT == 1) {
         reinterpret_cast<__nv_bfloat16*>(out)[(size_t)i * K + k] = __float2bfloat16_rn(v);
+      } else if constexpr (FMT == 3) {
+        uint32_t hi, lo;
+        split_tf32(v, hi, lo);
+        uint32_t* row = reinterpret_cast<uint32_t*>(out) + (size_t)i * 3 * K;
+        row[k] = hi;
+        row[K + k] = hi;
+        row[2 * K + k] = lo;
       } else {
         uint32_t tv;
         asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(tv) : "f"(v));
@@ -260,7 +281,7 @@ __global__ void prep_a_kernel(const float* __restrict__ a, int lda, int M, int K
   }
 }
 
-// B (K x N, column-major, K contiguous already) -> Bt (N rows of K entries).
+// B (K x N, column-major, K contiguous already) -> Bt (N rows of K entries, 3K for FMT 3).
 template <int FMT>
 __global__ void prep_b_kernel(const float* __restrict__ b, int ldb, int K, int N, void* __restrict__ out) {
   const size_t total = (size_t)K * N;
@@ -270,6 +291,13 @@ __global__ void prep_b_kernel(const float* __restrict__ b, int ldb, int K, int N
     const float v = b[k + j * (size_t)ldb];
     if constexpr (FMT == 1) {
       reinterpret_cast<__nv_bfloat16*>(out)[idx] = __float2bfloat16_rn(v);
+    } else if constexpr (FMT == 3) {
+      uint32_t hi, lo;
+      split_tf32(v, hi, lo);
+      uint32_t* row = reinterpret_cast<uint32_t*>(out) + j * 3 * (size_t)K;
+      row[k] = hi;
+      row[K + k] = lo;
+      row[2 * K + k] = hi;
     } else {
       uint32_t tv;
       asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(tv) : "f"(v));
@@ -316,10 +344,11 @@ template <int FMT>
 int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C,
               int ldc) {
   const int esz = FMT == 1 ? 2 : 4;
+  constexpr int KFMT = FMT == 3 ? 2 : FMT;  // the MMA's operand type (TF32x3 runs TF32 MMAs)
   // K padded to whole 128-byte slices so every TMA row stride is 16-byte aligned
   const int kslice = kSliceBytes / esz;
-  const int Kp = ((K + kslice - 1) / kslice) * kslice;
-  if (Kp != K) return ALG_BAD_SHAPE;  // K must be whole 128-byte slices (the LU's block widths are)
+  if (K % kslice != 0) return ALG_BAD_SHAPE;  // K must be whole 128-byte slices (the LU's block widths are)
+  const int Kp = FMT == 3 ? 3 * K : K;
   void* at = nullptr;
   void* bt = nullptr;
   ALG_TRY(ws_get(ctx, WS_KRYLOV, (size_t)esz * Kp * ((size_t)M + N) + 256, &at));
@@ -334,16 +363,16 @@ int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const 
     ALG_CUDA_TRY(cudaGetLastError());
   }
   CUtensorMap ma, mb;
-  ALG_TRY(make_map(&ma, at, FMT, M, Kp, BM));
-  ALG_TRY(make_map(&mb, bt, FMT, N, Kp, BN));
+  ALG_TRY(make_map(&ma, at, KFMT, M, Kp, BM));
+  ALG_TRY(make_map(&mb, bt, KFMT, N, Kp, BN));
   static bool configured = false;
   if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel<FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ALG_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel<KFMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kSmemBytes));
     configured = true;
   }
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-  gemm_tc_kernel<FMT><<<grid, kThreads, kSmemBytes, ctx->stream>>>(ma, mb, M, N, Kp, C, ldc, ctx->d_status);
+  gemm_tc_kernel<KFMT><<<grid, kThreads, kSmemBytes, ctx->stream>>>(ma, mb, M, N, Kp, C, ldc, ctx->d_status);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
@@ -358,6 +387,7 @@ int gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A,
   int rc;
   if (prec == ALG_PREC_BF16) rc = launch_tc<1>(ctx, M, N, K, A, lda, B, ldb, C, ldc);
   else if (prec == ALG_PREC_TF32) rc = launch_tc<2>(ctx, M, N, K, A, lda, B, ldb, C, ldc);
+  else if (prec == ALG_PREC_TF32X3) rc = launch_tc<3>(ctx, M, N, K, A, lda, B, ldb, C, ldc);
   else rc = ALG_INVALID_ARGUMENT;
   prof_end(ctx, tok, 2.0 * M * N * K, 4.0 * (2.0 * M * N + double(M) * K + double(K) * N));
   return rc;

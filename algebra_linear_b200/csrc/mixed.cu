@@ -157,6 +157,10 @@ int grid_for(size_t cnt, int sm) {
 
 int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, int* ipiv, int* perm) {
   LuPlan plan = default_plan(n, 4);
+  // tournament pivoting for the low-precision LU's panels (refinement in FP64
+  // restores the FP64 backward error); ALG_TSLU=0 keeps partial pivoting
+  const char* ts = std::getenv("ALG_TSLU");
+  plan.tslu = (ts != nullptr && ts[0] == '1') ? 1 : 0;
   if (precision != ALG_PREC_FP32) {
     plan.tc_prec = precision;
     plan.nb = 128;
@@ -458,7 +462,8 @@ int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, i
   alg_mixed_opts o;
   alg_mixed_opts_default(&o);
   if (opts) o = *opts;
-  if (o.precision != ALG_PREC_FP32 && o.precision != ALG_PREC_TF32 && o.precision != ALG_PREC_BF16)
+  if (o.precision != ALG_PREC_FP32 && o.precision != ALG_PREC_TF32 && o.precision != ALG_PREC_BF16 &&
+      o.precision != ALG_PREC_TF32X3)
     return ALG_INVALID_ARGUMENT;
   return alg::dgesv_mixed_dev(ctx, o, d_a, n, lda, d_b, nrhs, ldb, report);
 }

@@ -56,6 +56,8 @@ struct FrontPlan {
   std::vector<int32_t> small_level_ptr, small_level_fronts;  // batched levels (leaves first)
   std::vector<int32_t> big_order;                            // large fronts in postorder
   std::vector<int32_t> solve_level_ptr, solve_level_fronts;  // all fronts by height (leaves first)
+  std::vector<int64_t> csr_ptr, csr_map;                     // A by rows: row starts, CSC index of each entry
+  std::vector<int32_t> csr_col;                              //   and its column
   // sizes of the device arenas (doubles / ints)
   int64_t block_total = 0, l_total = 0, u_total = 0, rowid_total = 0;
   int64_t stack_total = 0, front_buf = 0;

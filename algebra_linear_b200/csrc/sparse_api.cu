@@ -29,6 +29,9 @@ struct alg_splu {
   alg::sp::DeviceLu dev;
   bool dev_ready = false;
   int cur = -1;  // factor set of the last successful factorization
+  int prec = -1;       // precision of the next factorization (-1: FP64)
+  double tol = 0.0;    // the mixed form's refinement target and step limit
+  int max_ir = 0;
   int has_stats = 0;
   alg_splu_stats stats{};
 };
@@ -70,6 +73,9 @@ int factor_loaded(alg_splu* lu) {
   const auto t0 = std::chrono::steady_clock::now();
   if (lu->plan.structurally_singular) return ALG_SP_SINGULAR;
   const int set = lu->cur < 0 ? 0 : 1 - lu->cur;
+  lu->dev.prec = lu->prec;
+  lu->dev.tol = lu->tol;
+  lu->dev.max_ir = lu->max_ir;
   ALG_TRY(lu->dev.factor(set));
   alg::sp::Stats st;
   const int rc = lu->dev.finish(set, &st);
@@ -200,9 +206,11 @@ int alg_splu_solve(const alg_splu* lu_c, double* b, size_t b_len) {
   if (lu->n == 0) return ALG_OK;
   cudaStream_t st = lu->ctx->stream;
   ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_rhs, b, sizeof(double) * lu->n, cudaMemcpyHostToDevice, st));
+  ALG_TRY(alg::status_reset(lu->ctx));
   ALG_TRY(lu->dev.solve(lu->cur));
   ALG_CUDA_TRY(cudaMemcpyAsync(b, lu->dev.d_rhs, sizeof(double) * lu->n, cudaMemcpyDeviceToHost, st));
-  ALG_CUDA_TRY(cudaStreamSynchronize(st));
+  ALG_TRY(alg::status_fetch(lu->ctx));  // synchronises
+  if (lu->ctx->h_status->timeout) return ALG_TIMEOUT;
   return ALG_OK;
 }
 
@@ -322,6 +330,9 @@ int alg_splu_clone(const alg_splu* src, alg_splu** out) {
   lu->ordering_time = src->ordering_time;
   lu->sym = src->sym;
   lu->plan = src->plan;
+  lu->prec = src->prec;
+  lu->tol = src->tol;
+  lu->max_ir = src->max_ir;
   *out = lu.release();
   return ALG_OK;
 }
@@ -339,6 +350,29 @@ int alg_splu_factorize_values(alg_splu* lu, const double* values) {
   ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_values, values, sizeof(double) * lu->nnz, cudaMemcpyHostToDevice,
                                lu->ctx->stream));
   return factor_loaded(lu);
+}
+
+int alg_splu_set_precision(alg_splu* lu, int precision, double tol, int max_ir) {
+  if (lu == nullptr) return ALG_INVALID_ARGUMENT;
+  if (precision != ALG_SPLU_FP64 && precision != ALG_PREC_FP32 && precision != ALG_PREC_TF32 &&
+      precision != ALG_PREC_BF16 && precision != ALG_PREC_TF32X3)
+    return ALG_INVALID_ARGUMENT;
+  if (!(tol == tol)) return ALG_INVALID_ARGUMENT;
+  lu->prec = precision;
+  lu->tol = tol;
+  lu->max_ir = max_ir;
+  return ALG_OK;
+}
+
+int alg_splu_last_solve(const alg_splu* lu, alg_splu_refine_report* out) {
+  if (lu == nullptr || out == nullptr) return ALG_INVALID_ARGUMENT;
+  if (lu->cur < 0) return ALG_SP_NOT_FACTORIZED;
+  out->precision = lu->dev.last.precision;
+  out->iterations = lu->dev.last.iterations;
+  out->fell_back = lu->dev.last.fell_back;
+  out->factor_precision = lu->dev_ready ? lu->dev.fac[lu->cur].prec : ALG_SPLU_FP64;
+  out->backward_error = lu->dev.last.backward_error;
+  return ALG_OK;
 }
 
 void alg_splu_free(alg_splu* lu) {

@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "dense.cuh"
@@ -28,6 +31,14 @@ namespace {
 
 constexpr int kSmallThreads = 256;
 
+template <typename T>
+__device__ __forceinline__ T fma_t(T a, T b, T c);
+template <>
+__device__ __forceinline__ double fma_t<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <>
+__device__ __forceinline__ float fma_t<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+template <typename T>
 struct SmallArgs {
   const FrontDesc* fronts;
   const int32_t* level_fronts;
@@ -39,9 +50,9 @@ struct SmallArgs {
   const int32_t* anew_col;
   const int32_t* new_rows;
   const double* values;
-  double* block;
-  double* L;
-  double* U;
+  T* block;
+  T* L;
+  T* U;
   int32_t* rowid;
   int* singular;
 };
@@ -82,28 +93,28 @@ __device__ int block_first_max(double key, int idx, double* rk, int* ri) {
 // C (mr x nc) -= A (mr x kd) B (kd x nc), all inside one front (column-major,
 // leading dimension ld), by one CTA of kSmallThreads: 64 x 64 tiles, each
 // thread a 4 x 4 register block, K staged through shared memory 16 at a time.
-__device__ void cta_gemm_sub(double* C, const double* A, const double* B, int ld, int mr, int nc, int kd,
-                             double* As, double* Bs) {
+template <typename T>
+__device__ void cta_gemm_sub(T* C, const T* A, const T* B, int ld, int mr, int nc, int kd, T* As, T* Bs) {
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   for (int i0 = 0; i0 < mr; i0 += 64)
     for (int j0 = 0; j0 < nc; j0 += 64) {
-      double acc[4][4];
+      T acc[4][4];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+        for (int c = 0; c < 4; ++c) acc[r][c] = T(0);
       for (int k0 = 0; k0 < kd; k0 += 16) {
         __syncthreads();
         for (int e = tid; e < 64 * 16; e += kSmallThreads) {
           const int r = e & 63, k = e >> 6;  // A tile, rows contiguous
-          As[k * 64 + r] = (i0 + r < mr && k0 + k < kd) ? A[(i0 + r) + (int64_t)(k0 + k) * ld] : 0.0;
+          As[k * 64 + r] = (i0 + r < mr && k0 + k < kd) ? A[(i0 + r) + (int64_t)(k0 + k) * ld] : T(0);
           const int kk = e & 15, c = e >> 4;  // B tile, k contiguous
-          Bs[kk * 64 + c] = (j0 + c < nc && k0 + kk < kd) ? B[(k0 + kk) + (int64_t)(j0 + c) * ld] : 0.0;
+          Bs[kk * 64 + c] = (j0 + c < nc && k0 + kk < kd) ? B[(k0 + kk) + (int64_t)(j0 + c) * ld] : T(0);
         }
         __syncthreads();
 #pragma unroll 4
         for (int k = 0; k < 16; ++k) {
-          double av[4], bv[4];
+          T av[4], bv[4];
 #pragma unroll
           for (int r = 0; r < 4; ++r) av[r] = As[k * 64 + tx * 4 + r];
 #pragma unroll
@@ -111,7 +122,7 @@ __device__ void cta_gemm_sub(double* C, const double* A, const double* B, int ld
 #pragma unroll
           for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+            for (int c = 0; c < 4; ++c) acc[r][c] = fma_t(av[r], bv[c], acc[r][c]);
         }
       }
 #pragma unroll
@@ -125,18 +136,19 @@ __device__ void cta_gemm_sub(double* C, const double* A, const double* B, int ld
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a) {
+template <typename T>
+__global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T> a) {
   __shared__ double rk[kSmallThreads / 32];
   __shared__ int ri[kSmallThreads / 32];
-  __shared__ double piv_s;
+  __shared__ T piv_s;
   const int s = a.level_fronts[blockIdx.x];
   const FrontDesc d = a.fronts[s];
   const int rows = d.rows, size = d.size, cols = d.size + d.ncb;
-  double* f = a.block + d.block_off;
+  T* f = a.block + d.block_off;
   int32_t* rid = a.rowid + d.rowid_off;
   const int tid = threadIdx.x;
   const int64_t total = (int64_t)rows * cols;
-  for (int64_t e = tid; e < total; e += kSmallThreads) f[e] = 0.0;
+  for (int64_t e = tid; e < total; e += kSmallThreads) f[e] = T(0);
   // slots: the children's unpivoted rows, then the rows entering here
   for (int k = d.child_begin; k < d.child_end; ++k) {
     const FrontDesc c = a.fronts[a.child_idx[k]];
@@ -149,12 +161,12 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
   }
   __syncthreads();
   for (int q = d.anew_begin + tid; q < d.anew_end; q += kSmallThreads)
-    f[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = a.values[a.anew_q[q]];
+    f[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = (T)a.values[a.anew_q[q]];
   for (int k = d.child_begin; k < d.child_end; ++k) {
     const FrontDesc c = a.fronts[a.child_idx[k]];
     const int slot0 = a.child_slot[k];
     const int crows = c.rows - c.size;
-    const double* cb = a.block + c.cb_off;
+    const T* cb = a.block + c.cb_off;
     const int64_t ce = (int64_t)crows * c.ncb;
     for (int64_t e = tid; e < ce; e += kSmallThreads) {
       const int i = (int)(e % crows), t = (int)(e / crows);
@@ -166,7 +178,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
     double key = -1.0;
     int idx = INT_MAX;
     for (int i = k + tid; i < rows; i += kSmallThreads) {
-      const double v = fabs(f[i + (int64_t)k * rows]);
+      const double v = fabs((double)f[i + (int64_t)k * rows]);
       if (v > key) {
         key = v;
         idx = i;
@@ -175,14 +187,14 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
     const int p = block_first_max(key, idx, rk, ri);
     if (tid == 0) piv_s = f[p + (int64_t)k * rows];
     __syncthreads();
-    const double pv = piv_s;
-    if (!(fabs(pv) > 0.0)) {
+    const T pv = piv_s;
+    if (!(fabs((double)pv) > 0.0)) {
       if (tid == 0) atomicExch(a.singular, 1);
       return;  // uniform: every thread read the same pivot
     }
     if (p != k) {
       for (int j = tid; j < cols; j += kSmallThreads) {
-        const double t = f[k + (int64_t)j * rows];
+        const T t = f[k + (int64_t)j * rows];
         f[k + (int64_t)j * rows] = f[p + (int64_t)j * rows];
         f[p + (int64_t)j * rows] = t;
       }
@@ -193,7 +205,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
       }
     }
     __syncthreads();
-    const double inv = 1.0 / pv;
+    const T inv = T(1) / pv;
     for (int i = k + 1 + tid; i < rows; i += kSmallThreads) f[i + (int64_t)k * rows] *= inv;
     __syncthreads();
     // rank-1 update of the front's own columns only
@@ -201,20 +213,20 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
     const int64_t upd = (int64_t)mr * mc;
     for (int64_t e = tid; e < upd; e += kSmallThreads) {
       const int i = k + 1 + (int)(e % mr), j = k + 1 + (int)(e / mr);
-      f[i + (int64_t)j * rows] = fma(-f[k + (int64_t)j * rows], f[i + (int64_t)k * rows], f[i + (int64_t)j * rows]);
+      f[i + (int64_t)j * rows] = fma_t(-f[k + (int64_t)j * rows], f[i + (int64_t)k * rows], f[i + (int64_t)j * rows]);
     }
     __syncthreads();
   }
-  __shared__ double As[64 * 16], Bs[16 * 64];
+  __shared__ T As[64 * 16], Bs[16 * 64];
   // U12 = L11^-1 A12 in 16-row blocks: forward substitution within the block
   // (a thread per column), then the rows below by the tiled update
   for (int kb = 0; kb < size; kb += 16) {
     const int ke = min(size, kb + 16);
     for (int c = size + tid; c < cols; c += kSmallThreads) {
-      double* col = f + (int64_t)c * rows;
+      T* col = f + (int64_t)c * rows;
       for (int k = kb; k < ke; ++k) {
-        const double uk = col[k];
-        for (int i = k + 1; i < ke; ++i) col[i] = fma(-f[i + (int64_t)k * rows], uk, col[i]);
+        const T uk = col[k];
+        for (int i = k + 1; i < ke; ++i) col[i] = fma_t(-f[i + (int64_t)k * rows], uk, col[i]);
       }
     }
     __syncthreads();
@@ -225,9 +237,9 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
   // contribution block: CB -= L21 U12 (register-tiled)
   cta_gemm_sub(f + size + (int64_t)size * rows, f + size, f + (int64_t)size * rows, rows, rows - size, d.ncb, size,
                As, Bs);
-  double* lp = a.L + d.l_off;
+  T* lp = a.L + d.l_off;
   for (int64_t e = tid; e < (int64_t)rows * size; e += kSmallThreads) lp[e] = f[e];
-  double* up = a.U + d.u_off;
+  T* up = a.U + d.u_off;
   for (int64_t e = tid; e < (int64_t)size * d.ncb; e += kSmallThreads) {
     const int kk = (int)(e % size), t = (int)(e / size);
     up[e] = f[kk + (int64_t)(size + t) * rows];
@@ -235,6 +247,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs a)
 }
 
 // ---- large fronts ----------------------------------------------------------
+template <typename T>
 struct BigArgs {
   FrontDesc d;
   const FrontDesc* fronts;
@@ -246,14 +259,15 @@ struct BigArgs {
   const int32_t* anew_col;
   const int32_t* new_rows;
   const double* values;
-  const double* block;  // small children's contribution blocks
-  const double* stack;  // large children's contribution blocks
-  double* front;        // rows x (size + ncb), ld = rows (zeroed before)
+  const T* block;  // small children's contribution blocks
+  const T* stack;  // large children's contribution blocks
+  T* front;        // rows x (size + ncb), ld = rows (zeroed before)
   const int32_t* rowid;
   int32_t* rowtmp;      // the front's slots before pivoting
 };
 
-__global__ void big_assemble_kernel(BigArgs a) {
+template <typename T>
+__global__ void big_assemble_kernel(BigArgs<T> a) {
   const FrontDesc& d = a.d;
   const int rows = d.rows;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -263,13 +277,13 @@ __global__ void big_assemble_kernel(BigArgs a) {
     for (int64_t i = tid; i < d.new_end - d.new_begin; i += nth) a.rowtmp[slotn + i] = a.new_rows[d.new_begin + i];
   }
   for (int64_t q = d.anew_begin + tid; q < d.anew_end; q += nth)
-    a.front[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = a.values[a.anew_q[q]];
+    a.front[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = (T)a.values[a.anew_q[q]];
   for (int k = d.child_begin; k < d.child_end; ++k) {
     const FrontDesc c = a.fronts[a.child_idx[k]];
     const int slot0 = a.child_slot[k];
     const int crows = c.rows - c.size;
     for (int64_t i = tid; i < crows; i += nth) a.rowtmp[slot0 + i] = a.rowid[c.rowid_off + c.size + i];
-    const double* cb = (c.small ? a.block : a.stack) + c.cb_off;
+    const T* cb = (c.small ? a.block : a.stack) + c.cb_off;
     const int64_t ce = (int64_t)crows * c.ncb;
     for (int64_t e = tid; e < ce; e += nth) {
       const int i = (int)(e % crows), t = (int)(e / crows);
@@ -279,20 +293,21 @@ __global__ void big_assemble_kernel(BigArgs a) {
 }
 
 // After the partial LU: rows of the slots, U12, and the contribution block.
-__global__ void big_finalize_kernel(FrontDesc d, const double* front, const int* perm, const int32_t* rowtmp,
-                                    int32_t* rowid, double* U, double* stack) {
+template <typename T>
+__global__ void big_finalize_kernel(FrontDesc d, const T* front, const int* perm, const int32_t* rowtmp,
+                                    int32_t* rowid, T* U, T* stack) {
   const int rows = d.rows, size = d.size;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = tid; i < rows; i += nth) rowid[d.rowid_off + i] = rowtmp[perm[i]];
-  double* up = U + d.u_off;
+  T* up = U + d.u_off;
   for (int64_t e = tid; e < (int64_t)size * d.ncb; e += nth) {
     const int kk = (int)(e % size), t = (int)(e / size);
     up[e] = front[kk + (int64_t)(size + t) * rows];
   }
   const int crows = rows - size;
   if (crows > 0) {
-    double* cb = stack + d.cb_off;
+    T* cb = stack + d.cb_off;
     for (int64_t e = tid; e < (int64_t)crows * d.ncb; e += nth) {
       const int i = (int)(e % crows), t = (int)(e / crows);
       cb[i + (int64_t)t * d.cb_ld] = front[(size + i) + (int64_t)(size + t) * rows];
@@ -303,8 +318,9 @@ __global__ void big_finalize_kernel(FrontDesc d, const double* front, const int*
 // ---- after the factorization -----------------------------------------------
 // Final position of every row, the row permutation, and the nonzero counts
 // of each column of L and U (exact zeros are not stored, as in the reference).
-__global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const int32_t* rowid, const double* L,
-                                        const double* U, const int32_t* struct_cols, int32_t* pos_of_row,
+template <typename T>
+__global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const int32_t* rowid, const T* L,
+                                        const T* U, const int32_t* struct_cols, int32_t* pos_of_row,
                                         int32_t* row_perm, int32_t* lcount, unsigned* ucount) {
   const int s = blockIdx.x;
   if (s >= ns) return;
@@ -315,14 +331,14 @@ __global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const i
     pos_of_row[r] = d.begin + k;
     row_perm[d.begin + k] = r;
   }
-  const double* lp = L + d.l_off;
+  const T* lp = L + d.l_off;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int jj = warp; jj < size; jj += nw) {
     int cl = 0, cu = 0;
     for (int i = lane; i < rows; i += 32) {
-      const double v = lp[i + (int64_t)jj * rows];
-      if (i > jj) cl += v != 0.0;
-      if (i < jj) cu += v != 0.0;
+      const T v = lp[i + (int64_t)jj * rows];
+      if (i > jj) cl += v != T(0);
+      if (i < jj) cu += v != T(0);
     }
     for (int off = 16; off > 0; off >>= 1) {
       cl += __shfl_xor_sync(0xffffffffu, cl, off);
@@ -333,10 +349,10 @@ __global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const i
       atomicAdd(&ucount[d.begin + jj], (unsigned)(cu + 1));
     }
   }
-  const double* up = U + d.u_off;
+  const T* up = U + d.u_off;
   for (int t = warp; t < d.ncb; t += nw) {
     int cu = 0;
-    for (int kk = lane; kk < size; kk += 32) cu += up[kk + (int64_t)t * size] != 0.0;
+    for (int kk = lane; kk < size; kk += 32) cu += up[kk + (int64_t)t * size] != T(0);
     for (int off = 16; off > 0; off >>= 1) cu += __shfl_xor_sync(0xffffffffu, cu, off);
     if (lane == 0 && cu) atomicAdd(&ucount[struct_cols[d.struct_begin + t]], (unsigned)cu);
   }
@@ -345,119 +361,268 @@ __global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const i
 // ---- solve ------------------------------------------------------------------
 constexpr int kSolveThreads = 256;
 
-__global__ void gather_rows_kernel(const double* b, const int32_t* row_perm, double* y, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = b[row_perm[i]];
+template <typename T>
+__global__ void gather_rows_kernel(const double* b, const int32_t* row_perm, T* y, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = (T)b[row_perm[i]];
 }
 
-__global__ void scatter_cols_kernel(const double* x, const int32_t* col_perm, double* b, int n) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) b[col_perm[j]] = x[j];
+template <typename T>
+__global__ void scatter_cols_kernel(const T* x, const int32_t* col_perm, double* b, int n) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) b[col_perm[j]] = (double)x[j];
 }
 
-constexpr int kRowChunk = 256;   // rows of L21 / U12 per CTA
-constexpr int kColChunk = 1024;  // columns of U12 per CTA
+constexpr int kRowChunk = 256;  // rows of L21 / U12 per CTA (one per thread)
+constexpr int kKChunk = 256;    // columns of L21 / U12 per CTA
+constexpr int kSolveBigSize = 512;  // larger diagonal blocks take the multi-CTA triangular sweep
 
-// Forward, diagonal block of each front of a level (one CTA per front):
-// unit-lower solve in 32-column blocks, a warp for the block, all threads
-// for the rows below it.
+// Forward, diagonal block of each front of a level (one CTA per front, for
+// fronts of at most kSolveBigSize columns by default): unit-lower solve in 32-column
+// blocks; the block's 32 x 32 triangle is staged in shared memory so the
+// warp's 32 dependent steps read no global memory, and the rows below it in
+// the diagonal block take the block's 32 terms with independent loads.
+template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) fwd_diag_kernel(const FrontDesc* fronts, const int32_t* level,
-                                                                 const double* L, double* y) {
+                                                                 const T* L, T* y) {
+  __shared__ T tri[32][33];
+  __shared__ T yb[32];
   const FrontDesc d = fronts[level[blockIdx.x]];
   const int rows = d.rows, m = d.size;
-  const double* lp = L + d.l_off;
-  double* ys = y + d.begin;
+  const T* lp = L + d.l_off;
+  T* ys = y + d.begin;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int kb = 0; kb < m; kb += 32) {
     const int w = min(32, m - kb);
+    for (int e = threadIdx.x; e < 32 * 32; e += kSolveThreads) {
+      const int r = e & 31, c = e >> 5;
+      tri[c][r] = (r < w && c < w && r > c) ? lp[(kb + r) + (int64_t)(kb + c) * rows] : T(0);
+    }
+    __syncthreads();
     if (warp == 0) {
-      double v = lane < w ? ys[kb + lane] : 0.0;
-      for (int k = 0; k < w; ++k) {
-        const double yk = __shfl_sync(0xffffffffu, v, k);
-        if (lane > k && lane < w) v -= lp[(kb + lane) + (int64_t)(kb + k) * rows] * yk;
+      T v = lane < w ? ys[kb + lane] : T(0);
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const T yk = __shfl_sync(0xffffffffu, v, k);
+        v -= tri[k][lane] * yk;  // zero on and above the diagonal and outside the block
       }
       if (lane < w) ys[kb + lane] = v;
+      yb[lane] = lane < w ? v : T(0);
     }
     __syncthreads();
     for (int i = kb + w + threadIdx.x; i < m; i += kSolveThreads) {
-      double acc = 0.0;
-      for (int k = 0; k < w; ++k) acc = fma(lp[i + (int64_t)(kb + k) * rows], ys[kb + k], acc);
+      const T* row = lp + i + (int64_t)kb * rows;
+      T acc = T(0);
+      if (w == 32) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc = fma_t(row[(int64_t)k * rows], yb[k], acc);
+      } else {
+        for (int k = 0; k < w; ++k) acc = fma_t(row[(int64_t)k * rows], yb[k], acc);
+      }
       ys[i] -= acc;
     }
     __syncthreads();
   }
 }
 
-// Forward, rows below the diagonal block: y[pos(row)] -= L21 y_s, a CTA per
-// chunk of rows (rows of different fronts of one level are distinct).
+// Forward, rows below the diagonal block: y[pos(row)] -= L21 y_s. A CTA per
+// (chunk of rows, chunk of columns); a front with one column chunk subtracts
+// directly (rows of different fronts of one level are distinct), otherwise
+// the chunks' partial sums are combined in a fixed order by fwd_finish_kernel.
+template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) fwd_l21_kernel(const FrontDesc* fronts, const SolveItem* items,
-                                                                const double* L, const int32_t* rowid,
-                                                                const int32_t* pos_of_row, double* y) {
+                                                                const T* L, const int32_t* rowid,
+                                                                const int32_t* pos_of_row, const int64_t* fpart_off,
+                                                                T* fpartial, T* y) {
   const SolveItem it = items[blockIdx.x];
   const FrontDesc d = fronts[it.front];
   const int i = d.size + it.chunk * kRowChunk + threadIdx.x;
   if (i >= d.rows) return;
-  const double* lp = L + d.l_off;
-  const double* ys = y + d.begin;
-  double acc = 0.0;
-  for (int k = 0; k < d.size; ++k) acc = fma(lp[i + (int64_t)k * d.rows], ys[k], acc);
+  const int k0 = it.tchunk * kKChunk, k1 = min(d.size, k0 + kKChunk);
+  const T* row = L + d.l_off + i;
+  const T* ys = y + d.begin;
+  T acc = T(0);
+  int k = k0;
+  for (; k + 8 <= k1; k += 8) {
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = row[(int64_t)(k + u) * d.rows];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = fma_t(v[u], ys[k + u], acc);
+  }
+  for (; k < k1; ++k) acc = fma_t(row[(int64_t)k * d.rows], ys[k], acc);
+  if (d.size <= kKChunk)
+    y[pos_of_row[rowid[d.rowid_off + i]]] -= acc;
+  else
+    fpartial[fpart_off[it.front] + (int64_t)it.tchunk * (d.rows - d.size) + (i - d.size)] = acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolveThreads) fwd_finish_kernel(const FrontDesc* fronts, const SolveItem* items,
+                                                                   const int32_t* rowid, const int32_t* pos_of_row,
+                                                                   const int64_t* fpart_off, const T* fpartial,
+                                                                   T* y) {
+  const SolveItem it = items[blockIdx.x];
+  const FrontDesc d = fronts[it.front];
+  const int i = d.size + it.chunk * kRowChunk + threadIdx.x;
+  if (i >= d.rows) return;
+  const int nk = (d.size + kKChunk - 1) / kKChunk;
+  const int64_t below = d.rows - d.size;
+  T acc = T(0);
+  for (int c = 0; c < nk; ++c) acc += fpartial[fpart_off[it.front] + c * below + (i - d.size)];
   y[pos_of_row[rowid[d.rowid_off + i]]] -= acc;
 }
 
 // Backward, U12 x[Struct(s)] in partial sums over column chunks (summed in a
-// fixed order by the diagonal kernel, so a solve is deterministic).
+// fixed order afterwards, so a solve is deterministic).
+template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) bwd_u12_kernel(const FrontDesc* fronts, const SolveItem* items,
-                                                                const double* U, const int32_t* struct_cols,
-                                                                const int64_t* part_off, const double* x,
-                                                                double* partial) {
+                                                                const T* U, const int32_t* struct_cols,
+                                                                const int64_t* part_off, const T* x,
+                                                                T* partial) {
   const SolveItem it = items[blockIdx.x];
   const FrontDesc d = fronts[it.front];
   const int kk = it.chunk * kRowChunk + threadIdx.x;
   if (kk >= d.size) return;
-  const double* up = U + d.u_off;
+  const T* up = U + d.u_off + kk;
   const int32_t* st = struct_cols + d.struct_begin;
-  const int t0 = it.tchunk * kColChunk, t1 = min(d.ncb, t0 + kColChunk);
-  double acc = 0.0;
-  for (int t = t0; t < t1; ++t) acc = fma(up[kk + (int64_t)t * d.size], x[st[t]], acc);
+  const int t0 = it.tchunk * kKChunk, t1 = min(d.ncb, t0 + kKChunk);
+  T acc = T(0);
+  int t = t0;
+  for (; t + 8 <= t1; t += 8) {
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = up[(int64_t)(t + u) * d.size];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = fma_t(v[u], x[st[t + u]], acc);
+  }
+  for (; t < t1; ++t) acc = fma_t(up[(int64_t)t * d.size], x[st[t]], acc);
   partial[part_off[it.front] + (int64_t)it.tchunk * d.size + kk] = acc;
 }
 
-// Backward, diagonal block (one CTA per front): subtract the U12 partial sums,
-// then the upper solve in 32-column blocks from the last, x_j times the
-// reciprocal of its diagonal as in the reference's upper sweep.
+// x_s -= (the U12 partial sums of front s), in chunk order
+template <typename T>
+__device__ __forceinline__ void subtract_partials(const FrontDesc& d, int64_t poff, const T* partial, T* xs) {
+  const int ntc = (d.ncb + kKChunk - 1) / kKChunk;
+  for (int kk = threadIdx.x; kk < d.size; kk += blockDim.x) {
+    T acc = T(0);
+    for (int tc = 0; tc < ntc; ++tc) acc += partial[poff + (int64_t)tc * d.size + kk];
+    xs[kk] -= acc;
+  }
+}
+
+// Backward, diagonal block (one CTA per front of at most kSolveBigSize
+// columns): subtract the U12 partial sums, then the upper solve in 32-column
+// blocks from the last, x_j times the reciprocal of its diagonal as in the
+// reference's upper sweep; the block's triangle is staged in shared memory.
+template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) bwd_diag_kernel(const FrontDesc* fronts, const int32_t* level,
-                                                                 const double* L, const int64_t* part_off,
-                                                                 const double* partial, double* x) {
+                                                                 const T* L, const int64_t* part_off,
+                                                                 const T* partial, T* x) {
+  __shared__ T tri[32][33];
+  __shared__ T xb[32];
   const int s = level[blockIdx.x];
   const FrontDesc d = fronts[s];
   const int rows = d.rows, m = d.size;
-  const double* lp = L + d.l_off;
-  double* xs = x + d.begin;
-  const int ntc = (d.ncb + kColChunk - 1) / kColChunk;
-  for (int kk = threadIdx.x; kk < m; kk += kSolveThreads) {
-    double acc = 0.0;
-    for (int tc = 0; tc < ntc; ++tc) acc += partial[part_off[s] + (int64_t)tc * m + kk];
-    xs[kk] -= acc;
-  }
+  const T* lp = L + d.l_off;
+  T* xs = x + d.begin;
+  subtract_partials(d, part_off[s], partial, xs);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int jb = m; jb > 0; jb -= 32) {
     const int j0 = max(0, jb - 32), w = jb - j0;
+    for (int e = threadIdx.x; e < 32 * 32; e += kSolveThreads) {
+      const int r = e & 31, c = e >> 5;
+      tri[c][r] = (r < w && c < w && r <= c) ? lp[(j0 + r) + (int64_t)(j0 + c) * rows] : T(0);
+    }
+    __syncthreads();
     if (warp == 0) {
-      double v = lane < w ? xs[j0 + lane] : 0.0;
+      T v = lane < w ? xs[j0 + lane] : T(0);
       for (int j = w - 1; j >= 0; --j) {
-        if (lane == j) v = v * (1.0 / lp[(j0 + j) + (int64_t)(j0 + j) * rows]);
-        const double xj = __shfl_sync(0xffffffffu, v, j);
-        if (lane < j) v -= lp[(j0 + lane) + (int64_t)(j0 + j) * rows] * xj;
+        if (lane == j) v = v * (T(1) / tri[j][j]);
+        const T xj = __shfl_sync(0xffffffffu, v, j);
+        if (lane < j) v -= tri[j][lane] * xj;
       }
       if (lane < w) xs[j0 + lane] = v;
+      xb[lane] = lane < w ? v : T(0);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < j0; i += kSolveThreads) {
-      double acc = 0.0;
-      for (int l = 0; l < w; ++l) acc = fma(lp[i + (int64_t)(j0 + l) * rows], xs[j0 + l], acc);
+      const T* row = lp + i + (int64_t)j0 * rows;
+      T acc = T(0);
+      if (w == 32) {
+#pragma unroll
+        for (int l = 0; l < 32; ++l) acc = fma_t(row[(int64_t)l * rows], xb[l], acc);
+      } else {
+        for (int l = 0; l < w; ++l) acc = fma_t(row[(int64_t)l * rows], xb[l], acc);
+      }
       xs[i] -= acc;
     }
     __syncthreads();
   }
+}
+
+// Backward, the U12 partial sums of one large front (its diagonal block is
+// then solved by the multi-CTA triangular solve).
+template <typename T>
+__global__ void __launch_bounds__(kSolveThreads) bwd_partials_kernel(const FrontDesc* fronts, int s,
+                                                                     const int64_t* part_off, const T* partial,
+                                                                     T* x) {
+  const FrontDesc d = fronts[s];
+  const int ntc = (d.ncb + kKChunk - 1) / kKChunk;
+  const int kk = blockIdx.x * kSolveThreads + threadIdx.x;
+  if (kk >= d.size) return;
+  T acc = T(0);
+  for (int tc = 0; tc < ntc; ++tc) acc += partial[part_off[s] + (int64_t)tc * d.size + kk];
+  x[d.begin + kk] -= acc;
+}
+
+// ---- the mixed form's refinement ---------------------------------------------
+// max that keeps a NaN (a diverged solve must not look converged)
+__device__ __forceinline__ double nanmax(double m, double v) { return (v != v || v > m) ? v : m; }
+
+// r = b - A x in FP64 (row by row, entries in column order) and the maxima
+// of |r|, |x| and |b| into norms[0..2] (atomic max on the bit patterns:
+// non-negative doubles order as integers and a NaN lies above all numbers)
+__global__ void residual_csr_kernel(int n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                                    const int64_t* __restrict__ map, const double* __restrict__ values,
+                                    const double* __restrict__ x, const double* __restrict__ b,
+                                    double* __restrict__ r, unsigned long long* norms) {
+  double mr = 0.0, mx = 0.0, mb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t q = ptr[i]; q < ptr[i + 1]; ++q) acc = __fma_rn(values[map[q]], x[col[q]], acc);
+    const double ri = b[i] - acc;
+    r[i] = ri;
+    mr = nanmax(mr, fabs(ri));
+    mx = nanmax(mx, fabs(x[i]));
+    mb = nanmax(mb, fabs(b[i]));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    mr = nanmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
+    mx = nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    mb = nanmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&norms[0], (unsigned long long)__double_as_longlong(mr));
+    atomicMax(&norms[1], (unsigned long long)__double_as_longlong(mx));
+    atomicMax(&norms[2], (unsigned long long)__double_as_longlong(mb));
+  }
+}
+
+// ||A||_inf into norms[3]
+__global__ void row_abs_sum_kernel(int n, const int64_t* __restrict__ ptr, const int64_t* __restrict__ map,
+                                   const double* __restrict__ values, unsigned long long* norms) {
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t q = ptr[i]; q < ptr[i + 1]; ++q) acc += fabs(values[map[q]]);
+    m = nanmax(m, acc);
+  }
+  for (int off = 16; off > 0; off >>= 1) m = nanmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(&norms[3], (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void axpy_kernel(const double* __restrict__ d, double* __restrict__ x, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += d[i];
 }
 
 template <typename T>
@@ -494,7 +659,6 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
   ALG_TRY(upload(F.anew_col, &d_anew_col));
   ALG_TRY(upload(F.new_rows, &d_new_rows));
   ALG_TRY(upload(F.small_level_fronts, &d_small_levels));
-  ALG_TRY(upload(F.solve_level_fronts, &d_solve_levels));
   ALG_TRY(upload(F.col_perm, &d_col_perm));
   const size_t n = (size_t)std::max<idx>(F.n, 1);
   ALG_TRY(dmalloc((void**)&d_values, sizeof(double) * std::max<idx>(F.nnz, 1)));
@@ -510,33 +674,62 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
   ALG_TRY(dmalloc((void**)&d_y, sizeof(double) * n));
   ALG_TRY(dmalloc((void**)&d_rhs, sizeof(double) * n));
   {
-    // solve work items per level and the U12 partial-sum offsets
-    std::vector<SolveItem> fwd, bwd;
-    std::vector<int64_t> poff(std::max<idx>(F.ns, 1), 0);
-    int64_t ptot = 0;
+    // solve schedule and the partial-sum offsets of the column chunks
+    std::vector<SolveItem> fwd, fin, bwd;
+    std::vector<int32_t> small_list;
+    std::vector<int64_t> poff(std::max<idx>(F.ns, 1), 0), fpoff(std::max<idx>(F.ns, 1), 0);
+    int64_t ptot = 0, fptot = 0;
+    int max_big = 0;
+    // fronts with more columns than this take the multi-CTA sweeps
+    // (ALG_SPLU_SOLVE_BIG overrides, for tests of that path on small grids)
+    int big_size = kSolveBigSize;
+    if (const char* e = std::getenv("ALG_SPLU_SOLVE_BIG")) big_size = std::max(32, std::atoi(e));
     for (idx s = 0; s < F.ns; ++s) {
       const FrontDesc& d = F.fronts[s];
       poff[s] = ptot;
-      ptot += (int64_t)((d.ncb + kColChunk - 1) / kColChunk) * d.size;
+      ptot += (int64_t)((d.ncb + kKChunk - 1) / kKChunk) * d.size;
+      fpoff[s] = fptot;
+      if (d.size > kKChunk) fptot += (int64_t)((d.size + kKChunk - 1) / kKChunk) * (d.rows - d.size);
     }
     const int nl = (int)F.solve_level_ptr.size() - 1;
     fwd_item_ptr.assign(std::max(nl, 0) + 1, 0);
+    fin_item_ptr.assign(std::max(nl, 0) + 1, 0);
     bwd_item_ptr.assign(std::max(nl, 0) + 1, 0);
+    solve_small_ptr.assign(std::max(nl, 0) + 1, 0);
+    solve_big.assign(std::max(nl, 0), {});
     for (int h = 0; h < nl; ++h) {
       for (int t = F.solve_level_ptr[h]; t < F.solve_level_ptr[h + 1]; ++t) {
         const int s = F.solve_level_fronts[t];
         const FrontDesc& d = F.fronts[s];
-        for (int c = 0; c * kRowChunk < d.rows - d.size; ++c) fwd.push_back(SolveItem{s, c, 0, 0});
+        if (d.size > big_size) {
+          solve_big[h].push_back(s);
+          max_big = std::max(max_big, (int)d.size);
+        } else {
+          small_list.push_back(s);
+        }
+        const int nk = (d.size + kKChunk - 1) / kKChunk;
+        for (int c = 0; c * kRowChunk < d.rows - d.size; ++c) {
+          for (int kc = 0; kc < nk; ++kc) fwd.push_back(SolveItem{s, c, kc, 0});
+          if (nk > 1) fin.push_back(SolveItem{s, c, 0, 0});
+        }
         for (int c = 0; c * kRowChunk < d.size; ++c)
-          for (int tc = 0; tc * kColChunk < d.ncb; ++tc) bwd.push_back(SolveItem{s, c, tc, 0});
+          for (int tc = 0; tc * kKChunk < d.ncb; ++tc) bwd.push_back(SolveItem{s, c, tc, 0});
       }
+      solve_small_ptr[h + 1] = (int)small_list.size();
       fwd_item_ptr[h + 1] = (int)fwd.size();
+      fin_item_ptr[h + 1] = (int)fin.size();
       bwd_item_ptr[h + 1] = (int)bwd.size();
     }
+    ALG_TRY(upload(small_list, &d_solve_small));
     ALG_TRY(upload(fwd, &d_fwd_items));
+    ALG_TRY(upload(fin, &d_fin_items));
     ALG_TRY(upload(bwd, &d_bwd_items));
     ALG_TRY(upload(poff, &d_part_off));
+    ALG_TRY(upload(fpoff, &d_fpart_off));
     ALG_TRY(dmalloc((void**)&d_partial, sizeof(double) * std::max<int64_t>(ptot, 1)));
+    ALG_TRY(dmalloc((void**)&d_fpartial, sizeof(double) * std::max<int64_t>(fptot, 1)));
+    tflag_count = max_big / 64 + 2;
+    ALG_TRY(dmalloc((void**)&d_tflags, sizeof(int) * (tflag_count + 1)));
   }
   for (int b = 0; b < 2; ++b) {
     ALG_TRY(dmalloc((void**)&fac[b].L, sizeof(double) * F.l_total));
@@ -550,32 +743,70 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
   return ALG_OK;
 }
 
+int DeviceLu::ensure_refine_buffers() {
+  if (d_csr_ptr != nullptr) return ALG_OK;
+  const FrontPlan& F = *plan;
+  const size_t n = (size_t)std::max<idx>(F.n, 1);
+  ALG_TRY(upload(F.csr_ptr, &d_csr_ptr));
+  ALG_TRY(upload(F.csr_col, &d_csr_col));
+  ALG_TRY(upload(F.csr_map, &d_csr_map));
+  ALG_TRY(dmalloc((void**)&d_b0, sizeof(double) * n));
+  ALG_TRY(dmalloc((void**)&d_x, sizeof(double) * n));
+  ALG_TRY(dmalloc((void**)&d_norms, sizeof(unsigned long long) * 4));
+  for (auto& f : fac) ALG_TRY(dmalloc((void**)&f.values, sizeof(double) * std::max<idx>(F.nnz, 1)));
+  return ALG_OK;
+}
+
 void DeviceLu::release() {
   for (void* q : {(void*)d_fronts, (void*)d_child_idx, (void*)d_child_slot, (void*)d_struct_cols,
                   (void*)d_cb_colmap, (void*)d_anew_q, (void*)d_anew_slot, (void*)d_anew_col, (void*)d_new_rows,
-                  (void*)d_small_levels, (void*)d_solve_levels, (void*)d_col_perm, (void*)d_values,
-                  (void*)d_block, (void*)d_stack, (void*)d_front, (void*)d_ipiv, (void*)d_perm, (void*)d_rowtmp,
-                  (void*)d_flag, (void*)d_y, (void*)d_rhs, (void*)d_fwd_items, (void*)d_bwd_items,
-                  (void*)d_part_off, (void*)d_partial})
+                  (void*)d_small_levels, (void*)d_col_perm, (void*)d_values, (void*)d_block, (void*)d_stack,
+                  (void*)d_front, (void*)d_ipiv, (void*)d_perm, (void*)d_rowtmp, (void*)d_flag, (void*)d_y,
+                  (void*)d_rhs, (void*)d_solve_small, (void*)d_fwd_items, (void*)d_fin_items, (void*)d_bwd_items,
+                  (void*)d_part_off, (void*)d_fpart_off, (void*)d_partial, (void*)d_fpartial, (void*)d_tflags,
+                  (void*)d_csr_ptr, (void*)d_csr_col, (void*)d_csr_map, (void*)d_b0, (void*)d_x, (void*)d_norms})
     if (q) cudaFree(q);
   for (auto& f : fac)
-    for (void* q : {(void*)f.L, (void*)f.U, (void*)f.rowid, (void*)f.pos_of_row, (void*)f.row_perm,
-                    (void*)f.lcount, (void*)f.ucount})
+    for (void* q : {(void*)f.values, (void*)f.L, (void*)f.U, (void*)f.rowid, (void*)f.pos_of_row,
+                    (void*)f.row_perm, (void*)f.lcount, (void*)f.ucount})
       if (q) cudaFree(q);
   *this = DeviceLu();
 }
 
-// Factors the values in d_values into factor set `b`. Stream-ordered; the
-// singular flag and the dense status block are read by the caller.
 int DeviceLu::factor(int b) {
+  if (prec < 0) return factor_t<double>(b, d_values, -1);
+  ALG_TRY(ensure_refine_buffers());
+  const FrontPlan& F = *plan;
+  cudaStream_t st = ctx->stream;
+  // the refinement's A and its norm belong to the factor set
+  ALG_CUDA_TRY(cudaMemcpyAsync(fac[b].values, d_values, sizeof(double) * std::max<idx>(F.nnz, 1),
+                               cudaMemcpyDeviceToDevice, st));
+  ALG_CUDA_TRY(cudaMemsetAsync(d_norms + 3, 0, sizeof(unsigned long long), st));
+  row_abs_sum_kernel<<<grid_for(ctx, F.n, 256), 256, 0, st>>>((int)F.n, d_csr_ptr, d_csr_map, fac[b].values,
+                                                               d_norms);
+  count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  return factor_t<float>(b, d_values, prec == ALG_PREC_FP32 ? -1 : prec);
+}
+
+// Factors `values` into factor set `b` in precision T. Stream-ordered; the
+// singular flag and the dense status block are read by finish().
+template <typename T>
+int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   const FrontPlan& F = *plan;
   Factors& out = fac[b];
+  out.prec = std::is_same<T, double>::value ? -1 : (tc_prec < 0 ? ALG_PREC_FP32 : tc_prec);
   cudaStream_t st = ctx->stream;
+  T* block = reinterpret_cast<T*>(d_block);
+  T* stack = reinterpret_cast<T*>(d_stack);
+  T* front = reinterpret_cast<T*>(d_front);
+  T* L = reinterpret_cast<T*>(out.L);
+  T* U = reinterpret_cast<T*>(out.U);
   const int tok = prof_begin(ctx, ALG_K_SPARSE);
   ALG_CUDA_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int) * 4, st));
   ALG_TRY(status_reset(ctx));
   // small fronts, one launch per level
-  SmallArgs sa;
+  SmallArgs<T> sa;
   sa.fronts = d_fronts;
   sa.child_idx = d_child_idx;
   sa.child_slot = d_child_slot;
@@ -584,10 +815,10 @@ int DeviceLu::factor(int b) {
   sa.anew_slot = d_anew_slot;
   sa.anew_col = d_anew_col;
   sa.new_rows = d_new_rows;
-  sa.values = d_values;
-  sa.block = d_block;
-  sa.L = out.L;
-  sa.U = out.U;
+  sa.values = values;
+  sa.block = block;
+  sa.L = L;
+  sa.U = U;
   sa.rowid = out.rowid;
   sa.singular = d_flag;
   const int tok_small = prof_begin(ctx, ALG_K_BATCH);
@@ -595,7 +826,7 @@ int DeviceLu::factor(int b) {
     const int cnt = F.small_level_ptr[h + 1] - F.small_level_ptr[h];
     if (cnt == 0) continue;
     sa.level_fronts = d_small_levels + F.small_level_ptr[h];
-    small_front_kernel<<<cnt, kSmallThreads, 0, st>>>(sa);
+    small_front_kernel<T><<<cnt, kSmallThreads, 0, st>>>(sa);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
@@ -604,11 +835,12 @@ int DeviceLu::factor(int b) {
   LuPlan lp;
   lp.nb = 64;
   lp.nbl = 16;
+  lp.tc_prec = tc_prec;
   for (int32_t s : F.big_order) {
     const FrontDesc& d = F.fronts[s];
     const int cols = d.size + d.ncb;
-    ALG_CUDA_TRY(cudaMemsetAsync(d_front, 0, sizeof(double) * (size_t)d.rows * cols, st));
-    BigArgs ba;
+    ALG_CUDA_TRY(cudaMemsetAsync(front, 0, sizeof(T) * (size_t)d.rows * cols, st));
+    BigArgs<T> ba;
     ba.d = d;
     ba.fronts = d_fronts;
     ba.child_idx = d_child_idx;
@@ -618,10 +850,10 @@ int DeviceLu::factor(int b) {
     ba.anew_slot = d_anew_slot;
     ba.anew_col = d_anew_col;
     ba.new_rows = d_new_rows;
-    ba.values = d_values;
-    ba.block = d_block;
-    ba.stack = d_stack;
-    ba.front = d_front;
+    ba.values = values;
+    ba.block = block;
+    ba.stack = stack;
+    ba.front = front;
     ba.rowid = out.rowid;
     ba.rowtmp = d_rowtmp;
     int64_t work = (int64_t)(d.anew_end - d.anew_begin) + d.rows;
@@ -629,23 +861,21 @@ int DeviceLu::factor(int b) {
       const FrontDesc& c = F.fronts[F.child_idx[k]];
       work = std::max<int64_t>(work, (int64_t)(c.rows - c.size) * c.ncb);
     }
-    big_assemble_kernel<<<grid_for(ctx, work, 256), 256, 0, st>>>(ba);
+    big_assemble_kernel<T><<<grid_for(ctx, work, 256), 256, 0, st>>>(ba);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
-    ALG_TRY((lu_factor_partial_dev<double, false>(ctx, d_front, d.rows, d.size, cols, d.rows, d_ipiv, d_perm, lp)));
-    ALG_CUDA_TRY(cudaMemcpyAsync(out.L + d.l_off, d_front, sizeof(double) * (size_t)d.rows * d.size,
-                                 cudaMemcpyDeviceToDevice, st));
+    ALG_TRY((lu_factor_partial_dev<T, false>(ctx, front, d.rows, d.size, cols, d.rows, d_ipiv, d_perm, lp)));
+    ALG_CUDA_TRY(cudaMemcpyAsync(L + d.l_off, front, sizeof(T) * (size_t)d.rows * d.size, cudaMemcpyDeviceToDevice,
+                                 st));
     const int64_t fw = std::max<int64_t>((int64_t)d.rows, (int64_t)d.rows * d.ncb);
-    big_finalize_kernel<<<grid_for(ctx, fw, 256), 256, 0, st>>>(d, d_front, d_perm, d_rowtmp, out.rowid, out.U,
-                                                                 d_stack);
+    big_finalize_kernel<T><<<grid_for(ctx, fw, 256), 256, 0, st>>>(d, front, d_perm, d_rowtmp, out.rowid, U, stack);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
   ALG_CUDA_TRY(cudaMemsetAsync(out.ucount, 0, sizeof(unsigned) * std::max<idx>(F.n, 1), st));
   if (F.ns > 0) {
-    positions_counts_kernel<<<(int)F.ns, 256, 0, st>>>(d_fronts, (int)F.ns, out.rowid, out.L, out.U,
-                                                        d_struct_cols, out.pos_of_row, out.row_perm, out.lcount,
-                                                        out.ucount);
+    positions_counts_kernel<T><<<(int)F.ns, 256, 0, st>>>(d_fronts, (int)F.ns, out.rowid, L, U, d_struct_cols,
+                                                           out.pos_of_row, out.row_perm, out.lcount, out.ucount);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
@@ -654,13 +884,24 @@ int DeviceLu::factor(int b) {
 }
 
 // Reads the factorization's outcome (synchronises): SP_OK or SP_SINGULAR.
+// The mixed form refactors in FP64 when its FP32 factorization met a zero
+// pivot (an FP32 underflow need not be a singular A).
 int DeviceLu::finish(int b, Stats* stats) {
   const FrontPlan& F = *plan;
   int h_flag[4] = {0, 0, 0, 0};
   ALG_CUDA_TRY(cudaMemcpyAsync(h_flag, d_flag, sizeof(h_flag), cudaMemcpyDeviceToHost, ctx->stream));
   ALG_TRY(status_fetch(ctx));
-  if (h_flag[0] != 0 || ctx->h_status->singular_col != INT_MAX) return SP_SINGULAR;
   if (ctx->h_status->timeout) return ALG_TIMEOUT;
+  if (h_flag[0] != 0 || ctx->h_status->singular_col != INT_MAX) {
+    if (fac[b].prec < 0) return SP_SINGULAR;
+    ALG_TRY(refactor_fp64(b));
+    return finish(b, stats);
+  }
+  if (fac[b].prec >= 0) {
+    unsigned long long bits = 0;
+    ALG_CUDA_TRY(cudaMemcpy(&bits, d_norms + 3, sizeof(bits), cudaMemcpyDeviceToHost));
+    std::memcpy(&fac[b].anorm, &bits, sizeof(double));
+  }
   if (stats) {
     const size_t n = (size_t)F.n;
     std::vector<int32_t> lc(n);
@@ -682,48 +923,149 @@ int DeviceLu::finish(int b, Stats* stats) {
   return SP_OK;
 }
 
-// x = A^-1 b for the factors of set `b`, with b (n) already on the device in
-// d_rhs; the result lands in d_rhs. Stream-ordered.
-int DeviceLu::solve(int b) {
+// The set's own values in FP64 (the mixed form's last resort).
+int DeviceLu::refactor_fp64(int b) {
+  return factor_t<double>(b, fac[b].values, -1);
+}
+
+// d_rhs <- (the set's LU)^-1 d_rhs in the set's precision. Stream-ordered.
+template <typename T>
+int DeviceLu::sweep_t(int b) {
   const FrontPlan& F = *plan;
   const Factors& f = fac[b];
+  const T* L = reinterpret_cast<const T*>(f.L);
+  const T* U = reinterpret_cast<const T*>(f.U);
+  T* y = reinterpret_cast<T*>(d_y);
+  T* partial = reinterpret_cast<T*>(d_partial);
+  T* fpartial = reinterpret_cast<T*>(d_fpartial);
+  int* abort_flag = d_tflags + tflag_count;
   cudaStream_t st = ctx->stream;
   const int n = (int)F.n;
-  if (n == 0) return ALG_OK;
   const int tok = prof_begin(ctx, ALG_K_SOLVE);
-  gather_rows_kernel<<<grid_for(ctx, n, 256), 256, 0, st>>>(d_rhs, f.row_perm, d_y, n);
+  gather_rows_kernel<T><<<grid_for(ctx, n, 256), 256, 0, st>>>(d_rhs, f.row_perm, y, n);
   count_launches();
+  ALG_CUDA_TRY(cudaMemsetAsync(abort_flag, 0, sizeof(int), st));
   const int nl = (int)F.solve_level_ptr.size() - 1;
   for (int h = 0; h < nl; ++h) {
-    const int cnt = F.solve_level_ptr[h + 1] - F.solve_level_ptr[h];
-    if (cnt == 0) continue;
-    fwd_diag_kernel<<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_levels + F.solve_level_ptr[h], f.L, d_y);
-    count_launches();
+    const int cnt = solve_small_ptr[h + 1] - solve_small_ptr[h];
+    if (cnt > 0) {
+      fwd_diag_kernel<T><<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_small + solve_small_ptr[h], L, y);
+      count_launches();
+    }
+    for (int32_t s : solve_big[h]) {
+      const FrontDesc& d = F.fronts[s];
+      ALG_TRY(tri_solve_dev<T>(ctx, L + d.l_off, d.rows, d.size, y + d.begin, false, d_tflags, abort_flag));
+    }
     const int ni = fwd_item_ptr[h + 1] - fwd_item_ptr[h];
     if (ni > 0) {
-      fwd_l21_kernel<<<ni, kSolveThreads, 0, st>>>(d_fronts, d_fwd_items + fwd_item_ptr[h], f.L, f.rowid,
-                                                   f.pos_of_row, d_y);
+      fwd_l21_kernel<T><<<ni, kSolveThreads, 0, st>>>(d_fronts, d_fwd_items + fwd_item_ptr[h], L, f.rowid,
+                                                      f.pos_of_row, d_fpart_off, fpartial, y);
+      count_launches();
+    }
+    const int nf = fin_item_ptr[h + 1] - fin_item_ptr[h];
+    if (nf > 0) {
+      fwd_finish_kernel<T><<<nf, kSolveThreads, 0, st>>>(d_fronts, d_fin_items + fin_item_ptr[h], f.rowid,
+                                                         f.pos_of_row, d_fpart_off, fpartial, y);
       count_launches();
     }
   }
   for (int h = nl - 1; h >= 0; --h) {
-    const int cnt = F.solve_level_ptr[h + 1] - F.solve_level_ptr[h];
-    if (cnt == 0) continue;
     const int ni = bwd_item_ptr[h + 1] - bwd_item_ptr[h];
     if (ni > 0) {
-      bwd_u12_kernel<<<ni, kSolveThreads, 0, st>>>(d_fronts, d_bwd_items + bwd_item_ptr[h], f.U, d_struct_cols,
-                                                   d_part_off, d_y, d_partial);
+      bwd_u12_kernel<T><<<ni, kSolveThreads, 0, st>>>(d_fronts, d_bwd_items + bwd_item_ptr[h], U, d_struct_cols,
+                                                      d_part_off, y, partial);
       count_launches();
     }
-    bwd_diag_kernel<<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_levels + F.solve_level_ptr[h], f.L,
-                                                    d_part_off, d_partial, d_y);
-    count_launches();
+    const int cnt = solve_small_ptr[h + 1] - solve_small_ptr[h];
+    if (cnt > 0) {
+      bwd_diag_kernel<T><<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_small + solve_small_ptr[h], L,
+                                                        d_part_off, partial, y);
+      count_launches();
+    }
+    for (int32_t s : solve_big[h]) {
+      const FrontDesc& d = F.fronts[s];
+      if (d.ncb > 0) {
+        bwd_partials_kernel<T><<<(d.size + kSolveThreads - 1) / kSolveThreads, kSolveThreads, 0, st>>>(
+            d_fronts, s, d_part_off, partial, y);
+        count_launches();
+      }
+      ALG_TRY(tri_solve_dev<T>(ctx, L + d.l_off, d.rows, d.size, y + d.begin, true, d_tflags, abort_flag));
+    }
   }
-  scatter_cols_kernel<<<grid_for(ctx, n, 256), 256, 0, st>>>(d_y, d_col_perm, d_rhs, n);
+  scatter_cols_kernel<T><<<grid_for(ctx, n, 256), 256, 0, st>>>(y, d_col_perm, d_rhs, n);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
-  prof_end(ctx, tok, 4.0 * (double)(F.l_total + F.u_total), 8.0 * (double)(F.l_total + F.u_total));
+  prof_end(ctx, tok, 4.0 * (double)(F.l_total + F.u_total), sizeof(T) * (double)(F.l_total + F.u_total));
   return ALG_OK;
+}
+
+// x = A^-1 b for the factors of set `b`, with b (n) already on the device in
+// d_rhs; the result lands in d_rhs.
+int DeviceLu::solve(int b) {
+  const FrontPlan& F = *plan;
+  if (F.n == 0) return ALG_OK;
+  last = RefineReport();
+  last.precision = fac[b].prec;
+  if (fac[b].prec < 0) return sweep_t<double>(b);
+  return refine(b);
+}
+
+// The mixed form: x_0 = 0, r_0 = b; x += LU32^-1 r, r = b - A x (FP64)
+// until ||r||_inf <= tol (||A||_inf ||x||_inf + ||b||_inf); a stall (less
+// than a halving twice running), divergence or max_ir steps refactor the set
+// in FP64 and solve directly.
+int DeviceLu::refine(int b) {
+  const FrontPlan& F = *plan;
+  const int n = (int)F.n;
+  cudaStream_t st = ctx->stream;
+  const double target = tol > 0 ? tol : 10.0 * (double)n * std::ldexp(1.0, -53);
+  const int steps = max_ir > 0 ? max_ir : 10;
+  const int g = grid_for(ctx, n, 256);
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_b0, d_rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  ALG_CUDA_TRY(cudaMemsetAsync(d_x, 0, sizeof(double) * n, st));
+  double prev = INFINITY;
+  int stall = 0;
+  for (int it = 0; it < steps; ++it) {
+    ALG_TRY(sweep_t<float>(b));  // d_rhs: r -> the correction
+    axpy_kernel<<<g, 256, 0, st>>>(d_rhs, d_x, n);
+    count_launches();
+    ALG_CUDA_TRY(cudaMemsetAsync(d_norms, 0, sizeof(unsigned long long) * 3, st));
+    residual_csr_kernel<<<g, 256, 0, st>>>(n, d_csr_ptr, d_csr_col, d_csr_map, fac[b].values, d_x, d_b0, d_rhs,
+                                           d_norms);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+    unsigned long long bits[3];
+    ALG_CUDA_TRY(cudaMemcpyAsync(bits, d_norms, sizeof(bits), cudaMemcpyDeviceToHost, st));
+    ALG_CUDA_TRY(cudaStreamSynchronize(st));
+    double nr, nx, nb;
+    std::memcpy(&nr, &bits[0], sizeof(double));
+    std::memcpy(&nx, &bits[1], sizeof(double));
+    std::memcpy(&nb, &bits[2], sizeof(double));
+    const double den = fac[b].anorm * nx + nb;
+    const double eta = den == 0.0 ? nr : nr / den;
+    last.iterations = it + 1;
+    last.backward_error = eta;
+    if (!(eta == eta) || std::isinf(eta)) break;
+    if (eta <= target) {
+      ALG_CUDA_TRY(cudaMemcpyAsync(d_rhs, d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      return ALG_OK;
+    }
+    if (eta > 0.5 * prev) {
+      if (++stall >= 2) break;
+    } else {
+      stall = 0;
+    }
+    prev = eta;
+  }
+  // FP64 refactorization of this set's values, then a direct solve
+  ALG_TRY(refactor_fp64(b));
+  const int rc = finish(b, nullptr);
+  if (rc != SP_OK) return rc;
+  last.fell_back = 1;
+  last.precision = -1;
+  last.backward_error = -1.0;
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_rhs, d_b0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  return sweep_t<double>(b);
 }
 
 }  // namespace sp

@@ -265,24 +265,49 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
            F.small_level_ptr[F.small_level_ptr.size() - 1] == F.small_level_ptr[F.small_level_ptr.size() - 2])
       F.small_level_ptr.pop_back();
   }
+  // A by rows (for the mixed form's FP64 residual): entries of each row in
+  // column order, with their CSC index
+  {
+    F.csr_ptr.assign(n + 1, 0);
+    for (idx q = 0; q < nnz; ++q) F.csr_ptr[p.row_idx[q] + 1] += 1;
+    for (idx i = 0; i < n; ++i) F.csr_ptr[i + 1] += F.csr_ptr[i];
+    F.csr_col.assign(nnz, 0);
+    F.csr_map.assign(nnz, 0);
+    std::vector<int64_t> next(F.csr_ptr.begin(), F.csr_ptr.end() - 1);
+    for (idx j = 0; j < n; ++j)
+      for (size_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
+        const int64_t at = next[p.row_idx[q]]++;
+        F.csr_col[at] = (int32_t)j;
+        F.csr_map[at] = (int64_t)q;
+      }
+  }
   return SP_OK;
 }
 
 
-// Merges chains of only-children into their parents when the merged front's
-// flops stay within (1 + tol) of the two separate fronts': a chain step no
-// longer copies its whole contribution block into the next front. The merged
-// front of a child c and its parent s has size_c + size_s columns,
-// rows_s + size_c rows and the parent's Struct (c's Struct outside s's
-// columns is contained in s's). Pivots do not depend on the partition.
+// Merges a front's last child (the one just before it in postorder, so the
+// merged columns stay contiguous) into it when the merged front's flops stay
+// within (1 + tol) of the two separate fronts', or, for two large fronts,
+// when the extra flops cost less than the child's contribution-block traffic
+// and launch chain: a merged step no longer copies the whole contribution
+// block into the next front. The merged front of a child c and its parent s
+// has size_c + size_s columns, rows_s + size_c rows and the parent's Struct
+// (c's Struct outside s's columns is contained in s's); the parent's other
+// children become the merged front's children (their rows are zero in c's
+// columns, as they are sibling subtrees of c). Pivots do not depend on the
+// partition.
+// Break-even of merging a chain child into its parent: FP64 tensor-core
+// flops per HBM byte of the dense updates (about 15 TFLOP/s against 3 TB/s
+// of effective front traffic), and the flops one front's launch chain
+// (panels, TRSM, assembly, about 50 us) is worth.
+constexpr double kFlopsPerByte = 5.0;
+constexpr double kFrontOverheadFlops = 7.5e8;
+
 void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std::vector<idx>* ptr_out) {
   const idx ns = F.ns;
   auto flops = [](double m, double k, double c) {
     return 2.0 * k * k * m - 2.0 / 3.0 * k * k * k + k * k * c + 2.0 * (m - k) * c * k;
   };
-  std::vector<int32_t> nkid(ns, 0);
-  for (idx s = 0; s < ns; ++s)
-    if (S.super_etree[s] >= 0) nkid[S.super_etree[s]] += 1;
   std::vector<double> gm(ns), gk(ns), gc(ns);
   std::vector<char> into_next(ns, 0);
   for (idx s = 0; s < ns; ++s) {
@@ -290,10 +315,20 @@ void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std:
     gm[s] = d.rows;
     gk[s] = d.size;
     gc[s] = d.ncb;
-    if (s > 0 && nkid[s] == 1 && S.super_etree[s - 1] == s) {
+    if (s > 0 && S.super_etree[s - 1] == s) {  // s - 1 is s's last child (postorder)
       const double m2 = d.rows + gk[s - 1], k2 = d.size + gk[s - 1], c2 = d.ncb;
       const double sep = flops(gm[s - 1], gk[s - 1], gc[s - 1]) + flops(d.rows, d.size, d.ncb);
-      if (flops(m2, k2, c2) <= (1.0 + tol) * sep) {
+      // a separate child front costs its contribution block's HBM traffic
+      // (written after its update, read back by the parent's assembly, about
+      // three passes) and a fixed launch chain; merged, those extra flops
+      // run inside the parent's updates instead
+      // (only between large fronts: a small front's columns stay in the
+      // batched kernel, off the large fronts' column-serial panel chain)
+      const double cb_bytes = 24.0 * (gm[s - 1] - gk[s - 1]) * gc[s - 1];
+      const double saved = kFlopsPerByte * cb_bytes + kFrontOverheadFlops;
+      const double merged = flops(m2, k2, c2);
+      const bool both_large = !F.fronts[s - 1].small && !d.small;
+      if (merged <= (1.0 + tol) * sep || (both_large && merged - sep <= saved)) {
         into_next[s - 1] = 1;
         gm[s] = m2;
         gk[s] = k2;

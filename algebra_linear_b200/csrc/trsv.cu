@@ -314,6 +314,18 @@ int lu_solve_dataflow_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* 
   return ALG_OK;
 }
 
+// One triangular sweep (non-exact arithmetic) over the leading n x n block
+// of column-major factors: unit-lower (upper = false) or upper. flags holds
+// n / 64 + 1 ints (cleared here); abort_flag must be zero.
+template <typename T>
+int tri_solve_dev(alg_ctx* ctx, const T* lu, int lda, int n, T* x, bool upper, int* flags, int* abort_flag) {
+  if (n <= 0) return ALG_OK;
+  if (upper) return launch_trsv<T, false, true>(ctx, lu, lda, n, x, n, 1, flags, abort_flag);
+  return launch_trsv<T, false, false>(ctx, lu, lda, n, x, n, 1, flags, abort_flag);
+}
+
+template int tri_solve_dev<double>(alg_ctx*, const double*, int, int, double*, bool, int*, int*);
+template int tri_solve_dev<float>(alg_ctx*, const float*, int, int, float*, bool, int*, int*);
 template int lu_solve_dataflow_dev<double, true>(alg_ctx*, const double*, int, int, const int*, double*, int, int);
 template int lu_solve_dataflow_dev<double, false>(alg_ctx*, const double*, int, int, const int*, double*, int, int);
 template int lu_solve_dataflow_dev<float, false>(alg_ctx*, const float*, int, int, const int*, float*, int, int);

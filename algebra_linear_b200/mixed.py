@@ -13,7 +13,7 @@ import ctypes as C
 from . import _lib
 from .lapack import LapackError, _KINDS
 
-PRECISIONS = {"fp32": 0, "tf32": 1, "bf16": 2}
+PRECISIONS = {"fp32": 0, "tf32": 1, "bf16": 2, "tf32x3": 3}
 PATHS = {1: "ir", 2: "gmres", 3: "fp64"}
 
 

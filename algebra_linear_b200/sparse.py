@@ -89,6 +89,16 @@ class _Plan(C.Structure):
                 ("structurally_singular", C.c_int)]
 
 
+class _Refine(C.Structure):
+    _fields_ = [("precision", C.c_int), ("iterations", C.c_int), ("fell_back", C.c_int),
+                ("factor_precision", C.c_int), ("backward_error", C.c_double)]
+
+
+# precisions of the factors (no counterpart in the reference, which is FP64 only)
+PRECISIONS = {"fp64": -1, "fp32": 0, "tf32": 1, "bf16": 2, "tf32x3": 3}
+_PREC_NAMES = {v: k for k, v in PRECISIONS.items()}
+
+
 def _idx(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint64)
 
@@ -163,6 +173,21 @@ class SparseLu:
         p = _Plan()
         _check(self._lib.alg_splu_plan_info(self._h, C.byref(p)))
         return {f: getattr(p, f) for f, _ in _Plan._fields_}
+
+    # ---- mixed precision (no reference counterpart) ----------------------------
+    def set_precision(self, precision: str = "fp64", tol: float = 0.0, max_ir: int = 0) -> None:
+        """Precision of the next factorizations: "fp64" (the reference's
+        arithmetic), or "fp32" / "tf32" / "tf32x3" / "bf16" fronts with every solve
+        refined in FP64 to the backward error tol (<= 0: 10 n 2^-53), else
+        the factors are recomputed in FP64."""
+        _check(self._lib.alg_splu_set_precision(self._h, PRECISIONS[precision], float(tol), int(max_ir)))
+
+    def last_solve(self) -> dict:
+        r = _Refine()
+        _check(self._lib.alg_splu_last_solve(self._h, C.byref(r)))
+        return {"precision": _PREC_NAMES[r.precision], "iterations": r.iterations, "fell_back": bool(r.fell_back),
+                "factor_precision": _PREC_NAMES[r.factor_precision],
+                "backward_error": r.backward_error if r.backward_error >= 0 else None}
 
     # ---- device-resident ------------------------------------------------------
     def bind(self, ctx) -> None:

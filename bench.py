@@ -69,6 +69,8 @@ def parse_args():
     ap.add_argument("--grid", type=int, default=48, help="sparse: grid points per side")
     ap.add_argument("--grid-nz", type=int, default=0, help="sparse: points along z (0: = grid; 1: 2-D)")
     ap.add_argument("--cpu-grid", type=int, default=16, help="sparse: grid side of the CPU-baseline sample")
+    ap.add_argument("--sparse-precision", choices=["fp64", "fp32", "tf32", "tf32x3", "bf16"], default="fp64",
+                    help="sparse: front precision (fp64 = the reference's arithmetic; others refine in FP64)")
     ap.add_argument("--requests", type=int, default=10000, help="serve: requests per rate")
     ap.add_argument("--rates", default="100,200,400", help="serve: Poisson arrival rates (requests/s)")
     ap.add_argument("--workers", type=int, default=4, help="serve: worker streams")
@@ -170,7 +172,7 @@ def form_registry():
     try:
         from algebra_linear_b200 import mixed  # noqa: F401
 
-        for prec in ("fp32", "tf32", "bf16"):
+        for prec in ("fp32", "tf32", "tf32x3", "bf16"):
             forms[f"mixed_{prec}"] = (False, (lambda p: lambda ctx, A, b, n, nrhs: mixed.dgesv_mixed_dev(
                 ctx, A, b, n, nrhs, precision=p))(prec))
     except ImportError:
@@ -452,6 +454,7 @@ def run_sparse(args, world, rank, local, pg):
     t0 = time.perf_counter()
     lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
     analyze_s = time.perf_counter() - t0
+    lu.set_precision(args.sparse_precision)
     lu.bind(ctx)
     b0 = torch.ones(n, dtype=torch.float64, device="cuda")
     b = b0.clone()
@@ -488,6 +491,7 @@ def run_sparse(args, world, rank, local, pg):
         ms = float(t.item())
     st = lu.stats()
     plan = lu.plan()
+    refine = lu.last_solve()
     # normwise backward error of the last round (host check)
     import scipy.sparse as sps
 
@@ -516,12 +520,14 @@ def run_sparse(args, world, rank, local, pg):
         "metric": "sparse LU refactorize+solve GFLOP/s (reference flop estimate); rounds/s",
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per_round, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": f"synthetic: convection-diffusion stencil, U(0,1) from the DLARNV stream seed {seed}",
+        "dtype": "f64" if args.sparse_precision == "fp64" else f"{args.sparse_precision} fronts + f64 refinement",
+        "data": f"synthetic: convection-diffusion stencil, U(0,1) from the DLARNV stream seed {seed}",
         "config": {"workload": f"{nx}x{nx}x{nz} grid, {'7' if nz > 1 else '5'}-point convection-diffusion, "
                                f"n={n}, nnz={nnz}; analyze once, then per round: values x (1 + 0.01 U(-1,1)), "
                                "factorize, solve", "n": n, "nnz": nnz, "parallelism": f"replicas x{world}",
                    "l2": "factors (GBs) larger than L2; no flush"},
         "rounds_per_s": 1e3 / per_round, "analyze_s": analyze_s, "backward_error": eta,
+        "precision": args.sparse_precision, "last_solve": refine,
         "stats": {k: st[k] for k in ("nnz_l", "nnz_u", "fill_ratio", "flops_estimate")},
         "plan": {k: plan[k] for k in ("n_fronts", "n_small_fronts", "max_front_rows", "max_front_cols",
                                        "plan_flops", "factor_bytes", "work_bytes")},
@@ -531,6 +537,7 @@ def run_sparse(args, world, rank, local, pg):
     }
     if not args.no_e2e and rank == 0:
         lu_h = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+        lu_h.set_precision(args.sparse_precision)
         hv = [r.cpu().numpy() for r in rounds[-3:]]
         lu_h.factorize(cp, ri, hv[0])
         ts = []

@@ -163,6 +163,10 @@ int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
 #define ALG_PREC_FP32 0
 #define ALG_PREC_TF32 1
 #define ALG_PREC_BF16 2
+/* TF32x3: each FP32 operand split into TF32 high and low parts and three
+ * TF32 products (hi hi + hi lo + lo hi) accumulated in FP32 on the tensor
+ * cores, FP32-level accuracy (Ootomo and Yokota, IJHPCA 2022). */
+#define ALG_PREC_TF32X3 3
 
 /* Stabilisation of the low-precision LU: partial pivoting (the reference's
  * strategy, column-serial panel), or a random butterfly transformation of A
@@ -239,8 +243,9 @@ void alg_batch_destroy(alg_batch* batch);
 
 /* The tensor-core trailing update of the low-precision LU on device buffers:
  * C (FP32, M x N) -= A (M x K) * B (K x N), all column-major, operands
- * rounded to prec (ALG_PREC_TF32 or ALG_PREC_BF16), FP32 accumulation.
- * K must be a multiple of 64 (BF16) or 32 (TF32). Synchronises. Exposed for
+ * rounded to prec (ALG_PREC_TF32 or ALG_PREC_BF16; ALG_PREC_TF32X3 splits
+ * them into TF32 pairs), FP32 accumulation. K must be a multiple of 64 (BF16)
+ * or 32 (TF32, TF32x3). Synchronises. Exposed for
  * tests and benchmarks of the kernel on its own. */
 int alg_gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda,
                         const float* B, int ldb, float* C, int ldc);
@@ -333,6 +338,29 @@ int alg_splu_clone(const alg_splu* src, alg_splu** out);
 /* factorize for the analyzed pattern itself: only the nnz values (host) are
  * passed; ALG_SP_NOT_FINITE, ALG_SP_SINGULAR as alg_splu_factorize. */
 int alg_splu_factorize_values(alg_splu* lu, const double* values);
+
+/* Mixed precision (no counterpart in the reference, whose sparse LU is FP64
+ * only): the precision of the next factorizations. ALG_SPLU_FP64 (the
+ * default) is the reference's arithmetic. ALG_PREC_FP32 / ALG_PREC_TF32 /
+ * ALG_PREC_TF32X3 / ALG_PREC_BF16 factor the fronts in FP32 (the large
+ * fronts' trailing updates in FP32, or on the tensor cores with TF32, split
+ * TF32x3 or BF16 operands and FP32 accumulation) and refine every solve in FP64 against A's values until the
+ * normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+ * is at most tol (<= 0: 10 n 2^-53); when max_ir steps (<= 0: 10) do not get
+ * there, or refinement stalls, the factor set is recomputed in FP64 from the
+ * same values and the solve is direct (an FP32 zero pivot at factorization
+ * time does the same). A mixed-form solve synchronises once per refinement
+ * step, solve_dev included. */
+#define ALG_SPLU_FP64 (-1)
+int alg_splu_set_precision(alg_splu* lu, int precision, double tol, int max_ir);
+typedef struct {
+  int precision;          /* ALG_SPLU_FP64 or ALG_PREC_* of the factors the last solve used */
+  int iterations;         /* refinement steps of the last solve (0 on the FP64 form) */
+  int fell_back;          /* 1: the last solve recomputed the factors in FP64 */
+  int factor_precision;   /* precision of the current factors */
+  double backward_error;  /* the last refined solve's backward error; -1 when not measured */
+} alg_splu_refine_report;
+int alg_splu_last_solve(const alg_splu* lu, alg_splu_refine_report* out);
 
 /* ---- serving loop (no counterpart in the reference) -----------------------
  * A device-resident request loop: requests are queued in arrival order and

@@ -111,6 +111,20 @@ def test_factorize_checks_before_numeric_work():
     assert lu.stats() is None
 
 
+def test_precision_settings_are_validated_on_the_host():
+    # the mixed form's settings (no reference counterpart) need no GPU
+    lu = SparseLu.analyze(COL_PTR, ROW_IDX, LuMethod.supernodal())
+    for p in ("fp64", "fp32", "tf32", "bf16"):
+        lu.set_precision(p, tol=1e-15, max_ir=5)
+    with pytest.raises(KeyError):
+        lu.set_precision("fp16")
+    from algebra_linear_b200 import _lib
+
+    assert lu._lib.alg_splu_set_precision(lu._h, 7, 0.0, 0) == _lib.INVALID_ARGUMENT
+    assert lu._lib.alg_splu_set_precision(lu._h, 0, float("nan"), 0) == _lib.INVALID_ARGUMENT
+    assert _raises("NotFactorized", lu.last_solve)
+
+
 def _tridiag(n, dense=False):
     cp, ri, v = [0], [], []
     for j in range(n):
