@@ -61,20 +61,22 @@ static cudaEvent_t prof_event(alg_ctx* ctx) {
 }
 
 int prof_begin(alg_ctx* ctx, int cls) {
-  if (!ctx->prof_on) return -1;
+  alg_ctx* pc = ctx->prof_parent ? ctx->prof_parent : ctx;
+  if (!pc->prof_on) return -1;
   alg_ctx::ProfPending pp;
   pp.cls = cls;
-  pp.e0 = prof_event(ctx);
-  pp.e1 = prof_event(ctx);
+  pp.e0 = prof_event(pc);
+  pp.e1 = prof_event(pc);
   pp.flops = pp.bytes = 0;
   cudaEventRecord(pp.e0, ctx->stream);
-  ctx->prof_pending.push_back(pp);
-  return (int)ctx->prof_pending.size() - 1;
+  pc->prof_pending.push_back(pp);
+  return (int)pc->prof_pending.size() - 1;
 }
 
 void prof_end(alg_ctx* ctx, int token, double flops, double bytes) {
-  if (token < 0 || !ctx->prof_on) return;
-  auto& pp = ctx->prof_pending[token];
+  alg_ctx* pc = ctx->prof_parent ? ctx->prof_parent : ctx;
+  if (token < 0 || !pc->prof_on) return;
+  auto& pp = pc->prof_pending[token];
   pp.flops = flops;
   pp.bytes = bytes;
   cudaEventRecord(pp.e1, ctx->stream);

@@ -40,7 +40,10 @@ struct alg_ctx {
   };
   std::vector<Buf> bufs;
   std::mutex mu;  // serialises the shared per-device contexts of the drop-ins
-  // profiler: event pairs around launches of the timed classes
+  // profiler: event pairs around launches of the timed classes; a context
+  // with a parent records its launches (on its own stream) in the parent's
+  // profile (the lanes of a sparse factorization)
+  alg_ctx* prof_parent = nullptr;
   bool prof_on = false;
   struct ProfPending {
     int cls;

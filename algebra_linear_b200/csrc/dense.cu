@@ -225,7 +225,6 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   void* tslu_ws = nullptr;
   if (std::is_same<T, float>::value && plan.tslu) {
     ALG_TRY(ws_get(ctx, WS_TSLU, tslu_scratch_bytes(), &tslu_ws));
-    ALG_CUDA_TRY(cudaMemsetAsync(tslu_ws, 0, tslu_scratch_bytes(), ctx->stream));  // arrival counters
   }
   if (perm != nullptr) {
     iota_kernel<<<std::min(1024, (m + 255) / 256), 256, 0, ctx->stream>>>(perm, m);

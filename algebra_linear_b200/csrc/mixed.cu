@@ -30,6 +30,9 @@ namespace alg {
 namespace {
 
 constexpr int kVecThreads = 256;
+// from this order on, AUTO pivoting uses tournament pivoting (below it the
+// panels are short and partial pivoting's chain is cheap)
+constexpr int kTournamentMinOrder = 2048;
 
 __global__ void cast_f64_f32_kernel(const double* __restrict__ a, int lda, float* __restrict__ o, int ldo,
                                     int m, int n) {
@@ -155,12 +158,10 @@ int grid_for(size_t cnt, int sm) {
 
 }  // namespace
 
-int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, int* ipiv, int* perm) {
+int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, int* ipiv, int* perm,
+                       bool tournament) {
   LuPlan plan = default_plan(n, 4);
-  // tournament pivoting for the low-precision LU's panels (refinement in FP64
-  // restores the FP64 backward error); ALG_TSLU=0 keeps partial pivoting
-  const char* ts = std::getenv("ALG_TSLU");
-  plan.tslu = (ts != nullptr && ts[0] == '1') ? 1 : 0;
+  plan.tslu = tournament ? 1 : 0;
   if (precision != ALG_PREC_FP32) {
     plan.tc_prec = precision;
     plan.nb = 128;
@@ -317,9 +318,10 @@ int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, i
   ALG_TRY(ws_get(ctx, WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&ipiv)));
 
   // ---- factorize in low precision --------------------------------------
-  // AUTO keeps partial pivoting: on matrices that are already random (the
-  // dense workloads here) LU without pivoting has large growth even after the
-  // butterflies, so the butterfly form is an explicit choice.
+  // AUTO pivots (tournament pivoting from kTournamentMinOrder on): on
+  // matrices that are already random (the dense workloads here) LU without
+  // pivoting has large growth even after the butterflies, so the butterfly
+  // form is an explicit choice.
   bool use_rbt = o.pivoting == ALG_PIVOT_RBT;
   if (o.pivoting == ALG_PIVOT_RBT && n % 4 != 0) return ALG_BAD_SHAPE;
   bool lowp_singular = false;
@@ -347,7 +349,10 @@ int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, i
       prof_end(ctx, tok, 0.0, 12.0 * n * n);
       ALG_CUDA_TRY(cudaGetLastError());
     }
-    ALG_TRY(lu_factor_lowp_dev(ctx, o.precision, F.a32, n, n, ipiv, F.perm));
+    const bool tournament =
+        o.pivoting == ALG_PIVOT_TOURNAMENT || (o.pivoting == ALG_PIVOT_AUTO && n >= kTournamentMinOrder);
+    R.reserved[1] = tournament ? 1.0 : 0.0;
+    ALG_TRY(lu_factor_lowp_dev(ctx, o.precision, F.a32, n, n, ipiv, F.perm, tournament));
     ALG_TRY(status_fetch(ctx));
     lowp_singular = ctx->h_status->singular_col != INT_MAX;
   }
@@ -465,6 +470,7 @@ int alg_dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts* opts, double* d_a, i
   if (o.precision != ALG_PREC_FP32 && o.precision != ALG_PREC_TF32 && o.precision != ALG_PREC_BF16 &&
       o.precision != ALG_PREC_TF32X3)
     return ALG_INVALID_ARGUMENT;
+  if (o.pivoting < ALG_PIVOT_AUTO || o.pivoting > ALG_PIVOT_TOURNAMENT) return ALG_INVALID_ARGUMENT;
   return alg::dgesv_mixed_dev(ctx, o, d_a, n, lda, d_b, nrhs, ldb, report);
 }
 

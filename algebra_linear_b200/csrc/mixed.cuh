@@ -7,7 +7,8 @@ namespace alg {
 
 // LU of the n x n FP32 matrix a32 (leading dim lda) with trailing updates in
 // the chosen precision (ALG_PREC_*). Stream-ordered; status in ctx.
-int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, int* ipiv, int* perm);
+int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, int* ipiv, int* perm,
+                       bool tournament);
 
 // ||A||_inf of an n x n FP64 matrix (synchronises).
 int inf_norm_dev(alg_ctx* ctx, const double* a, int n, int lda, double* out_host);

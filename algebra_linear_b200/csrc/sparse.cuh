@@ -55,6 +55,10 @@ struct FrontPlan {
   // schedule
   std::vector<int32_t> small_level_ptr, small_level_fronts;  // batched levels (leaves first)
   std::vector<int32_t> big_order;                            // large fronts in postorder
+  int n_lanes = 1;                                           // concurrent lanes of large fronts
+  std::vector<int32_t> lane_ptr, lane_fronts;                // each lane's large fronts, postorder
+  std::vector<int32_t> top_fronts;                           // large fronts after all lanes, postorder
+  std::vector<int64_t> lane_front_buf;                       // front buffer (entries) per lane
   std::vector<int32_t> solve_level_ptr, solve_level_fronts;  // all fronts by height (leaves first)
   std::vector<int64_t> csr_ptr, csr_map;                     // A by rows: row starts, CSC index of each entry
   std::vector<int32_t> csr_col;                              //   and its column
@@ -66,8 +70,9 @@ struct FrontPlan {
 
 // Builds the front plan from the validated pattern and the supernodal symbolic
 // structure. small_rows: fronts with at most this many rows whose children are
-// all small go to the batched kernel.
-int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, FrontPlan* out);
+// all small go to the batched kernel. lanes: independent subtrees of large
+// fronts are spread over up to this many concurrent lanes.
+int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, int lanes, FrontPlan* out);
 
 // A coarser partition for the GPU plan: chains of only-children merged into
 // their parents while the merged front's flops grow by at most tol.

@@ -8,6 +8,7 @@
 // statistics in place (sparse_lu.rs:82-83, 114-115).
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 
@@ -40,6 +41,7 @@ namespace {
 
 constexpr int kSmallFrontRows = 256;
 constexpr double kChainTolerance = 0.05;
+constexpr int kLanes = 2;
 
 // CscView::new for an n x n matrix (csc.rs:39-76, 178-189).
 int check_view(const alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx,
@@ -149,10 +151,13 @@ int alg_splu_analyze(const size_t* col_ptr, size_t col_ptr_len, const size_t* ro
     lu->effective = lu->flop_ratio > flop_ratio_threshold ? ALG_SPLU_SUPERNODAL : ALG_SPLU_SIMPLICIAL;
   else
     lu->effective = ALG_SPLU_SIMPLICIAL;
-  // GPU plan: the reference's partition with chains of only-children merged
+  // GPU plan: the reference's partition with chains of children merged;
+  // large fronts in kLanes concurrent lanes (ALG_SPLU_LANES overrides)
   {
+    int lanes = kLanes;
+    if (const char* e = std::getenv("ALG_SPLU_LANES")) lanes = std::max(1, std::min(8, std::atoi(e)));
     alg::sp::FrontPlan first;
-    rc = alg::sp::build_front_plan(p, lu->sym, kSmallFrontRows, &first);
+    rc = alg::sp::build_front_plan(p, lu->sym, kSmallFrontRows, lanes, &first);
     if (rc != ALG_OK) return rc;
     std::vector<idx> ptr;
     alg::sp::amalgamate_chains(first, lu->sym, kChainTolerance, &ptr);
@@ -161,7 +166,7 @@ int alg_splu_analyze(const size_t* col_ptr, size_t col_ptr_len, const size_t* ro
     } else {
       alg::sp::Supernodal coarse;
       alg::sp::repartition(lu->sym, ptr, &coarse);
-      rc = alg::sp::build_front_plan(p, coarse, kSmallFrontRows, &lu->plan);
+      rc = alg::sp::build_front_plan(p, coarse, kSmallFrontRows, lanes, &lu->plan);
       if (rc != ALG_OK) return rc;
     }
   }
@@ -273,6 +278,8 @@ int alg_splu_plan_info(const alg_splu* lu, alg_splu_plan* out) {
   out->work_bytes = 8 * (size_t)(F.block_total + F.stack_total + F.front_buf);
   out->plan_flops = F.flops;
   out->structurally_singular = F.structurally_singular ? 1 : 0;
+  out->n_lanes = F.n_lanes;
+  out->top_fronts = F.top_fronts.size();
   return ALG_OK;
 }
 

@@ -664,12 +664,23 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
   ALG_TRY(dmalloc((void**)&d_values, sizeof(double) * std::max<idx>(F.nnz, 1)));
   ALG_TRY(dmalloc((void**)&d_block, sizeof(double) * F.block_total));
   ALG_TRY(dmalloc((void**)&d_stack, sizeof(double) * F.stack_total));
-  ALG_TRY(dmalloc((void**)&d_front, sizeof(double) * F.front_buf));
+  n_lanes = std::max(1, std::min(F.n_lanes, kMaxLanes));
+  lane_ctx[0] = ctx;
   int64_t max_rows = 1;
   for (const auto& d : F.fronts) max_rows = std::max<int64_t>(max_rows, d.rows);
-  ALG_TRY(dmalloc((void**)&d_ipiv, sizeof(int) * max_rows));
-  ALG_TRY(dmalloc((void**)&d_perm, sizeof(int) * max_rows));
-  ALG_TRY(dmalloc((void**)&d_rowtmp, sizeof(int32_t) * max_rows));
+  for (int k = 0; k < n_lanes; ++k) {
+    if (k > 0) {
+      ALG_TRY(alg_ctx_create(nullptr, &lane_ctx[k]));
+      lane_ctx[k]->prof_parent = ctx;  // the lanes' launches show in the handle's profile
+      ALG_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    }
+    const int64_t fb = k < (int)F.lane_front_buf.size() ? F.lane_front_buf[k] : F.front_buf;
+    ALG_TRY(dmalloc((void**)&d_front[k], sizeof(double) * std::max<int64_t>(fb, 1)));
+    ALG_TRY(dmalloc((void**)&d_ipiv[k], sizeof(int) * max_rows));
+    ALG_TRY(dmalloc((void**)&d_perm[k], sizeof(int) * max_rows));
+    ALG_TRY(dmalloc((void**)&d_rowtmp[k], sizeof(int32_t) * max_rows));
+  }
+  ALG_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   ALG_TRY(dmalloc((void**)&d_flag, sizeof(int) * 4));
   ALG_TRY(dmalloc((void**)&d_y, sizeof(double) * n));
   ALG_TRY(dmalloc((void**)&d_rhs, sizeof(double) * n));
@@ -758,10 +769,17 @@ int DeviceLu::ensure_refine_buffers() {
 }
 
 void DeviceLu::release() {
+  for (int k = 0; k < kMaxLanes; ++k) {
+    for (void* q : {(void*)d_front[k], (void*)d_ipiv[k], (void*)d_perm[k], (void*)d_rowtmp[k]})
+      if (q) cudaFree(q);
+    if (k > 0 && lane_ctx[k]) alg_ctx_destroy(lane_ctx[k]);
+    if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+  }
+  if (ev_fork) cudaEventDestroy(ev_fork);
   for (void* q : {(void*)d_fronts, (void*)d_child_idx, (void*)d_child_slot, (void*)d_struct_cols,
                   (void*)d_cb_colmap, (void*)d_anew_q, (void*)d_anew_slot, (void*)d_anew_col, (void*)d_new_rows,
                   (void*)d_small_levels, (void*)d_col_perm, (void*)d_values, (void*)d_block, (void*)d_stack,
-                  (void*)d_front, (void*)d_ipiv, (void*)d_perm, (void*)d_rowtmp, (void*)d_flag, (void*)d_y,
+                  (void*)d_flag, (void*)d_y,
                   (void*)d_rhs, (void*)d_solve_small, (void*)d_fwd_items, (void*)d_fin_items, (void*)d_bwd_items,
                   (void*)d_part_off, (void*)d_fpart_off, (void*)d_partial, (void*)d_fpartial, (void*)d_tflags,
                   (void*)d_csr_ptr, (void*)d_csr_col, (void*)d_csr_map, (void*)d_b0, (void*)d_x, (void*)d_norms})
@@ -798,8 +816,6 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   out.prec = std::is_same<T, double>::value ? -1 : (tc_prec < 0 ? ALG_PREC_FP32 : tc_prec);
   cudaStream_t st = ctx->stream;
   T* block = reinterpret_cast<T*>(d_block);
-  T* stack = reinterpret_cast<T*>(d_stack);
-  T* front = reinterpret_cast<T*>(d_front);
   T* L = reinterpret_cast<T*>(out.L);
   T* U = reinterpret_cast<T*>(out.U);
   const int tok = prof_begin(ctx, ALG_K_SPARSE);
@@ -831,47 +847,30 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
     ALG_CUDA_TRY(cudaGetLastError());
   }
   prof_end(ctx, tok_small, 0.0, 0.0);
-  // large fronts in postorder
-  LuPlan lp;
-  lp.nb = 64;
-  lp.nbl = 16;
-  lp.tc_prec = tc_prec;
-  for (int32_t s : F.big_order) {
-    const FrontDesc& d = F.fronts[s];
-    const int cols = d.size + d.ncb;
-    ALG_CUDA_TRY(cudaMemsetAsync(front, 0, sizeof(T) * (size_t)d.rows * cols, st));
-    BigArgs<T> ba;
-    ba.d = d;
-    ba.fronts = d_fronts;
-    ba.child_idx = d_child_idx;
-    ba.child_slot = d_child_slot;
-    ba.cb_colmap = d_cb_colmap;
-    ba.anew_q = d_anew_q;
-    ba.anew_slot = d_anew_slot;
-    ba.anew_col = d_anew_col;
-    ba.new_rows = d_new_rows;
-    ba.values = values;
-    ba.block = block;
-    ba.stack = stack;
-    ba.front = front;
-    ba.rowid = out.rowid;
-    ba.rowtmp = d_rowtmp;
-    int64_t work = (int64_t)(d.anew_end - d.anew_begin) + d.rows;
-    for (int k = d.child_begin; k < d.child_end; ++k) {
-      const FrontDesc& c = F.fronts[F.child_idx[k]];
-      work = std::max<int64_t>(work, (int64_t)(c.rows - c.size) * c.ncb);
+  // large fronts: the lanes' subtrees concurrently (issued front by front in
+  // turn), then the fronts above them on the handle's stream
+  if (n_lanes > 1) {
+    ALG_CUDA_TRY(cudaEventRecord(ev_fork, st));
+    for (int k = 1; k < n_lanes; ++k) {
+      ALG_CUDA_TRY(cudaStreamWaitEvent(lane_ctx[k]->stream, ev_fork, 0));
+      ALG_TRY(status_reset(lane_ctx[k]));
     }
-    big_assemble_kernel<T><<<grid_for(ctx, work, 256), 256, 0, st>>>(ba);
-    count_launches();
-    ALG_CUDA_TRY(cudaGetLastError());
-    ALG_TRY((lu_factor_partial_dev<T, false>(ctx, front, d.rows, d.size, cols, d.rows, d_ipiv, d_perm, lp)));
-    ALG_CUDA_TRY(cudaMemcpyAsync(L + d.l_off, front, sizeof(T) * (size_t)d.rows * d.size, cudaMemcpyDeviceToDevice,
-                                 st));
-    const int64_t fw = std::max<int64_t>((int64_t)d.rows, (int64_t)d.rows * d.ncb);
-    big_finalize_kernel<T><<<grid_for(ctx, fw, 256), 256, 0, st>>>(d, front, d_perm, d_rowtmp, out.rowid, U, stack);
-    count_launches();
-    ALG_CUDA_TRY(cudaGetLastError());
   }
+  std::vector<int> next(n_lanes);
+  for (int k = 0; k < n_lanes; ++k) next[k] = F.lane_ptr[k];
+  for (bool more = true; more;) {
+    more = false;
+    for (int k = 0; k < n_lanes; ++k) {
+      if (next[k] >= F.lane_ptr[k + 1]) continue;
+      ALG_TRY(factor_big<T>(b, F.lane_fronts[next[k]++], k, values, tc_prec));
+      more = true;
+    }
+  }
+  for (int k = 1; k < n_lanes; ++k) {
+    ALG_CUDA_TRY(cudaEventRecord(ev_join[k], lane_ctx[k]->stream));
+    ALG_CUDA_TRY(cudaStreamWaitEvent(st, ev_join[k], 0));
+  }
+  for (int32_t s : F.top_fronts) ALG_TRY(factor_big<T>(b, s, 0, values, tc_prec));
   ALG_CUDA_TRY(cudaMemsetAsync(out.ucount, 0, sizeof(unsigned) * std::max<idx>(F.n, 1), st));
   if (F.ns > 0) {
     positions_counts_kernel<T><<<(int)F.ns, 256, 0, st>>>(d_fronts, (int)F.ns, out.rowid, L, U, d_struct_cols,
@@ -883,6 +882,58 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   return ALG_OK;
 }
 
+// One large front on lane `lane`: assemble, blocked partial-pivoting LU of
+// its columns over all its rows, then its rows, U12 and contribution block.
+template <typename T>
+int DeviceLu::factor_big(int b, int32_t s, int lane, const double* values, int tc_prec) {
+  const FrontPlan& F = *plan;
+  Factors& out = fac[b];
+  alg_ctx* lc = lane_ctx[lane];
+  cudaStream_t st = lc->stream;
+  T* front = reinterpret_cast<T*>(d_front[lane]);
+  const FrontDesc& d = F.fronts[s];
+  const int cols = d.size + d.ncb;
+  ALG_CUDA_TRY(cudaMemsetAsync(front, 0, sizeof(T) * (size_t)d.rows * cols, st));
+  BigArgs<T> ba;
+  ba.d = d;
+  ba.fronts = d_fronts;
+  ba.child_idx = d_child_idx;
+  ba.child_slot = d_child_slot;
+  ba.cb_colmap = d_cb_colmap;
+  ba.anew_q = d_anew_q;
+  ba.anew_slot = d_anew_slot;
+  ba.anew_col = d_anew_col;
+  ba.new_rows = d_new_rows;
+  ba.values = values;
+  ba.block = reinterpret_cast<T*>(d_block);
+  ba.stack = reinterpret_cast<T*>(d_stack);
+  ba.front = front;
+  ba.rowid = out.rowid;
+  ba.rowtmp = d_rowtmp[lane];
+  int64_t work = (int64_t)(d.anew_end - d.anew_begin) + d.rows;
+  for (int k = d.child_begin; k < d.child_end; ++k) {
+    const FrontDesc& c = F.fronts[F.child_idx[k]];
+    work = std::max<int64_t>(work, (int64_t)(c.rows - c.size) * c.ncb);
+  }
+  big_assemble_kernel<T><<<grid_for(lc, work, 256), 256, 0, st>>>(ba);
+  count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  LuPlan lp;
+  lp.nb = 64;
+  lp.nbl = 16;
+  lp.tc_prec = tc_prec;
+  ALG_TRY((lu_factor_partial_dev<T, false>(lc, front, d.rows, d.size, cols, d.rows, d_ipiv[lane], d_perm[lane], lp)));
+  T* L = reinterpret_cast<T*>(out.L);
+  T* U = reinterpret_cast<T*>(out.U);
+  ALG_CUDA_TRY(cudaMemcpyAsync(L + d.l_off, front, sizeof(T) * (size_t)d.rows * d.size, cudaMemcpyDeviceToDevice, st));
+  const int64_t fw = std::max<int64_t>((int64_t)d.rows, (int64_t)d.rows * d.ncb);
+  big_finalize_kernel<T><<<grid_for(lc, fw, 256), 256, 0, st>>>(d, front, d_perm[lane], d_rowtmp[lane], out.rowid, U,
+                                                                 reinterpret_cast<T*>(d_stack));
+  count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
 // Reads the factorization's outcome (synchronises): SP_OK or SP_SINGULAR.
 // The mixed form refactors in FP64 when its FP32 factorization met a zero
 // pivot (an FP32 underflow need not be a singular A).
@@ -891,8 +942,14 @@ int DeviceLu::finish(int b, Stats* stats) {
   int h_flag[4] = {0, 0, 0, 0};
   ALG_CUDA_TRY(cudaMemcpyAsync(h_flag, d_flag, sizeof(h_flag), cudaMemcpyDeviceToHost, ctx->stream));
   ALG_TRY(status_fetch(ctx));
-  if (ctx->h_status->timeout) return ALG_TIMEOUT;
-  if (h_flag[0] != 0 || ctx->h_status->singular_col != INT_MAX) {
+  bool timeout = ctx->h_status->timeout != 0, singular = ctx->h_status->singular_col != INT_MAX;
+  for (int k = 1; k < n_lanes; ++k) {
+    ALG_TRY(status_fetch(lane_ctx[k]));
+    timeout = timeout || lane_ctx[k]->h_status->timeout != 0;
+    singular = singular || lane_ctx[k]->h_status->singular_col != INT_MAX;
+  }
+  if (timeout) return ALG_TIMEOUT;
+  if (h_flag[0] != 0 || singular) {
     if (fac[b].prec < 0) return SP_SINGULAR;
     ALG_TRY(refactor_fp64(b));
     return finish(b, stats);

@@ -51,9 +51,17 @@ struct DeviceLu {
   // arenas sized in doubles; the FP32 form uses their first halves as floats
   double* d_block = nullptr;   // small fronts' blocks
   double* d_stack = nullptr;   // large fronts' contribution blocks
-  double* d_front = nullptr;   // the large front being factored
-  int *d_ipiv = nullptr, *d_perm = nullptr;
-  int32_t* d_rowtmp = nullptr;
+  // per lane (independent subtrees of large fronts run concurrently): a
+  // context (stream, workspaces; lane 0 is the handle's own), the front
+  // being factored and the pivot scratch
+  static constexpr int kMaxLanes = 8;
+  int n_lanes = 1;
+  alg_ctx* lane_ctx[kMaxLanes] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kMaxLanes] = {};
+  double* d_front[kMaxLanes] = {};
+  int* d_ipiv[kMaxLanes] = {};
+  int* d_perm[kMaxLanes] = {};
+  int32_t* d_rowtmp[kMaxLanes] = {};
   int* d_flag = nullptr;       // [0]: a small front met a zero pivot
   double *d_y = nullptr, *d_rhs = nullptr;
   // solve schedule: per level the fronts solved by the one-CTA diagonal
@@ -97,6 +105,8 @@ struct DeviceLu {
  private:
   template <typename T>
   int factor_t(int set, const double* values, int tc_prec);
+  template <typename T>
+  int factor_big(int set, int32_t s, int lane, const double* values, int tc_prec);
   template <typename T>
   int sweep_t(int set);                // d_rhs -> d_rhs with the set's factors, stream-ordered
   int refine(int set);

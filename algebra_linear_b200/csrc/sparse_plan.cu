@@ -8,7 +8,7 @@
 namespace alg {
 namespace sp {
 
-int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, FrontPlan* out) {
+int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, int lanes, FrontPlan* out) {
   FrontPlan& F = *out;
   F = FrontPlan();
   const idx n = p.n, ns = S.n_supernodes(), nnz = p.nnz();
@@ -213,30 +213,118 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, Fron
   F.u_total = uo;
   F.rowid_total = ro;
   F.block_total = bo;
-  // large fronts: postorder, contribution blocks on a stack
+  // large fronts: postorder, split into lanes (independent subtrees factored
+  // concurrently, one stream each) and the fronts above them; contribution
+  // blocks on one stack per lane and one for the top, in disjoint regions
   {
-    std::vector<std::pair<int64_t, int64_t>> stack;  // (offset, length)
-    int64_t top = 0, peak = 0, fbuf = 0;
+    std::vector<int32_t> big_parent(ns, -1);
+    std::vector<double> cost(ns, 0.0), sub(ns, 0.0);
     for (idx s = 0; s < ns; ++s) {
       FrontDesc& d = F.fronts[s];
       if (d.small) continue;
       F.big_order.push_back((int32_t)s);
-      fbuf = std::max(fbuf, (int64_t)d.rows * (d.size + d.ncb));
-      int nbig = 0;
-      for (int32_t k = d.child_begin; k < d.child_end; ++k) nbig += F.fronts[F.child_idx[k]].small ? 0 : 1;
-      for (int i = 0; i < nbig; ++i) {
-        top = stack.back().first;
-        stack.pop_back();
-      }
-      d.cb_off = top;
-      d.cb_ld = std::max(1, d.rows - d.size);
-      const int64_t len = (int64_t)(d.rows - d.size) * d.ncb;
-      stack.push_back({top, len});
-      top += len;
-      peak = std::max(peak, top);
+      for (int32_t k = d.child_begin; k < d.child_end; ++k)
+        if (!F.fronts[F.child_idx[k]].small) big_parent[F.child_idx[k]] = (int32_t)s;
+      // seconds: updates at ~15 TFLOP/s, contribution-block traffic at ~3 TB/s,
+      // a launch chain and a column-serial panel
+      const double m = d.rows, k = d.size, c = d.ncb;
+      const double fl = 2.0 * k * k * m - 2.0 / 3.0 * k * k * k + k * k * c + 2.0 * (m - k) * c * k;
+      cost[s] = fl / 15e12 + 24.0 * (m - k) * c / 3e12 + 50e-6 + 5e-6 * k;
     }
-    F.stack_total = peak;
-    F.front_buf = fbuf;
+    for (int32_t s : F.big_order) {  // children precede parents
+      sub[s] += cost[s];
+      if (big_parent[s] >= 0) sub[big_parent[s]] += sub[s];
+    }
+    // split the heaviest subtree at its root (the root goes to the top) until
+    // the lanes can be balanced
+    std::vector<int32_t> tasks;
+    std::vector<char> is_top(ns, 0);
+    for (int32_t s : F.big_order)
+      if (big_parent[s] < 0) tasks.push_back(s);
+    const int K = std::max(1, std::min(lanes, 8));
+    while (K > 1 && !tasks.empty() && tasks.size() < 64) {
+      size_t hi = 0;
+      double total = 0.0;
+      for (size_t i = 0; i < tasks.size(); ++i) {
+        total += sub[tasks[i]];
+        if (sub[tasks[i]] > sub[tasks[hi]]) hi = i;
+      }
+      const int32_t r = tasks[hi];
+      if ((int)tasks.size() >= K && sub[r] <= 1.1 * total / K) break;
+      const FrontDesc& d = F.fronts[r];
+      std::vector<int32_t> kids;
+      for (int32_t k = d.child_begin; k < d.child_end; ++k)
+        if (!F.fronts[F.child_idx[k]].small) kids.push_back(F.child_idx[k]);
+      if (kids.empty()) break;
+      is_top[r] = 1;
+      tasks.erase(tasks.begin() + hi);
+      tasks.insert(tasks.end(), kids.begin(), kids.end());
+    }
+    // longest-processing-time assignment of the subtrees to lanes
+    std::sort(tasks.begin(), tasks.end(), [&](int32_t x, int32_t y) { return sub[x] > sub[y]; });
+    std::vector<double> load(K, 0.0);
+    std::vector<int32_t> lane_of(ns, -1);
+    for (int32_t r : tasks) {
+      const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[k] += sub[r];
+      lane_of[r] = k;
+    }
+    // every front of a task's subtree takes the task's lane (parents come
+    // later in postorder, so walk the order backwards)
+    for (auto it = F.big_order.rbegin(); it != F.big_order.rend(); ++it) {
+      const int32_t s = *it;
+      if (is_top[s] || lane_of[s] >= 0) continue;
+      lane_of[s] = lane_of[big_parent[s]];
+    }
+    F.n_lanes = K;
+    F.lane_ptr.assign(K + 1, 0);
+    F.lane_front_buf.assign(K, 0);
+    for (int32_t s : F.big_order)
+      if (!is_top[s]) F.lane_ptr[lane_of[s] + 1] += 1;
+    for (int k = 0; k < K; ++k) F.lane_ptr[k + 1] += F.lane_ptr[k];
+    F.lane_fronts.assign(F.lane_ptr[K], 0);
+    std::vector<int32_t> fill(F.lane_ptr.begin(), F.lane_ptr.end() - 1);
+    for (int32_t s : F.big_order) {
+      if (is_top[s])
+        F.top_fronts.push_back(s);
+      else
+        F.lane_fronts[fill[lane_of[s]]++] = s;
+    }
+    // stacks: lane k's region, then the top's; a front pops the contribution
+    // blocks of its large children on its own stack (the lanes' roots are
+    // read in place by the top fronts)
+    int64_t base = 0;
+    auto run_stack = [&](const int32_t* list, int cnt, bool top, int64_t* fbuf) {
+      std::vector<std::pair<int64_t, int64_t>> stack;  // (offset, length)
+      int64_t at = base, peak = base;
+      for (int i = 0; i < cnt; ++i) {
+        FrontDesc& d = F.fronts[list[i]];
+        *fbuf = std::max(*fbuf, (int64_t)d.rows * (d.size + d.ncb));
+        int npop = 0;
+        for (int32_t k = d.child_begin; k < d.child_end; ++k) {
+          const int32_t c = F.child_idx[k];
+          if (!F.fronts[c].small && (!top || is_top[c])) ++npop;
+        }
+        for (int q = 0; q < npop; ++q) {
+          at = stack.back().first;
+          stack.pop_back();
+        }
+        d.cb_off = at;
+        d.cb_ld = std::max(1, d.rows - d.size);
+        const int64_t len = (int64_t)(d.rows - d.size) * d.ncb;
+        stack.push_back({at, len});
+        at += len;
+        peak = std::max(peak, at);
+      }
+      base = peak;
+    };
+    for (int k = 0; k < K; ++k)
+      run_stack(F.lane_fronts.data() + F.lane_ptr[k], F.lane_ptr[k + 1] - F.lane_ptr[k], false,
+                &F.lane_front_buf[k]);
+    run_stack(F.top_fronts.data(), (int)F.top_fronts.size(), true, &F.lane_front_buf[0]);
+    F.stack_total = base;
+    F.front_buf = 0;
+    for (int64_t fb : F.lane_front_buf) F.front_buf = std::max(F.front_buf, fb);
   }
   // levels: small fronts (batched kernel) and all fronts (solve)
   {

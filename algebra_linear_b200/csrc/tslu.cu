@@ -6,18 +6,20 @@
 // (TSLU: Grigori, Demmel, Xiang, "CALU: a communication optimal LU
 // factorization algorithm", SIAM J. Matrix Anal. Appl. 32, 2011) chooses the
 // panel's w pivot rows first and factors afterwards:
-//   1. select: each CTA runs partial-pivoting LU on its own chunk of rows (in
-//      shared memory) and proposes the w rows it pivoted on;
-//   2. merge: one CTA runs partial-pivoting LU on the proposed rows'
-//      original values; its w pivots are the panel's pivots and its leading
-//      w x w block is L11 \ U11;
+//   1. select: each CTA runs partial-pivoting LU on its own chunk of 256 rows
+//      (one row per thread, the chunk in shared memory) and proposes the w
+//      rows it pivoted on, with their original values;
+//   2. merge: a CTA runs the same LU on the up to 8 x w rows its 8 children
+//      proposed (original values), level after level, until one CTA holds
+//      the panel's w pivots in order and, as its LU's leading rows,
+//      L11 \ U11 of the winners;
 //   3. apply: the interchanges (LAPACK sequential form, as the partial-
 //      pivoting panel records them) move the winners to the top, every other
-//      row gets its multipliers l = a U11^-1, the labels of the moved rows
+//      row gets its multipliers l = a U11^-1, and the labels of the moved rows
 //      and the block panel's other columns follow the interchanges.
 // The factorization differs from partial pivoting's (other pivots); the
 // mixed form's refinement in FP64 then brings the solution to the FP64
-// backward error, which is its contract.
+// backward error, which is its contract. No kernel waits on another CTA.
 #include <algorithm>
 #include <climits>
 
@@ -26,41 +28,53 @@
 namespace alg {
 namespace {
 
-constexpr int kW = 32;             // widest leaf
-constexpr int kChunk = 64;         // rows per warp at the tree's leaves
-constexpr int kMaxChunks = 1024;   // up to 65 536 panel rows
-constexpr int kTreeWarps = 2;      // warps per CTA of the tournament kernel (2 x 16 KB of shared memory)
+constexpr int kW = 32;            // widest leaf
+constexpr int kRows = 256;        // rows per CTA (one per thread)
+constexpr int kFan = 8;           // children merged by one CTA (8 x 32 = 256 rows)
+constexpr int kMaxGroups = 1024;  // CTAs of the first level: up to 262 144 panel rows
 constexpr int kMaxMoves = 2 * kW;
 
 struct TsluScratch {
-  int node_cand[2 * kMaxChunks][kW];  // each tree node's proposed rows (absolute), -1 = none
-  float node_vals[2 * kMaxChunks][kW * kW];  // their original values ([col][row], stride kW)
-  int counter[2 * kMaxChunks];        // arrivals per node (reset by the merging warp)
+  int cand_rows[2][kMaxGroups][kW];        // proposals of each CTA of a level, in step order
+  int cand_cnt[2][kMaxGroups];
+  float cand_vals[2][kMaxGroups][kW * kW];  // their original values, [col][k]
+  int win[kW];                              // the panel's pivot rows in order
   int nmoves;
-  int move_pos[kMaxMoves];            // a position whose row changed
-  int move_src[kMaxMoves];            // the position that row came from (at the leaf's start)
-  int move_lab[kMaxMoves];            // its new label
-  float top_lu[kW * kW];              // L11 \ U11 of the winners (column-major w x w)
-  float top_orig[kW * kW];            // original values of the rows at the top positions
+  int move_pos[kMaxMoves];                  // a position whose row changed
+  int move_src[kMaxMoves];                  // the position that row came from (at the leaf's start)
+  int move_lab[kMaxMoves];                  // its new label
+  float top_lu[kW * kW];                    // L11 \ U11 of the winners ([col][k], stride kW)
+  float top_orig[kW * kW];                  // original values of the rows at the top positions
 };
 
-// Partial-pivoting LU, by one warp, of the first w columns of nr <= 64 rows
-// held in shared memory ([col][row], stride kChunk), swapping the row ids
-// along; returns the first column whose pivot is zero, or -1.
-__device__ int warp_gepp(float* s, int* sid, int nr, int w) {
-  const int lane = threadIdx.x & 31;
-  int zero_col = -1;
-  const int kmax = min(w, nr);
-  for (int k = 0; k < kmax; ++k) {
-    float key = -1.0f;
-    int idx = INT_MAX;
-    for (int r = k + lane; r < nr; r += 32) {
-      const float v = fabsf(s[k * kChunk + r]);
-      if (v > key) {
-        key = v;
-        idx = r;
-      }
-    }
+// Partial-pivoting LU of the first w columns of nr <= 256 rows, row t in
+// thread t's registers v[], rows left in place. One barrier per column: each
+// warp publishes its best candidate (key, index and the whole row) in a
+// mailbox double-buffered by column parity, and every warp reduces the
+// mailboxes itself. Returns the step at which this thread's row was chosen
+// (-1: not chosen); the chosen row's v[] then holds its multipliers (columns
+// before its step) and its U entries (from its step on). zero_col: first
+// column whose pivot was zero (thread 0's copy).
+constexpr int kWarps = kRows / 32;
+
+struct GeppBox {
+  float row[2][kWarps][kW];
+  float key[2][kWarps];
+  int idx[2][kWarps];
+};
+
+__device__ __forceinline__ int block_gepp(float (&v)[kW], int nr, int w, GeppBox& box, int* zero_col) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  int chosen = -1;
+  for (int j = 0; j < w; ++j) {
+    const int par = j & 1;
+    float vj = v[0];
+#pragma unroll
+    for (int c = 1; c < kW; ++c)
+      if (c == j) vj = v[c];
+    float key = (t < nr && chosen < 0) ? fabsf(vj) : -1.0f;
+    int idx = t;
+#pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const float ok = __shfl_xor_sync(0xffffffffu, key, off);
       const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
@@ -69,247 +83,287 @@ __device__ int warp_gepp(float* s, int* sid, int nr, int w) {
         idx = oi;
       }
     }
-    const int p = idx;
-    if (p != k) {
-      if (lane < w) {
-        const float t = s[lane * kChunk + k];
-        s[lane * kChunk + k] = s[lane * kChunk + p];
-        s[lane * kChunk + p] = t;
-      }
+    if (key < 0.0f) {
       if (lane == 0) {
-        const int t = sid[k];
-        sid[k] = sid[p];
-        sid[p] = t;
+        box.key[par][warp] = -1.0f;
+        box.idx[par][warp] = INT_MAX;
+      }
+    } else if (idx == t) {
+      box.key[par][warp] = key;
+      box.idx[par][warp] = idx;
+#pragma unroll
+      for (int c = 0; c < kW; ++c) box.row[par][warp][c] = v[c];
+    }
+    __syncthreads();
+    float bk = lane < kWarps ? box.key[par][lane] : -1.0f;
+    int bi = lane < kWarps ? box.idx[par][lane] : INT_MAX;
+    int bw = lane;
+#pragma unroll
+    for (int off = kWarps / 2; off > 0; off >>= 1) {
+      const float ok = __shfl_xor_sync(0xffffffffu, bk, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      const int ow = __shfl_xor_sync(0xffffffffu, bw, off);
+      if (ok > bk || (ok == bk && oi < bi)) {
+        bk = ok;
+        bi = oi;
+        bw = ow;
       }
     }
-    __syncwarp();
-    const float d = s[k * kChunk + k];
-    if (d == 0.0f) {
-      if (zero_col < 0) zero_col = k;
-    } else {
-      const float inv = 1.0f / d;
-      for (int r = k + 1 + lane; r < nr; r += 32) s[k * kChunk + r] *= inv;
+    bk = __shfl_sync(0xffffffffu, bk, 0);
+    bi = __shfl_sync(0xffffffffu, bi, 0);
+    bw = __shfl_sync(0xffffffffu, bw, 0);
+    if (bk < 0.0f) break;  // fewer rows than columns: every row is chosen
+    if (t == bi) chosen = j;
+    const float* prow = box.row[par][bw];
+    const float pv = prow[j];
+    if (pv == 0.0f && t == 0 && *zero_col < 0) *zero_col = j;
+    if (t < nr && chosen < 0) {
+      const float l = pv != 0.0f ? vj / pv : 0.0f;
+#pragma unroll
+      for (int c = 0; c < kW; ++c) {
+        if (c == j) v[c] = l;
+        if (c > j && c < w) v[c] = fmaf(-l, prow[c], v[c]);
+      }
     }
-    __syncwarp();
-    for (int r = k + 1 + lane; r < nr; r += 32) {
-      const float l = s[k * kChunk + r];
-      for (int c = k + 1; c < w; ++c) s[c * kChunk + r] = fmaf(-s[c * kChunk + k], l, s[c * kChunk + r]);
-    }
-    __syncwarp();
   }
-  return zero_col;
+  __syncthreads();
+  return chosen;
 }
 
-// 1 + 2. The tournament, one launch: warp g factors rows
-// [c0 + 64 g, c0 + 64 (g + 1)) and proposes its w pivot rows, with their
-// original values, to its tree node; up a binary tree, the second of two
-// sibling warps to finish merges their proposals (partial-pivoting LU of the
-// up to 2 w proposed rows' original values, read contiguously from the
-// scratch); the warp that merges the root holds the panel's pivots and
-// L11 \ U11 and records the interchanges, the moved rows and their labels.
-// No warp waits for another: arrivals are counted with atomics after a fence.
-__global__ void __launch_bounds__(kTreeWarps * 32) tslu_tree_kernel(const float* a, int lda, int n, int c0, int w,
-                                                                    int nchunks, int* ipiv, const int* lab,
-                                                                    int first_leaf, DevStatus* status,
-                                                                    TsluScratch* ws) {
-  __shared__ float work_s[kTreeWarps][kW * kChunk];
-  __shared__ float orig_s[kTreeWarps][kW * kChunk];
-  __shared__ int sids[kTreeWarps][kChunk];
-  __shared__ int rows_s[kTreeWarps][kChunk];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int g = blockIdx.x * kTreeWarps + wl;
-  if (g >= nchunks) return;
-  float* s = work_s[wl];
-  float* o = orig_s[wl];
-  int* sid = sids[wl];  // local indices into rows / o
-  int* rows = rows_s[wl];
-  // leaf: this warp's own chunk
-  const int r0 = c0 + g * kChunk;
-  int nr = max(0, min(n, r0 + kChunk) - r0);
-  for (int e = lane; e < nr * w; e += 32) {
-    const int r = e % nr, c = e / nr;
-    const float v = a[(size_t)(r0 + r) + (size_t)(c0 + c) * lda];
-    o[c * kChunk + r] = v;
-    s[c * kChunk + r] = v;
-  }
-  for (int r = lane; r < nr; r += 32) {
-    rows[r] = r0 + r;
-    sid[r] = r;
-  }
-  __syncwarp();
-  int zc = warp_gepp(s, sid, nr, w);
-  int node = g, base = 0, width = nchunks;  // node index within its level, level's first slot, level width
-  auto publish = [&]() {
-    const int cnt = min(w, nr);
-    for (int k = lane; k < kW; k += 32) ws->node_cand[base + node][k] = k < cnt ? rows[sid[k]] : -1;
-    for (int e = lane; e < cnt * w; e += 32) {
-      const int k = e % cnt, c = e / cnt;
-      ws->node_vals[base + node][c * kW + k] = o[c * kChunk + sid[k]];
+// One level of the tournament. Level 0 (src < 0) reads rows [c0 + 256 g, ...)
+// of the panel; later levels read the proposals of children [8 g, 8 g + 8)
+// from scratch slot src. Writes this CTA's proposals to slot dst; the single
+// CTA of the last level (root) also writes the winners, L11 \ U11, the rows
+// at the top before anything moves, ipiv and the list of moved rows.
+__global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __restrict__ a, int lda, int n, int c0,
+                                                           int w, int src, int nchild, int dst, int root,
+                                                           int* ipiv, const int* lab, int first_leaf,
+                                                           DevStatus* status, TsluScratch* ws) {
+  __shared__ GeppBox box;
+  __shared__ int zero_col;
+  __shared__ int coff[kFan + 1];
+  const int t = threadIdx.x, g = blockIdx.x;
+  float o[kW];  // this row's original values
+#pragma unroll
+  for (int c = 0; c < kW; ++c) o[c] = 0.0f;
+  int row = -1, nr = 0;
+  if (src < 0) {
+    const int r0 = c0 + g * kRows;
+    nr = max(0, min(n, r0 + kRows) - r0);
+    if (t < nr) {
+      row = r0 + t;
+#pragma unroll
+      for (int c = 0; c < kW; ++c) o[c] = c < w ? a[(size_t)row + (size_t)(c0 + c) * lda] : 0.0f;
     }
-  };
-  publish();
-  // up the tree
-  while (width > 1) {
-    const int parent = node >> 1, pwidth = (width + 1) >> 1, pbase = base + width;
-    const bool has_sibling = (node ^ 1) < width;
-    __syncwarp();
-    if (has_sibling) {
-      __threadfence();
-      int arrived = 0;
-      if (lane == 0) arrived = atomicAdd(&ws->counter[pbase + parent], 1);
-      arrived = __shfl_sync(0xffffffffu, arrived, 0);
-      if (arrived == 0) return;  // the sibling merges
-      __threadfence();
-      if (lane == 0) ws->counter[pbase + parent] = 0;  // ready for the next panel
-    }
-    // gather the children's proposals and their original values
-    nr = 0;
-    for (int ch = 2 * parent; ch < min(2 * parent + 2, width); ++ch) {
-      const volatile int* cand = ws->node_cand[base + ch];
-      const volatile float* vals = ws->node_vals[base + ch];
-      int cnt = 0;
-      while (cnt < kW && cand[cnt] >= 0) ++cnt;
-      for (int k = lane; k < cnt; k += 32) rows[nr + k] = cand[k];
-      for (int e = lane; e < cnt * w; e += 32) {
-        const int k = e % cnt, c = e / cnt;
-        const float v = vals[c * kW + k];
-        o[c * kChunk + nr + k] = v;
-        s[c * kChunk + nr + k] = v;
+  } else {
+    if (t == 0) {
+      int acc = 0;
+      for (int k = 0; k < kFan; ++k) {
+        coff[k] = acc;
+        const int ch = g * kFan + k;
+        acc += ch < nchild ? ws->cand_cnt[src][ch] : 0;
       }
-      nr += cnt;
+      coff[kFan] = acc;
     }
-    for (int r = lane; r < nr; r += 32) sid[r] = r;
-    __syncwarp();
-    zc = warp_gepp(s, sid, nr, w);
-    node = parent;
-    base = pbase;
-    width = pwidth;
-    publish();
+    __syncthreads();
+    nr = coff[kFan];
+    if (t < nr) {
+      int k = 0;
+      while (k + 1 < kFan && coff[k + 1] <= t) ++k;
+      const int ch = g * kFan + k, q = t - coff[k];
+      row = ws->cand_rows[src][ch][q];
+#pragma unroll
+      for (int c = 0; c < kW; ++c) o[c] = c < w ? ws->cand_vals[src][ch][c * kW + q] : 0.0f;
+    }
   }
-  __syncwarp();
-  // the root: pivots, L11 \ U11, the rows at the top before anything moves
-  for (int e = lane; e < w * w; e += 32) {
+  float v[kW];
+#pragma unroll
+  for (int c = 0; c < kW; ++c) v[c] = o[c];
+  if (t == 0) zero_col = -1;
+  __syncthreads();
+  const int step = block_gepp(v, nr, w, box, &zero_col);
+  const int cnt = min(w, nr);
+  if (!root) {
+    if (step >= 0) {
+      ws->cand_rows[dst][g][step] = row;
+#pragma unroll
+      for (int c = 0; c < kW; ++c)
+        if (c < w) ws->cand_vals[dst][g][c * kW + step] = o[c];
+    }
+    if (t == 0) ws->cand_cnt[dst][g] = cnt;
+    return;
+  }
+  // ---- root: winners, L11 \ U11, the top rows' original values ------------
+  if (step >= 0) {
+    ws->win[step] = row;
+#pragma unroll
+    for (int c = 0; c < kW; ++c)
+      if (c < w) ws->top_lu[c * kW + step] = v[c];
+  }
+  for (int e = t; e < w * w; e += kRows) {
     const int r = e % w, c = e / w;
-    ws->top_lu[r + c * kW] = s[c * kChunk + r];
-    ws->top_orig[r + c * kW] = a[(size_t)(c0 + r) + (size_t)(c0 + c) * lda];
+    ws->top_orig[c * kW + r] = a[(size_t)(c0 + r) + (size_t)(c0 + c) * lda];
   }
-  if (lane == 0) {
-    if (zc >= 0) atomicMin(&status->singular_col, c0 + zc);
-    // LAPACK sequential interchanges that bring winner j to position c0 + j;
-    // occupant tracking over the touched positions only
-    int pos[kMaxMoves], occ[kMaxMoves];
+  if (t == 0 && zero_col >= 0) atomicMin(&status->singular_col, c0 + zero_col);
+  __syncthreads();
+  // ---- LAPACK sequential interchanges bringing winner j to position c0 + j,
+  //      tracked over the touched positions only (one warp) ------------------
+  if (t < 32) {
+    __shared__ int pos[kMaxMoves], occ[kMaxMoves];
+    const int lane = t;
     int nt = 0;
-    auto find_pos = [&](int p) {
-      for (int t = 0; t < nt; ++t)
-        if (pos[t] == p) return t;
-      pos[nt] = p;
-      occ[nt] = p;  // untouched: the row that started there
-      return nt++;
+    auto find = [&](const int* arr, int v) -> int {  // index t with arr[t] == v, or -1
+      int hit = -1;
+      for (int b = 0; b < nt; b += 32) {
+        const int i = b + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, i < nt && arr[i] == v);
+        if (m != 0u && hit < 0) hit = b + __ffs(m) - 1;
+      }
+      return hit;
     };
     for (int j = 0; j < w; ++j) {
-      const int gr = rows[sid[j]];
-      int pr = gr;  // current position of row gr
-      for (int t = 0; t < nt; ++t)
-        if (occ[t] == gr) {
-          pr = pos[t];
-          break;
+      const int gr = ws->win[j];
+      const int to = find(occ, gr);
+      const int pr = to >= 0 ? pos[to] : gr;  // current position of row gr
+      int tj = find(pos, c0 + j);
+      if (tj < 0) {
+        if (lane == 0) {
+          pos[nt] = c0 + j;
+          occ[nt] = c0 + j;  // untouched: the row that started there
         }
-      ipiv[c0 + j] = pr;
-      const int tj = find_pos(c0 + j);
-      const int tp = find_pos(pr);
-      const int h = occ[tj];
-      occ[tj] = gr;
-      occ[tp] = h;
-    }
-    int nm = 0;
-    for (int t = 0; t < nt; ++t)
-      if (occ[t] != pos[t]) {
-        ws->move_pos[nm] = pos[t];
-        ws->move_src[nm] = occ[t];
-        ws->move_lab[nm] = first_leaf ? occ[t] : lab[occ[t]];
-        ++nm;
+        tj = nt++;
       }
-    ws->nmoves = nm;
+      __syncwarp();
+      int tp = find(pos, pr);
+      if (tp < 0) {
+        if (lane == 0) {
+          pos[nt] = pr;
+          occ[nt] = pr;
+        }
+        tp = nt++;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        ipiv[c0 + j] = pr;
+        const int h = occ[tj];
+        occ[tj] = gr;
+        occ[tp] = h;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      int nm = 0;
+      for (int i = 0; i < nt; ++i)
+        if (occ[i] != pos[i]) {
+          ws->move_pos[nm] = pos[i];
+          ws->move_src[nm] = occ[i];
+          ws->move_lab[nm] = first_leaf ? occ[i] : lab[occ[i]];
+          ++nm;
+        }
+      ws->nmoves = nm;
+    }
   }
 }
 
-// 3. multipliers of every row below the top, the top block, labels and the
-//    block panel's other columns
+// 3. Blocks [0, side_blocks): the block panel's other columns follow the
+//    interchanges (all reads of a column's moved entries before its writes).
+//    The rest: rows below the top get l = a U11^-1 (a from the row that ends
+//    up there), the top block and the labels.
+constexpr int kSideCols = 8;
+
 __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int n, int c0, int w, int kb0, int kb1,
-                                                         const int* ipiv, int* lab, int first_leaf,
+                                                         int* lab, int first_leaf, int side_blocks,
                                                          const TsluScratch* ws) {
   __shared__ float U[kW * kW];
   __shared__ int mpos[kMaxMoves], msrc[kMaxMoves], mlab[kMaxMoves];
-  __shared__ int nm;
-  for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = ws->top_lu[e];
-  if (threadIdx.x == 0) nm = ws->nmoves;
+  __shared__ int nm_s;
+  if (threadIdx.x == 0) nm_s = ws->nmoves;
   for (int t = threadIdx.x; t < kMaxMoves; t += blockDim.x) {
     mpos[t] = ws->move_pos[t];
     msrc[t] = ws->move_src[t];
     mlab[t] = ws->move_lab[t];
   }
-  __syncthreads();
-  const int nmv = nm;
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nth = gridDim.x * blockDim.x;
-  // rows below the top: l = a U11^-1 (a from the row that ends up there)
-  for (int r = c0 + w + gtid; r < n; r += nth) {
-    int src = r, t_hit = -1;
-    for (int t = 0; t < nmv; ++t)
-      if (mpos[t] == r) {
-        src = msrc[t];
-        t_hit = t;
+  const int side = (kb1 - kb0) - w;
+  if ((int)blockIdx.x < side_blocks) {
+    __syncthreads();
+    const int nm = nm_s;
+    // kSideCols columns x the moves: read all, then write all
+    float v[(kSideCols * kMaxMoves + 255) / 256];
+#pragma unroll
+    for (int u = 0; u < (kSideCols * kMaxMoves + 255) / 256; ++u) {
+      const int e = threadIdx.x + u * 256;
+      const int cl = e / kMaxMoves, mv = e % kMaxMoves;
+      const int cidx = blockIdx.x * kSideCols + cl;
+      v[u] = 0.0f;
+      if (cl < kSideCols && cidx < side && mv < nm) {
+        int col = kb0 + cidx;
+        if (col >= c0) col += w;
+        v[u] = a[(size_t)msrc[mv] + (size_t)col * lda];
       }
-    float l[kW];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < (kSideCols * kMaxMoves + 255) / 256; ++u) {
+      const int e = threadIdx.x + u * 256;
+      const int cl = e / kMaxMoves, mv = e % kMaxMoves;
+      const int cidx = blockIdx.x * kSideCols + cl;
+      if (cl < kSideCols && cidx < side && mv < nm) {
+        int col = kb0 + cidx;
+        if (col >= c0) col += w;
+        a[(size_t)mpos[mv] + (size_t)col * lda] = v[u];
+      }
+    }
+    return;
+  }
+  for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = ws->top_lu[e];
+  __syncthreads();
+  const int nm = nm_s;
+  const int gtid = (blockIdx.x - side_blocks) * blockDim.x + threadIdx.x;
+  const int nth = (gridDim.x - side_blocks) * blockDim.x;
+  // rows below the top
+  for (int r = c0 + w + gtid; r < n; r += nth) {
+    int src = r, hit = -1;
+    for (int q = 0; q < nm; ++q)
+      if (mpos[q] == r) hit = q;
+    if (hit >= 0) src = msrc[hit];
+    // a row below the top either stays or is a row displaced from the top
+    const bool from_top = src < c0 + w;
+    float x[kW];
+#pragma unroll
+    for (int j = 0; j < kW; ++j)
+      x[j] = j < w ? (from_top ? ws->top_orig[j * kW + (src - c0)] : a[(size_t)src + (size_t)(c0 + j) * lda]) : 0.0f;
 #pragma unroll
     for (int j = 0; j < kW; ++j) {
       if (j < w) {
-        // a row displaced from the top reads its saved original values
-        float s = src >= c0 + w || src < c0 ? a[(size_t)src + (size_t)(c0 + j) * lda]
-                                            : ws->top_orig[(src - c0) + j * kW];
+        float s = x[j];
 #pragma unroll
         for (int i = 0; i < kW; ++i)
-          if (i < j) s = fmaf(-l[i], U[i + j * kW], s);
-        l[j] = s / U[j + j * kW];
+          if (i < j) s = fmaf(-x[i], U[i + j * kW], s);
+        const float d = U[j + j * kW];
+        x[j] = d != 0.0f ? s / d : 0.0f;
       }
     }
-    // write after every read of this row's source (a source below the top is the row itself)
 #pragma unroll
     for (int j = 0; j < kW; ++j)
-      if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = l[j];
-    if (t_hit >= 0)
-      lab[r] = mlab[t_hit];
+      if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = x[j];
+    if (hit >= 0)
+      lab[r] = mlab[hit];
     else if (first_leaf)
       lab[r] = r;
   }
-  // the top block and the top positions' labels
+  // the top block (row k = winner k's factored row) and the top labels
   for (int e = gtid; e < w * w; e += nth) {
     const int r = e % w, c = e / w;
     a[(size_t)(c0 + r) + (size_t)(c0 + c) * lda] = U[r + c * kW];
   }
   for (int r = c0 + gtid; r < c0 + w; r += nth) {
-    int t_hit = -1;
-    for (int t = 0; t < nmv; ++t)
-      if (mpos[t] == r) t_hit = t;
-    if (t_hit >= 0)
-      lab[r] = mlab[t_hit];
+    int hit = -1;
+    for (int q = 0; q < nm; ++q)
+      if (mpos[q] == r) hit = q;
+    if (hit >= 0)
+      lab[r] = mlab[hit];
     else if (first_leaf)
       lab[r] = r;
-  }
-  // the block panel's other columns follow the interchanges (in order)
-  const int side = (kb1 - kb0) - w;
-  for (int cidx = gtid; cidx < side; cidx += nth) {
-    int col = kb0 + cidx;
-    if (col >= c0) col += w;
-    float* cp = a + (size_t)col * lda;
-    for (int j = 0; j < w; ++j) {
-      const int pr = ipiv[c0 + j];
-      if (pr != c0 + j) {
-        const float t = cp[c0 + j];
-        cp[c0 + j] = cp[pr];
-        cp[pr] = t;
-      }
-    }
   }
 }
 
@@ -320,21 +374,34 @@ size_t tslu_scratch_bytes() { return sizeof(TsluScratch); }
 // A leaf panel of the FP32 LU by tournament pivoting; same outputs as the
 // partial-pivoting cluster kernel (factored panel, ipiv, labels, side
 // columns). Returns ALG_NOT_IMPLEMENTED when the panel does not fit its
-// limits (the caller then uses partial pivoting). The scratch's arrival
-// counters must be zero on the first call (the caller clears it once).
+// limits (the caller then uses partial pivoting). Nothing in the scratch
+// needs clearing between calls.
 int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch) {
   const int m = p.n - p.c0, w = p.w;
   if (w > kW || w < 1 || m < w) return ALG_NOT_IMPLEMENTED;
-  const int nchunks = (m + kChunk - 1) / kChunk;
-  if (nchunks > kMaxChunks) return ALG_NOT_IMPLEMENTED;
+  const int groups0 = (m + kRows - 1) / kRows;
+  if (groups0 > kMaxGroups) return ALG_NOT_IMPLEMENTED;
   auto* ws = static_cast<TsluScratch*>(scratch);
   const int tok = prof_begin(ctx, ALG_K_PANEL);
-  tslu_tree_kernel<<<(nchunks + kTreeWarps - 1) / kTreeWarps, kTreeWarps * 32, 0, ctx->stream>>>(
-      p.a, p.lda, p.n, p.c0, w, nchunks, p.ipiv, p.lab, p.first_leaf, p.status, ws);
-  const int grid = std::max(1, std::min(2 * ctx->sm_count, (m + 255) / 256));
-  tslu_apply_kernel<<<grid, 256, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, p.kb0, p.kb1, p.ipiv, p.lab,
-                                                   p.first_leaf, ws);
-  count_launches(2);
+  // level 0 reads the panel; each later level merges kFan proposals per CTA
+  int groups = groups0, src = -1, dst = 0, nchild = 0, launches = 0;
+  for (;;) {
+    const bool root = groups == 1;
+    tslu_level_kernel<<<groups, kRows, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, src, nchild, dst, root ? 1 : 0,
+                                                          p.ipiv, p.lab, p.first_leaf, p.status, ws);
+    ++launches;
+    if (root) break;
+    nchild = groups;
+    groups = (groups + kFan - 1) / kFan;
+    src = dst;
+    dst = 1 - dst;
+  }
+  const int side = (p.kb1 - p.kb0) - w;
+  const int side_blocks = side > 0 ? (side + kSideCols - 1) / kSideCols : 0;
+  const int row_blocks = std::max(1, std::min(2 * ctx->sm_count, (m + 255) / 256));
+  tslu_apply_kernel<<<side_blocks + row_blocks, 256, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, p.kb0, p.kb1,
+                                                                       p.lab, p.first_leaf, side_blocks, ws);
+  count_launches(launches + 1);
   double pflops = 0;
   for (int j = 0; j < w; ++j) pflops += double(m - j - 1) * (1.0 + 2.0 * (w - j - 1));
   prof_end(ctx, tok, pflops, 2.0 * sizeof(float) * m * w);

@@ -29,10 +29,10 @@ class Report(C.Structure):
     def as_dict(self) -> dict:
         return {"path": PATHS.get(self.path, "none"), "ir_iterations": self.ir_iterations,
                 "gmres_iterations": self.gmres_iterations, "backward_error": self.backward_error,
-                "butterfly": bool(self.reserved[0])}
+                "butterfly": bool(self.reserved[0]), "tournament": bool(self.reserved[1])}
 
 
-PIVOTING = {"auto": 0, "partial": 1, "rbt": 2}
+PIVOTING = {"auto": 0, "partial": 1, "rbt": 2, "tournament": 3}
 
 
 def opts(precision: str = "fp32", tol: float = 0.0, max_ir: int = 30, no_fallback: bool = False,

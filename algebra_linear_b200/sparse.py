@@ -86,7 +86,7 @@ class _Plan(C.Structure):
     _fields_ = [("n_fronts", C.c_size_t), ("n_small_fronts", C.c_size_t), ("small_levels", C.c_size_t),
                 ("solve_levels", C.c_size_t), ("max_front_rows", C.c_size_t), ("max_front_cols", C.c_size_t),
                 ("factor_bytes", C.c_size_t), ("work_bytes", C.c_size_t), ("plan_flops", C.c_double),
-                ("structurally_singular", C.c_int)]
+                ("structurally_singular", C.c_int), ("n_lanes", C.c_int), ("top_fronts", C.c_size_t)]
 
 
 class _Refine(C.Structure):

@@ -169,14 +169,19 @@ int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda,
 #define ALG_PREC_TF32X3 3
 
 /* Stabilisation of the low-precision LU: partial pivoting (the reference's
- * strategy, column-serial panel), or a random butterfly transformation of A
- * followed by LU without pivoting (Baboulin, Dongarra, Herrmann, Tomov, ACM
- * TOMS 2013; needs n divisible by 4; falls back to pivoting on a zero pivot).
- * AUTO means partial pivoting: LU without pivoting keeps a large growth factor
- * on matrices that are random to begin with, butterflies or not. */
+ * strategy, column-serial panel); tournament pivoting (CALU's TSLU, Grigori,
+ * Demmel and Xiang, SIMAX 2011: each leaf panel's pivot rows are chosen by a
+ * reduction tree of partial-pivoting LUs over row blocks, so the column-serial
+ * chain runs on 256-row blocks instead of the whole panel); or a random
+ * butterfly transformation of A followed by LU without pivoting (Baboulin,
+ * Dongarra, Herrmann, Tomov, ACM TOMS 2013; needs n divisible by 4; falls back
+ * to pivoting on a zero pivot). AUTO: tournament pivoting for n >= 2048,
+ * partial pivoting below; LU without pivoting keeps a large growth factor on
+ * matrices that are random to begin with, butterflies or not. */
 #define ALG_PIVOT_AUTO 0
 #define ALG_PIVOT_PARTIAL 1
 #define ALG_PIVOT_RBT 2
+#define ALG_PIVOT_TOURNAMENT 3
 
 #define ALG_MIXED_PATH_IR 1
 #define ALG_MIXED_PATH_GMRES 2
@@ -199,7 +204,7 @@ typedef struct {
   int ir_iterations;
   int gmres_iterations;
   double backward_error;  /* worst over the right-hand sides; -1 on the FP64 path */
-  double reserved[4];
+  double reserved[4];     /* [0]: 1 when the butterfly form ran; [1]: 1 when tournament pivoting ran */
 } alg_mixed_report;
 
 void alg_mixed_opts_default(alg_mixed_opts* opts);
@@ -320,6 +325,8 @@ typedef struct {
   size_t factor_bytes, work_bytes;
   double plan_flops;
   int structurally_singular;
+  int n_lanes;            /* concurrent lanes of large fronts (independent subtrees) */
+  size_t top_fronts;      /* large fronts factored after the lanes */
 } alg_splu_plan;
 int alg_splu_plan_info(const alg_splu* lu, alg_splu_plan* out);
 

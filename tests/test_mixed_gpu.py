@@ -67,7 +67,7 @@ def test_tensor_core_update_matches_reference(gpu, prec, shape):
         assert err <= 1e-5 * scale, (err, scale)
 
 
-@pytest.mark.parametrize("pivoting", ["partial"])
+@pytest.mark.parametrize("pivoting", ["partial", "tournament"])
 @pytest.mark.parametrize("prec", ["fp32", "tf32", "tf32x3", "bf16"])
 def test_mixed_solve_reaches_fp64_backward_error(gpu, oracle, prec, pivoting):
     import torch
@@ -149,4 +149,27 @@ def test_butterfly_form_on_a_diagonally_dominant_system(gpu, oracle):
         x = B.cpu().numpy()
         assert np.array_equal(A.cpu().numpy(), a)
     assert rep["butterfly"] and rep["path"] in ("ir", "gmres"), rep
+    assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53
+
+
+@pytest.mark.parametrize("n", [1536, 5000])
+@pytest.mark.parametrize("prec", ["fp32", "tf32x3"])
+def test_tournament_pivoting_panels(gpu, oracle, n, prec):
+    """Tournament-pivoting leaf panels: the FP32 LU stays a good
+    preconditioner (plain refinement, few steps) and x reaches the FP64
+    backward error; n = 5000 takes two merge levels."""
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    a, _, b = oracle.c1_system(n, seed=[3, 1, 4, 1])
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        B = torch.from_numpy(b.copy()).cuda()
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision=prec, pivoting="tournament", no_gmres=True,
+                                    no_fallback=True)
+        assert rep["tournament"], rep
+        x = B.cpu().numpy()
+        assert np.array_equal(A.cpu().numpy(), a)
+    assert rep["path"] == "ir" and rep["ir_iterations"] <= 8, rep
     assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53

@@ -125,6 +125,26 @@ def test_precision_settings_are_validated_on_the_host():
     assert _raises("NotFactorized", lu.last_solve)
 
 
+def test_large_fronts_split_into_lanes(monkeypatch):
+    """Analyze spreads independent subtrees of large fronts over concurrent
+    lanes (host-only plan; the 24^3 grid's tree splits into two heavy
+    subtrees below a chain of top fronts)."""
+    from oracle import sparse as osp
+
+    cp, ri, _ = osp.grid_pattern(24, 24, 24)
+    for lanes in ("1", "2"):
+        monkeypatch.setenv("ALG_SPLU_LANES", lanes)
+        plan = SparseLu.analyze(cp, ri, LuMethod.supernodal()).plan()
+        assert plan["n_lanes"] == int(lanes)
+        if lanes == "1":
+            assert plan["top_fronts"] == 0
+            one = plan
+        else:
+            assert plan["top_fronts"] >= 1
+            # same fronts and flops; the lanes only reorder independent work
+            assert plan["n_fronts"] == one["n_fronts"] and plan["plan_flops"] == one["plan_flops"]
+
+
 def _tridiag(n, dense=False):
     cp, ri, v = [0], [], []
     for j in range(n):

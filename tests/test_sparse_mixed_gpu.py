@@ -182,3 +182,22 @@ def test_device_resident_mixed_solve_is_deterministic(gpu, osp):
         assert lu.last_solve()["iterations"] >= 1
         lu.close()
     assert np.array_equal(xh, xd)
+
+
+def test_lanes_do_not_change_the_result(gpu, osp, monkeypatch):
+    """Independent subtrees factored on two concurrent lanes give the same
+    factors, bit for bit, as one lane (no arithmetic depends on the order)."""
+    cp, ri, kind = osp.grid_pattern(20, 20, 20)
+    v, _ = osp.convection_diffusion_values(kind, SEED)
+    n = len(cp) - 1
+    b, _ = osp.dense.larnv("Symmetric", [7, 7, 7, 7], n)
+    xs = []
+    for lanes in ("1", "2"):
+        monkeypatch.setenv("ALG_SPLU_LANES", lanes)
+        lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+        assert lu.plan()["n_lanes"] == int(lanes)
+        lu.factorize(cp, ri, v)
+        x = b.copy()
+        lu.solve(x)
+        xs.append((x, lu.row_perm(), lu.stats()["nnz_l"]))
+    assert np.array_equal(xs[0][0], xs[1][0]) and np.array_equal(xs[0][1], xs[1][1]) and xs[0][2] == xs[1][2]
