@@ -922,6 +922,12 @@ int DeviceLu::factor_big(int b, int32_t s, int lane, const double* values, int t
   lp.nb = 64;
   lp.nbl = 16;
   lp.tc_prec = tc_prec;
+  if constexpr (std::is_same<T, float>::value) {
+    // the mixed form's FP32 fronts pivot by tournament (refinement restores
+    // the FP64 backward error); the FP64 form keeps the reference's pivots
+    lp.tslu = 1;
+    lp.nbl = 32;
+  }
   ALG_TRY((lu_factor_partial_dev<T, false>(lc, front, d.rows, d.size, cols, d.rows, d_ipiv[lane], d_perm[lane], lp)));
   T* L = reinterpret_cast<T*>(out.L);
   T* U = reinterpret_cast<T*>(out.U);
