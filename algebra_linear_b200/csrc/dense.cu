@@ -152,8 +152,31 @@ int launch_panel(alg_ctx* ctx, const PanelArgs<T>& args) {
 }
 
 template <typename T, bool EXACT>
+int launch_trsm_reg(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
+  const size_t smem = sizeof(T) * (size_t)kb * kb;
+  auto kern = kb <= 32 ? trsm_lower_unit_reg_kernel<T, EXACT, 1>
+                       : (kb <= 64 ? trsm_lower_unit_reg_kernel<T, EXACT, 2> : trsm_lower_unit_reg_kernel<T, EXACT, 4>);
+  static bool configured = false;
+  if (!configured) {
+    for (auto k : {trsm_lower_unit_reg_kernel<T, EXACT, 1>, trsm_lower_unit_reg_kernel<T, EXACT, 2>,
+                   trsm_lower_unit_reg_kernel<T, EXACT, 4>})
+      ALG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    configured = true;
+  }
+  const int grid = (ce - cb + kTrsmRegCols - 1) / kTrsmRegCols;
+  const int tok = prof_begin(ctx, ALG_K_TRSM);
+  kern<<<grid, kTrsmThreads, smem, ctx->stream>>>(a, lda, r0, kb, cb, ce);
+  count_launches();
+  prof_end(ctx, tok, double(kb) * (kb - 1) * (ce - cb), sizeof(T) * (double(kb) * kb / 2 + 2.0 * kb * (ce - cb)));
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
+template <typename T, bool EXACT>
 int launch_trsm(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
   if (ce <= cb || kb <= 1) return ALG_OK;
+  // register form for the LU's block widths (<= 128); the shared-memory form beyond
+  if (kb <= 128) return launch_trsm_reg<T, EXACT>(ctx, a, lda, r0, kb, cb, ce);
   const size_t smem = sizeof(T) * ((size_t)kb * kb + (size_t)kb * kTrsmCols);
   static bool configured = false;
   if (!configured) {

@@ -915,6 +915,70 @@ __global__ void __launch_bounds__(kTrsmThreads) trsm_lower_unit_kernel(
   }
 }
 
+// The same solve with no block barrier inside: L11 (kb <= 128) staged in
+// shared memory, each warp owns kTrsmRegCols / 8 whole columns with lane l
+// holding rows l, l + 32, ... in registers; step k broadcasts x_k from its
+// owner lane by a shuffle. Every entry still takes its terms in increasing k
+// as one rounded multiply-subtract each, so the result is bit-identical.
+constexpr int kTrsmRegCols = 64;
+
+template <typename T, bool EXACT, int RPT>
+__global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T* a, int lda, int r0, int kb, int cb,
+                                                                           int ce) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* L = reinterpret_cast<T*>(smem_raw);  // kb x kb, column-major
+  constexpr int kWarpCols = kTrsmRegCols / (kTrsmThreads / 32);
+  const int c_first = cb + blockIdx.x * kTrsmRegCols;
+  const int ncol = min(kTrsmRegCols, ce - c_first);
+  if (ncol <= 0) return;
+  for (int idx = threadIdx.x; idx < kb * kb; idx += kTrsmThreads) {
+    const int i = idx % kb, k = idx / kb;
+    L[idx] = a[(size_t)(r0 + i) + (size_t)(r0 + k) * lda];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T x[kWarpCols][RPT];
+#pragma unroll
+  for (int c = 0; c < kWarpCols; ++c) {
+    const int cc = warp * kWarpCols + c;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int i = lane + 32 * r;
+      x[c][r] = (cc < ncol && i < kb) ? a[(size_t)(r0 + i) + (size_t)(c_first + cc) * lda] : T(0);
+    }
+  }
+  __syncthreads();
+  for (int k = 0; k + 1 < kb; ++k) {
+    const int owner = k & 31, rk = k >> 5;
+    T u[kWarpCols];
+#pragma unroll
+    for (int c = 0; c < kWarpCols; ++c) {
+      T xv = x[c][0];
+#pragma unroll
+      for (int r = 1; r < RPT; ++r)
+        if (r == rk) xv = x[c][r];
+      u[c] = __shfl_sync(0xffffffffu, xv, owner);
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int i = lane + 32 * r;
+      if (i > k && i < kb) {
+        const T l = L[i + (size_t)k * kb];
+#pragma unroll
+        for (int c = 0; c < kWarpCols; ++c) x[c][r] = msub<EXACT>(x[c][r], l, u[c]);
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kWarpCols; ++c) {
+    const int cc = warp * kWarpCols + c;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int i = lane + 32 * r;
+      if (cc < ncol && i < kb) a[(size_t)(r0 + i) + (size_t)(c_first + cc) * lda] = x[c][r];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K4 (CUDA-core form): C -= A * B with C M x N, A M x K, B K x N, all
 // column-major. Each thread owns an 8 x 8 block of C in registers, loads it

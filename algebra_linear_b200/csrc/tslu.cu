@@ -63,15 +63,36 @@ struct GeppBox {
   int idx[2][kWarps];
 };
 
-__device__ __forceinline__ int block_gepp(float (&v)[kW], int nr, int w, GeppBox& box, int* zero_col) {
+// v[j] for a run-time j by a log-depth select tree (a linear scan would be a
+// W-long dependent chain)
+template <int W>
+__device__ __forceinline__ float select_col(const float (&v)[W], int j) {
+  float t16[(W + 1) / 2];
+  if constexpr (W == 32) {
+    float t[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) t[i] = (j & 16) ? v[i + 16] : v[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t16[i] = (j & 8) ? t[i + 8] : t[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t16[i] = (j & 8) ? v[i + 8] : v[i];
+  }
+  float t4[4], t2[2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t16[i + 4] : t16[i];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) t2[i] = (j & 2) ? t4[i + 2] : t4[i];
+  return (j & 1) ? t2[1] : t2[0];
+}
+
+template <int W>
+__device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppBox& box, int* zero_col) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   int chosen = -1;
   for (int j = 0; j < w; ++j) {
     const int par = j & 1;
-    float vj = v[0];
-#pragma unroll
-    for (int c = 1; c < kW; ++c)
-      if (c == j) vj = v[c];
+    const float vj = select_col<W>(v, j);
     float key = (t < nr && chosen < 0) ? fabsf(vj) : -1.0f;
     int idx = t;
 #pragma unroll
@@ -92,7 +113,7 @@ __device__ __forceinline__ int block_gepp(float (&v)[kW], int nr, int w, GeppBox
       box.key[par][warp] = key;
       box.idx[par][warp] = idx;
 #pragma unroll
-      for (int c = 0; c < kW; ++c) box.row[par][warp][c] = v[c];
+      for (int c = 0; c < W; ++c) box.row[par][warp][c] = v[c];
     }
     __syncthreads();
     float bk = lane < kWarps ? box.key[par][lane] : -1.0f;
@@ -120,9 +141,9 @@ __device__ __forceinline__ int block_gepp(float (&v)[kW], int nr, int w, GeppBox
     if (t < nr && chosen < 0) {
       const float l = pv != 0.0f ? vj / pv : 0.0f;
 #pragma unroll
-      for (int c = 0; c < kW; ++c) {
+      for (int c = 0; c < W; ++c) {
         if (c == j) v[c] = l;
-        if (c > j && c < w) v[c] = fmaf(-l, prow[c], v[c]);
+        if (c > j) v[c] = fmaf(-l, prow[c], v[c]);  // columns >= w stay zero (prow is zero there)
       }
     }
   }
@@ -135,6 +156,7 @@ __device__ __forceinline__ int block_gepp(float (&v)[kW], int nr, int w, GeppBox
 // from scratch slot src. Writes this CTA's proposals to slot dst; the single
 // CTA of the last level (root) also writes the winners, L11 \ U11, the rows
 // at the top before anything moves, ipiv and the list of moved rows.
+template <int W>
 __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __restrict__ a, int lda, int n, int c0,
                                                            int w, int src, int nchild, int dst, int root,
                                                            int* ipiv, const int* lab, int first_leaf,
@@ -143,9 +165,9 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
   __shared__ int zero_col;
   __shared__ int coff[kFan + 1];
   const int t = threadIdx.x, g = blockIdx.x;
-  float o[kW];  // this row's original values
+  float o[W];  // this row's original values
 #pragma unroll
-  for (int c = 0; c < kW; ++c) o[c] = 0.0f;
+  for (int c = 0; c < W; ++c) o[c] = 0.0f;
   int row = -1, nr = 0;
   if (src < 0) {
     const int r0 = c0 + g * kRows;
@@ -153,7 +175,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
     if (t < nr) {
       row = r0 + t;
 #pragma unroll
-      for (int c = 0; c < kW; ++c) o[c] = c < w ? a[(size_t)row + (size_t)(c0 + c) * lda] : 0.0f;
+      for (int c = 0; c < W; ++c) o[c] = c < w ? a[(size_t)row + (size_t)(c0 + c) * lda] : 0.0f;
     }
   } else {
     if (t == 0) {
@@ -173,21 +195,21 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
       const int ch = g * kFan + k, q = t - coff[k];
       row = ws->cand_rows[src][ch][q];
 #pragma unroll
-      for (int c = 0; c < kW; ++c) o[c] = c < w ? ws->cand_vals[src][ch][c * kW + q] : 0.0f;
+      for (int c = 0; c < W; ++c) o[c] = c < w ? ws->cand_vals[src][ch][c * kW + q] : 0.0f;
     }
   }
-  float v[kW];
+  float v[W];
 #pragma unroll
-  for (int c = 0; c < kW; ++c) v[c] = o[c];
+  for (int c = 0; c < W; ++c) v[c] = o[c];
   if (t == 0) zero_col = -1;
   __syncthreads();
-  const int step = block_gepp(v, nr, w, box, &zero_col);
+  const int step = block_gepp<W>(v, nr, w, box, &zero_col);
   const int cnt = min(w, nr);
   if (!root) {
     if (step >= 0) {
       ws->cand_rows[dst][g][step] = row;
 #pragma unroll
-      for (int c = 0; c < kW; ++c)
+      for (int c = 0; c < W; ++c)
         if (c < w) ws->cand_vals[dst][g][c * kW + step] = o[c];
     }
     if (t == 0) ws->cand_cnt[dst][g] = cnt;
@@ -197,7 +219,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
   if (step >= 0) {
     ws->win[step] = row;
 #pragma unroll
-    for (int c = 0; c < kW; ++c)
+    for (int c = 0; c < W; ++c)
       if (c < w) ws->top_lu[c * kW + step] = v[c];
   }
   for (int e = t; e < w * w; e += kRows) {
@@ -271,6 +293,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
 //    up there), the top block and the labels.
 constexpr int kSideCols = 8;
 
+template <int W>
 __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int n, int c0, int w, int kb0, int kb1,
                                                          int* lab, int first_leaf, int side_blocks,
                                                          const TsluScratch* ws) {
@@ -328,23 +351,22 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int 
     if (hit >= 0) src = msrc[hit];
     // a row below the top either stays or is a row displaced from the top
     const bool from_top = src < c0 + w;
-    float x[kW];
+    float x[W];
 #pragma unroll
-    for (int j = 0; j < kW; ++j)
+    for (int j = 0; j < W; ++j)
       x[j] = j < w ? (from_top ? ws->top_orig[j * kW + (src - c0)] : a[(size_t)src + (size_t)(c0 + j) * lda]) : 0.0f;
 #pragma unroll
-    for (int j = 0; j < kW; ++j) {
+    for (int j = 0; j < W; ++j) {
       if (j < w) {
         float s = x[j];
 #pragma unroll
-        for (int i = 0; i < kW; ++i)
-          if (i < j) s = fmaf(-x[i], U[i + j * kW], s);
+        for (int i = 0; i < j; ++i) s = fmaf(-x[i], U[i + j * kW], s);
         const float d = U[j + j * kW];
         x[j] = d != 0.0f ? s / d : 0.0f;
       }
     }
 #pragma unroll
-    for (int j = 0; j < kW; ++j)
+    for (int j = 0; j < W; ++j)
       if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = x[j];
     if (hit >= 0)
       lab[r] = mlab[hit];
@@ -387,8 +409,14 @@ int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch) {
   int groups = groups0, src = -1, dst = 0, nchild = 0, launches = 0;
   for (;;) {
     const bool root = groups == 1;
-    tslu_level_kernel<<<groups, kRows, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, src, nchild, dst, root ? 1 : 0,
-                                                          p.ipiv, p.lab, p.first_leaf, p.status, ws);
+    if (w <= 16)
+      tslu_level_kernel<16><<<groups, kRows, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, src, nchild, dst,
+                                                                root ? 1 : 0, p.ipiv, p.lab, p.first_leaf, p.status,
+                                                                ws);
+    else
+      tslu_level_kernel<32><<<groups, kRows, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, src, nchild, dst,
+                                                                root ? 1 : 0, p.ipiv, p.lab, p.first_leaf, p.status,
+                                                                ws);
     ++launches;
     if (root) break;
     nchild = groups;
@@ -399,8 +427,14 @@ int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch) {
   const int side = (p.kb1 - p.kb0) - w;
   const int side_blocks = side > 0 ? (side + kSideCols - 1) / kSideCols : 0;
   const int row_blocks = std::max(1, std::min(2 * ctx->sm_count, (m + 255) / 256));
-  tslu_apply_kernel<<<side_blocks + row_blocks, 256, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, p.kb0, p.kb1,
-                                                                       p.lab, p.first_leaf, side_blocks, ws);
+  if (w <= 16)
+    tslu_apply_kernel<16><<<side_blocks + row_blocks, 256, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, p.kb0,
+                                                                             p.kb1, p.lab, p.first_leaf,
+                                                                             side_blocks, ws);
+  else
+    tslu_apply_kernel<32><<<side_blocks + row_blocks, 256, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, p.kb0,
+                                                                             p.kb1, p.lab, p.first_leaf,
+                                                                             side_blocks, ws);
   count_launches(launches + 1);
   double pflops = 0;
   for (int j = 0; j < w; ++j) pflops += double(m - j - 1) * (1.0 + 2.0 * (w - j - 1));
