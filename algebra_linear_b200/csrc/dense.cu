@@ -172,24 +172,23 @@ int launch_trsm_reg(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce)
   return ALG_OK;
 }
 
+// U12 = L11^-1 A12 for the kb x kb unit-lower block at (r0, r0) and columns
+// [cb, ce): the register kernel for kb <= 128, else by 128-row diagonal
+// blocks with the rows below updated by the trailing GEMM in between (every
+// entry still takes its terms in increasing k, so the exact form is kept).
 template <typename T, bool EXACT>
 int launch_trsm(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
   if (ce <= cb || kb <= 1) return ALG_OK;
-  // register form for the LU's block widths (<= 128); the shared-memory form beyond
   if (kb <= 128) return launch_trsm_reg<T, EXACT>(ctx, a, lda, r0, kb, cb, ce);
-  const size_t smem = sizeof(T) * ((size_t)kb * kb + (size_t)kb * kTrsmCols);
-  static bool configured = false;
-  if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(trsm_lower_unit_kernel<T, EXACT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    configured = true;
+  for (int k0 = 0; k0 < kb; k0 += 128) {
+    const int bk = std::min(128, kb - k0);
+    ALG_TRY((launch_trsm_reg<T, EXACT>(ctx, a, lda, r0 + k0, bk, cb, ce)));
+    const int below = kb - k0 - bk;
+    if (below > 0)
+      ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, below, ce - cb, bk, a + (size_t)(r0 + k0 + bk) + (size_t)(r0 + k0) * lda,
+                                      lda, a + (size_t)(r0 + k0) + (size_t)cb * lda, lda,
+                                      a + (size_t)(r0 + k0 + bk) + (size_t)cb * lda, lda)));
   }
-  const int grid = (ce - cb + kTrsmCols - 1) / kTrsmCols;
-  const int tok = prof_begin(ctx, ALG_K_TRSM);
-  trsm_lower_unit_kernel<T, EXACT><<<grid, kTrsmThreads, smem, ctx->stream>>>(a, lda, r0, kb, cb, ce);
-  count_launches();
-  prof_end(ctx, tok, double(kb) * (kb - 1) * (ce - cb), sizeof(T) * (double(kb) * kb / 2 + 2.0 * kb * (ce - cb)));
-  ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
 }
 

@@ -875,51 +875,13 @@ __global__ void iota_kernel(int* v, int n) {
 // ---------------------------------------------------------------------------
 // K3: U12 = L11^{-1} A12 for rows [r0, r0+kb) of columns [cb, ce), unit lower
 // L11 = a[r0:r0+kb, r0:r0+kb]. Entry (i, c) receives `-= l_ik * u_kc` for
-// k = r0 .. i-1 in that order, the reference's order for those entries.
-// One CTA owns 32 columns; a step k updates every row below k in parallel.
+// k = r0 .. i-1 in that order (one rounded multiply-subtract each in the
+// exact form), the reference's order for those entries. No block barrier
+// inside: L11 (kb <= 128) staged in shared memory, each warp owns
+// kTrsmRegCols / 8 whole columns with lane l holding rows l, l + 32, ... in
+// registers; step k broadcasts x_k from its owner lane by a shuffle.
 // ---------------------------------------------------------------------------
 constexpr int kTrsmThreads = 256;
-constexpr int kTrsmCols = 32;
-
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_lower_unit_kernel(
-    T* a, int lda, int r0, int kb, int cb, int ce) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* L = reinterpret_cast<T*>(smem_raw);     // kb x kb, column-major
-  T* X = L + (size_t)kb * kb;                 // kb x kTrsmCols, row-major
-  const int c_first = cb + blockIdx.x * kTrsmCols;
-  const int ncol = min(kTrsmCols, ce - c_first);
-  if (ncol <= 0) return;
-  for (int idx = threadIdx.x; idx < kb * kb; idx += kTrsmThreads) {
-    const int i = idx % kb, k = idx / kb;
-    L[idx] = a[(size_t)(r0 + i) + (size_t)(r0 + k) * lda];
-  }
-  for (int idx = threadIdx.x; idx < kb * kTrsmCols; idx += kTrsmThreads) {
-    const int i = idx % kb, c = idx / kb;
-    X[i * kTrsmCols + c] = c < ncol ? a[(size_t)(r0 + i) + (size_t)(c_first + c) * lda] : T(0);
-  }
-  __syncthreads();
-  const int c = threadIdx.x % kTrsmCols;
-  const int g = threadIdx.x / kTrsmCols;
-  constexpr int G = kTrsmThreads / kTrsmCols;
-  for (int k = 0; k + 1 < kb; ++k) {
-    const T u = X[k * kTrsmCols + c];
-    for (int i = k + 1 + g; i < kb; i += G) {
-      X[i * kTrsmCols + c] = msub<EXACT>(X[i * kTrsmCols + c], L[i + (size_t)k * kb], u);
-    }
-    __syncthreads();
-  }
-  for (int idx = threadIdx.x; idx < kb * kTrsmCols; idx += kTrsmThreads) {
-    const int i = idx % kb, cc = idx / kb;
-    if (cc < ncol) a[(size_t)(r0 + i) + (size_t)(c_first + cc) * lda] = X[i * kTrsmCols + cc];
-  }
-}
-
-// The same solve with no block barrier inside: L11 (kb <= 128) staged in
-// shared memory, each warp owns kTrsmRegCols / 8 whole columns with lane l
-// holding rows l, l + 32, ... in registers; step k broadcasts x_k from its
-// owner lane by a shuffle. Every entry still takes its terms in increasing k
-// as one rounded multiply-subtract each, so the result is bit-identical.
 constexpr int kTrsmRegCols = 64;
 
 template <typename T, bool EXACT, int RPT>

@@ -47,103 +47,127 @@ struct TsluScratch {
   float top_orig[kW * kW];                  // original values of the rows at the top positions
 };
 
-// Partial-pivoting LU of the first w columns of nr <= 256 rows, row t in
-// thread t's registers v[], rows left in place. One barrier per column: each
-// warp publishes its best candidate (key, index and the whole row) in a
-// mailbox double-buffered by column parity, and every warp reduces the
-// mailboxes itself. Returns the step at which this thread's row was chosen
-// (-1: not chosen); the chosen row's v[] then holds its multipliers (columns
-// before its step) and its U entries (from its step on). zero_col: first
-// column whose pivot was zero (thread 0's copy).
 constexpr int kWarps = kRows / 32;
 
-struct GeppBox {
-  float row[2][kWarps][kW];
+// Partial-pivoting LU of the first w columns of nr <= 256 rows, row t in
+// thread t's registers v[], rows left in place, blocked by kSub columns:
+// inside a sub-block each column costs one barrier — every warp publishes its
+// best candidate (key, index and the row's kSub sub-block entries) in a
+// mailbox double-buffered by column parity and every warp reduces the
+// mailboxes itself — and only the sub-block's columns are updated; after the
+// sub-block its pivot rows' entries right of it become U12 by a forward
+// substitution in shared memory and every other row takes the rank-kSub
+// update at once. Returns the step at which this thread's row was chosen
+// (-1: not chosen); the chosen row's v[] then holds its multipliers (columns
+// before its step) and its U entries (from its step on). zero_col: first
+// column whose pivot was zero.
+constexpr int kSub = 8;
+
+struct GeppShared {
+  float row[2][kWarps][kSub];  // mailboxes: each warp's best row, sub-block entries
   float key[2][kWarps];
   int idx[2][kWarps];
+  float prow[kSub][kW];        // the sub-block's pivot rows (then U12 right of the sub-block)
 };
 
-// v[j] for a run-time j by a log-depth select tree (a linear scan would be a
-// W-long dependent chain)
 template <int W>
-__device__ __forceinline__ float select_col(const float (&v)[W], int j) {
-  float t16[(W + 1) / 2];
-  if constexpr (W == 32) {
-    float t[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) t[i] = (j & 16) ? v[i + 16] : v[i];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) t16[i] = (j & 8) ? t[i + 8] : t[i];
-  } else {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) t16[i] = (j & 8) ? v[i + 8] : v[i];
-  }
-  float t4[4], t2[2];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) t4[i] = (j & 4) ? t16[i + 4] : t16[i];
-#pragma unroll
-  for (int i = 0; i < 2; ++i) t2[i] = (j & 2) ? t4[i + 2] : t4[i];
-  return (j & 1) ? t2[1] : t2[0];
-}
-
-template <int W>
-__device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppBox& box, int* zero_col) {
+__device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShared& sh, int* zero_col) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   int chosen = -1;
-  for (int j = 0; j < w; ++j) {
-    const int par = j & 1;
-    const float vj = select_col<W>(v, j);
-    float key = (t < nr && chosen < 0) ? fabsf(vj) : -1.0f;
-    int idx = t;
+  bool done = false;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const float ok = __shfl_xor_sync(0xffffffffu, key, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
-      if (ok > key || (ok == key && oi < idx)) {
-        key = ok;
-        idx = oi;
+  for (int jb = 0; jb < W; jb += kSub) {
+    if (done || jb >= w) break;
+    const int nsub = min(kSub, w - jb);
+    for (int jj = 0; jj < nsub; ++jj) {
+      const int j = jb + jj, par = j & 1;
+      float vj = v[jb];
+#pragma unroll
+      for (int cc = 1; cc < kSub; ++cc)
+        if (cc == jj) vj = v[jb + cc];
+      float key = (t < nr && chosen < 0) ? fabsf(vj) : -1.0f;
+      int idx = t;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const float ok = __shfl_xor_sync(0xffffffffu, key, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
+        if (ok > key || (ok == key && oi < idx)) {
+          key = ok;
+          idx = oi;
+        }
+      }
+      if (key < 0.0f) {
+        if (lane == 0) {
+          sh.key[par][warp] = -1.0f;
+          sh.idx[par][warp] = INT_MAX;
+        }
+      } else if (idx == t) {
+        sh.key[par][warp] = key;
+        sh.idx[par][warp] = idx;
+#pragma unroll
+        for (int cc = 0; cc < kSub; ++cc) sh.row[par][warp][cc] = v[jb + cc];
+      }
+      __syncthreads();
+      float bk = lane < kWarps ? sh.key[par][lane] : -1.0f;
+      int bi = lane < kWarps ? sh.idx[par][lane] : INT_MAX;
+      int bw = lane;
+#pragma unroll
+      for (int off = kWarps / 2; off > 0; off >>= 1) {
+        const float ok = __shfl_xor_sync(0xffffffffu, bk, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        const int ow = __shfl_xor_sync(0xffffffffu, bw, off);
+        if (ok > bk || (ok == bk && oi < bi)) {
+          bk = ok;
+          bi = oi;
+          bw = ow;
+        }
+      }
+      bk = __shfl_sync(0xffffffffu, bk, 0);
+      bi = __shfl_sync(0xffffffffu, bi, 0);
+      bw = __shfl_sync(0xffffffffu, bw, 0);
+      if (bk < 0.0f) {  // fewer rows than columns: every row is chosen
+        done = true;
+        break;
+      }
+      if (t == bi) chosen = j;
+      const float* pr = sh.row[par][bw];
+      const float pv = pr[jj];
+      if (pv == 0.0f && t == 0 && *zero_col < 0) *zero_col = j;
+      if (t < nr && chosen < 0) {
+        const float l = pv != 0.0f ? vj / pv : 0.0f;
+#pragma unroll
+        for (int cc = 0; cc < kSub; ++cc) {
+          if (cc == jj) v[jb + cc] = l;
+          if (cc > jj) v[jb + cc] = fmaf(-l, pr[cc], v[jb + cc]);
+        }
       }
     }
-    if (key < 0.0f) {
-      if (lane == 0) {
-        box.key[par][warp] = -1.0f;
-        box.idx[par][warp] = INT_MAX;
-      }
-    } else if (idx == t) {
-      box.key[par][warp] = key;
-      box.idx[par][warp] = idx;
+    if (jb + kSub >= W) break;  // no columns right of the last sub-block
+    // the sub-block's pivot rows, then U12 = L11^-1 (their entries right of it)
+    const bool mine = chosen >= jb && chosen < jb + kSub;
+    if (mine) {
 #pragma unroll
-      for (int c = 0; c < W; ++c) box.row[par][warp][c] = v[c];
+      for (int c = jb; c < W; ++c) sh.prow[chosen - jb][c] = v[c];
     }
     __syncthreads();
-    float bk = lane < kWarps ? box.key[par][lane] : -1.0f;
-    int bi = lane < kWarps ? box.idx[par][lane] : INT_MAX;
-    int bw = lane;
-#pragma unroll
-    for (int off = kWarps / 2; off > 0; off >>= 1) {
-      const float ok = __shfl_xor_sync(0xffffffffu, bk, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-      const int ow = __shfl_xor_sync(0xffffffffu, bw, off);
-      if (ok > bk || (ok == bk && oi < bi)) {
-        bk = ok;
-        bi = oi;
-        bw = ow;
+    if (t < W - jb - kSub) {
+      const int c = jb + kSub + t;
+      for (int i = 1; i < nsub; ++i) {
+        float u = sh.prow[i][c];
+        for (int k = 0; k < i; ++k) u = fmaf(-sh.prow[i][jb + k], sh.prow[k][c], u);
+        sh.prow[i][c] = u;
       }
     }
-    bk = __shfl_sync(0xffffffffu, bk, 0);
-    bi = __shfl_sync(0xffffffffu, bi, 0);
-    bw = __shfl_sync(0xffffffffu, bw, 0);
-    if (bk < 0.0f) break;  // fewer rows than columns: every row is chosen
-    if (t == bi) chosen = j;
-    const float* prow = box.row[par][bw];
-    const float pv = prow[j];
-    if (pv == 0.0f && t == 0 && *zero_col < 0) *zero_col = j;
-    if (t < nr && chosen < 0) {
-      const float l = pv != 0.0f ? vj / pv : 0.0f;
+    __syncthreads();
+    if (mine) {
 #pragma unroll
-      for (int c = 0; c < W; ++c) {
-        if (c == j) v[c] = l;
-        if (c > j) v[c] = fmaf(-l, prow[c], v[c]);  // columns >= w stay zero (prow is zero there)
+      for (int c = jb + kSub; c < W; ++c) v[c] = sh.prow[chosen - jb][c];
+    } else if (t < nr && chosen < 0) {
+#pragma unroll
+      for (int k = 0; k < kSub; ++k) {
+        const float l = k < nsub ? v[jb + k] : 0.0f;
+#pragma unroll
+        for (int c = jb + kSub; c < W; ++c) v[c] = fmaf(-l, sh.prow[k][c], v[c]);
       }
     }
   }
@@ -161,7 +185,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
                                                            int w, int src, int nchild, int dst, int root,
                                                            int* ipiv, const int* lab, int first_leaf,
                                                            DevStatus* status, TsluScratch* ws) {
-  __shared__ GeppBox box;
+  __shared__ GeppShared box;
   __shared__ int zero_col;
   __shared__ int coff[kFan + 1];
   const int t = threadIdx.x, g = blockIdx.x;
