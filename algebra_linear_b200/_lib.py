@@ -53,6 +53,7 @@ SIGNATURES = [
     ("alg_dgetrf", _I, [_P, _SZ, _P, _P]),
     ("alg_dgetrf_rect", _I, [_P, _SZ, _SZ, _P]),
     ("alg_dgesv", _I, [_P, _P, _SZ]),
+    ("alg_dgetri", _I, [_P, _SZ, _P]),
     ("alg_dgesv_nrhs", _I, [_P, _P, _SZ, _SZ]),
     ("alg_dgesv_ex", _I, [_I, _P, _P, _SZ, _SZ, _P]),
     ("alg_ctx_create", _I, [_P, C.POINTER(_P)]),
@@ -61,6 +62,7 @@ SIGNATURES = [
     ("alg_dgetrf_dev", _I, [_P, _I, _P, _I, _I, _P, _P]),
     ("alg_dgetrf_rect_dev", _I, [_P, _I, _P, _I, _I, _I, _P]),
     ("alg_dgetrs_dev", _I, [_P, _P, _I, _I, _P, _P, _I, _I]),
+    ("alg_dgetri_dev", _I, [_P, _P, _I, _I, _P]),
     ("alg_dgesv_dev", _I, [_P, _I, _P, _I, _I, _P, _I, _I, _P]),
     ("alg_larnv_dev", _I, [_P, _I, _P, _SZ, _P, _P]),
     ("alg_mixed_opts_default", None, [_P]),

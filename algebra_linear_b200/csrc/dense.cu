@@ -247,6 +247,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   void* tslu_ws = nullptr;
   if (std::is_same<T, float>::value && plan.tslu) {
     ALG_TRY(ws_get(ctx, WS_TSLU, tslu_scratch_bytes(), &tslu_ws));
+    ALG_TRY(tslu_scratch_reset(ctx, tslu_ws));
   }
   if (perm != nullptr) {
     iota_kernel<<<std::min(1024, (m + 255) / 256), 256, 0, ctx->stream>>>(perm, m);
@@ -482,9 +483,82 @@ int host_lu(int update, double* a, size_t m, size_t nc, size_t* ipiv, double* de
   return ALG_OK;
 }
 
+// B = I (n x n, leading dimension ld) and a flag if some u_ii of the
+// factors is zero.
+__global__ void identity_and_zero_diag_kernel(const double* __restrict__ lu, int lda, double* __restrict__ b,
+                                              int ld, int n, int* zero_diag) {
+  const size_t total = (size_t)n * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), j = (int)(e / n);
+    b[i + (size_t)j * ld] = i == j ? 1.0 : 0.0;
+    if (i == j && lu[i + (size_t)i * lda] == 0.0) atomicExch(zero_diag, 1);
+  }
+}
+
+// The inverse from dgetrf's factors (mod.rs:249-298): the columns of the
+// identity through the exact solve (the interchanges, the unit-lower row-dot
+// sweep, the upper sweep dividing by u_ii, each entry in the reference's
+// order), into d_inv (ld n); ALG_SINGULAR, with nothing written, when some
+// u_ii is zero.
+int inverse_dev(alg_ctx* ctx, const double* d_lu, int n, int lda, const int* d_perm, double* d_inv) {
+  int* flag = nullptr;
+  ALG_TRY(alg::ws_get(ctx, alg::WS_MISC, sizeof(int), reinterpret_cast<void**>(&flag)));
+  ALG_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
+  const int grid = (int)std::max<size_t>(1, std::min<size_t>(((size_t)n * n + 255) / 256, 8 * (size_t)ctx->sm_count));
+  identity_and_zero_diag_kernel<<<grid, 256, 0, ctx->stream>>>(d_lu, lda, d_inv, n, n, flag);
+  alg::count_launches();
+  ALG_CUDA_TRY(cudaGetLastError());
+  int zero = 0;
+  ALG_CUDA_TRY(cudaMemcpyAsync(&zero, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (zero) return ALG_SINGULAR;
+  return solve_any(ctx, ALG_UPDATE_EXACT, d_lu, n, lda, d_perm, d_inv, n, n);
+}
+
 }  // namespace
 
 extern "C" {
+
+int alg_dgetri(double* lu, size_t n, const size_t* ipiv) {
+  if (n == 0) return ALG_OK;
+  if (lu == nullptr || ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  if (!size_ok(n)) return ALG_BAD_SHAPE;
+  for (size_t k = 0; k < n; ++k)
+    if (ipiv[k] >= n) return ALG_BAD_SHAPE;
+  // the sequential interchanges as one gather: row i of P b is row perm[i] of b
+  std::vector<int> perm(n);
+  for (size_t i = 0; i < n; ++i) perm[i] = (int)i;
+  for (size_t k = 0; k < n; ++k) std::swap(perm[k], perm[ipiv[k]]);
+  CtxLock L;
+  if (L.rc != ALG_OK) return L.rc;
+  alg_ctx* ctx = L.ctx;
+  const int N = (int)n;
+  double* d_a = nullptr;
+  double* d_b = nullptr;
+  int* d_perm = nullptr;
+  ALG_TRY(alg::ws_get(ctx, alg::WS_A, sizeof(double) * n * n, reinterpret_cast<void**>(&d_a)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_B, sizeof(double) * n * n, reinterpret_cast<void**>(&d_b)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_PERM, sizeof(int) * n, reinterpret_cast<void**>(&d_perm)));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_a, lu, sizeof(double) * n * n, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_TRY(alg::status_reset(ctx));
+  ALG_TRY(inverse_dev(ctx, d_a, N, N, d_perm, d_b));
+  ALG_CUDA_TRY(cudaMemcpyAsync(lu, d_b, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return alg::status_fetch(ctx);  // synchronises; reports a timed-out sweep
+}
+
+int alg_dgetri_dev(alg_ctx* ctx, double* d_lu, int n, int lda, const int32_t* d_perm) {
+  if (ctx == nullptr || (n > 0 && (d_lu == nullptr || d_perm == nullptr))) return ALG_INVALID_ARGUMENT;
+  if (n < 0 || lda < std::max(1, n)) return ALG_BAD_SHAPE;
+  if (n == 0) return ALG_OK;
+  double* d_b = nullptr;
+  ALG_TRY(alg::ws_get(ctx, alg::WS_B, sizeof(double) * (size_t)n * n, reinterpret_cast<void**>(&d_b)));
+  ALG_TRY(alg::status_reset(ctx));
+  ALG_TRY(inverse_dev(ctx, d_lu, n, lda, d_perm, d_b));
+  ALG_CUDA_TRY(cudaMemcpy2DAsync(d_lu, sizeof(double) * (size_t)lda, d_b, sizeof(double) * (size_t)n,
+                                 sizeof(double) * (size_t)n, n, cudaMemcpyDeviceToDevice, ctx->stream));
+  return alg::status_fetch(ctx);
+}
 
 int alg_dgetrf(double* a, size_t n, size_t* ipiv, double* det) {
   if (n == 0) {

@@ -30,6 +30,7 @@ template <typename T>
 int tri_solve_dev(alg_ctx* ctx, const T* lu, int lda, int n, T* x, bool upper, int* flags, int* abort_flag);
 
 size_t tslu_scratch_bytes();
+int tslu_scratch_reset(alg_ctx* ctx, void* scratch);
 int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch);
 
 // C -= A B on the tensor cores (tcgen05, FP32 accumulation in TMEM) with the

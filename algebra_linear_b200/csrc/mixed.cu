@@ -164,7 +164,9 @@ int lu_factor_lowp_dev(alg_ctx* ctx, int precision, float* a32, int n, int lda, 
   plan.tslu = tournament ? 1 : 0;
   if (precision != ALG_PREC_FP32) {
     plan.tc_prec = precision;
-    plan.nb = 128;
+    // deep blocks for the tensor-core update: K = 256 halves the update's
+    // C traffic per flop and the passes of deferred interchanges
+    plan.nb = n >= 8192 ? 256 : 128;
     if (const char* e = std::getenv("ALG_NB_TC")) plan.nb = std::max(32, std::atoi(e));
   }
   return lu_factor_dev<float, false>(ctx, a32, n, n, lda, ipiv, perm, plan);

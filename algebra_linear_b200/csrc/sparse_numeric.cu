@@ -175,10 +175,10 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
     const int slot0 = a.child_slot[k];
     const int crows = c.rows - c.size;
     const T* cb = a.block + c.cb_off;
-    const int64_t ce = (int64_t)crows * c.ncb;
-    for (int64_t e = tid; e < ce; e += kSmallThreads) {
-      const int i = (int)(e % crows), t = (int)(e / crows);
-      f[(slot0 + i) + (int64_t)a.cb_colmap[c.struct_begin + t] * rows] = cb[i + (int64_t)t * c.cb_ld];
+    for (int t = 0; t < c.ncb; ++t) {
+      T* dst = f + slot0 + a.cb_colmap[c.struct_begin + t] * rows;
+      const T* src = cb + t * c.cb_ld;
+      for (int i = tid; i < crows; i += kSmallThreads) dst[i] = src[i];
     }
   }
   __syncthreads();
@@ -214,14 +214,13 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
     }
     __syncthreads();
     const T inv = T(1) / pv;
-    for (int i = k + 1 + tid; i < rows; i += kSmallThreads) f[i + (int64_t)k * rows] *= inv;
+    for (int i = k + 1 + tid; i < rows; i += kSmallThreads) f[i + k * rows] *= inv;
     __syncthreads();
-    // rank-1 update of the front's own columns only
+    // rank-1 update of the front's own columns, spread over all threads
     const int mr = rows - k - 1, mc = size - k - 1;
-    const int64_t upd = (int64_t)mr * mc;
-    for (int64_t e = tid; e < upd; e += kSmallThreads) {
-      const int i = k + 1 + (int)(e % mr), j = k + 1 + (int)(e / mr);
-      f[i + (int64_t)j * rows] = fma_t(-f[k + (int64_t)j * rows], f[i + (int64_t)k * rows], f[i + (int64_t)j * rows]);
+    for (int e = tid; e < mr * mc; e += kSmallThreads) {
+      const int i = k + 1 + e % mr, j = k + 1 + e / mr;
+      f[i + j * rows] = fma_t(-f[k + j * rows], f[i + k * rows], f[i + j * rows]);
     }
     __syncthreads();
   }
@@ -246,19 +245,14 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
   cta_gemm_sub(f + size + (int64_t)size * rows, f + size, f + (int64_t)size * rows, rows, rows - size, d.ncb, size,
                As, Bs);
   T* lp = a.L + d.l_off;
-  for (int64_t e = tid; e < (int64_t)rows * size; e += kSmallThreads) lp[e] = f[e];
+  for (int e = tid; e < rows * size; e += kSmallThreads) lp[e] = f[e];
   T* up = a.U + d.u_off;
-  for (int64_t e = tid; e < (int64_t)size * d.ncb; e += kSmallThreads) {
-    const int kk = (int)(e % size), t = (int)(e / size);
-    up[e] = f[kk + (int64_t)(size + t) * rows];
-  }
+  for (int t = 0; t < d.ncb; ++t)
+    for (int kk = tid; kk < size; kk += kSmallThreads) up[kk + t * size] = f[kk + (size + t) * rows];
   if (in_smem) {
     const int crows = rows - size;
-    for (int64_t e = tid; e < (int64_t)crows * d.ncb; e += kSmallThreads) {
-      const int i = (int)(e % crows), t = (int)(e / crows);
-      const int64_t at = (size + i) + (int64_t)(size + t) * rows;
-      fg[at] = f[at];
-    }
+    for (int t = 0; t < d.ncb; ++t)
+      for (int i = tid; i < crows; i += kSmallThreads) fg[(size + i) + (size + t) * rows] = f[(size + i) + (size + t) * rows];
   }
 }
 
@@ -853,7 +847,10 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   sa.U = U;
   sa.rowid = out.rowid;
   sa.singular = d_flag;
-  sa.smem_entries = (int)(kSmallSmemBytes / sizeof(T));
+  // ALG_SPLU_SMALL_SMEM=0 keeps every small front in the block arena
+  const char* sm_env = std::getenv("ALG_SPLU_SMALL_SMEM");
+  const bool use_smem = sm_env == nullptr || sm_env[0] != '0';
+  sa.smem_entries = use_smem ? (int)(kSmallSmemBytes / sizeof(T)) : 0;
   {
     static bool configured[2] = {false, false};
     bool& done = configured[sizeof(T) == 8 ? 1 : 0];
@@ -868,7 +865,7 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
     const int cnt = F.small_level_ptr[h + 1] - F.small_level_ptr[h];
     if (cnt == 0) continue;
     sa.level_fronts = d_small_levels + F.small_level_ptr[h];
-    small_front_kernel<T><<<cnt, kSmallThreads, kSmallSmemBytes, st>>>(sa);
+    small_front_kernel<T><<<cnt, kSmallThreads, use_smem ? kSmallSmemBytes : 0, st>>>(sa);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }

@@ -21,7 +21,10 @@
 // mixed form's refinement in FP64 then brings the solution to the FP64
 // backward error, which is its contract. No kernel waits on another CTA.
 #include <algorithm>
+#include <atomic>
 #include <climits>
+#include <cstddef>
+#include <cstdlib>
 
 #include "dense.cuh"
 
@@ -34,7 +37,14 @@ constexpr int kFan = 8;           // children merged by one CTA (8 x 32 = 256 ro
 constexpr int kMaxGroups = 1024;  // CTAs of the first level: up to 262 144 panel rows
 constexpr int kMaxMoves = 2 * kW;
 
+constexpr int kMaxLevels = 4;
+constexpr int kFusedMaxGroups = 32;  // panels of up to 8192 rows take the single launch  // merge levels: 1024 -> 128 -> 16 -> 2 -> 1
+
 struct TsluScratch {
+  // single-launch form: arrivals per parent and level (the last arrival merges
+  // and resets the count) and the root's release flag (the launch's epoch)
+  int counter[kMaxLevels][kMaxGroups / kFan];
+  unsigned ready;
   int cand_rows[2][kMaxGroups][kW];        // proposals of each CTA of a level, in step order
   int cand_cnt[2][kMaxGroups];
   float cand_vals[2][kMaxGroups][kW * kW];  // their original values, [col][k]
@@ -180,15 +190,27 @@ __device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShar
 // from scratch slot src. Writes this CTA's proposals to slot dst; the single
 // CTA of the last level (root) also writes the winners, L11 \ U11, the rows
 // at the top before anything moves, ipiv and the list of moved rows.
+struct LevelIn {
+  const float* a;
+  int lda, n, c0, w;
+  int* ipiv;
+  const int* lab;
+  int first_leaf;
+  DevStatus* status;
+};
+
+// Proposals written by other CTAs are read through L2 (__ldcg): in the
+// single-launch form they were written during this launch by other SMs.
 template <int W>
-__global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __restrict__ a, int lda, int n, int c0,
-                                                           int w, int src, int nchild, int dst, int root,
-                                                           int* ipiv, const int* lab, int first_leaf,
-                                                           DevStatus* status, TsluScratch* ws) {
+__device__ void level_body(const LevelIn& in, int g, int src, int nchild, int dst, bool root, TsluScratch* ws) {
   __shared__ GeppShared box;
   __shared__ int zero_col;
   __shared__ int coff[kFan + 1];
-  const int t = threadIdx.x, g = blockIdx.x;
+  const float* a = in.a;
+  const int lda = in.lda, n = in.n, c0 = in.c0, w = in.w, first_leaf = in.first_leaf;
+  int* ipiv = in.ipiv;
+  const int* lab = in.lab;
+  const int t = threadIdx.x;
   float o[W];  // this row's original values
 #pragma unroll
   for (int c = 0; c < W; ++c) o[c] = 0.0f;
@@ -207,7 +229,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
       for (int k = 0; k < kFan; ++k) {
         coff[k] = acc;
         const int ch = g * kFan + k;
-        acc += ch < nchild ? ws->cand_cnt[src][ch] : 0;
+        acc += ch < nchild ? __ldcg(&ws->cand_cnt[src][ch]) : 0;
       }
       coff[kFan] = acc;
     }
@@ -217,9 +239,9 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
       int k = 0;
       while (k + 1 < kFan && coff[k + 1] <= t) ++k;
       const int ch = g * kFan + k, q = t - coff[k];
-      row = ws->cand_rows[src][ch][q];
+      row = __ldcg(&ws->cand_rows[src][ch][q]);
 #pragma unroll
-      for (int c = 0; c < W; ++c) o[c] = c < w ? ws->cand_vals[src][ch][c * kW + q] : 0.0f;
+      for (int c = 0; c < W; ++c) o[c] = c < w ? __ldcg(&ws->cand_vals[src][ch][c * kW + q]) : 0.0f;
     }
   }
   float v[W];
@@ -237,6 +259,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
         if (c < w) ws->cand_vals[dst][g][c * kW + step] = o[c];
     }
     if (t == 0) ws->cand_cnt[dst][g] = cnt;
+    __syncthreads();  // the block's shared state is reused by the next level
     return;
   }
   // ---- root: winners, L11 \ U11, the top rows' original values ------------
@@ -250,7 +273,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
     const int r = e % w, c = e / w;
     ws->top_orig[c * kW + r] = a[(size_t)(c0 + r) + (size_t)(c0 + c) * lda];
   }
-  if (t == 0 && zero_col >= 0) atomicMin(&status->singular_col, c0 + zero_col);
+  if (t == 0 && zero_col >= 0) atomicMin(&in.status->singular_col, c0 + zero_col);
   __syncthreads();
   // ---- LAPACK sequential interchanges bringing winner j to position c0 + j,
   //      tracked over the touched positions only (one warp) ------------------
@@ -309,6 +332,14 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
       ws->nmoves = nm;
     }
   }
+  __syncthreads();
+}
+
+// One level of the multi-launch form.
+template <int W>
+__global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(LevelIn in, int src, int nchild, int dst, int root,
+                                                           TsluScratch* ws) {
+  level_body<W>(in, blockIdx.x, src, nchild, dst, root != 0, ws);
 }
 
 // 3. Blocks [0, side_blocks): the block panel's other columns follow the
@@ -317,22 +348,24 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(const float* __res
 //    up there), the top block and the labels.
 constexpr int kSideCols = 8;
 
+// CTA `cta` of `ncta`: the first side_blocks CTAs permute the block panel's
+// other columns (side_rows: whether they also take rows); rows are spread
+// over the CTAs from row_cta0 on.
 template <int W>
-__global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int n, int c0, int w, int kb0, int kb1,
-                                                         int* lab, int first_leaf, int side_blocks,
-                                                         const TsluScratch* ws) {
+__device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab, int first_leaf,
+                           int cta, int ncta, int side_blocks, int row_cta0, const TsluScratch* ws) {
   __shared__ float U[kW * kW];
   __shared__ int mpos[kMaxMoves], msrc[kMaxMoves], mlab[kMaxMoves];
   __shared__ int nm_s;
-  if (threadIdx.x == 0) nm_s = ws->nmoves;
+  if (threadIdx.x == 0) nm_s = __ldcg(&ws->nmoves);
   for (int t = threadIdx.x; t < kMaxMoves; t += blockDim.x) {
-    mpos[t] = ws->move_pos[t];
-    msrc[t] = ws->move_src[t];
-    mlab[t] = ws->move_lab[t];
+    mpos[t] = __ldcg(&ws->move_pos[t]);
+    msrc[t] = __ldcg(&ws->move_src[t]);
+    mlab[t] = __ldcg(&ws->move_lab[t]);
   }
   const int side = (kb1 - kb0) - w;
-  if ((int)blockIdx.x < side_blocks) {
-    __syncthreads();
+  __syncthreads();
+  if (cta < side_blocks) {
     const int nm = nm_s;
     // kSideCols columns x the moves: read all, then write all
     float v[(kSideCols * kMaxMoves + 255) / 256];
@@ -340,7 +373,7 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int 
     for (int u = 0; u < (kSideCols * kMaxMoves + 255) / 256; ++u) {
       const int e = threadIdx.x + u * 256;
       const int cl = e / kMaxMoves, mv = e % kMaxMoves;
-      const int cidx = blockIdx.x * kSideCols + cl;
+      const int cidx = cta * kSideCols + cl;
       v[u] = 0.0f;
       if (cl < kSideCols && cidx < side && mv < nm) {
         int col = kb0 + cidx;
@@ -353,20 +386,20 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int 
     for (int u = 0; u < (kSideCols * kMaxMoves + 255) / 256; ++u) {
       const int e = threadIdx.x + u * 256;
       const int cl = e / kMaxMoves, mv = e % kMaxMoves;
-      const int cidx = blockIdx.x * kSideCols + cl;
+      const int cidx = cta * kSideCols + cl;
       if (cl < kSideCols && cidx < side && mv < nm) {
         int col = kb0 + cidx;
         if (col >= c0) col += w;
         a[(size_t)mpos[mv] + (size_t)col * lda] = v[u];
       }
     }
-    return;
   }
-  for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = ws->top_lu[e];
+  if (cta < row_cta0) return;
+  for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = __ldcg(&ws->top_lu[e]);
   __syncthreads();
   const int nm = nm_s;
-  const int gtid = (blockIdx.x - side_blocks) * blockDim.x + threadIdx.x;
-  const int nth = (gridDim.x - side_blocks) * blockDim.x;
+  const int gtid = (cta - row_cta0) * blockDim.x + threadIdx.x;
+  const int nth = (ncta - row_cta0) * blockDim.x;
   // rows below the top
   for (int r = c0 + w + gtid; r < n; r += nth) {
     int src = r, hit = -1;
@@ -378,7 +411,8 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int 
     float x[W];
 #pragma unroll
     for (int j = 0; j < W; ++j)
-      x[j] = j < w ? (from_top ? ws->top_orig[j * kW + (src - c0)] : a[(size_t)src + (size_t)(c0 + j) * lda]) : 0.0f;
+      x[j] = j < w ? (from_top ? __ldcg(&ws->top_orig[j * kW + (src - c0)]) : a[(size_t)src + (size_t)(c0 + j) * lda])
+                    : 0.0f;
 #pragma unroll
     for (int j = 0; j < W; ++j) {
       if (j < w) {
@@ -413,34 +447,169 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int 
   }
 }
 
+template <int W>
+__global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int n, int c0, int w, int kb0, int kb1,
+                                                         int* lab, int first_leaf, int side_blocks,
+                                                         const TsluScratch* ws) {
+  apply_body<W>(a, lda, n, c0, w, kb0, kb1, lab, first_leaf, blockIdx.x, gridDim.x, side_blocks, side_blocks, ws);
+}
+
+__device__ __forceinline__ uint64_t tslu_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// The single-launch form (a cooperative launch, so every CTA is resident):
+// each CTA factors its 256-row block; the last of each kFan siblings to
+// arrive (an atomic count after a fence) merges their proposals and climbs
+// on; the CTA that factors the root publishes its results and releases the
+// launch's epoch; every CTA waits for it (bounded: 2 s, then the timeout flag)
+// and takes its share of the apply step.
+template <int W>
+__global__ void __launch_bounds__(kRows, 1) tslu_fused_kernel(LevelIn in, int groups0, int kb0, int kb1, int* lab,
+                                                           int side_blocks, unsigned epoch, TsluScratch* ws) {
+  __shared__ int last_s;
+  __shared__ int ok_s;
+  int g = blockIdx.x, groups = groups0, src = -1, dst = 0, nchild = 0, level = 0;
+  bool ran_root = false;
+  // CTAs beyond the level-0 blocks (there only for the side columns) take
+  // no part in the tree
+  for (; (int)blockIdx.x < groups0;) {
+    const bool root = groups == 1;
+    level_body<W>(in, g, src, nchild, dst, root, ws);
+    if (root) {
+      ran_root = true;
+      break;
+    }
+    __threadfence();
+    __syncthreads();
+    const int parent = g / kFan;
+    const int nkids = min(kFan, groups - parent * kFan);
+    if (threadIdx.x == 0) {
+      const int prev = atomicAdd(&ws->counter[level][parent], 1);
+      last_s = prev == nkids - 1 ? 1 : 0;
+      if (last_s) ws->counter[level][parent] = 0;  // ready for the next panel
+    }
+    __syncthreads();
+    if (!last_s) break;
+    __threadfence();
+    nchild = groups;
+    groups = (groups + kFan - 1) / kFan;
+    src = dst;
+    dst = 1 - dst;
+    g = parent;
+    ++level;
+  }
+  if (ran_root) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&ws->ready), "r"(epoch) : "memory");
+  }
+  if (threadIdx.x == 0) {
+    const uint64_t t0 = tslu_timer_ns();
+    int ok = 0;
+    for (;;) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&ws->ready) : "memory");
+      if (v == epoch) {
+        ok = 1;
+        break;
+      }
+      if (tslu_timer_ns() - t0 > 2000000000ull) break;
+      __nanosleep(64);
+    }
+    ok_s = ok;
+    if (!ok) atomicExch(&in.status->timeout, 1);
+  }
+  __syncthreads();
+  if (!ok_s) return;
+  apply_body<W>(const_cast<float*>(in.a), in.lda, in.n, in.c0, in.w, kb0, kb1, lab, in.first_leaf, blockIdx.x,
+                gridDim.x, side_blocks, 0, ws);
+}
+
 }  // namespace
 
 size_t tslu_scratch_bytes() { return sizeof(TsluScratch); }
 
+// The arrival counts and the release flag start at zero (once per
+// factorization; the counts are left at zero by every merge).
+int tslu_scratch_reset(alg_ctx* ctx, void* scratch) {
+  ALG_CUDA_TRY(cudaMemsetAsync(scratch, 0, offsetof(TsluScratch, cand_rows), ctx->stream));
+  return ALG_OK;
+}
+
+namespace {
+
+template <int W>
+int launch_fused(alg_ctx* ctx, const TsluArgs& p, int groups0, int side_blocks, TsluScratch* ws, bool* done) {
+  static int max_ctas = -1;
+  if (max_ctas < 0) {
+    int per_sm = 0;
+    ALG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tslu_fused_kernel<W>, kRows, 0));
+    max_ctas = per_sm * ctx->sm_count;
+  }
+  *done = false;
+  const int grid = std::max(groups0, side_blocks);
+  // the waiting CTAs hold their SMs until the root is done, which the
+  // concurrent trailing update of a large matrix needs: tall panels take the
+  // multi-launch form (as do grids that cannot be co-resident)
+  if (groups0 > kFusedMaxGroups || grid > max_ctas) return ALG_OK;
+  static std::atomic<unsigned> epochs{1};
+  unsigned epoch = epochs.fetch_add(1);
+  if (epoch == 0) epoch = epochs.fetch_add(1);
+  LevelIn in{p.a, p.lda, p.n, p.c0, p.w, p.ipiv, p.lab, p.first_leaf, p.status};
+  int kb0 = p.kb0, kb1 = p.kb1;
+  int* lab = p.lab;
+  void* args[] = {(void*)&in, (void*)&groups0, (void*)&kb0, (void*)&kb1, (void*)&lab, (void*)&side_blocks,
+                  (void*)&epoch, (void*)&ws};
+  ALG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)tslu_fused_kernel<W>, dim3(grid), dim3(kRows), args, 0,
+                                           ctx->stream));
+  *done = true;
+  return ALG_OK;
+}
+
+}  // namespace
+
 // A leaf panel of the FP32 LU by tournament pivoting; same outputs as the
 // partial-pivoting cluster kernel (factored panel, ipiv, labels, side
 // columns). Returns ALG_NOT_IMPLEMENTED when the panel does not fit its
-// limits (the caller then uses partial pivoting). Nothing in the scratch
-// needs clearing between calls.
+// limits (the caller then uses partial pivoting). One cooperative launch when
+// the level-0 CTAs fit on the device at once, else one launch per tree level
+// and one for the apply step. The scratch is reset once per factorization.
 int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch) {
   const int m = p.n - p.c0, w = p.w;
   if (w > kW || w < 1 || m < w) return ALG_NOT_IMPLEMENTED;
   const int groups0 = (m + kRows - 1) / kRows;
   if (groups0 > kMaxGroups) return ALG_NOT_IMPLEMENTED;
   auto* ws = static_cast<TsluScratch*>(scratch);
+  const int side = (p.kb1 - p.kb0) - w;
+  const int side_blocks = side > 0 ? (side + kSideCols - 1) / kSideCols : 0;
+  double pflops = 0;
+  for (int j = 0; j < w; ++j) pflops += double(m - j - 1) * (1.0 + 2.0 * (w - j - 1));
   const int tok = prof_begin(ctx, ALG_K_PANEL);
+  if (!std::getenv("ALG_TSLU_SPLIT")) {
+    bool done = false;
+    if (w <= 16)
+      ALG_TRY(launch_fused<16>(ctx, p, groups0, side_blocks, ws, &done));
+    else
+      ALG_TRY(launch_fused<32>(ctx, p, groups0, side_blocks, ws, &done));
+    if (done) {
+      count_launches(1);
+      prof_end(ctx, tok, pflops, 2.0 * sizeof(float) * m * w);
+      ALG_CUDA_TRY(cudaGetLastError());
+      return ALG_OK;
+    }
+  }
+  LevelIn in{p.a, p.lda, p.n, p.c0, w, p.ipiv, p.lab, p.first_leaf, p.status};
   // level 0 reads the panel; each later level merges kFan proposals per CTA
   int groups = groups0, src = -1, dst = 0, nchild = 0, launches = 0;
   for (;;) {
     const bool root = groups == 1;
     if (w <= 16)
-      tslu_level_kernel<16><<<groups, kRows, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, src, nchild, dst,
-                                                                root ? 1 : 0, p.ipiv, p.lab, p.first_leaf, p.status,
-                                                                ws);
+      tslu_level_kernel<16><<<groups, kRows, 0, ctx->stream>>>(in, src, nchild, dst, root ? 1 : 0, ws);
     else
-      tslu_level_kernel<32><<<groups, kRows, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, src, nchild, dst,
-                                                                root ? 1 : 0, p.ipiv, p.lab, p.first_leaf, p.status,
-                                                                ws);
+      tslu_level_kernel<32><<<groups, kRows, 0, ctx->stream>>>(in, src, nchild, dst, root ? 1 : 0, ws);
     ++launches;
     if (root) break;
     nchild = groups;
@@ -448,8 +617,6 @@ int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch) {
     src = dst;
     dst = 1 - dst;
   }
-  const int side = (p.kb1 - p.kb0) - w;
-  const int side_blocks = side > 0 ? (side + kSideCols - 1) / kSideCols : 0;
   const int row_blocks = std::max(1, std::min(2 * ctx->sm_count, (m + 255) / 256));
   if (w <= 16)
     tslu_apply_kernel<16><<<side_blocks + row_blocks, 256, 0, ctx->stream>>>(p.a, p.lda, p.n, p.c0, w, p.kb0,
@@ -460,8 +627,6 @@ int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch) {
                                                                              p.kb1, p.lab, p.first_leaf,
                                                                              side_blocks, ws);
   count_launches(launches + 1);
-  double pflops = 0;
-  for (int j = 0; j < w; ++j) pflops += double(m - j - 1) * (1.0 + 2.0 * (w - j - 1));
   prof_end(ctx, tok, pflops, 2.0 * sizeof(float) * m * w);
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;

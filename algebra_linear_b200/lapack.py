@@ -79,6 +79,17 @@ def dgetrf_rect(a: np.ndarray, nrows: int, ncols: int, ipiv) -> None:
         ipiv[k] = int(buf[k])
 
 
+def dgetri(lu: np.ndarray, n: int, ipiv) -> None:
+    """Inverse from dgetrf's factors, in place (mod.rs:249-298)."""
+    _f64(lu, "lu")
+    if lu.size != n * n or len(ipiv) != n:
+        raise LapackError("BadShape", _lib.BAD_SHAPE)
+    if n == 0:
+        return
+    iv = np.ascontiguousarray(ipiv, dtype=np.uint64)
+    _check(_lib.load().alg_dgetri(_lib.ptr(lu), n, _lib.ptr(iv)))
+
+
 def dgesv(a: np.ndarray, b: np.ndarray) -> None:
     """Solves A x = b for one right-hand side; n = len(b) (mod.rs:309)."""
     _f64(a, "a")

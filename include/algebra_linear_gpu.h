@@ -90,6 +90,14 @@ int alg_dgetrf_rect(double* a, size_t nrows, size_t ncols, size_t* ipiv);
  * a is destroyed (holds the LU factors); b becomes x. */
 int alg_dgesv(double* a, double* b, size_t n);
 
+/* Replaces `pub fn dgetri(lu: &mut [f64], n: usize, ipiv: &[usize])
+ *   -> Result<(), LapackError>` (src/lapack/mod.rs:249-298): lu (n*n, the
+ * factors from alg_dgetrf) becomes the inverse, computed column by column
+ * with the reference's interchange, row-dot and division order (bit-identical
+ * results). ALG_SINGULAR, with lu unchanged, when some u_ii is zero;
+ * ALG_BAD_SHAPE when an ipiv entry is out of range. */
+int alg_dgetri(double* lu, size_t n, const size_t* ipiv);
+
 /* dgesv with nrhs right-hand sides, b n x nrhs column-major: the reference's
  * dgetrf followed by its dgetrs (src/lapack/mod.rs:330-354) per column. */
 int alg_dgesv_nrhs(double* a, double* b, size_t n, size_t nrhs);
@@ -128,6 +136,11 @@ int alg_dgetrf_rect_dev(alg_ctx* ctx, int update, double* d_a, int nrows, int nc
  * overwritten with x. */
 int alg_dgetrs_dev(alg_ctx* ctx, const double* d_lu, int n, int lda,
                    const int32_t* d_perm, double* d_b, int nrhs, int ldb);
+
+/* The device form of alg_dgetri: d_lu (factors from alg_dgetrf_dev, leading
+ * dimension lda) becomes the inverse; d_perm is the net permutation that
+ * alg_dgetrf_dev returned. */
+int alg_dgetri_dev(alg_ctx* ctx, double* d_lu, int n, int lda, const int32_t* d_perm);
 
 /* Per-kernel-class timing of a context's launches with CUDA events, for
  * roofline reporting. Classes: 0 panel, 1 row interchange, 2 trsm,

@@ -36,6 +36,7 @@ def load() -> C.CDLL:
         lib.oracle_dgetrf_rect.argtypes = [P, SZ, SZ, P]
         lib.oracle_dgetrs.argtypes = [P, P, P, SZ, SZ]
         lib.oracle_dgesv.argtypes = [P, P, SZ, SZ, P]
+        lib.oracle_dgetri.argtypes = [P, SZ, P]
         lib.oracle_dgemv.argtypes = [P, P, P, SZ, SZ]
         lib.oracle_idamax.argtypes = [P, SZ]
         lib.oracle_idamax.restype = SZ
@@ -78,6 +79,13 @@ def dgetrf_rect(a: np.ndarray, nrows: int, ncols: int):
 def dgetrs(lu: np.ndarray, ipiv, b: np.ndarray, n: int, nrhs: int = 1) -> None:
     iv = np.asarray(ipiv, dtype=np.uint64)
     load().oracle_dgetrs(_p(lu), _p(iv), _p(b), n, nrhs)
+
+
+def dgetri(lu: np.ndarray, n: int, ipiv) -> int:
+    """mod.rs:249-298: lu (n*n, column-major) becomes the inverse; returns
+    the status (0, or OR_SINGULAR leaving lu unchanged)."""
+    iv = np.ascontiguousarray(ipiv, dtype=np.uint64)
+    return int(load().oracle_dgetri(_p(lu), n, _p(iv)))
 
 
 def dgesv(a: np.ndarray, b: np.ndarray, n: int, nrhs: int = 1):

@@ -14,6 +14,7 @@
 // src/lapack/families.rs:1183-1261 (captured by the reference from LAPACK's
 // libtmglib) and the dense-LU unit tests of src/lapack/mod.rs:461-752.
 
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -212,6 +213,37 @@ void oracle_dgetrs(const double* lu, const size_t* ipiv, double* b, size_t n, si
       x[i] = sum / lu[i + i * n];
     }
   }
+}
+
+// mod.rs:249-298 (dgetri): the inverse from dgetrf's factors, column by
+// column (the interchanges in dgetrf's order, the unit-lower row-dot sweep,
+// the upper sweep dividing by u_ii), written over lu only when every column
+// succeeded; OR_SINGULAR on a zero diagonal of U.
+int oracle_dgetri(double* lu, size_t n, const size_t* ipiv) {
+  if (n == 0) return OR_OK;
+  std::vector<double> inverse(n * n, 0.0), b(n);
+  for (size_t col = 0; col < n; ++col) {
+    std::fill(b.begin(), b.end(), 0.0);
+    b[col] = 1.0;
+    for (size_t k = 0; k < n; ++k) {
+      const double t = b[k]; b[k] = b[ipiv[k]]; b[ipiv[k]] = t;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      double sum = b[i];
+      for (size_t j = 0; j < i; ++j) sum -= lu[i + j * n] * b[j];
+      b[i] = sum;
+    }
+    for (size_t i = n; i-- > 0;) {
+      double sum = b[i];
+      for (size_t j = i + 1; j < n; ++j) sum -= lu[i + j * n] * b[j];
+      const double d = lu[i + i * n];
+      if (d == 0.0) return OR_SINGULAR;
+      b[i] = sum / d;
+    }
+    for (size_t i = 0; i < n; ++i) inverse[i + col * n] = b[i];
+  }
+  std::memcpy(lu, inverse.data(), n * n * sizeof(double));
+  return OR_OK;
 }
 
 // mod.rs:309-323 (dgesv) generalised to nrhs columns: dgetrf then dgetrs.

@@ -293,3 +293,58 @@ def test_fp64_tensor_core_update_matches_torch(gpu, shape):
     assert err <= 4 * K * 2.0**-53 * scale, (err, scale)
     # padding rows between the leading dimension and M are untouched
     assert torch.equal(C[:, M:], C0[:, M:])
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 64, 333, 1024])
+def test_dgetri_is_bit_identical_to_the_oracle(gpu, oracle, n):
+    """dgetri (mod.rs:249-298) on the GPU from the same factors: the inverse
+    equals the oracle's bit for bit (same interchange, row-dot and division
+    order per column)."""
+    from algebra_linear_b200 import lapack
+
+    a, _ = oracle.larnv("Symmetric", [5, 6, 7, 2 * n + 1], n * n)
+    lu = a.copy()
+    rc, ipiv, _, _ = oracle.dgetrf(lu, n)
+    assert rc == 0
+    ref = lu.copy()
+    assert oracle.dgetri(ref, n, ipiv) == 0
+    got = lu.copy()
+    lapack.dgetri(got, n, ipiv)
+    assert np.array_equal(got, ref)
+
+
+def test_dgetri_rejects_zero_pivots_and_bad_shapes(gpu):
+    from algebra_linear_b200 import lapack
+    from algebra_linear_b200.lapack import LapackError
+
+    lu = np.array([2.0, 0.5, 1.0, 0.0])  # U = [[2, 1], [0, 0]]
+    before = lu.copy()
+    with pytest.raises(LapackError) as e:
+        lapack.dgetri(lu, 2, [0, 1])
+    assert e.value.kind == "Singular" and np.array_equal(lu, before)
+    with pytest.raises(LapackError):
+        lapack.dgetri(np.zeros(4), 2, [0])
+    with pytest.raises(LapackError):
+        lapack.dgetri(np.eye(2).reshape(-1), 2, [0, 5])
+
+
+def test_dgetri_device_form_matches_the_host_form(gpu, oracle):
+    import ctypes as C
+
+    import torch
+
+    from algebra_linear_b200 import _lib, device
+
+    n = 200
+    a, _ = oracle.larnv("Symmetric", [3, 3, 3, 3], n * n)
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        perm = torch.zeros(n, dtype=torch.int32, device="cuda")
+        lib = _lib.load()
+        assert lib.alg_dgetrf_dev(ctx.handle, _lib.UPDATE_EXACT, A.data_ptr(), n, n, None, perm.data_ptr()) == 0
+        assert lib.alg_dgetri_dev(ctx.handle, A.data_ptr(), n, n, perm.data_ptr()) == 0
+        inv = A.cpu().numpy()
+    lu = a.copy()
+    rc, ipiv, _, _ = oracle.dgetrf(lu, n)
+    assert oracle.dgetri(lu, n, ipiv) == 0
+    assert np.array_equal(inv, lu)

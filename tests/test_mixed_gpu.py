@@ -173,3 +173,26 @@ def test_tournament_pivoting_panels(gpu, oracle, n, prec):
         assert np.array_equal(A.cpu().numpy(), a)
     assert rep["path"] == "ir" and rep["ir_iterations"] <= 8, rep
     assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53
+
+
+def test_tournament_single_launch_matches_level_launches(gpu, oracle, monkeypatch):
+    """The single cooperative launch per leaf and the one-launch-per-level
+    form run the same arithmetic: bit-identical solutions."""
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    n = 5000
+    a, _, b = oracle.c1_system(n, seed=[2, 7, 1, 9])
+    xs = []
+    for split in ("0", "1"):
+        if split == "1":
+            monkeypatch.setenv("ALG_TSLU_SPLIT", "1")
+        with device.Context() as ctx:
+            A = torch.from_numpy(a.copy()).cuda()
+            B = torch.from_numpy(b.copy()).cuda()
+            rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision="tf32x3", pivoting="tournament",
+                                        no_gmres=True, no_fallback=True)
+            assert rep["tournament"] and rep["path"] == "ir", rep
+            xs.append(B.cpu().numpy())
+    assert np.array_equal(xs[0], xs[1])

@@ -65,6 +65,50 @@ def test_dgetrf_detects_a_singular_matrix(oracle):
     assert rc == 1
 
 
+def spd(n):
+    # checkers.rs:260-279: A = L L^T with integer entries
+    l = np.zeros((n, n))
+    for j in range(n):
+        l[j, j] = j + 2
+        for i in range(j + 1, n):
+            l[i, j] = (i + j) % 3 - 1.0
+    return (l @ l.T).T.reshape(-1).copy()  # column-major storage of the symmetric product
+
+
+def test_dgetri_inverts_correctly(oracle):
+    # mod.rs:510-534: A * A^-1 e_j = e_j for the 4 x 4 sample
+    a = sample4()
+    lu = a.copy()
+    rc, ipiv, _, _ = oracle.dgetrf(lu, 4)
+    assert rc == 0
+    assert oracle.dgetri(lu, 4, ipiv) == 0
+    for j in range(4):
+        e = np.zeros(4)
+        e[j] = 1.0
+        back = oracle.dgemv(lu, oracle.dgemv(a, e, 4, 4), 4, 4)
+        assert np.all(np.abs(back - e) < 1e-12)
+
+
+def test_dgetri_residual_on_spd_matrices(oracle):
+    # checkers.rs:307-330 (the DGET03 use): ||I - A A^-1|| small on spd(n)
+    for n in (1, 2, 5, 8):
+        a = spd(n)
+        lu = a.copy()
+        rc, ipiv, _, _ = oracle.dgetrf(lu, n)
+        assert rc == 0 and oracle.dgetri(lu, n, ipiv) == 0
+        am, inv = a.reshape(n, n).T, lu.reshape(n, n).T
+        resid = np.abs(np.eye(n) - am @ inv).sum(axis=0).max()
+        anorm, inorm = np.abs(am).sum(axis=0).max(), np.abs(inv).sum(axis=0).max()
+        assert resid / (n * anorm * inorm * 2.0**-52) <= 20.0
+
+
+def test_dgetri_reports_a_zero_pivot_and_keeps_the_factors(oracle):
+    lu = np.array([2.0, 0.5, 1.0, 0.0])  # U = [[2, 1], [0, 0]]
+    before = lu.copy()
+    assert oracle.dgetri(lu, 2, [0, 1]) == 1
+    assert np.array_equal(lu, before)
+
+
 def test_dgesv_solves_a_system(oracle):
     # mod.rs:537-551
     a = sample4()
