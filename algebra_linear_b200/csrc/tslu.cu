@@ -37,8 +37,8 @@ constexpr int kFan = 8;           // children merged by one CTA (8 x 32 = 256 ro
 constexpr int kMaxGroups = 1024;  // CTAs of the first level: up to 262 144 panel rows
 constexpr int kMaxMoves = 2 * kW;
 
-constexpr int kMaxLevels = 4;
-constexpr int kFusedMaxGroups = 32;  // panels of up to 8192 rows take the single launch  // merge levels: 1024 -> 128 -> 16 -> 2 -> 1
+constexpr int kMaxLevels = 4;        // merge levels: 1024 -> 128 -> 16 -> 2 -> 1
+constexpr int kFusedMaxGroups = 32;  // panels of up to 8192 rows take the single launch
 
 struct TsluScratch {
   // single-launch form: arrivals per parent and level (the last arrival merges
