@@ -483,36 +483,63 @@ int host_lu(int update, double* a, size_t m, size_t nc, size_t* ipiv, double* de
   return ALG_OK;
 }
 
-// B = I (n x n, leading dimension ld) and a flag if some u_ii of the
-// factors is zero.
-__global__ void identity_and_zero_diag_kernel(const double* __restrict__ lu, int lda, double* __restrict__ b,
-                                              int ld, int n, int* zero_diag) {
-  const size_t total = (size_t)n * n;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e % n), j = (int)(e / n);
-    b[i + (size_t)j * ld] = i == j ? 1.0 : 0.0;
-    if (i == j && lu[i + (size_t)i * lda] == 0.0) atomicExch(zero_diag, 1);
-  }
+// A flag if some u_ii of the factors is zero.
+__global__ void zero_diag_kernel(const double* __restrict__ lu, int lda, int n, int* zero_diag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (lu[i + (size_t)i * lda] == 0.0) atomicExch(zero_diag, 1);
 }
 
-// The inverse from dgetrf's factors (mod.rs:249-298): the columns of the
-// identity through the exact solve (the interchanges, the unit-lower row-dot
-// sweep, the upper sweep dividing by u_ii, each entry in the reference's
-// order), into d_inv (ld n); ALG_SINGULAR, with nothing written, when some
-// u_ii is zero.
+// Column `col` of the inverse (mod.rs:249-298), one thread per column and the
+// reference's loops as they are: b = e_col with dgetrf's interchanges
+// applied (row i of P e_col is entry perm[i]), the unit-lower sweep
+// sum -= l_ij b_j in increasing j, then the upper sweep sum -= u_ij b_j in
+// increasing j and b_i = sum / u_ii, each product and difference rounded on
+// its own — so every entry equals the reference's bit for bit. The working
+// column lives in w (n x n, w[i * n + col]) so a warp's accesses coalesce.
+__global__ void __launch_bounds__(128) inverse_columns_kernel(const double* __restrict__ lu, int lda, int n,
+                                                              const int* __restrict__ perm, double* __restrict__ w,
+                                                              double* __restrict__ inv) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  double* x = w + col;
+  for (int i = 0; i < n; ++i) x[(size_t)i * n] = perm[i] == col ? 1.0 : 0.0;
+  for (int i = 0; i < n; ++i) {
+    double sum = x[(size_t)i * n];
+#pragma unroll 8
+    for (int j = 0; j < i; ++j) sum = __dsub_rn(sum, __dmul_rn(lu[i + (size_t)j * lda], x[(size_t)j * n]));
+    x[(size_t)i * n] = sum;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double sum = x[(size_t)i * n];
+#pragma unroll 8
+    for (int j = i + 1; j < n; ++j) sum = __dsub_rn(sum, __dmul_rn(lu[i + (size_t)j * lda], x[(size_t)j * n]));
+    x[(size_t)i * n] = __ddiv_rn(sum, lu[i + (size_t)i * lda]);
+  }
+  for (int i = 0; i < n; ++i) inv[i + (size_t)col * n] = x[(size_t)i * n];
+}
+
+// The inverse from dgetrf's factors (mod.rs:249-298) into d_inv (ld n);
+// ALG_SINGULAR, with nothing written, when some u_ii is zero.
 int inverse_dev(alg_ctx* ctx, const double* d_lu, int n, int lda, const int* d_perm, double* d_inv) {
   int* flag = nullptr;
+  double* w = nullptr;
   ALG_TRY(alg::ws_get(ctx, alg::WS_MISC, sizeof(int), reinterpret_cast<void**>(&flag)));
+  ALG_TRY(alg::ws_get(ctx, alg::WS_X, sizeof(double) * (size_t)n * n, reinterpret_cast<void**>(&w)));
   ALG_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
-  const int grid = (int)std::max<size_t>(1, std::min<size_t>(((size_t)n * n + 255) / 256, 8 * (size_t)ctx->sm_count));
-  identity_and_zero_diag_kernel<<<grid, 256, 0, ctx->stream>>>(d_lu, lda, d_inv, n, n, flag);
+  zero_diag_kernel<<<std::max(1, std::min(ctx->sm_count, (n + 255) / 256)), 256, 0, ctx->stream>>>(d_lu, lda, n,
+                                                                                                    flag);
   alg::count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   int zero = 0;
   ALG_CUDA_TRY(cudaMemcpyAsync(&zero, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   if (zero) return ALG_SINGULAR;
-  return solve_any(ctx, ALG_UPDATE_EXACT, d_lu, n, lda, d_perm, d_inv, n, n);
+  const int tok = alg::prof_begin(ctx, ALG_K_SOLVE);
+  inverse_columns_kernel<<<(n + 127) / 128, 128, 0, ctx->stream>>>(d_lu, lda, n, d_perm, w, d_inv);
+  alg::count_launches();
+  alg::prof_end(ctx, tok, 2.0 * (double)n * n * n, 8.0 * (double)n * n * 3);
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
 }
 
 }  // namespace

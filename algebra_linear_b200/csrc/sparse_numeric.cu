@@ -30,7 +30,6 @@ namespace sp {
 namespace {
 
 constexpr int kSmallThreads = 256;
-constexpr size_t kSmallSmemBytes = 96 * 1024;  // a front that fits is worked in shared memory (two CTAs per SM)
 
 template <typename T>
 __device__ __forceinline__ T fma_t(T a, T b, T c);
@@ -56,7 +55,6 @@ struct SmallArgs {
   T* U;
   int32_t* rowid;
   int* singular;
-  int smem_entries;  // fronts of at most this many entries are worked in shared memory
 };
 
 // First index of the largest key over the block (ties to the lower index).
@@ -140,19 +138,13 @@ __device__ void cta_gemm_sub(T* C, const T* A, const T* B, int ld, int mr, int n
 
 template <typename T>
 __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char small_smem[];
   __shared__ double rk[kSmallThreads / 32];
   __shared__ int ri[kSmallThreads / 32];
   __shared__ T piv_s;
   const int s = a.level_fronts[blockIdx.x];
   const FrontDesc d = a.fronts[s];
   const int rows = d.rows, size = d.size, cols = d.size + d.ncb;
-  // the front is assembled and factored in shared memory when it fits (the
-  // column-serial pivot steps then wait on shared, not global, memory); its
-  // contribution block is written back to the block arena for the parent
-  T* const fg = a.block + d.block_off;
-  const bool in_smem = (int64_t)rows * cols <= a.smem_entries;
-  T* f = in_smem ? reinterpret_cast<T*>(small_smem) : fg;
+  T* f = a.block + d.block_off;
   int32_t* rid = a.rowid + d.rowid_off;
   const int tid = threadIdx.x;
   const int64_t total = (int64_t)rows * cols;
@@ -249,11 +241,6 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
   T* up = a.U + d.u_off;
   for (int t = 0; t < d.ncb; ++t)
     for (int kk = tid; kk < size; kk += kSmallThreads) up[kk + t * size] = f[kk + (size + t) * rows];
-  if (in_smem) {
-    const int crows = rows - size;
-    for (int t = 0; t < d.ncb; ++t)
-      for (int i = tid; i < crows; i += kSmallThreads) fg[(size + i) + (size + t) * rows] = f[(size + i) + (size + t) * rows];
-  }
 }
 
 // ---- large fronts ----------------------------------------------------------
@@ -847,25 +834,12 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   sa.U = U;
   sa.rowid = out.rowid;
   sa.singular = d_flag;
-  // ALG_SPLU_SMALL_SMEM=0 keeps every small front in the block arena
-  const char* sm_env = std::getenv("ALG_SPLU_SMALL_SMEM");
-  const bool use_smem = sm_env == nullptr || sm_env[0] != '0';
-  sa.smem_entries = use_smem ? (int)(kSmallSmemBytes / sizeof(T)) : 0;
-  {
-    static bool configured[2] = {false, false};
-    bool& done = configured[sizeof(T) == 8 ? 1 : 0];
-    if (!done) {
-      ALG_CUDA_TRY(cudaFuncSetAttribute(small_front_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kSmallSmemBytes));
-      done = true;
-    }
-  }
   const int tok_small = prof_begin(ctx, ALG_K_BATCH);
   for (size_t h = 0; h + 1 < F.small_level_ptr.size(); ++h) {
     const int cnt = F.small_level_ptr[h + 1] - F.small_level_ptr[h];
     if (cnt == 0) continue;
     sa.level_fronts = d_small_levels + F.small_level_ptr[h];
-    small_front_kernel<T><<<cnt, kSmallThreads, use_smem ? kSmallSmemBytes : 0, st>>>(sa);
+    small_front_kernel<T><<<cnt, kSmallThreads, 0, st>>>(sa);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
