@@ -154,16 +154,24 @@ int launch_panel(alg_ctx* ctx, const PanelArgs<T>& args) {
 template <typename T, bool EXACT>
 int launch_trsm_reg(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce) {
   const size_t smem = sizeof(T) * (size_t)kb * kb;
-  auto kern = kb <= 32 ? trsm_lower_unit_reg_kernel<T, EXACT, 1>
-                       : (kb <= 64 ? trsm_lower_unit_reg_kernel<T, EXACT, 2> : trsm_lower_unit_reg_kernel<T, EXACT, 4>);
+  // narrow right-hand sides (a block's columns on the look-ahead chain): two
+  // columns per warp for more CTAs; wide ones: eight
+  const bool narrow = ce - cb <= 1024;
+  auto pick = [&](auto k1, auto k2, auto k4) { return kb <= 32 ? k1 : (kb <= 64 ? k2 : k4); };
+  auto kern = narrow ? pick(trsm_lower_unit_reg_kernel<T, EXACT, 1, 2>, trsm_lower_unit_reg_kernel<T, EXACT, 2, 2>,
+                            trsm_lower_unit_reg_kernel<T, EXACT, 4, 2>)
+                     : pick(trsm_lower_unit_reg_kernel<T, EXACT, 1, 8>, trsm_lower_unit_reg_kernel<T, EXACT, 2, 8>,
+                            trsm_lower_unit_reg_kernel<T, EXACT, 4, 8>);
   static bool configured = false;
   if (!configured) {
-    for (auto k : {trsm_lower_unit_reg_kernel<T, EXACT, 1>, trsm_lower_unit_reg_kernel<T, EXACT, 2>,
-                   trsm_lower_unit_reg_kernel<T, EXACT, 4>})
+    for (auto k : {trsm_lower_unit_reg_kernel<T, EXACT, 1, 2>, trsm_lower_unit_reg_kernel<T, EXACT, 2, 2>,
+                   trsm_lower_unit_reg_kernel<T, EXACT, 4, 2>, trsm_lower_unit_reg_kernel<T, EXACT, 1, 8>,
+                   trsm_lower_unit_reg_kernel<T, EXACT, 2, 8>, trsm_lower_unit_reg_kernel<T, EXACT, 4, 8>})
       ALG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     configured = true;
   }
-  const int grid = (ce - cb + kTrsmRegCols - 1) / kTrsmRegCols;
+  const int cta_cols = (narrow ? 2 : 8) * (kTrsmThreads / 32);
+  const int grid = (ce - cb + cta_cols - 1) / cta_cols;
   const int tok = prof_begin(ctx, ALG_K_TRSM);
   kern<<<grid, kTrsmThreads, smem, ctx->stream>>>(a, lda, r0, kb, cb, ce);
   count_launches();

@@ -878,20 +878,21 @@ __global__ void iota_kernel(int* v, int n) {
 // k = r0 .. i-1 in that order (one rounded multiply-subtract each in the
 // exact form), the reference's order for those entries. No block barrier
 // inside: L11 (kb <= 128) staged in shared memory, each warp owns
-// kTrsmRegCols / 8 whole columns with lane l holding rows l, l + 32, ... in
+// CPW whole columns with lane l holding rows l, l + 32, ... in
 // registers; step k broadcasts x_k from its owner lane by a shuffle.
 // ---------------------------------------------------------------------------
 constexpr int kTrsmThreads = 256;
-constexpr int kTrsmRegCols = 64;
-
-template <typename T, bool EXACT, int RPT>
+// CPW columns per warp: 8 for wide right-hand sides, 2 for narrow ones (more
+// CTAs and a shorter per-step chain when only a block's columns are solved).
+template <typename T, bool EXACT, int RPT, int CPW>
 __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T* a, int lda, int r0, int kb, int cb,
                                                                            int ce) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* L = reinterpret_cast<T*>(smem_raw);  // kb x kb, column-major
-  constexpr int kWarpCols = kTrsmRegCols / (kTrsmThreads / 32);
-  const int c_first = cb + blockIdx.x * kTrsmRegCols;
-  const int ncol = min(kTrsmRegCols, ce - c_first);
+  constexpr int kWarpCols = CPW;
+  constexpr int kCtaCols = CPW * (kTrsmThreads / 32);
+  const int c_first = cb + blockIdx.x * kCtaCols;
+  const int ncol = min(kCtaCols, ce - c_first);
   if (ncol <= 0) return;
   for (int idx = threadIdx.x; idx < kb * kb; idx += kTrsmThreads) {
     const int i = idx % kb, k = idx / kb;

@@ -57,39 +57,6 @@ struct SmallArgs {
   int* singular;
 };
 
-// First index of the largest key over the block (ties to the lower index).
-__device__ int block_first_max(double key, int idx, double* rk, int* ri) {
-  for (int off = 16; off > 0; off >>= 1) {
-    const double ok = __shfl_down_sync(0xffffffffu, key, off);
-    const int oi = __shfl_down_sync(0xffffffffu, idx, off);
-    if (ok > key || (ok == key && oi < idx)) {
-      key = ok;
-      idx = oi;
-    }
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    rk[warp] = key;
-    ri[warp] = idx;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double k = rk[0];
-    int i = ri[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-      if (rk[w] > k || (rk[w] == k && ri[w] < i)) {
-        k = rk[w];
-        i = ri[w];
-      }
-    rk[0] = k;
-    ri[0] = i;
-  }
-  __syncthreads();
-  const int r = ri[0];
-  __syncthreads();
-  return r;
-}
-
 // C (mr x nc) -= A (mr x kd) B (kd x nc), all inside one front (column-major,
 // leading dimension ld), by one CTA of kSmallThreads: 64 x 64 tiles, each
 // thread a 4 x 4 register block, K staged through shared memory 16 at a time.
@@ -138,9 +105,6 @@ __device__ void cta_gemm_sub(T* C, const T* A, const T* B, int ld, int mr, int n
 
 template <typename T>
 __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T> a) {
-  __shared__ double rk[kSmallThreads / 32];
-  __shared__ int ri[kSmallThreads / 32];
-  __shared__ T piv_s;
   const int s = a.level_fronts[blockIdx.x];
   const FrontDesc d = a.fronts[s];
   const int rows = d.rows, size = d.size, cols = d.size + d.ncb;
@@ -174,7 +138,20 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
     }
   }
   __syncthreads();
+  // Three barriers per column: (1) the previous column's multipliers are
+  // scaled and this column's pivot is searched, each warp posting its
+  // candidate in a mailbox double-buffered by column parity that every
+  // thread then reduces itself; (2) the row interchange (the pivot is read
+  // from row k only after it); (3) the rank-1 update, which forms each
+  // multiplier a_ik * (1 / pivot) itself, exactly as it is stored (so the
+  // arithmetic is that of scale-then-update).
+  __shared__ double mk[2][kSmallThreads / 32];
+  __shared__ int mi[2][kSmallThreads / 32];
+  const int lane = tid & 31, warp = tid >> 5;
+  T inv_prev = T(0);
   for (int k = 0; k < size; ++k) {
+    if (k > 0)
+      for (int i = k + tid; i < rows; i += kSmallThreads) f[i + (k - 1) * rows] *= inv_prev;
     double key = -1.0;
     int idx = INT_MAX;
     for (int i = k + tid; i < rows; i += kSmallThreads) {
@@ -184,13 +161,30 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
         idx = i;
       }
     }
-    const int p = block_first_max(key, idx, rk, ri);
-    if (tid == 0) piv_s = f[p + (int64_t)k * rows];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ok = __shfl_down_sync(0xffffffffu, key, off);
+      const int oi = __shfl_down_sync(0xffffffffu, idx, off);
+      if (ok > key || (ok == key && oi < idx)) {
+        key = ok;
+        idx = oi;
+      }
+    }
+    const int par = k & 1;
+    if (lane == 0) {
+      mk[par][warp] = key;
+      mi[par][warp] = idx;
+    }
     __syncthreads();
-    const T pv = piv_s;
-    if (!(fabs((double)pv) > 0.0)) {
+    double bk = mk[par][0];
+    int p = mi[par][0];
+    for (int w = 1; w < kSmallThreads / 32; ++w)
+      if (mk[par][w] > bk || (mk[par][w] == bk && mi[par][w] < p)) {
+        bk = mk[par][w];
+        p = mi[par][w];
+      }
+    if (!(bk > 0.0)) {  // bk = |pivot|
       if (tid == 0) atomicExch(a.singular, 1);
-      return;  // uniform: every thread read the same pivot
+      return;  // uniform: every thread reduced the same mailboxes
     }
     if (p != k) {
       for (int j = tid; j < cols; j += kSmallThreads) {
@@ -205,15 +199,18 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
       }
     }
     __syncthreads();
-    const T inv = T(1) / pv;
-    for (int i = k + 1 + tid; i < rows; i += kSmallThreads) f[i + k * rows] *= inv;
-    __syncthreads();
+    const T inv = T(1) / f[k + (int64_t)k * rows];  // the pivot, swapped into row k
     // rank-1 update of the front's own columns, spread over all threads
     const int mr = rows - k - 1, mc = size - k - 1;
     for (int e = tid; e < mr * mc; e += kSmallThreads) {
       const int i = k + 1 + e % mr, j = k + 1 + e / mr;
-      f[i + j * rows] = fma_t(-f[k + j * rows], f[i + k * rows], f[i + j * rows]);
+      f[i + j * rows] = fma_t(-f[k + j * rows], f[i + k * rows] * inv, f[i + j * rows]);
     }
+    inv_prev = inv;
+    __syncthreads();
+  }
+  if (size > 0) {
+    for (int i = size + tid; i < rows; i += kSmallThreads) f[i + (size - 1) * rows] *= inv_prev;
     __syncthreads();
   }
   __shared__ T As[64 * 16], Bs[16 * 64];

@@ -155,3 +155,26 @@ def test_device_resident_refactorization(gpu, osp):
     ref = osp.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], sym["supernode_ptr"])
     xr = ref.solve(b)
     assert np.max(np.abs(x - xr) / np.maximum(np.abs(xr), 1.0)) <= 1e-12
+
+
+@pytest.mark.parametrize("dims", [(150, 150, 1), (200, 120, 1)], ids=lambda d: "x".join(map(str, d)))
+def test_large_two_dimensional_grid_backward_error(gpu, osp, dims):
+    """A 2-D grid with thousands of small fronts per tree level (the serving
+    workload's shape, too large for the oracle): x must be at the FP64
+    backward-error level and the refactorization must agree with it."""
+    import scipy.sparse as ss
+
+    cp, ri, kind = osp.grid_pattern(*dims)
+    v, s = osp.convection_diffusion_values(kind, [1988, 1989, 1990, 1991])
+    n = len(cp) - 1
+    lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+    assert lu.plan()["n_small_fronts"] > 1000
+    for vals in (v, osp.perturb(v, s)[0]):
+        lu.factorize(cp, ri, vals)
+        b, _ = osp.dense.larnv("Symmetric", [4, 3, 2, 1], n)
+        x = b.copy()
+        lu.solve(x)
+        a = ss.csc_matrix((np.asarray(vals), np.asarray(ri, dtype=np.int64), np.asarray(cp, dtype=np.int64)),
+                          shape=(n, n))
+        eta = np.max(np.abs(b - a @ x)) / (np.max(abs(a).sum(axis=1)) * np.max(np.abs(x)) + np.max(np.abs(b)))
+        assert eta <= 1e-14, eta
