@@ -73,9 +73,15 @@ constexpr int kWarps = kRows / 32;
 // column whose pivot was zero.
 constexpr int kSub = 8;
 
+// Pivot keys as ordered integers: |v|'s bit pattern + 1 (bit patterns of
+// non-negative floats order like the values), 0 for a row that is out of the
+// running, so one warp-wide integer max (redux) and a ballot for its first
+// lane find the largest |v| and, among equals, the lowest row.
+__device__ __forceinline__ unsigned pivot_key(float v, bool live) { return live ? __float_as_uint(fabsf(v)) + 1u : 0u; }
+
 struct GeppShared {
   float row[2][kWarps][kSub];  // mailboxes: each warp's best row, sub-block entries
-  float key[2][kWarps];
+  unsigned key[2][kWarps];
   int idx[2][kWarps];
   float prow[kSub][kW];        // the sub-block's pivot rows (then U12 right of the sub-block)
 };
@@ -95,50 +101,30 @@ __device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShar
 #pragma unroll
       for (int cc = 1; cc < kSub; ++cc)
         if (cc == jj) vj = v[jb + cc];
-      float key = (t < nr && chosen < 0) ? fabsf(vj) : -1.0f;
-      int idx = t;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const float ok = __shfl_xor_sync(0xffffffffu, key, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
-        if (ok > key || (ok == key && oi < idx)) {
-          key = ok;
-          idx = oi;
-        }
-      }
-      if (key < 0.0f) {
+      const unsigned key = pivot_key(vj, t < nr && chosen < 0);
+      const unsigned wmax = __reduce_max_sync(0xffffffffu, key);
+      if (wmax == 0u) {
         if (lane == 0) {
-          sh.key[par][warp] = -1.0f;
+          sh.key[par][warp] = 0u;
           sh.idx[par][warp] = INT_MAX;
         }
-      } else if (idx == t) {
-        sh.key[par][warp] = key;
-        sh.idx[par][warp] = idx;
+      } else if (lane == __ffs(__ballot_sync(0xffffffffu, key == wmax)) - 1) {
+        sh.key[par][warp] = wmax;
+        sh.idx[par][warp] = t;
 #pragma unroll
         for (int cc = 0; cc < kSub; ++cc) sh.row[par][warp][cc] = v[jb + cc];
       }
       __syncthreads();
-      float bk = lane < kWarps ? sh.key[par][lane] : -1.0f;
-      int bi = lane < kWarps ? sh.idx[par][lane] : INT_MAX;
-      int bw = lane;
-#pragma unroll
-      for (int off = kWarps / 2; off > 0; off >>= 1) {
-        const float ok = __shfl_xor_sync(0xffffffffu, bk, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        const int ow = __shfl_xor_sync(0xffffffffu, bw, off);
-        if (ok > bk || (ok == bk && oi < bi)) {
-          bk = ok;
-          bi = oi;
-          bw = ow;
-        }
-      }
-      bk = __shfl_sync(0xffffffffu, bk, 0);
-      bi = __shfl_sync(0xffffffffu, bi, 0);
-      bw = __shfl_sync(0xffffffffu, bw, 0);
-      if (bk < 0.0f) {  // fewer rows than columns: every row is chosen
+      // every warp reduces the mailboxes itself (warps in row order, so the
+      // first warp holding the maximum holds its lowest row)
+      const unsigned mk = lane < kWarps ? sh.key[par][lane] : 0u;
+      const unsigned bmax = __reduce_max_sync(0xffffffffu, mk);
+      if (bmax == 0u) {  // fewer rows than columns: every row is chosen
         done = true;
         break;
       }
+      const int bw = __ffs(__ballot_sync(0xffffffffu, mk == bmax)) - 1;
+      const int bi = sh.idx[par][bw];
       if (t == bi) chosen = j;
       const float* pr = sh.row[par][bw];
       const float pv = pr[jj];
