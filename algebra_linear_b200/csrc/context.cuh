@@ -85,6 +85,7 @@ enum WsSlot : int {
   WS_IDENT,       // identity permutation
   WS_BATCH,       // batched-solve queues
   WS_TSLU,        // tournament-pivoting panel scratch
+  WS_TC_CHAIN,    // tensor-core operands of the look-ahead chain's narrow update
   WS_COUNT
 };
 

@@ -312,18 +312,20 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
     return ALG_OK;
   };
   // U12 and the trailing update of columns [cb, ce) by block [k0, k0 + kb);
-  // tc: the tensor-core kernel may take it (one stream at a time uses its
-  // operand workspace: the wide update, never the look-ahead's narrow one)
-  auto update = [&](int k0, int kb, int cb, int ce, bool tc) -> int {
+  // wide: the update of the rest of the matrix (off the look-ahead chain);
+  // the chain's narrow update converts its tensor-core operands in a
+  // workspace of its own, since both can be in flight at once
+  auto update = [&](int k0, int kb, int cb, int ce, bool wide) -> int {
     if (ce <= cb) return ALG_OK;
     const int kr = k0 + kb;
     ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, k0, kb, cb, ce)));
     if (kr >= m) return ALG_OK;
     if constexpr (std::is_same<T, float>::value) {
       // the tensor-core kernel takes whole 128-byte K slices; a ragged last block stays in FP32
-      if (tc && plan.tc_prec >= 0 && kb % (plan.tc_prec == ALG_PREC_BF16 ? 64 : 32) == 0)
+      if (plan.tc_prec >= 0 && kb % (plan.tc_prec == ALG_PREC_BF16 ? 64 : 32) == 0)
         return gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
-                               a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
+                               a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda,
+                               wide ? WS_KRYLOV : WS_TC_CHAIN);
     }
     return gemm_sub_dev<T, EXACT>(ctx, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                   a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);

@@ -34,9 +34,11 @@ int tslu_scratch_reset(alg_ctx* ctx, void* scratch);
 int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch);
 
 // C -= A B on the tensor cores (tcgen05, FP32 accumulation in TMEM) with the
-// operands rounded to TF32 or BF16; A, B, C FP32 column-major.
+// operands rounded to TF32 or BF16 (or split into TF32 pairs); A, B, C FP32
+// column-major. ws_slot: the workspace that holds the converted operands
+// (two updates in flight on two streams need two).
 int gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda, const float* B,
-                    int ldb, float* C, int ldc);
+                    int ldb, float* C, int ldc, int ws_slot = WS_KRYLOV);
 
 // In-place LU of the m x nc (m >= nc) device matrix a (leading dim lda).
 // ipiv: nc global interchanges; perm: m net permutation (may be null).

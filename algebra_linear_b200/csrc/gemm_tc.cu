@@ -342,7 +342,7 @@ int make_map(CUtensorMap* map, const void* ptr, int fmt, int rows, int K, int bo
 
 template <int FMT>
 int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C,
-              int ldc) {
+              int ldc, int ws_slot) {
   const int esz = FMT == 1 ? 2 : 4;
   constexpr int KFMT = FMT == 3 ? 2 : FMT;  // the MMA's operand type (TF32x3 runs TF32 MMAs)
   // K padded to whole 128-byte slices so every TMA row stride is 16-byte aligned
@@ -351,7 +351,7 @@ int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const 
   const int Kp = FMT == 3 ? 3 * K : K;
   void* at = nullptr;
   void* bt = nullptr;
-  ALG_TRY(ws_get(ctx, WS_KRYLOV, (size_t)esz * Kp * ((size_t)M + N) + 256, &at));
+  ALG_TRY(ws_get(ctx, ws_slot, (size_t)esz * Kp * ((size_t)M + N) + 256, &at));
   bt = static_cast<unsigned char*>(at) + (((size_t)esz * Kp * M + 255) & ~size_t(255));
   {
     dim3 grid((M + 31) / 32, (K + 31) / 32);
@@ -381,13 +381,13 @@ int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const 
 }  // namespace
 
 int gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda, const float* B,
-                    int ldb, float* C, int ldc) {
+                    int ldb, float* C, int ldc, int ws_slot) {
   if (M <= 0 || N <= 0 || K <= 0) return ALG_OK;
   const int tok = prof_begin(ctx, ALG_K_GEMM_TC);
   int rc;
-  if (prec == ALG_PREC_BF16) rc = launch_tc<1>(ctx, M, N, K, A, lda, B, ldb, C, ldc);
-  else if (prec == ALG_PREC_TF32) rc = launch_tc<2>(ctx, M, N, K, A, lda, B, ldb, C, ldc);
-  else if (prec == ALG_PREC_TF32X3) rc = launch_tc<3>(ctx, M, N, K, A, lda, B, ldb, C, ldc);
+  if (prec == ALG_PREC_BF16) rc = launch_tc<1>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot);
+  else if (prec == ALG_PREC_TF32) rc = launch_tc<2>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot);
+  else if (prec == ALG_PREC_TF32X3) rc = launch_tc<3>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot);
   else rc = ALG_INVALID_ARGUMENT;
   prof_end(ctx, tok, 2.0 * M * N * K, 4.0 * (2.0 * M * N + double(M) * K + double(K) * N));
   return rc;
