@@ -200,7 +200,9 @@ def run_form(name, spec, ctx, A0, b0, xt, n, nrhs, steps, warmup, pg, sample_clo
 
     lib = _lib.load()
     needs_restore, solve = spec
-    A = A0.clone() if needs_restore else A0
+    # every form works on its own copy: the mixed forms only read A, unless
+    # their FP64 fallback runs, which must not reach the next form's input
+    A = A0.clone()
     b = b0.clone()
     for _ in range(warmup):
         if needs_restore:
@@ -240,8 +242,14 @@ def run_form(name, spec, ctx, A0, b0, xt, n, nrhs, steps, warmup, pg, sample_clo
         pg.barrier()
     eta = backward_error(A0, b, b0, n, nrhs)
     fwd = float((b - xt).abs().max() / xt.abs().max())
+    report = None
+    if name.startswith("mixed"):
+        from algebra_linear_b200 import mixed
+
+        report = dict(mixed.last_report)  # the last timed step's path and refinement steps
     return {
         "ms_per_step": ms / steps,
+        "refinement": report,
         "gflops": flops_dgesv(n, nrhs) / (ms / steps) / 1e6,
         "backward_error": eta,
         "forward_error": fwd,
