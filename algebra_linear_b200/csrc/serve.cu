@@ -83,6 +83,11 @@ int run_dense(alg_server::Worker& w, alg_request* r) {
   if (r->precision == ALG_REQ_MIXED) {
     alg_mixed_opts o;
     alg_mixed_opts_default(&o);
+    // requests share the GPU with the other workers' kernels: the
+    // tournament's single-launch form is a cooperative launch that waits for
+    // enough idle SMs, while partial pivoting is nearly as fast at the
+    // orders served here
+    o.pivoting = ALG_PIVOT_PARTIAL;
     alg_mixed_report rep;
     rc = alg_dgesv_mixed_dev(w.ctx, &o, w.d_a, (int)n, (int)n, w.d_b, 1, (int)n, &rep);
     r->backward_error = rep.backward_error;

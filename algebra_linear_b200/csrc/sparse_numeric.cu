@@ -913,7 +913,12 @@ int DeviceLu::factor_big(int b, int32_t s, int lane, const double* values, int t
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   LuPlan lp;
-  lp.nb = 64;
+  // block width of a large front's LU (ALG_SPLU_NB: measurement switch)
+  static const int splu_nb = [] {
+    const char* e = std::getenv("ALG_SPLU_NB");
+    return e ? std::max(16, std::atoi(e)) : 64;
+  }();
+  lp.nb = splu_nb;
   lp.nbl = 16;
   lp.tc_prec = tc_prec;
   if constexpr (std::is_same<T, float>::value) {
