@@ -87,3 +87,13 @@ def test_dense_shape_errors_match_the_reference():
     with pytest.raises(LapackError) as e:
         dgesv(np.zeros(5), np.zeros(2))
     assert e.value.kind == "BadShape"
+    # mod.rs:250-255 (dgetri: lengths checked first, n = 0 succeeds)
+    from algebra_linear_b200.lapack import dgetri
+
+    with pytest.raises(LapackError) as e:
+        dgetri(np.zeros(4), 2, [0])
+    assert e.value.kind == "BadShape"
+    with pytest.raises(LapackError) as e:
+        dgetri(np.zeros(3), 2, [0, 1])
+    assert e.value.kind == "BadShape"
+    dgetri(np.zeros(0), 0, [])
