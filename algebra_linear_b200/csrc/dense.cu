@@ -243,6 +243,18 @@ bool lookahead_enabled() {
   return on;
 }
 
+// SMs the look-ahead's wide tensor-core update leaves to the critical chain:
+// its CTAs are persistent, so the chain's kernels (the tournament's
+// cooperative launch needs up to 32 SMs at once) run only on SMs it does not
+// hold. ALG_TC_RESERVE_SMS overrides the count (tuning).
+int tc_reserve_sms() {
+  static const int v = [] {
+    const char* e = std::getenv("ALG_TC_RESERVE_SMS");
+    return e ? std::max(0, std::atoi(e)) : 64;
+  }();
+  return v;
+}
+
 template <typename T, bool EXACT>
 int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, int* ipiv, int* perm,
                           const LuPlan& plan) {
@@ -315,6 +327,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   // wide: the update of the rest of the matrix (off the look-ahead chain);
   // the chain's narrow update converts its tensor-core operands in a
   // workspace of its own, since both can be in flight at once
+  int wide_ctas = 0;  // cap of the wide update's persistent grid (0: every SM)
   auto update = [&](int k0, int kb, int cb, int ce, bool wide) -> int {
     if (ce <= cb) return ALG_OK;
     const int kr = k0 + kb;
@@ -325,7 +338,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
       if (plan.tc_prec >= 0 && kb % (plan.tc_prec == ALG_PREC_BF16 ? 64 : 32) == 0)
         return gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda,
-                               wide ? WS_KRYLOV : WS_TC_CHAIN);
+                               wide ? WS_KRYLOV : WS_TC_CHAIN, wide ? wide_ctas : 0);
     }
     return gemm_sub_dev<T, EXACT>(ctx, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                   a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
@@ -347,6 +360,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   // columns, then block k + 1's panels) while the low-priority stream applies
   // block k to everything else; the two meet once per block.
   ALG_TRY(ctx_lookahead_streams(ctx));
+  wide_ctas = std::max(1, ctx->sm_count - tc_reserve_sms());
   cudaStream_t user = ctx->stream, sa = ctx->la_stream[0], sb = ctx->la_stream[1];
   cudaEvent_t ev_a = ctx->la_event[0], ev_b = ctx->la_event[1], ev_in = ctx->la_event[2];
   ALG_CUDA_TRY(cudaEventRecord(ev_in, user));

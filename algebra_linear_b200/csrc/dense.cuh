@@ -36,9 +36,10 @@ int tslu_panel(alg_ctx* ctx, const TsluArgs& p, void* scratch);
 // C -= A B on the tensor cores (tcgen05, FP32 accumulation in TMEM) with the
 // operands rounded to TF32 or BF16 (or split into TF32 pairs); A, B, C FP32
 // column-major. ws_slot: the workspace that holds the converted operands
-// (two updates in flight on two streams need two).
+// (two updates in flight on two streams need two); max_ctas > 0 caps the
+// persistent grid below the SM count (SMs left to another stream's kernels).
 int gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda, const float* B,
-                    int ldb, float* C, int ldc, int ws_slot = WS_KRYLOV);
+                    int ldb, float* C, int ldc, int ws_slot = WS_KRYLOV, int max_ctas = 0);
 
 // In-place LU of the m x nc (m >= nc) device matrix a (leading dim lda).
 // ipiv: nc global interchanges; perm: m net permutation (may be null).

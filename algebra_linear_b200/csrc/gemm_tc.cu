@@ -8,14 +8,20 @@
 //  1. prep kernels copy A and B into K-major operand buffers (A as M rows of
 //     K entries, B as N rows of K entries) in the operand type (BF16, or FP32
 //     rounded to TF32), so both MMA operands are K-major;
-//  2. the GEMM kernel, one CTA per 128 x 256 output tile:
+//  2. the GEMM kernel, persistent: each CTA takes 128 x 256 output tiles
+//     tile, tile + grid, ... (the grid may be capped below the SM count so
+//     that kernels of another stream find free SMs):
 //       warp 0   TMA producer: 128-byte K slices of the A and B tiles into a
-//                4-stage shared-memory ring (128B swizzle, no multicast);
-//       warp 1   allocates 256 TMEM columns; one lane issues tcgen05.mma
-//                (M=128, N=256, FP32 accumulator in TMEM) per 32-byte K step
-//                and commits each stage back to the producer;
-//       8 warps  epilogue: tcgen05.ld of the accumulator, C -= acc with
-//                coalesced column accesses (thread = row).
+//                4-stage shared-memory ring (128B swizzle, no multicast),
+//                running ahead across tiles;
+//       warp 1   allocates 512 TMEM columns (two accumulators); one lane
+//                issues tcgen05.mma (M=128, N=256, FP32 accumulator) per
+//                32-byte K step into the tile's accumulator, commits each
+//                stage back to the producer and the finished accumulator to
+//                the epilogue;
+//       8 warps  epilogue: tcgen05.ld of the accumulator (then handed back
+//                to the MMA lane), C -= acc with coalesced column accesses
+//                (thread = row), while the MMAs fill the other accumulator.
 // Every wait on an mbarrier is bounded; on expiry the kernel raises the
 // timeout flag of the status block and skips ahead.
 #include <cuda.h>
@@ -39,8 +45,10 @@ constexpr int kSliceBytes = 128;                  // one 128B-swizzle atom along
 constexpr int kABytes = BM * kSliceBytes;         // 16 KB per stage
 constexpr int kBBytes = BN * kSliceBytes;         // 32 KB per stage
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kThreads = 256;
-constexpr int kTmemCols = 256;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
+constexpr int kAccCols = BN;                    // one FP32 accumulator: 128 lanes x 256 columns
+constexpr int kTmemCols = 2 * kAccCols;
 constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -49,6 +57,9 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -137,11 +148,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char* stage_a = base;                                  // [kStages][kABytes]
   unsigned char* stage_b = base + (size_t)kStages * kABytes;      // [kStages][kBBytes]
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)kStages * kStageBytes);
-  // bars[0..S): full, bars[S..2S): empty, bars[2S]: accumulator done
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
+  // bars[0..S): stage full, [S..2S): stage empty, 2S + b: accumulator b full,
+  // 2S + 2 + b: accumulator b drained, 2S + 4: every MMA done
+  uint64_t* acc_full = bars + 2 * kStages;
+  uint64_t* acc_empty = bars + 2 * kStages + 2;
+  uint64_t* mma_done = bars + 2 * kStages + 4;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int mtiles = (M + BM - 1) / BM;
+  const int tiles = mtiles * ((N + BN - 1) / BN);
   const int kslice = kSliceBytes / (FMT == 1 ? 2 : 4);  // K entries per slice
   const int nslices = (K + kslice - 1) / kslice;
 
@@ -150,7 +166,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(smem_addr(&bars[s]), 1);
       mbar_init(smem_addr(&bars[kStages + s]), 1);
     }
-    mbar_init(smem_addr(&bars[2 * kStages]), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_addr(&acc_full[b]), 1);
+      mbar_init(smem_addr(&acc_empty[b]), kEpiWarps);
+    }
+    mbar_init(smem_addr(mma_done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -164,68 +184,105 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  if (warp == 0 && lane == 0) {
-    // ---- TMA producer -------------------------------------------------------
-    for (int ks = 0; ks < nslices; ++ks) {
-      const int s = ks % kStages;
-      const uint32_t round = ks / kStages;
-      if (ks >= kStages && !mbar_wait_bounded(smem_addr(&bars[kStages + s]), (round - 1) & 1)) {
-        ok = false;
-        break;
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer: slice g of this CTA's sequence goes to stage g % S --
+      uint32_t g = 0;
+      for (int tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x) {
+        const int m0 = (tile % mtiles) * BM, n0 = (tile / mtiles) * BN;
+        for (int ks = 0; ks < nslices; ++ks, ++g) {
+          const int s = g % kStages;
+          if (g >= kStages && !mbar_wait_bounded(smem_addr(&bars[kStages + s]), ((g / kStages) - 1) & 1)) {
+            ok = false;
+            break;
+          }
+          const uint32_t full = smem_addr(&bars[s]);
+          mbar_expect_tx(full, kStageBytes);
+          tma_load_2d(smem_addr(stage_a + (size_t)s * kABytes), &map_a, ks * kslice, m0, full);
+          tma_load_2d(smem_addr(stage_b + (size_t)s * kBBytes), &map_b, ks * kslice, n0, full);
+        }
       }
-      const uint32_t full = smem_addr(&bars[s]);
-      mbar_expect_tx(full, kStageBytes);
-      tma_load_2d(smem_addr(stage_a + (size_t)s * kABytes), &map_a, ks * kslice, m0, full);
-      tma_load_2d(smem_addr(stage_b + (size_t)s * kBBytes), &map_b, ks * kslice, n0, full);
     }
-  } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer -----------------------------------------------------------
-    const int ksteps = kSliceBytes / 32;  // 32-byte K steps per slice
-    for (int ks = 0; ks < nslices; ++ks) {
-      const int s = ks % kStages;
-      if (!mbar_wait_bounded(smem_addr(&bars[s]), (ks / kStages) & 1)) {
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer: tile i of this CTA accumulates in accumulator i & 1 --
+      const int ksteps = kSliceBytes / 32;  // 32-byte K steps per slice
+      uint32_t g = 0;
+      int li = 0;
+      for (int tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x, ++li) {
+        const int b = li & 1;
+        // the epilogue has drained this accumulator's previous tile
+        if (li >= 2 && !mbar_wait_bounded(smem_addr(&acc_empty[b]), ((li >> 1) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(b * kAccCols);
+        for (int ks = 0; ks < nslices; ++ks, ++g) {
+          const int s = g % kStages;
+          if (!mbar_wait_bounded(smem_addr(&bars[s]), (g / kStages) & 1)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint64_t adesc = smem_desc_sw128(smem_addr(stage_a + (size_t)s * kABytes));
+          const uint64_t bdesc = smem_desc_sw128(smem_addr(stage_b + (size_t)s * kBBytes));
+          for (int kk = 0; kk < ksteps; ++kk) {
+            // advance the start address by 32 bytes per K step inside the swizzle atom
+            mma_issue<FMT>(d, adesc + (uint64_t)(2 * kk), bdesc + (uint64_t)(2 * kk), (ks | kk) != 0);
+          }
+          mma_commit(smem_addr(&bars[kStages + s]));  // stage free once these MMAs finish
+        }
+        if (!ok) break;
+        mma_commit(smem_addr(&acc_full[b]));  // accumulator complete
+      }
+      // every MMA issued here has finished before TMEM is released
+      mma_commit(smem_addr(mma_done));
+      if (!mbar_wait_bounded(smem_addr(mma_done), 0)) ok = false;
+    }
+  } else {
+    // ---- epilogue: C -= acc ----------------------------------------------------
+    const int lane_base = 32 * (warp & 3);  // TMEM lanes this warp may read
+    const int col_half = ((warp - 2) >> 2) * (BN / 2);
+    int li = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++li) {
+      const int m0 = (tile % mtiles) * BM, n0 = (tile / mtiles) * BN;
+      const int b = li & 1;
+      if (!mbar_wait_bounded(smem_addr(&acc_full[b]), (li >> 1) & 1)) {
         ok = false;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint64_t adesc = smem_desc_sw128(smem_addr(stage_a + (size_t)s * kABytes));
-      const uint64_t bdesc = smem_desc_sw128(smem_addr(stage_b + (size_t)s * kBBytes));
-      for (int kk = 0; kk < ksteps; ++kk) {
-        // advance the start address by 32 bytes per K step inside the swizzle atom
-        mma_issue<FMT>(tmem, adesc + (uint64_t)(2 * kk), bdesc + (uint64_t)(2 * kk), (ks | kk) != 0);
+      const int row = m0 + lane_base + lane;
+      for (int cb = 0; cb < BN / 2; cb += 32) {
+        uint32_t r[32];
+        const uint32_t taddr =
+            tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kAccCols + col_half + cb);
+        TMEM_LD_X32(taddr, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (cb + 32 == BN / 2) {
+          // this warp's share of the accumulator is in registers: hand it back
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_addr(&acc_empty[b]));
+        }
+        if (row < M) {
+          float cv[32];
+#pragma unroll
+          for (int t = 0; t < 32; ++t) {
+            const int col = n0 + col_half + cb + t;
+            cv[t] = col < N ? C[(size_t)row + (size_t)col * ldc] : 0.f;
+          }
+#pragma unroll
+          for (int t = 0; t < 32; ++t) {
+            const int col = n0 + col_half + cb + t;
+            if (col < N) C[(size_t)row + (size_t)col * ldc] = cv[t] - __uint_as_float(r[t]);
+          }
+        }
       }
-      mma_commit(smem_addr(&bars[kStages + s]));  // stage free once these MMAs finish
     }
-    mma_commit(smem_addr(&bars[2 * kStages]));    // accumulator complete
   }
-  __syncwarp();
-
-  // ---- epilogue: C -= acc ------------------------------------------------------
-  if (!mbar_wait_bounded(smem_addr(&bars[2 * kStages]), 0)) ok = false;
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!ok) atomicExch(&status->timeout, 1);
-  const int lane_base = 32 * (warp & 3);   // TMEM lanes this warp may read
-  const int col_half = (warp >> 2) * (BN / 2);
-  const int row = m0 + lane_base + lane;
-  for (int cb = 0; cb < BN / 2; cb += 32) {
-    uint32_t r[32];
-    const uint32_t taddr = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(col_half + cb);
-    TMEM_LD_X32(taddr, r);
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (ok && row < M) {
-      float cv[32];
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = n0 + col_half + cb + t;
-        cv[t] = col < N ? C[(size_t)row + (size_t)col * ldc] : 0.f;
-      }
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = n0 + col_half + cb + t;
-        if (col < N) C[(size_t)row + (size_t)col * ldc] = cv[t] - __uint_as_float(r[t]);
-      }
-    }
-  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 1) {
@@ -342,7 +399,7 @@ int make_map(CUtensorMap* map, const void* ptr, int fmt, int rows, int K, int bo
 
 template <int FMT>
 int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C,
-              int ldc, int ws_slot) {
+              int ldc, int ws_slot, int max_ctas) {
   const int esz = FMT == 1 ? 2 : 4;
   constexpr int KFMT = FMT == 3 ? 2 : FMT;  // the MMA's operand type (TF32x3 runs TF32 MMAs)
   // K padded to whole 128-byte slices so every TMA row stride is 16-byte aligned
@@ -371,8 +428,12 @@ int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const 
                                       (int)kSmemBytes));
     configured = true;
   }
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-  gemm_tc_kernel<KFMT><<<grid, kThreads, kSmemBytes, ctx->stream>>>(ma, mb, M, N, Kp, C, ldc, ctx->d_status);
+  // persistent CTAs, at most one per SM (the shared-memory ring and the 512
+  // TMEM columns take a whole SM), fewer when the caller keeps SMs free
+  const long tiles = (long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  int ctas = max_ctas > 0 ? std::min(max_ctas, ctx->sm_count) : ctx->sm_count;
+  ctas = (int)std::max<long>(1, std::min<long>(ctas, tiles));
+  gemm_tc_kernel<KFMT><<<ctas, kThreads, kSmemBytes, ctx->stream>>>(ma, mb, M, N, Kp, C, ldc, ctx->d_status);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
@@ -381,13 +442,13 @@ int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const 
 }  // namespace
 
 int gemm_tc_sub_dev(alg_ctx* ctx, int prec, int M, int N, int K, const float* A, int lda, const float* B,
-                    int ldb, float* C, int ldc, int ws_slot) {
+                    int ldb, float* C, int ldc, int ws_slot, int max_ctas) {
   if (M <= 0 || N <= 0 || K <= 0) return ALG_OK;
   const int tok = prof_begin(ctx, ALG_K_GEMM_TC);
   int rc;
-  if (prec == ALG_PREC_BF16) rc = launch_tc<1>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot);
-  else if (prec == ALG_PREC_TF32) rc = launch_tc<2>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot);
-  else if (prec == ALG_PREC_TF32X3) rc = launch_tc<3>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot);
+  if (prec == ALG_PREC_BF16) rc = launch_tc<1>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot, max_ctas);
+  else if (prec == ALG_PREC_TF32) rc = launch_tc<2>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot, max_ctas);
+  else if (prec == ALG_PREC_TF32X3) rc = launch_tc<3>(ctx, M, N, K, A, lda, B, ldb, C, ldc, ws_slot, max_ctas);
   else rc = ALG_INVALID_ARGUMENT;
   prof_end(ctx, tok, 2.0 * M * N * K, 4.0 * (2.0 * M * N + double(M) * K + double(K) * N));
   return rc;

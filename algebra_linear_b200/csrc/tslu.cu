@@ -19,7 +19,8 @@
 //      and the block panel's other columns follow the interchanges.
 // The factorization differs from partial pivoting's (other pivots); the
 // mixed form's refinement in FP64 then brings the solution to the FP64
-// backward error, which is its contract. No kernel waits on another CTA.
+// backward error, which is its contract. In the single-launch form every CTA
+// waits (bounded) for the root's release; the multi-launch form has no waits.
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -91,16 +92,17 @@ __device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShar
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   int chosen = -1;
   bool done = false;
+  // both loops unroll completely, so every column index below is a
+  // compile-time constant (the row stays in registers, no selects)
 #pragma unroll
   for (int jb = 0; jb < W; jb += kSub) {
     if (done || jb >= w) break;
     const int nsub = min(kSub, w - jb);
-    for (int jj = 0; jj < nsub; ++jj) {
-      const int j = jb + jj, par = j & 1;
-      float vj = v[jb];
 #pragma unroll
-      for (int cc = 1; cc < kSub; ++cc)
-        if (cc == jj) vj = v[jb + cc];
+    for (int jj = 0; jj < kSub; ++jj) {
+      if (jj >= nsub) break;
+      const int j = jb + jj, par = j & 1;
+      const float vj = v[j];
       const unsigned key = pivot_key(vj, t < nr && chosen < 0);
       const unsigned wmax = __reduce_max_sync(0xffffffffu, key);
       if (wmax == 0u) {
@@ -112,7 +114,7 @@ __device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShar
         sh.key[par][warp] = wmax;
         sh.idx[par][warp] = t;
 #pragma unroll
-        for (int cc = 0; cc < kSub; ++cc) sh.row[par][warp][cc] = v[jb + cc];
+        for (int cc = jj; cc < kSub; ++cc) sh.row[par][warp][cc] = v[jb + cc];
       }
       __syncthreads();
       // every warp reduces the mailboxes itself (warps in row order, so the
@@ -131,11 +133,9 @@ __device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShar
       if (pv == 0.0f && t == 0 && *zero_col < 0) *zero_col = j;
       if (t < nr && chosen < 0) {
         const float l = pv != 0.0f ? vj / pv : 0.0f;
+        v[j] = l;
 #pragma unroll
-        for (int cc = 0; cc < kSub; ++cc) {
-          if (cc == jj) v[jb + cc] = l;
-          if (cc > jj) v[jb + cc] = fmaf(-l, pr[cc], v[jb + cc]);
-        }
+        for (int cc = jj + 1; cc < kSub; ++cc) v[jb + cc] = fmaf(-l, pr[cc], v[jb + cc]);
       }
     }
     if (jb + kSub >= W) break;  // no columns right of the last sub-block
@@ -148,10 +148,14 @@ __device__ __forceinline__ int block_gepp(float (&v)[W], int nr, int w, GeppShar
     __syncthreads();
     if (t < W - jb - kSub) {
       const int c = jb + kSub + t;
-      for (int i = 1; i < nsub; ++i) {
-        float u = sh.prow[i][c];
-        for (int k = 0; k < i; ++k) u = fmaf(-sh.prow[i][jb + k], sh.prow[k][c], u);
-        sh.prow[i][c] = u;
+#pragma unroll
+      for (int i = 1; i < kSub; ++i) {
+        if (i < nsub) {
+          float u = sh.prow[i][c];
+#pragma unroll
+          for (int k = 0; k < i; ++k) u = fmaf(-sh.prow[i][jb + k], sh.prow[k][c], u);
+          sh.prow[i][c] = u;
+        }
       }
     }
     __syncthreads();
@@ -261,60 +265,64 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
   }
   if (t == 0 && zero_col >= 0) atomicMin(&in.status->singular_col, c0 + zero_col);
   __syncthreads();
-  // ---- LAPACK sequential interchanges bringing winner j to position c0 + j,
-  //      tracked over the touched positions only (one warp) ------------------
+  // ---- LAPACK sequential interchanges bringing winner j to position c0 + j.
+  // Only two kinds of position are ever touched: the top positions c0 + i
+  // (i < w) and the original positions of the winners from below the top. A
+  // winner from below sits at its original position until its own step, and
+  // a row that started in the top moves only by the steps, so one lane keeps
+  // the occupant of every touched position and the location of every
+  // top-started row in shared memory and runs the w steps in O(1) each.
   if (t < 32) {
-    __shared__ int pos[kMaxMoves], occ[kMaxMoves];
+    __shared__ int occ_top[kW];  // row at top position c0 + i
+    __shared__ int occ_out[kW];  // row at the original position of winner j (a winner from below)
+    __shared__ int loc_top[kW];  // where the row that started at c0 + i is: i' < kW top, kW + j outside
     const int lane = t;
-    int nt = 0;
-    auto find = [&](const int* arr, int v) -> int {  // index t with arr[t] == v, or -1
-      int hit = -1;
-      for (int b = 0; b < nt; b += 32) {
-        const int i = b + lane;
-        const unsigned m = __ballot_sync(0xffffffffu, i < nt && arr[i] == v);
-        if (m != 0u && hit < 0) hit = b + __ffs(m) - 1;
-      }
-      return hit;
-    };
-    for (int j = 0; j < w; ++j) {
-      const int gr = ws->win[j];
-      const int to = find(occ, gr);
-      const int pr = to >= 0 ? pos[to] : gr;  // current position of row gr
-      int tj = find(pos, c0 + j);
-      if (tj < 0) {
-        if (lane == 0) {
-          pos[nt] = c0 + j;
-          occ[nt] = c0 + j;  // untouched: the row that started there
-        }
-        tj = nt++;
-      }
-      __syncwarp();
-      int tp = find(pos, pr);
-      if (tp < 0) {
-        if (lane == 0) {
-          pos[nt] = pr;
-          occ[nt] = pr;
-        }
-        tp = nt++;
-      }
-      __syncwarp();
-      if (lane == 0) {
-        ipiv[c0 + j] = pr;
-        const int h = occ[tj];
-        occ[tj] = gr;
-        occ[tp] = h;
-      }
-      __syncwarp();
+    if (lane < w) {
+      occ_top[lane] = c0 + lane;
+      loc_top[lane] = lane;
+      const int gr = ws->win[lane];
+      occ_out[lane] = gr;
     }
+    __syncwarp();
+    if (lane == 0) {
+      for (int j = 0; j < w; ++j) {
+        const int gr = ws->win[j];
+        const bool g_top = gr < c0 + w;  // candidates are rows >= c0
+        const int cur = g_top ? loc_top[gr - c0] : kW + j;
+        const int pr = cur < kW ? c0 + cur : ws->win[cur - kW];
+        ipiv[c0 + j] = pr;
+        const int h = occ_top[j];  // the row at c0 + j goes where gr was
+        occ_top[j] = gr;
+        if (g_top) loc_top[gr - c0] = j;
+        if (cur < kW) {
+          if (cur != j) occ_top[cur] = h;
+        } else {
+          occ_out[cur - kW] = h;
+        }
+        if (h < c0 + w && h != gr) loc_top[h - c0] = cur;
+      }
+    }
+    __syncwarp();
+    // the moved rows: top positions and the below-top winners' positions
+    // whose occupant changed (a set; the apply step's order does not matter)
     if (lane == 0) {
       int nm = 0;
-      for (int i = 0; i < nt; ++i)
-        if (occ[i] != pos[i]) {
-          ws->move_pos[nm] = pos[i];
-          ws->move_src[nm] = occ[i];
-          ws->move_lab[nm] = first_leaf ? occ[i] : lab[occ[i]];
+      for (int i = 0; i < w; ++i)
+        if (occ_top[i] != c0 + i) {
+          ws->move_pos[nm] = c0 + i;
+          ws->move_src[nm] = occ_top[i];
+          ws->move_lab[nm] = first_leaf ? occ_top[i] : lab[occ_top[i]];
           ++nm;
         }
+      for (int j = 0; j < w; ++j) {
+        const int gr = ws->win[j];
+        if (gr >= c0 + w && occ_out[j] != gr) {
+          ws->move_pos[nm] = gr;
+          ws->move_src[nm] = occ_out[j];
+          ws->move_lab[nm] = first_leaf ? occ_out[j] : lab[occ_out[j]];
+          ++nm;
+        }
+      }
       ws->nmoves = nm;
     }
   }
