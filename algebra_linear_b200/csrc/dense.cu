@@ -294,16 +294,19 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
       pa.first_leaf = (c0 == k0) ? 1 : 0;
       pa.status = ctx->d_status;
       int prc = ALG_NOT_IMPLEMENTED;
+      bool u12_done = false;  // the tournament's apply step also forms U12 of the block's trailing columns
       if constexpr (std::is_same<T, float>::value) {
-        if (tslu_ws)
+        if (tslu_ws) {
           prc = tslu_panel(ctx, TsluArgs{a, lda, m, c0, w, k0, k0 + kb, ipiv, lb, pa.first_leaf, ctx->d_status},
                            tslu_ws);
+          u12_done = prc == ALG_OK;
+        }
       }
       if (prc == ALG_NOT_IMPLEMENTED) prc = launch_panel<T, EXACT>(ctx, pa);
       ALG_TRY(prc);
       const int cr = c0 + w;  // first column right of the leaf
       if (cr < k0 + kb) {
-        ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, c0, w, cr, k0 + kb)));
+        if (!u12_done) ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, c0, w, cr, k0 + kb)));
         ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - cr, k0 + kb - cr, w, a + (size_t)cr + (size_t)c0 * lda, lda,
                                         a + (size_t)c0 + (size_t)cr * lda, lda,
                                         a + (size_t)cr + (size_t)cr * lda, lda)));

@@ -894,10 +894,6 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T*
   const int c_first = cb + blockIdx.x * kCtaCols;
   const int ncol = min(kCtaCols, ce - c_first);
   if (ncol <= 0) return;
-  for (int idx = threadIdx.x; idx < kb * kb; idx += kTrsmThreads) {
-    const int i = idx % kb, k = idx / kb;
-    L[idx] = a[(size_t)(r0 + i) + (size_t)(r0 + k) * lda];
-  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   T x[kWarpCols][RPT];
 #pragma unroll
@@ -907,6 +903,24 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T*
     for (int r = 0; r < RPT; ++r) {
       const int i = lane + 32 * r;
       x[c][r] = (cc < ncol && i < kb) ? a[(size_t)(r0 + i) + (size_t)(c_first + cc) * lda] : T(0);
+    }
+  }
+  // L's strictly lower part (the rest is never read), kBatch loads in flight
+  // per thread before any is stored
+  constexpr int kBatch = 16;
+  const int total = kb * kb;
+  for (int base = threadIdx.x; base < total; base += kTrsmThreads * kBatch) {
+    T tmp[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int idx = base + u * kTrsmThreads;
+      const int i = idx % kb, k = idx / kb;
+      tmp[u] = (idx < total && i > k) ? a[(size_t)(r0 + i) + (size_t)(r0 + k) * lda] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int idx = base + u * kTrsmThreads;
+      if (idx < total) L[idx] = tmp[u];
     }
   }
   __syncthreads();

@@ -15,8 +15,9 @@
 //      L11 \ U11 of the winners;
 //   3. apply: the interchanges (LAPACK sequential form, as the partial-
 //      pivoting panel records them) move the winners to the top, every other
-//      row gets its multipliers l = a U11^-1, and the labels of the moved rows
-//      and the block panel's other columns follow the interchanges.
+//      row gets its multipliers l = a U11^-1, the labels of the moved rows
+//      and the block panel's other columns follow the interchanges, and the
+//      top rows of the block panel's trailing columns become U12.
 // The factorization differs from partial pivoting's (other pivots); the
 // mixed form's refinement in FP64 then brings the solution to the FP64
 // backward error, which is its contract. In the single-launch form every CTA
@@ -343,8 +344,8 @@ __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(LevelIn in, int sr
 constexpr int kSideCols = 8;
 
 // CTA `cta` of `ncta`: the first side_blocks CTAs permute the block panel's
-// other columns (side_rows: whether they also take rows); rows are spread
-// over the CTAs from row_cta0 on.
+// other columns and turn the top rows of its trailing columns into U12; rows
+// are spread over the CTAs from row_cta0 on.
 template <int W>
 __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab, int first_leaf,
                            int cta, int ncta, int side_blocks, int row_cta0, const TsluScratch* ws) {
@@ -386,6 +387,30 @@ __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int
         if (col >= c0) col += w;
         a[(size_t)mpos[mv] + (size_t)col * lda] = v[u];
       }
+    }
+    // U12 = L11^-1 A12 on this CTA's columns right of the leaf (the block
+    // panel's trailing columns), from the permuted top rows this CTA just
+    // wrote: one warp per column, top row i in lane i, step k's value
+    // broadcast by a shuffle; each entry takes its terms in increasing k with
+    // one FMA each, the arithmetic of the separate FP32 TRSM kernel
+    __syncthreads();
+    const int lane = threadIdx.x & 31, cl = threadIdx.x >> 5;
+    const int cidx = cta * kSideCols + cl;
+    int col = kb0 + cidx;
+    if (col >= c0) col += w;
+    if (cl < kSideCols && cidx < side && col >= c0 + w) {
+      float lrow[kW];  // row `lane` of L11
+#pragma unroll
+      for (int k = 0; k < kW; ++k) lrow[k] = (k < lane && lane < w) ? __ldcg(&ws->top_lu[k * kW + lane]) : 0.0f;
+      float x = lane < w ? a[(size_t)(c0 + lane) + (size_t)col * lda] : 0.0f;
+#pragma unroll
+      for (int k = 0; k + 1 < kW; ++k) {
+        if (k + 1 < w) {
+          const float u = __shfl_sync(0xffffffffu, x, k);
+          if (lane > k && lane < w) x = __fmaf_rn(-lrow[k], u, x);
+        }
+      }
+      if (lane < w) a[(size_t)(c0 + lane) + (size_t)col * lda] = x;
     }
   }
   if (cta < row_cta0) return;
@@ -565,9 +590,9 @@ int launch_fused(alg_ctx* ctx, const TsluArgs& p, int groups0, int side_blocks, 
 
 }  // namespace
 
-// A leaf panel of the FP32 LU by tournament pivoting; same outputs as the
+// A leaf panel of the FP32 LU by tournament pivoting; the outputs of the
 // partial-pivoting cluster kernel (factored panel, ipiv, labels, side
-// columns). Returns ALG_NOT_IMPLEMENTED when the panel does not fit its
+// columns) and U12 of the block panel's trailing columns (the in-block TRSM). Returns ALG_NOT_IMPLEMENTED when the panel does not fit its
 // limits (the caller then uses partial pivoting). One cooperative launch when
 // the level-0 CTAs fit on the device at once, else one launch per tree level
 // and one for the apply step. The scratch is reset once per factorization.
