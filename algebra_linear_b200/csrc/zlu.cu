@@ -1,0 +1,299 @@
+// Complex twins of the dense LU (src/lapack/complex.rs): zgetrf, zgetrf_rect
+// and zgesv on the GPU, bit-identical to the reference.
+//
+// The reference's Complex64 is num_complex::Complex<f64> (num-complex 0.4),
+// whose operators are
+//   (a + ib)(c + id) = (ac - bd) + i(ad + bc)
+//   (a + ib)/(c + id) = ((ac + bd) + i(bc - ad)) / (cc + dd)
+//   (a + ib) - (c + id) = (a - c) + i(b - d)
+// each product, sum and quotient rounded on its own (rustc contracts
+// nothing); the kernels below spell every operation with the _rn intrinsics
+// so that nvcc cannot fuse them. The pivot measure is |Re| + |Im|.
+//
+// Layout: a complex entry is a double2 (re, im), the interleaved layout of
+// the host's complex arrays; matrices column-major, a[i + j * lda].
+//
+// Factorization (complex.rs:67-124 zgetf2, 169-208 zgetrf_rect): one step per
+// column, as the reference's loop:
+//   zpivot_kernel   one CTA: the first row with the largest |Re| + |Im| at or
+//                   below the diagonal (the reference's strict-greater scan,
+//                   NaN included), the zero-pivot test, the whole-row swap,
+//                   the column below the pivot divided by it;
+//   zupdate_kernel  the rank-1 update a_ik -= l_i u_k of the trailing block.
+// Every entry therefore takes its terms in increasing column order, exactly
+// as in the reference. After a zero pivot both kernels do nothing, so the
+// matrix is left as the reference leaves it.
+//
+// Solve (complex.rs:279-312): the interchanges applied to b in order; the
+// unit-lower sweep as a column pipeline (one CTA; row i takes its term for
+// b_j, j = 0, 1, ..., as each b_j becomes final); the upper sweep row
+// by row from the bottom: the products u_ij b_j of a row in parallel, then
+// subtracted from b_i in increasing j by one thread (the reference's order)
+// and divided by u_ii.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstddef>
+#include <mutex>
+#include <vector>
+
+#include "dense.cuh"
+
+namespace alg {
+namespace {
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) {
+  return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
+  const double norm_sqr = __dadd_rn(__dmul_rn(b.x, b.x), __dmul_rn(b.y, b.y));
+  const double re = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+  const double im = __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y));
+  return make_double2(__ddiv_rn(re, norm_sqr), __ddiv_rn(im, norm_sqr));
+}
+__device__ __forceinline__ double zabs1(double2 z) { return __dadd_rn(fabs(z.x), fabs(z.y)); }
+
+__device__ __forceinline__ bool stopped(const DevStatus* st) {
+  return *reinterpret_cast<const volatile int*>(&st->singular_col) != INT_MAX;
+}
+
+constexpr int kPivThreads = 1024;
+
+// Step j of the factorization of an m x nc matrix (m >= nc): pivot, swap of
+// the whole rows (all nc columns), scaling of column j below the diagonal.
+__global__ void __launch_bounds__(kPivThreads) zpivot_kernel(double2* __restrict__ a, int lda, int m, int nc, int j,
+                                                             int* __restrict__ ipiv, DevStatus* st) {
+  __shared__ double sb[kPivThreads / 32];
+  __shared__ int si[kPivThreads / 32];
+  __shared__ int piv_s;
+  if (stopped(st)) return;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  double2* col = a + (size_t)j * lda;
+  // first maximum over this thread's rows below the diagonal (a NaN is never
+  // greater, as in the reference's scan); -1 means none
+  double best = -1.0;
+  int bi = INT_MAX;
+  for (int i = j + 1 + t; i < m; i += kPivThreads) {
+    const double c = zabs1(col[i]);
+    if (c > best) {
+      best = c;
+      bi = i;
+    }
+  }
+  // larger value wins, the lower row among equals
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ob = __shfl_down_sync(0xffffffffu, best, off);
+    const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
+    }
+  }
+  if (lane == 0) {
+    sb[warp] = best;
+    si[warp] = bi;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double gb = sb[0];
+    int gi = si[0];
+    for (int w = 1; w < kPivThreads / 32; ++w)
+      if (sb[w] > gb || (sb[w] == gb && si[w] < gi)) {
+        gb = sb[w];
+        gi = si[w];
+      }
+    // the diagonal entry comes first in the reference's scan: a row below
+    // replaces it only when strictly greater (never when it is NaN)
+    const double vj = zabs1(col[j]);
+    int jp = j;
+    double pbest = vj;
+    if (gi != INT_MAX && gb > vj) {
+      jp = gi;
+      pbest = gb;
+    }
+    if (pbest <= 0.0) {  // ZERO_DETERMINANT = 0.0
+      atomicMin(&st->singular_col, j);
+      jp = -1;
+    } else {
+      ipiv[j] = jp;
+    }
+    piv_s = jp;
+  }
+  __syncthreads();
+  const int jp = piv_s;
+  if (jp < 0) return;
+  if (jp != j) {
+    for (int k = t; k < nc; k += kPivThreads) {
+      double2* c = a + (size_t)k * lda;
+      const double2 x = c[j];
+      c[j] = c[jp];
+      c[jp] = x;
+    }
+  }
+  __syncthreads();
+  const double2 d = col[j];
+  for (int i = j + 1 + t; i < m; i += kPivThreads) col[i] = zdiv(col[i], d);
+}
+
+// Step j's rank-1 update: a[i, k] -= a[i, j] * a[j, k] for i in (j, m),
+// k in (j, nc); a thread per row, a CTA row per column (grid-strided).
+__global__ void __launch_bounds__(256) zupdate_kernel(double2* __restrict__ a, int lda, int m, int nc, int j,
+                                                      const DevStatus* st) {
+  if (stopped(st)) return;
+  const int i = j + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double2 l = a[i + (size_t)j * lda];
+  for (int k = j + 1 + blockIdx.y; k < nc; k += gridDim.y) {
+    double2* c = a + (size_t)k * lda;
+    c[i] = zsub(c[i], zmul(l, c[j]));
+  }
+}
+
+constexpr int kSolveThreads = 1024;
+constexpr int kFoldChunk = 2048;  // products per chunk of the upper sweep (32 KB of shared memory)
+
+// zgesv's interchanges and unit-lower sweep (complex.rs:287-301), one CTA:
+// at step j every row below j takes its term l_ij b_j, so each row's terms
+// arrive in increasing j and b_j is final when step j starts.
+__global__ void __launch_bounds__(kSolveThreads) zforward_kernel(const double2* __restrict__ lu, int lda, int n,
+                                                                 const int* __restrict__ ipiv, double2* b) {
+  const int t = threadIdx.x;
+  if (t == 0)
+    for (int k = 0; k < n; ++k) {
+      const int p = ipiv[k];
+      const double2 x = b[k];
+      b[k] = b[p];
+      b[p] = x;
+    }
+  for (int j = 0; j + 1 < n; ++j) {
+    __syncthreads();  // step j - 1's updates (b_j's last term among them) are in place
+    const double2 bj = b[j];
+    const double2* lcol = lu + (size_t)j * lda;
+    for (int i = j + 1 + t; i < n; i += kSolveThreads) b[i] = zsub(b[i], zmul(lcol[i], bj));
+  }
+}
+
+// zgesv's upper sweep (complex.rs:304-311), one CTA: row i's products in
+// parallel (by chunks), folded into b_i in increasing j by thread 0.
+__global__ void __launch_bounds__(kSolveThreads) zbackward_kernel(const double2* __restrict__ lu, int lda, int n,
+                                                                  double2* b) {
+  __shared__ double2 p[kFoldChunk];
+  __shared__ double2 sum_s;
+  const int t = threadIdx.x;
+  for (int i = n - 1; i >= 0; --i) {
+    if (t == 0) sum_s = b[i];
+    for (int j0 = i + 1; j0 < n; j0 += kFoldChunk) {
+      const int j1 = min(n, j0 + kFoldChunk);
+      for (int j = j0 + t; j < j1; j += kSolveThreads) p[j - j0] = zmul(lu[i + (size_t)j * lda], b[j]);
+      __syncthreads();
+      if (t == 0) {
+        double2 s = sum_s;
+        for (int j = j0; j < j1; ++j) s = zsub(s, p[j - j0]);
+        sum_s = s;
+      }
+      __syncthreads();
+    }
+    if (t == 0) b[i] = zdiv(sum_s, lu[i + (size_t)i * lda]);
+    __syncthreads();
+  }
+}
+
+// Factorization of the m x nc device matrix (m >= nc), stream-ordered; a zero
+// pivot lands in the status block's singular_col.
+int zlu_factor_dev(alg_ctx* ctx, double2* d_a, int m, int nc, int lda, int* d_ipiv) {
+  for (int j = 0; j < nc; ++j) {
+    zpivot_kernel<<<1, kPivThreads, 0, ctx->stream>>>(d_a, lda, m, nc, j, d_ipiv, ctx->d_status);
+    const int rows = m - j - 1, cols = nc - j - 1;
+    int launches = 1;
+    if (rows > 0 && cols > 0) {
+      dim3 grid((rows + 255) / 256, std::min(cols, 65535));
+      zupdate_kernel<<<grid, 256, 0, ctx->stream>>>(d_a, lda, m, nc, j, ctx->d_status);
+      ++launches;
+    }
+    count_launches(launches);
+  }
+  ALG_CUDA_TRY(cudaGetLastError());
+  return ALG_OK;
+}
+
+bool zsize_ok(size_t n) { return n <= (size_t)INT_MAX / 4; }
+
+struct ZCtxLock {
+  alg_ctx* ctx = nullptr;
+  std::unique_lock<std::mutex> lk;
+  int rc = ALG_OK;
+  ZCtxLock() {
+    rc = default_ctx(&ctx);
+    if (rc == ALG_OK) lk = std::unique_lock<std::mutex>(ctx->mu);
+  }
+};
+
+// Host drop-in core: a (m x nc complex, interleaved) and b (m complex, or
+// null) copied in, factored (and solved), copied back.
+int host_zlu(double* a, size_t m, size_t nc, size_t* ipiv, double* b) {
+  if (!zsize_ok(m) || !zsize_ok(nc)) return ALG_BAD_SHAPE;
+  ZCtxLock L;
+  if (L.rc != ALG_OK) return L.rc;
+  alg_ctx* ctx = L.ctx;
+  const int M = (int)m, N = (int)nc;
+  const size_t abytes = 2 * sizeof(double) * m * nc;
+  double2* d_a = nullptr;
+  double2* d_b = nullptr;
+  int* d_ipiv = nullptr;
+  ALG_TRY(ws_get(ctx, WS_A, abytes, reinterpret_cast<void**>(&d_a)));
+  ALG_TRY(ws_get(ctx, WS_IPIV, sizeof(int) * std::max<size_t>(nc, 1), reinterpret_cast<void**>(&d_ipiv)));
+  if (b != nullptr) ALG_TRY(ws_get(ctx, WS_B, 2 * sizeof(double) * m, reinterpret_cast<void**>(&d_b)));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_a, a, abytes, cudaMemcpyHostToDevice, ctx->stream));
+  if (d_b) ALG_CUDA_TRY(cudaMemcpyAsync(d_b, b, 2 * sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_TRY(status_reset(ctx));
+  ALG_TRY(zlu_factor_dev(ctx, d_a, M, N, M, d_ipiv));
+  ALG_TRY(status_fetch(ctx));
+  const bool singular = ctx->h_status->singular_col != INT_MAX;
+  if (!singular && d_b) {
+    zforward_kernel<<<1, kSolveThreads, 0, ctx->stream>>>(d_a, M, M, d_ipiv, d_b);
+    zbackward_kernel<<<1, kSolveThreads, 0, ctx->stream>>>(d_a, M, M, d_b);
+    count_launches(2);
+    ALG_CUDA_TRY(cudaGetLastError());
+    ALG_CUDA_TRY(cudaMemcpyAsync(b, d_b, 2 * sizeof(double) * m, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ALG_CUDA_TRY(cudaMemcpyAsync(a, d_a, abytes, cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<int> h_ipiv(std::max<size_t>(nc, 1));
+  ALG_CUDA_TRY(cudaMemcpyAsync(h_ipiv.data(), d_ipiv, sizeof(int) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (singular) return ALG_SINGULAR;
+  if (ipiv)
+    for (size_t k = 0; k < nc; ++k) ipiv[k] = (size_t)h_ipiv[k];
+  return ALG_OK;
+}
+
+}  // namespace
+}  // namespace alg
+
+// complex.rs:67 zgetrf(a, n) -> ipiv
+extern "C" int alg_zgetrf(double* a, size_t n, size_t* ipiv) {
+  if (n == 0) return ALG_OK;
+  if (a == nullptr || ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  return alg::host_zlu(a, n, n, ipiv, nullptr);
+}
+
+// complex.rs:169 zgetrf_rect(a, nrows, ncols, ipiv)
+extern "C" int alg_zgetrf_rect(double* a, size_t nrows, size_t ncols, size_t* ipiv) {
+  if (nrows < ncols) return ALG_BAD_SHAPE;
+  if (ncols == 0) return ALG_OK;
+  if (a == nullptr || ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  return alg::host_zlu(a, nrows, ncols, ipiv, nullptr);
+}
+
+// complex.rs:279 zgesv(a, b)
+extern "C" int alg_zgesv(double* a, double* b, size_t n) {
+  if (n == 0) return ALG_OK;
+  if (a == nullptr || b == nullptr) return ALG_INVALID_ARGUMENT;
+  std::vector<size_t> ipiv(n);
+  return alg::host_zlu(a, n, n, ipiv.data(), b);
+}

@@ -5,9 +5,13 @@ Mirrors `algebra_linear::lapack` (src/lapack/mod.rs):
     dgetrf(a, n) -> (ipiv, det)            mod.rs:181-185
     dgetrf_rect(a, nrows, ncols, ipiv)     mod.rs:202-238
     dgesv(a, b)                            mod.rs:309-323
+    zgetrf(a, n) -> ipiv                   complex.rs:67-124
+    zgetrf_rect(a, nrows, ncols, ipiv)     complex.rs:169-208
+    zgesv(a, b)                            complex.rs:279-312
 
-`a` and `b` are 1-D float64 numpy arrays holding column-major data
-(`a[i + j*n]`), modified in place exactly as the Rust slices are. Errors are
+`a` and `b` are 1-D float64 (complex128 for the z functions) numpy arrays
+holding column-major data (`a[i + j*n]`), modified in place exactly as the
+Rust slices are. Errors are
 raised as LapackError with the reference's variant name. The arithmetic runs
 on the GPU through libalgebra_linear_gpu.so; nothing here computes on the CPU.
 """
@@ -100,6 +104,49 @@ def dgesv(a: np.ndarray, b: np.ndarray) -> None:
     if n == 0:
         return
     _check(_lib.load().alg_dgesv(_lib.ptr(a), _lib.ptr(b), n))
+
+
+def _c128(a, name: str) -> np.ndarray:
+    if not isinstance(a, np.ndarray) or a.dtype != np.complex128 or a.ndim != 1 or not a.flags.c_contiguous:
+        raise TypeError(f"{name} must be a contiguous 1-D complex128 numpy array")
+    return a
+
+
+def zgetrf(a: np.ndarray, n: int):
+    """Complex LU with partial pivoting in place; returns ipiv (complex.rs:67)."""
+    _c128(a, "a")
+    if a.size != n * n:
+        raise LapackError("BadShape", _lib.BAD_SHAPE)
+    if n == 0:
+        return []
+    ipiv = np.zeros(n, dtype=np.uint64)
+    _check(_lib.load().alg_zgetrf(_lib.ptr(a), n, _lib.ptr(ipiv)))
+    return [int(v) for v in ipiv]
+
+
+def zgetrf_rect(a: np.ndarray, nrows: int, ncols: int, ipiv) -> None:
+    """Complex LU of an nrows x ncols panel, ipiv filled in place (complex.rs:169)."""
+    _c128(a, "a")
+    if nrows < ncols or a.size != nrows * ncols or len(ipiv) != ncols:
+        raise LapackError("BadShape", _lib.BAD_SHAPE)
+    if ncols == 0:
+        return
+    buf = np.zeros(ncols, dtype=np.uint64)
+    _check(_lib.load().alg_zgetrf_rect(_lib.ptr(a), nrows, ncols, _lib.ptr(buf)))
+    for k in range(ncols):
+        ipiv[k] = int(buf[k])
+
+
+def zgesv(a: np.ndarray, b: np.ndarray) -> None:
+    """Solves A x = b for one complex right-hand side; n = len(b) (complex.rs:279)."""
+    _c128(a, "a")
+    _c128(b, "b")
+    n = b.size
+    if a.size != n * n:
+        raise LapackError("BadShape", _lib.BAD_SHAPE)
+    if n == 0:
+        return
+    _check(_lib.load().alg_zgesv(_lib.ptr(a), _lib.ptr(b), n))
 
 
 def dgesv_nrhs(a: np.ndarray, b: np.ndarray, n: int, nrhs: int, update: int = _lib.UPDATE_EXACT):

@@ -98,6 +98,33 @@ int alg_dgesv(double* a, double* b, size_t n);
  * ALG_BAD_SHAPE when an ipiv entry is out of range. */
 int alg_dgetri(double* lu, size_t n, const size_t* ipiv);
 
+/* ---- complex twins (src/lapack/complex.rs) ------------------------------
+ * A complex entry is an interleaved (re, im) pair of doubles, the layout of
+ * the reference's Complex64 (num_complex::Complex<f64>), of C99 double
+ * complex and of numpy complex128; matrices are column-major, so an n x n
+ * matrix is 2 n^2 doubles. Results are bit-identical to the reference: the
+ * same |Re| + |Im| pivots and the num-complex 0.4 operator formulas with every
+ * product, sum and quotient rounded on its own. */
+
+/* Replaces `pub fn zgetrf(a: &mut [Complex64], n: usize)
+ *   -> Result<Vec<usize>, LapackError>` (src/lapack/complex.rs:67-124): a is
+ * factored in place (unit-lower L below the diagonal, U on and above it);
+ * ipiv (n entries, 0-based: rows k and ipiv[k] swapped at step k). On
+ * ALG_SINGULAR, a holds the reference's partial state and ipiv is not
+ * written. */
+int alg_zgetrf(double* a, size_t n, size_t* ipiv);
+
+/* Replaces `pub fn zgetrf_rect(a: &mut [Complex64], nrows: usize, ncols:
+ *   usize, ipiv: &mut [usize]) -> Result<(), LapackError>`
+ * (src/lapack/complex.rs:169-208): the nrows x ncols panel (nrows >= ncols,
+ * else ALG_BAD_SHAPE) factored in place, ipiv ncols entries. */
+int alg_zgetrf_rect(double* a, size_t nrows, size_t ncols, size_t* ipiv);
+
+/* Replaces `pub fn zgesv(a: &mut [Complex64], b: &mut [Complex64])
+ *   -> Result<(), LapackError>` (src/lapack/complex.rs:279-312): a (2 n^2
+ * doubles) is left holding its LU factors, b (2 n doubles) holds x. */
+int alg_zgesv(double* a, double* b, size_t n);
+
 /* dgesv with nrhs right-hand sides, b n x nrhs column-major: the reference's
  * dgetrf followed by its dgetrs (src/lapack/mod.rs:330-354) per column. */
 int alg_dgesv_nrhs(double* a, double* b, size_t n, size_t nrhs);

@@ -97,3 +97,28 @@ def test_dense_shape_errors_match_the_reference():
         dgetri(np.zeros(3), 2, [0, 1])
     assert e.value.kind == "BadShape"
     dgetri(np.zeros(0), 0, [])
+
+
+def test_complex_shape_errors_match_the_reference():
+    # complex.rs:518-529, 582-590, 640-645: lengths checked before any work,
+    # n = 0 succeeds; the C ABI rejects nrows < ncols without touching a GPU
+    from algebra_linear_b200 import _lib
+    from algebra_linear_b200.lapack import LapackError, zgesv, zgetrf, zgetrf_rect
+
+    with pytest.raises(LapackError) as e:
+        zgetrf(np.ones(3, dtype=np.complex128), 2)
+    assert e.value.kind == "BadShape"
+    with pytest.raises(LapackError) as e:
+        zgesv(np.ones(3, dtype=np.complex128), np.ones(2, dtype=np.complex128))
+    assert e.value.kind == "BadShape"
+    with pytest.raises(LapackError) as e:
+        zgetrf_rect(np.ones(4, dtype=np.complex128), 1, 2, [0, 0])
+    assert e.value.kind == "BadShape"
+    with pytest.raises(TypeError):
+        zgetrf(np.ones(4), 2)  # float64 is not a complex matrix
+    assert zgetrf(np.zeros(0, dtype=np.complex128), 0) == []
+    zgesv(np.zeros(0, dtype=np.complex128), np.zeros(0, dtype=np.complex128))
+    lib = _lib.load()
+    assert lib.alg_zgetrf_rect(None, 1, 2, None) == _lib.BAD_SHAPE
+    assert lib.alg_zgetrf(None, 0, None) == _lib.OK
+    assert lib.alg_zgesv(None, None, 0) == _lib.OK
