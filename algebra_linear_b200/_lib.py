@@ -57,6 +57,7 @@ SIGNATURES = [
     ("alg_zgetrf", _I, [_P, _SZ, _P]),
     ("alg_zgetrf_rect", _I, [_P, _SZ, _SZ, _P]),
     ("alg_zgesv", _I, [_P, _P, _SZ]),
+    ("alg_zgetri", _I, [_P, _SZ, _P]),
     ("alg_dgesv_nrhs", _I, [_P, _P, _SZ, _SZ]),
     ("alg_dgesv_ex", _I, [_I, _P, _P, _SZ, _SZ, _P]),
     ("alg_ctx_create", _I, [_P, C.POINTER(_P)]),

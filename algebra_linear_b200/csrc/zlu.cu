@@ -1,5 +1,5 @@
-// Complex twins of the dense LU (src/lapack/complex.rs): zgetrf, zgetrf_rect
-// and zgesv on the GPU, bit-identical to the reference.
+// Complex twins of the dense LU (src/lapack/complex.rs): zgetrf, zgetrf_rect,
+// zgesv and zgetri on the GPU, bit-identical to the reference.
 //
 // The reference's Complex64 is num_complex::Complex<f64> (num-complex 0.4),
 // whose operators are
@@ -55,6 +55,9 @@ __device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
   const double re = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
   const double im = __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y));
   return make_double2(__ddiv_rn(re, norm_sqr), __ddiv_rn(im, norm_sqr));
+}
+__device__ __forceinline__ double2 zadd(double2 a, double2 b) {
+  return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
 }
 __device__ __forceinline__ double zabs1(double2 z) { return __dadd_rn(fabs(z.x), fabs(z.y)); }
 
@@ -204,6 +207,75 @@ __global__ void __launch_bounds__(kSolveThreads) zbackward_kernel(const double2*
   }
 }
 
+// zgetri (complex.rs:130-158 ztrti2 'Upper' 'Non-unit', then 217-271), in
+// three parts. U is inverted in place in one CTA, column after column: the
+// diagonal becomes 1/u_jj, and row i < j of the column becomes
+// -(1/u_jj) * (sum over k = i..j-1 of a_ik a_kj, summed from zero in
+// increasing k) with a_ik already inverted; x holds the sums so that no
+// entry of the column is overwritten before every row has read it. A zero
+// u_jj stops with the columns before it inverted, as in the reference.
+__global__ void __launch_bounds__(kSolveThreads) ztrti2_kernel(double2* __restrict__ a, int lda, int n,
+                                                              double2* __restrict__ x, DevStatus* st) {
+  const int t = threadIdx.x;
+  for (int j = 0; j < n; ++j) {
+    const double2 ujj = a[j + (size_t)j * lda];  // columns before j never write it
+    if (ujj.x == 0.0 && ujj.y == 0.0) {
+      if (t == 0) atomicMin(&st->singular_col, j);
+      return;
+    }
+    const double2 inv = zdiv(make_double2(1.0, 0.0), ujj);
+    const double2 ajj = make_double2(-inv.x, -inv.y);
+    for (int i = t; i < j; i += kSolveThreads) {
+      double2 sum = make_double2(0.0, 0.0);
+      for (int k = i; k < j; ++k) sum = zadd(sum, zmul(a[i + (size_t)k * lda], a[k + (size_t)j * lda]));
+      x[i] = sum;
+    }
+    __syncthreads();  // every row has read column j
+    if (t == 0) a[j + (size_t)j * lda] = inv;
+    for (int i = t; i < j; i += kSolveThreads) a[i + (size_t)j * lda] = zmul(ajj, x[i]);
+    __syncthreads();  // column j is final before column j + 1 reads it
+  }
+}
+
+// Column j of inv(A) L = inv(U) (columns right of j already final): the L
+// entries below the diagonal move to work and become zero ...
+__global__ void __launch_bounds__(256) zgetri_work_kernel(double2* __restrict__ a, int lda, int n, int j,
+                                                          double2* __restrict__ work) {
+  for (int i = j + 1 + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2* e = a + i + (size_t)j * lda;
+    work[i] = *e;
+    *e = make_double2(0.0, 0.0);
+  }
+}
+
+// ... then a_ij -= sum over k > j of a_ik work_k (from zero, increasing k), a
+// thread per row.
+__global__ void __launch_bounds__(256) zgetri_col_kernel(double2* __restrict__ a, int lda, int n, int j,
+                                                         const double2* __restrict__ work) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double2 sum = make_double2(0.0, 0.0);
+  for (int k = j + 1; k < n; ++k) sum = zadd(sum, zmul(a[i + (size_t)k * lda], work[k]));
+  double2* e = a + i + (size_t)j * lda;
+  *e = zsub(*e, sum);
+}
+
+// The interchanges undone as column swaps, from the second-to-last pivot
+// down; a thread per row.
+__global__ void __launch_bounds__(256) zgetri_swap_kernel(double2* __restrict__ a, int lda, int n,
+                                                          const int* __restrict__ ipiv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = n - 2; j >= 0; --j) {
+    const int jp = ipiv[j];
+    if (jp != j) {
+      const double2 v = a[i + (size_t)j * lda];
+      a[i + (size_t)j * lda] = a[i + (size_t)jp * lda];
+      a[i + (size_t)jp * lda] = v;
+    }
+  }
+}
+
 // Factorization of the m x nc device matrix (m >= nc), stream-ordered; a zero
 // pivot lands in the status block's singular_col.
 int zlu_factor_dev(alg_ctx* ctx, double2* d_a, int m, int nc, int lda, int* d_ipiv) {
@@ -272,8 +344,58 @@ int host_zlu(double* a, size_t m, size_t nc, size_t* ipiv, double* b) {
   return ALG_OK;
 }
 
+// Host drop-in core of zgetri: the factors copied in, inverted, copied back
+// (also on ALG_SINGULAR, with the reference's partial state).
+int host_zgetri(double* lu, size_t n, const size_t* ipiv) {
+  if (!zsize_ok(n)) return ALG_BAD_SHAPE;
+  std::vector<int> h_ipiv(n);
+  for (size_t k = 0; k < n; ++k) {
+    if (ipiv[k] >= n) return ALG_BAD_SHAPE;
+    h_ipiv[k] = (int)ipiv[k];
+  }
+  ZCtxLock L;
+  if (L.rc != ALG_OK) return L.rc;
+  alg_ctx* ctx = L.ctx;
+  const int N = (int)n;
+  const size_t abytes = 2 * sizeof(double) * n * n;
+  double2* d_a = nullptr;
+  double2* d_x = nullptr;
+  int* d_ipiv = nullptr;
+  ALG_TRY(ws_get(ctx, WS_A, abytes, reinterpret_cast<void**>(&d_a)));
+  ALG_TRY(ws_get(ctx, WS_X, 2 * sizeof(double) * n, reinterpret_cast<void**>(&d_x)));
+  ALG_TRY(ws_get(ctx, WS_IPIV, sizeof(int) * n, reinterpret_cast<void**>(&d_ipiv)));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_a, lu, abytes, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_CUDA_TRY(cudaMemcpyAsync(d_ipiv, h_ipiv.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
+  ALG_TRY(status_reset(ctx));
+  ztrti2_kernel<<<1, kSolveThreads, 0, ctx->stream>>>(d_a, N, N, d_x, ctx->d_status);
+  count_launches();
+  ALG_TRY(status_fetch(ctx));
+  const bool singular = ctx->h_status->singular_col != INT_MAX;
+  if (!singular) {
+    const int grid = (N + 255) / 256;
+    for (int j = N - 2; j >= 0; --j) {
+      zgetri_work_kernel<<<std::max(1, (N - j - 1 + 255) / 256), 256, 0, ctx->stream>>>(d_a, N, N, j, d_x);
+      zgetri_col_kernel<<<grid, 256, 0, ctx->stream>>>(d_a, N, N, j, d_x);
+      count_launches(2);
+    }
+    zgetri_swap_kernel<<<grid, 256, 0, ctx->stream>>>(d_a, N, N, d_ipiv);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  ALG_CUDA_TRY(cudaMemcpyAsync(lu, d_a, abytes, cudaMemcpyDeviceToHost, ctx->stream));
+  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return singular ? ALG_SINGULAR : ALG_OK;
+}
+
 }  // namespace
 }  // namespace alg
+
+// complex.rs:217 zgetri(lu, n, ipiv)
+extern "C" int alg_zgetri(double* lu, size_t n, const size_t* ipiv) {
+  if (n == 0) return ALG_OK;
+  if (lu == nullptr || ipiv == nullptr) return ALG_INVALID_ARGUMENT;
+  return alg::host_zgetri(lu, n, ipiv);
+}
 
 // complex.rs:67 zgetrf(a, n) -> ipiv
 extern "C" int alg_zgetrf(double* a, size_t n, size_t* ipiv) {

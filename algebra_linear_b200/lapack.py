@@ -8,6 +8,7 @@ Mirrors `algebra_linear::lapack` (src/lapack/mod.rs):
     zgetrf(a, n) -> ipiv                   complex.rs:67-124
     zgetrf_rect(a, nrows, ncols, ipiv)     complex.rs:169-208
     zgesv(a, b)                            complex.rs:279-312
+    zgetri(lu, n, ipiv)                    complex.rs:217-271
 
 `a` and `b` are 1-D float64 (complex128 for the z functions) numpy arrays
 holding column-major data (`a[i + j*n]`), modified in place exactly as the
@@ -147,6 +148,17 @@ def zgesv(a: np.ndarray, b: np.ndarray) -> None:
     if n == 0:
         return
     _check(_lib.load().alg_zgesv(_lib.ptr(a), _lib.ptr(b), n))
+
+
+def zgetri(lu: np.ndarray, n: int, ipiv) -> None:
+    """Complex inverse from zgetrf's factors, in place (complex.rs:217)."""
+    _c128(lu, "lu")
+    if lu.size != n * n or len(ipiv) != n:
+        raise LapackError("BadShape", _lib.BAD_SHAPE)
+    if n == 0:
+        return
+    iv = np.ascontiguousarray(ipiv, dtype=np.uint64)
+    _check(_lib.load().alg_zgetri(_lib.ptr(lu), n, _lib.ptr(iv)))
 
 
 def dgesv_nrhs(a: np.ndarray, b: np.ndarray, n: int, nrhs: int, update: int = _lib.UPDATE_EXACT):

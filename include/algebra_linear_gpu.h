@@ -125,6 +125,15 @@ int alg_zgetrf_rect(double* a, size_t nrows, size_t ncols, size_t* ipiv);
  * doubles) is left holding its LU factors, b (2 n doubles) holds x. */
 int alg_zgesv(double* a, double* b, size_t n);
 
+/* Replaces `pub fn zgetri(lu: &mut [Complex64], n: usize, ipiv: &[usize])
+ *   -> Result<(), LapackError>` (src/lapack/complex.rs:217-271): lu (the
+ * factors and pivots from alg_zgetrf) becomes the inverse (U inverted in
+ * place, inv(A) L = inv(U) solved from the last column down, the
+ * interchanges undone as column swaps). ALG_SINGULAR on a zero u_jj, with the
+ * columns before j already inverted as the reference leaves them;
+ * ALG_BAD_SHAPE when an ipiv entry is out of range. */
+int alg_zgetri(double* lu, size_t n, const size_t* ipiv);
+
 /* dgesv with nrhs right-hand sides, b n x nrhs column-major: the reference's
  * dgetrf followed by its dgetrs (src/lapack/mod.rs:330-354) per column. */
 int alg_dgesv_nrhs(double* a, double* b, size_t n, size_t nrhs);

@@ -1,5 +1,5 @@
 """ORACLE — test infrastructure only: ctypes wrapper of oracle_complex.cpp,
-the C++ restatement of src/lapack/complex.rs (zgetrf, zgetrf_rect, zgesv) with
+the C++ restatement of src/lapack/complex.rs (zgetrf, zgetrf_rect, zgesv, zgetri) with
 num-complex 0.4's operator formulas. Matrices are numpy complex128,
 column-major (`a[i + j * n]`), as the reference stores them.
 """
@@ -25,6 +25,7 @@ def _lib() -> C.CDLL:
         lib.oracle_zgetrf.argtypes = [P, SZ, P]
         lib.oracle_zgetrf_rect.argtypes = [P, SZ, SZ, P]
         lib.oracle_zgesv.argtypes = [P, P, SZ, P]
+        lib.oracle_zgetri.argtypes = [P, SZ, P]
         _bound = True
     return lib
 
@@ -65,6 +66,16 @@ def zgesv(a, b):
     ipiv = np.zeros(max(n, 1), dtype=np.uintp)
     rc = _lib().oracle_zgesv(lu.ctypes.data, x.ctypes.data, n, ipiv.ctypes.data)
     return rc, lu, x, ipiv[:n]
+
+
+def zgetri(lu, n: int, ipiv):
+    """complex.rs:217-271 on a copy of the factors; returns (status, inverse)."""
+    inv = _cm(lu)
+    iv = np.ascontiguousarray(ipiv, dtype=np.uintp)
+    if inv.size != n * n or iv.size != n:
+        return BAD_SHAPE, inv
+    rc = _lib().oracle_zgetri(inv.ctypes.data, n, iv.ctypes.data if n else None)
+    return rc, inv
 
 
 def complex_sample(n: int) -> np.ndarray:

@@ -1,6 +1,6 @@
 // ORACLE — test infrastructure only. Not part of the product.
 //
-// A CPU restatement of the reference crate's complex dense LU
+// A CPU restatement of the reference crate's complex dense LU and inverse
 // (cpmech/algebra_linear 4.0.0, src/lapack/complex.rs), used only by tests/
 // as the checker of the GPU complex path. Built by oracle/Makefile with
 // -ffp-contract=off -fno-fast-math (rustc's release codegen: every product,
@@ -23,6 +23,7 @@
 
 #include <cmath>
 #include <cstddef>
+#include <vector>
 
 namespace {
 
@@ -39,6 +40,7 @@ inline cplx cdiv(cplx a, cplx b) {
 }
 inline cplx csub(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
 inline double abs1(cplx z) { return std::fabs(z.re) + std::fabs(z.im); }
+inline cplx cadd(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
 
 }  // namespace
 
@@ -137,6 +139,55 @@ int oracle_zgesv(cplx* a, cplx* b, size_t n, size_t* ipiv) {
     cplx sum = b[ii];
     for (size_t j = ii + 1; j < n; ++j) sum = csub(sum, cmul(a[ii + j * n], b[j]));
     b[ii] = cdiv(sum, a[ii + ii * n]);
+  }
+  return OZ_OK;
+}
+
+// complex.rs:130-158 (ztrti2 'Upper', 'Non-unit') and 217-271 (zgetri): U
+// inverted in place column by column (the diagonal replaced by its
+// reciprocal, the column above it by -inv * (sum over k of a_ik a_kj, k in
+// increasing order, from zero)); then, from the last column down, the
+// column's L part moved to a work vector and zeroed and the column reduced by
+// sum_k a_ik work_k (k increasing, from zero); then the interchanges undone as
+// column swaps from the second-to-last pivot down. A zero u_jj returns
+// OZ_SINGULAR with the columns before j already inverted.
+int oracle_zgetri(cplx* a, size_t n, const size_t* ipiv) {
+  for (size_t j = 0; j < n; ++j) {
+    if (a[j + j * n].re == 0.0 && a[j + j * n].im == 0.0) return OZ_SINGULAR;
+    const cplx inv = cdiv(cplx{1.0, 0.0}, a[j + j * n]);
+    a[j + j * n] = inv;
+    const cplx ajj{-inv.re, -inv.im};
+    std::vector<cplx> x(j);
+    for (size_t i = 0; i < j; ++i) {
+      cplx sum{0.0, 0.0};
+      for (size_t k = i; k < j; ++k) sum = cadd(sum, cmul(a[i + k * n], a[k + j * n]));
+      x[i] = sum;
+    }
+    for (size_t i = 0; i < j; ++i) a[i + j * n] = cmul(ajj, x[i]);
+  }
+  std::vector<cplx> work(n), y(n);
+  for (size_t j = n; j-- > 0;) {
+    for (size_t i = j + 1; i < n; ++i) {
+      work[i] = a[i + j * n];
+      a[i + j * n] = cplx{0.0, 0.0};
+    }
+    if (j + 1 < n) {
+      for (size_t i = 0; i < n; ++i) {
+        cplx sum{0.0, 0.0};
+        for (size_t k = j + 1; k < n; ++k) sum = cadd(sum, cmul(a[i + k * n], work[k]));
+        y[i] = sum;
+      }
+      for (size_t i = 0; i < n; ++i) a[i + j * n] = csub(a[i + j * n], y[i]);
+    }
+  }
+  for (size_t j = n > 0 ? n - 1 : 0; j-- > 0;) {
+    const size_t jp = ipiv[j];
+    if (jp != j)
+      for (size_t i = 0; i < n; ++i) {
+        const cplx t = a[i + j * n];
+        a[i + j * n] = a[i + jp * n];
+        a[i + jp * n] = t;
+      }
   }
   return OZ_OK;
 }

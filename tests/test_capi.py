@@ -122,3 +122,10 @@ def test_complex_shape_errors_match_the_reference():
     assert lib.alg_zgetrf_rect(None, 1, 2, None) == _lib.BAD_SHAPE
     assert lib.alg_zgetrf(None, 0, None) == _lib.OK
     assert lib.alg_zgesv(None, None, 0) == _lib.OK
+    from algebra_linear_b200.lapack import zgetri
+
+    with pytest.raises(LapackError) as e:
+        zgetri(np.zeros(4, dtype=np.complex128), 2, [0])
+    assert e.value.kind == "BadShape"
+    zgetri(np.zeros(0, dtype=np.complex128), 0, [])
+    assert lib.alg_zgetri(None, 0, None) == _lib.OK

@@ -1,5 +1,5 @@
 """GPU parity of the complex twins (src/lapack/complex.rs: zgetrf,
-zgetrf_rect, zgesv) against the complex oracle: identical pivots and
+zgetrf_rect, zgesv, zgetri) against the complex oracle: identical pivots and
 bit-identical factors and solutions (both run the reference's operations in
 the reference's order), on the reference's own test matrices, on sizes whose
 rows and columns exceed one CTA's threads, on pivot ties, on NaN entries, and
@@ -8,7 +8,7 @@ on the partial state a zero pivot leaves."""
 import numpy as np
 import pytest
 
-from algebra_linear_b200.lapack import LapackError, zgesv, zgetrf, zgetrf_rect
+from algebra_linear_b200.lapack import LapackError, zgesv, zgetrf, zgetri, zgetrf_rect
 
 pytestmark = pytest.mark.gpu
 
@@ -127,3 +127,31 @@ def test_zero_pivot_leaves_the_reference_partial_state(gpu, oz):
     M[:, 2] = M[:, 0] + M[:, 1]
     M[2:, 3:] = rng.standard_normal((3, 2)) + 1j * rng.standard_normal((3, 2))
     assert _agrees(oz, M.T.ravel().copy(), n) == oz.SINGULAR
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 8, 100, 1030])
+def test_zgetri_is_bit_identical(gpu, oz, n):
+    # complex.rs:463-486 / parity.rs:463-510: zgetrf then zgetri
+    a0 = oz.general3() if n == 3 else (oz.complex_sample(n) if n <= 8 else _rand(n * n, 5 * n))
+    rc, lu_ref, ipiv_ref = oz.zgetrf(a0, n)
+    rc, inv_ref = oz.zgetri(lu_ref, n, ipiv_ref)
+    assert rc == oz.OK
+    lu = lu_ref.copy()
+    zgetri(lu, n, [int(v) for v in ipiv_ref])
+    assert _same(lu, inv_ref)
+    if n == 3:
+        back = a0.reshape(3, 3).T @ lu.reshape(3, 3).T
+        assert np.all(np.abs(back - np.eye(3)) < 1e-12)
+
+
+def test_zgetri_zero_diagonal_leaves_the_partial_inverse(gpu, oz):
+    n = 4
+    lu0 = _rand(n * n, 9)
+    lu0[2 + 2 * n] = 0j  # u_22 = 0: columns 0-1 inverted, then Singular
+    rc, inv_ref = oz.zgetri(lu0, n, [0, 1, 2, 3])
+    assert rc == oz.SINGULAR
+    lu = lu0.copy()
+    with pytest.raises(LapackError) as e:
+        zgetri(lu, n, [0, 1, 2, 3])
+    assert e.value.kind == "Singular"
+    assert _same(lu, inv_ref)

@@ -93,3 +93,33 @@ def test_pivots_and_factors_agree_with_lapack(n):
     lu_ref, piv_ref = sl.lu_factor(A)
     assert np.array_equal(ipiv.astype(np.int64), piv_ref.astype(np.int64))
     np.testing.assert_allclose(lu.reshape(n, n).T, lu_ref, rtol=0, atol=1e-12 * n)
+
+
+def test_zgetrf_then_zgetri_inverts():
+    # complex.rs:463-486: A * inv(A) = I to 1e-12
+    a = oz.general3()
+    rc, lu, ipiv = oz.zgetrf(a, 3)
+    rc, inv = oz.zgetri(lu, 3, ipiv)
+    assert rc == oz.OK
+    back = a.reshape(3, 3).T @ inv.reshape(3, 3).T
+    assert np.all(np.abs(back - np.eye(3)) < 1e-12)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8])
+def test_complex_inverse_agrees_with_lapack(n):
+    # parity.rs:463-510 compares with the reference LAPACK at TOL 1e-10 (relative to max(|want|, 1))
+    a = oz.complex_sample(n)
+    rc, lu, ipiv = oz.zgetrf(a, n)
+    rc, inv = oz.zgetri(lu, n, ipiv)
+    assert rc == oz.OK
+    want = np.linalg.inv(a.reshape(n, n).T)
+    got = inv.reshape(n, n).T
+    assert np.all(np.abs(got - want) / np.maximum(np.abs(want), 1.0) < 1e-10)
+
+
+def test_zgetri_zero_diagonal_is_singular():
+    # ztrti2's test (complex.rs:134-137): an exactly zero u_jj
+    lu = np.array([2 + 0j, 0.5 + 0j, 1 + 1j, 0j])  # u_11 = 0
+    rc, inv = oz.zgetri(lu, 2, [0, 1])
+    assert rc == oz.SINGULAR
+    assert inv[0] == 0.5  # column 0 already inverted: 1 / 2
