@@ -380,6 +380,42 @@ def e2e_run(form, A0, b0, n, nrhs, steps):
             "api": "alg_dgesv_ex" if not form.startswith("mixed") else "alg_dgesv_mixed"}
 
 
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+class _OneCore:
+    """Pins the calling thread to one of its allowed cores while the CPU path
+    is timed (the reference is single-threaded) and restores the affinity."""
+
+    def __enter__(self):
+        self.old, self.core = None, None
+        try:
+            self.old = os.sched_getaffinity(0)
+            self.core = max(self.old)
+            os.sched_setaffinity(0, {self.core})
+        except (AttributeError, OSError):
+            self.old = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.old is not None:
+            os.sched_setaffinity(0, self.old)
+        return False
+
+    def info(self) -> dict:
+        return {"cpu_model": _cpu_model(), "pinned_core": self.core}
+
+
 def cpu_baseline(n_cpu: int, reps: int = 3):
     """The oracle (C++ restatement of lapack::dgesv, mod.rs:309-354) on one
     host core, dgesv at order n_cpu, median of reps."""
@@ -387,16 +423,17 @@ def cpu_baseline(n_cpu: int, reps: int = 3):
 
     a, _, b = oracle.c1_system(n_cpu)
     ts = []
-    for _ in range(reps):
-        aw, bw = a.copy(), b.copy()
-        t0 = time.perf_counter()
-        rc, _ = oracle.dgesv(aw, bw, n_cpu)
-        ts.append(time.perf_counter() - t0)
-        assert rc == 0
+    with _OneCore() as pin:
+        for _ in range(reps):
+            aw, bw = a.copy(), b.copy()
+            t0 = time.perf_counter()
+            rc, _ = oracle.dgesv(aw, bw, n_cpu)
+            ts.append(time.perf_counter() - t0)
+            assert rc == 0
     t = statistics.median(ts)
     return {"value": flops_dgesv(n_cpu, 1) / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
             "sample": f"dgesv n={n_cpu}, 1 RHS, same larnv workload, median of {reps} "
-                      f"({t:.2f} s each); the reference path is single-threaded"}
+                      f"({t:.2f} s each); the reference path is single-threaded", **pin.info()}
 
 
 
@@ -440,13 +477,15 @@ def sparse_cpu_baseline(side: int):
     cp, ri, kind = grid_csc(side, side, side)
     v, _ = osp.convection_diffusion_values(kind, SEEDY)
     sym = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
-    t0 = time.perf_counter()
-    f = osp.Factors(len(cp) - 1, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], sym["supernode_ptr"])
-    f.solve(np.ones(len(cp) - 1))
-    t = time.perf_counter() - t0
+    with _OneCore() as pin:
+        t0 = time.perf_counter()
+        f = osp.Factors(len(cp) - 1, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], sym["supernode_ptr"])
+        f.solve(np.ones(len(cp) - 1))
+        t = time.perf_counter() - t0
     fl = 2.0 * f.flops_estimate() + 2.0 * (f.nnz_l + f.nnz_u)
     return {"value": fl / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
-            "sample": f"one factorize+solve of the {side}^3 grid ({t:.1f} s); the reference path is single-threaded"}
+            "sample": f"one factorize+solve of the {side}^3 grid ({t:.1f} s); the reference path is single-threaded",
+            **pin.info()}
 
 
 def run_sparse(args, world, rank, local, pg):
@@ -685,12 +724,13 @@ def run_reference(args, world, rank, pg):
 
     n_cpu = args.cpu_n
     a, _, b = oracle.c1_system(n_cpu)
-    for _ in range(args.warmup):
-        oracle.dgesv(a.copy(), b.copy(), n_cpu)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        oracle.dgesv(a.copy(), b.copy(), n_cpu)
-    dt = (time.perf_counter() - t0) / args.steps
+    with _OneCore() as pin:
+        for _ in range(args.warmup):
+            oracle.dgesv(a.copy(), b.copy(), n_cpu)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            oracle.dgesv(a.copy(), b.copy(), n_cpu)
+        dt = (time.perf_counter() - t0) / args.steps
     v = flops_dgesv(n_cpu, 1) / dt / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
@@ -701,7 +741,8 @@ def run_reference(args, world, rank, pg):
                    "n": n_cpu, "nrhs": 1, "parallelism": "1 host core"},
         "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": 1, "kind": "port",
                          "sample": f"one dgesv of order {n_cpu} per step (the reference is single-threaded; "
-                                   "its Rust crate cannot be built here, so the oracle's C++ restatement runs)"},
+                                   "its Rust crate cannot be built here, so the oracle's C++ restatement runs)",
+                         **pin.info()},
         "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
