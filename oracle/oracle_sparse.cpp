@@ -1,6 +1,7 @@
 // TEST INFRASTRUCTURE ONLY. A CPU restatement of the reference's numeric
-// supernodal sparse LU and its solve, used by the tests and the bench's CPU
-// baseline to check the GPU path; nothing in the product links or calls it.
+// supernodal sparse LU, its simplicial LU and their solve, used by the tests
+// and the bench's CPU baseline to check the GPU path; nothing in the product
+// links or calls it.
 //
 // Follows src/sparse/faer/supernodal_lu.rs (factorize :145-480, lu_front
 // :490-533, solve :118-133) and src/sparse/faer/lu.rs (unit_lower_solve
@@ -323,5 +324,113 @@ void oracle_splu_solve(const void* h, double* b) {
 }
 
 void oracle_splu_free(void* h) { delete static_cast<Factors*>(h); }
+
+// The simplicial path, lu.rs:209-327 (SymbolicLu::factorize) with
+// l_incomplete_solve_sparse, reach and depth_first_search (:349-436), over
+// the same column order: for the j-th column, the rows reachable from A's
+// column through the L columns stored so far, in the depth-first search's
+// finishing order (each search from A's rows in stored order, children in
+// stored L order); x = L \ a over that reach; U takes x of the reach's
+// pivoted rows at their positions, then the pivot; the pivot is the first
+// unpivoted row of the reach with the largest |x| (a NaN, which compares as
+// unordered, takes it); L takes 1 for the pivot row, then x_i * (1 / x_piv)
+// for every other unpivoted row of the reach, zeros included. L's rows
+// become positions at the end; no sorting (L's pivot first, U's diagonal
+// last, as the sweeps expect). Same status codes as oracle_splu_factorize.
+int oracle_simplicial_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val,
+                                const size_t* col_perm, const size_t* col_perm_inv, void** out) {
+  *out = nullptr;
+  for (size_t q = 0; q < cp[n]; ++q)
+    if (!std::isfinite(val[q])) return 107;
+  auto* f = new Factors;
+  f->n = n;
+  f->lp.assign(n + 1, 0);
+  f->up.assign(n + 1, 0);
+  std::vector<double> x(n, 0.0);
+  std::vector<size_t> marked(n, 0), reach(n), stack(n), rpi(n, n);
+  for (size_t j = 0; j < n; ++j) {
+    const size_t pj = col_perm[j], mark = j + 1;
+    // depth-first search from b over the L columns 0..j-1; the head of the
+    // path lives at reach[0..), finished rows are written down from `tail`
+    auto dfs = [&](size_t b0, size_t tail) -> size_t {
+      size_t head = 1;
+      reach[0] = b0;
+      while (head > 0) {
+        const size_t b = reach[head - 1];
+        const size_t pb = rpi[b];
+        const size_t lo = pb < j ? f->lp[pb] : 0, hi = pb < j ? f->lp[pb + 1] : 0;
+        if (marked[b] < mark) {
+          marked[b] = mark;
+          stack[head - 1] = lo;
+        }
+        bool pushed = false;
+        for (size_t ptr = stack[head - 1]; ptr < hi; ++ptr) {
+          const size_t i = f->li[ptr];
+          if (marked[i] == mark) continue;
+          stack[head - 1] = ptr;
+          reach[head] = i;
+          ++head;
+          pushed = true;
+          break;
+        }
+        if (pushed) continue;
+        --head;
+        reach[--tail] = b;
+      }
+      return tail;
+    };
+    size_t tail = n;
+    for (size_t q = cp[pj]; q < cp[pj + 1]; ++q)
+      if (marked[ri[q]] < mark) tail = dfs(ri[q], tail);
+    for (size_t q = cp[pj]; q < cp[pj + 1]; ++q) x[ri[q]] += val[q];
+    for (size_t t = tail; t < n; ++t) {
+      const size_t i = reach[t], pi = rpi[i];
+      if (pi >= j) continue;
+      const double xi = x[i];
+      for (size_t k = f->lp[pi] + 1; k < f->lp[pi + 1]; ++k) x[f->li[k]] -= f->lv[k] * xi;
+    }
+    size_t piv = n;
+    double pval = -1.0;
+    for (size_t t = tail; t < n; ++t) {
+      const size_t i = reach[t];
+      if (rpi[i] == n) {
+        const double v = std::fabs(x[i]);
+        if (std::isnan(v) || std::isnan(pval) || v > pval) {
+          piv = i;
+          pval = v;
+        }
+      } else {
+        f->ui.push_back(rpi[i]);
+        f->uv.push_back(x[i]);
+      }
+    }
+    if (piv == n || pval == 0.0) {
+      delete f;
+      return 104;
+    }
+    const double xp = x[piv], xp_inv = 1.0 / xp;
+    rpi[piv] = j;
+    f->ui.push_back(j);
+    f->uv.push_back(xp);
+    f->up[j + 1] = f->ui.size();
+    f->li.push_back(piv);
+    f->lv.push_back(1.0);
+    for (size_t t = tail; t < n; ++t) {
+      const size_t i = reach[t];
+      if (rpi[i] == n) {
+        f->li.push_back(i);
+        f->lv.push_back(x[i] * xp_inv);
+      }
+      x[i] = 0.0;
+    }
+    f->lp[j + 1] = f->li.size();
+  }
+  for (auto& r : f->li) r = rpi[r];
+  f->row_perm.assign(n, 0);
+  for (size_t i = 0; i < n; ++i) f->row_perm[rpi[i]] = i;
+  f->col_perm_inv.assign(col_perm_inv, col_perm_inv + n);
+  *out = f;
+  return 0;
+}
 
 }  // extern "C"

@@ -24,6 +24,7 @@ def _lib():
         lib.oracle_splu_get.argtypes = [P, P, P, P, P, P, P, P]
         lib.oracle_splu_solve.argtypes = [P, P]
         lib.oracle_splu_free.argtypes = [P]
+        lib.oracle_simplicial_factorize.argtypes = [SZ, P, P, P, P, P, C.POINTER(C.c_void_p)]
         lib._sparse_bound = True
     return lib
 
@@ -33,18 +34,24 @@ def _u(a) -> np.ndarray:
 
 
 class Factors:
-    """The reference's supernodal factors of one matrix (positions, CSC)."""
+    """The reference's supernodal factors of one matrix (positions, CSC);
+    with supernode_ptr None, its simplicial factors (lu.rs:209-327)."""
 
     def __init__(self, n, col_ptr, row_idx, values, col_perm, col_perm_inv, supernode_ptr):
         lib = _lib()
         self.n = int(n)
         cp, ri = _u(col_ptr), _u(row_idx)
         v = np.ascontiguousarray(values, dtype=np.float64)
-        cpm, cpi, snp = _u(col_perm), _u(col_perm_inv), _u(supernode_ptr)
+        cpm, cpi = _u(col_perm), _u(col_perm_inv)
+        snp = _u(supernode_ptr) if supernode_ptr is not None else None
         h = C.c_void_p()
-        self.status = lib.oracle_splu_factorize(self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data,
-                                                cpm.ctypes.data, cpi.ctypes.data, snp.ctypes.data,
-                                                len(snp) - 1, C.byref(h))
+        if supernode_ptr is None:  # the simplicial path
+            self.status = lib.oracle_simplicial_factorize(self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data,
+                                                          cpm.ctypes.data, cpi.ctypes.data, C.byref(h))
+        else:
+            self.status = lib.oracle_splu_factorize(self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data,
+                                                    cpm.ctypes.data, cpi.ctypes.data, snp.ctypes.data,
+                                                    len(snp) - 1, C.byref(h))
         self.h = h if self.status == 0 else None
         if self.h is None:
             return

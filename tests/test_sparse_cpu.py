@@ -240,3 +240,93 @@ def test_grid_values_follow_the_stencil(oracle_sparse):
     assert np.all(v[kind == 3] == -1.0)
     assert np.all((v[kind == 2] >= -1.0) & (v[kind == 2] <= -0.7))
     assert np.all((v[kind == 1] >= -1.3) & (v[kind == 1] <= -1.0))
+
+
+def _simplicial(osp, cp, ri, v):
+    sym = SparseLu.analyze(cp, ri, LuMethod.simplicial()).symbolic()
+    return osp.Factors(len(cp) - 1, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], None), sym
+
+
+def _csc_dense(cp, ri, v, n):
+    A = np.zeros((n, n))
+    for j in range(n):
+        A[ri[cp[j]:cp[j + 1]], j] = v[cp[j]:cp[j + 1]]
+    return A
+
+
+def _lu_dense(f):
+    n = f.n
+    L, U = np.zeros((n, n)), np.zeros((n, n))
+    for j in range(n):
+        for k in range(int(f.l_col_ptr[j]), int(f.l_col_ptr[j + 1])):
+            L[int(f.l_row_idx[k]), j] = f.l_val[k]
+        for k in range(int(f.u_col_ptr[j]), int(f.u_col_ptr[j + 1])):
+            U[int(f.u_row_idx[k]), j] = f.u_val[k]
+    return L, U
+
+
+def test_simplicial_oracle_pins(oracle_sparse):
+    # lu.rs:527-533: [4 1; 1 3] x = [1, 2]
+    f, _ = _simplicial(oracle_sparse, COL_PTR, ROW_IDX, VALUES)
+    assert f.status == 0
+    np.testing.assert_allclose(f.solve([1.0, 2.0]), [1 / 11, 7 / 11], rtol=0, atol=1e-14 * 2)
+    # lu.rs:536-557: P A Q = L U on the 4 x 4 fill pattern
+    cp, ri = [0, 2, 5, 8, 10], [0, 1, 0, 1, 2, 1, 2, 3, 0, 3]
+    v = np.array([4.0, 1.0, 1.0, 3.0, 1.0, 1.0, 5.0, 1.0, 1.0, 4.0])
+    f, sym = _simplicial(oracle_sparse, cp, ri, v)
+    L, U = _lu_dense(f)
+    A = _csc_dense(cp, ri, v, 4)
+    np.testing.assert_allclose(L @ U, A[f.row_perm.astype(int)][:, sym["col_perm"]], rtol=0, atol=1e-12 * 2)
+    # the pivot is stored first in each L column, the diagonal last in each U column
+    assert all(f.l_val[int(f.l_col_ptr[j])] == 1.0 for j in range(4))
+    assert all(int(f.u_row_idx[int(f.u_col_ptr[j + 1]) - 1]) == j for j in range(4))
+    # lu.rs:559-587: banded 8 x 8, x = i + 1/2
+    n = 8
+    cp, ri, v = [0], [], []
+    for j in range(n):
+        for i, a in ((j - 1, -1.0), (j, 4.0), (j + 1, -1.0)):
+            if 0 <= i < n:
+                ri.append(i)
+                v.append(a)
+        cp.append(len(ri))
+    f, _ = _simplicial(oracle_sparse, cp, ri, np.array(v))
+    x = np.arange(n) + 0.5
+    b = _csc_dense(cp, ri, np.array(v), n) @ x
+    np.testing.assert_allclose(f.solve(b), x, rtol=1e-12, atol=1e-12)
+    # lu.rs:589-625: diagonal, then an arrow (dense first row and column)
+    f, _ = _simplicial(oracle_sparse, list(range(6)), list(range(5)), np.array([2.0, 3.0, 4.0, 5.0, 6.0]))
+    np.testing.assert_allclose(f.solve([2.0, 6.0, 12.0, 20.0, 30.0]), [1, 2, 3, 4, 5], rtol=0, atol=1e-15 * 6)
+    n = 6
+    cp, ri, v = [0], [], []
+    for j in range(n):
+        col = [(i, 5.0 if i == 0 else 1.0) for i in range(n)] if j == 0 else [(0, 1.0), (j, 4.0)]
+        for i, a in col:
+            ri.append(i)
+            v.append(a)
+        cp.append(len(ri))
+    f, _ = _simplicial(oracle_sparse, cp, ri, np.array(v))
+    x = np.arange(1.0, n + 1)
+    np.testing.assert_allclose(f.solve(_csc_dense(cp, ri, np.array(v), n) @ x), x, rtol=1e-12, atol=1e-12)
+    # a structurally singular column
+    f, _ = _simplicial(oracle_sparse, COL_PTR, ROW_IDX, [1.0, 1.0, 1.0, 1.0])
+    assert f.status == 104
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8), (30, 30, 1)], ids=lambda d: "x".join(map(str, d)))
+def test_simplicial_and_supernodal_oracles_agree(oracle_sparse, dims):
+    """The two reference paths share the column order and, without ties, the
+    pivots; their solutions agree to rounding, and the simplicial factors keep
+    the exact zeros of each column's reach (at least as many entries)."""
+    cp, ri, kind = oracle_sparse.grid_pattern(*dims)
+    v, _ = oracle_sparse.convection_diffusion_values(kind, [4, 3, 2, 1])
+    n = len(cp) - 1
+    fs, sym = _simplicial(oracle_sparse, cp, ri, v)
+    sup = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
+    assert np.array_equal(sym["col_perm"], sup["col_perm"])
+    f = oracle_sparse.Factors(n, cp, ri, v, sup["col_perm"], sup["col_perm_inv"], sup["supernode_ptr"])
+    assert fs.status == 0 and f.status == 0
+    assert np.array_equal(fs.row_perm, f.row_perm)
+    b = np.linspace(-1.0, 2.0, n)
+    xs, x = fs.solve(b), f.solve(b)
+    assert np.max(np.abs(xs - x)) / np.max(np.abs(x)) <= 1e-12
+    assert fs.nnz_l >= f.nnz_l and fs.nnz_u >= f.nnz_u, (fs.nnz_l, f.nnz_l, fs.nnz_u, f.nnz_u)

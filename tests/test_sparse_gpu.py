@@ -178,3 +178,34 @@ def test_large_two_dimensional_grid_backward_error(gpu, osp, dims):
                           shape=(n, n))
         eta = np.max(np.abs(b - a @ x)) / (np.max(abs(a).sum(axis=1)) * np.max(np.abs(x)) + np.max(np.abs(b)))
         assert eta <= 1e-14, eta
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8), (30, 30, 1), (9, 8, 7)], ids=lambda d: "x".join(map(str, d)))
+def test_simplicial_request_matches_the_simplicial_oracle(gpu, osp, dims):
+    """A handle analyzed with LuMethod::Simplicial (lu.rs:209-327) is factored
+    by the GPU's multifrontal path: the same column order and, without ties,
+    the same pivots as the reference's simplicial factorization, its solution
+    to rounding (and, without exact cancellation, the same nnz)."""
+    cp, ri, kind = osp.grid_pattern(*dims)
+    if dims == (9, 8, 7):  # weak diagonal: partial pivoting swaps rows
+        u, _ = osp.dense.larnv("Uniform", [11, 12, 13, 15], kind.size)
+        v = np.where(kind == 0, 0.5 + 0.1 * u, -1.0 - 0.3 * u)
+    else:
+        v, _ = osp.convection_diffusion_values(kind, [1988, 1989, 1990, 1991])
+    n = len(cp) - 1
+    lu = SparseLu.analyze(cp, ri, LuMethod.simplicial())
+    assert lu.effective_method() == "Simplicial"
+    lu.factorize(cp, ri, v)
+    sym = lu.symbolic()
+    ref = osp.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], None)
+    assert ref.status == 0
+    assert np.array_equal(lu.row_perm(), ref.row_perm.astype(np.int64)), "pivot sequence"
+    b, _ = osp.dense.larnv("Symmetric", [3, 5, 7, 9], n)
+    x = b.copy()
+    lu.solve(x)
+    xr = ref.solve(b)
+    tol = 1e-9 if dims == (9, 8, 7) else 1e-12
+    assert np.max(np.abs(x - xr) / np.maximum(np.abs(xr), 1.0)) <= tol
+    if dims != (9, 8, 7):
+        s = lu.stats()
+        assert (s["nnz_l"], s["nnz_u"]) == (ref.nnz_l, ref.nnz_u)
