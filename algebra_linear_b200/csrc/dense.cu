@@ -61,14 +61,16 @@ int launch_panel_w(alg_ctx* ctx, const PanelArgs<T>& args) {
     smem = panel_smem_bytes<T, W>((m + C - 1) / C);
   }
   if (smem > kMaxSmem) return ALG_BAD_SHAPE;  // panel too tall for one cluster
-  static bool configured = false;
-  if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, W, EXACT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_cluster_kernel<T, W, EXACT>,
-                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    configured = true;
-  }
+  // kernel attributes set once per process (a thread-safe static initializer)
+  static const cudaError_t configured = [] {
+    cudaError_t e = cudaFuncSetAttribute(panel_cluster_kernel<T, W, EXACT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(panel_cluster_kernel<T, W, EXACT>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                               1);
+    return e;
+  }();
+  ALG_CUDA_TRY(configured);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C, 1, 1);
   cfg.blockDim = dim3(kPanelThreads, 1, 1);
@@ -92,12 +94,9 @@ int launch_panel_w(alg_ctx* ctx, const PanelArgs<T>& args) {
 
 template <typename T, int W, int RPT, bool EXACT>
 int launch_panel_reg(alg_ctx* ctx, const PanelArgs<T>& args, int C) {
-  static bool configured = false;
-  if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(panel_reg_kernel<T, W, RPT, EXACT>,
-                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    configured = true;
-  }
+  static const cudaError_t configured =
+      cudaFuncSetAttribute(panel_reg_kernel<T, W, RPT, EXACT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  ALG_CUDA_TRY(configured);
   const int m = args.n - args.c0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C, 1, 1);
@@ -162,14 +161,16 @@ int launch_trsm_reg(alg_ctx* ctx, T* a, int lda, int r0, int kb, int cb, int ce)
                             trsm_lower_unit_reg_kernel<T, EXACT, 4, 2>)
                      : pick(trsm_lower_unit_reg_kernel<T, EXACT, 1, 8>, trsm_lower_unit_reg_kernel<T, EXACT, 2, 8>,
                             trsm_lower_unit_reg_kernel<T, EXACT, 4, 8>);
-  static bool configured = false;
-  if (!configured) {
+  static const cudaError_t configured = [] {
     for (auto k : {trsm_lower_unit_reg_kernel<T, EXACT, 1, 2>, trsm_lower_unit_reg_kernel<T, EXACT, 2, 2>,
                    trsm_lower_unit_reg_kernel<T, EXACT, 4, 2>, trsm_lower_unit_reg_kernel<T, EXACT, 1, 8>,
-                   trsm_lower_unit_reg_kernel<T, EXACT, 2, 8>, trsm_lower_unit_reg_kernel<T, EXACT, 4, 8>})
-      ALG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    configured = true;
-  }
+                   trsm_lower_unit_reg_kernel<T, EXACT, 2, 8>, trsm_lower_unit_reg_kernel<T, EXACT, 4, 8>}) {
+      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }();
+  ALG_CUDA_TRY(configured);
   const int cta_cols = (narrow ? 2 : 8) * (kTrsmThreads / 32);
   const int grid = (ce - cb + cta_cols - 1) / cta_cols;
   const int tok = prof_begin(ctx, ALG_K_TRSM);

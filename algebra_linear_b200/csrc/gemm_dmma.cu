@@ -128,12 +128,9 @@ __global__ void __launch_bounds__(kThreads, 1) dmma_gemm_sub_kernel(int M, int N
 int gemm_dmma_sub_dev(alg_ctx* ctx, int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                       double* C, int ldc) {
   if (M <= 0 || N <= 0 || K <= 0) return ALG_OK;
-  static bool configured = false;
-  if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(dmma_gemm_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSmemBytes));
-    configured = true;
-  }
+  static const cudaError_t configured =
+      cudaFuncSetAttribute(dmma_gemm_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  ALG_CUDA_TRY(configured);
   dim3 grid((M + kBM - 1) / kBM, (N + kBN - 1) / kBN);
   const int tok = prof_begin(ctx, ALG_K_GEMM);
   dmma_gemm_sub_kernel<<<grid, kThreads, kSmemBytes, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);

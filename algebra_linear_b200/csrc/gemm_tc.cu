@@ -422,12 +422,9 @@ int launch_tc(alg_ctx* ctx, int M, int N, int K, const float* A, int lda, const 
   CUtensorMap ma, mb;
   ALG_TRY(make_map(&ma, at, KFMT, M, Kp, BM));
   ALG_TRY(make_map(&mb, bt, KFMT, N, Kp, BN));
-  static bool configured = false;
-  if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel<KFMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSmemBytes));
-    configured = true;
-  }
+  static const cudaError_t configured =
+      cudaFuncSetAttribute(gemm_tc_kernel<KFMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  ALG_CUDA_TRY(configured);
   // persistent CTAs, at most one per SM (the shared-memory ring and the 512
   // TMEM columns take a whole SM), fewer when the caller keeps SMs free
   const long tiles = (long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);

@@ -245,12 +245,13 @@ int genp_factor(alg_ctx* ctx, int prec, float* a, int n, int lda, int nb) {
   ALG_TRY(ws_get(ctx, WS_PRECOND, sizeof(float) * 128 * 128 + sizeof(float) * (size_t)n,
                  reinterpret_cast<void**>(&inv)));
   inv += n;  // the first n floats are the preconditioner's FP32 vector
-  static bool configured = false;
-  if (!configured) {
-    ALG_CUDA_TRY(cudaFuncSetAttribute(genp_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024));
-    ALG_CUDA_TRY(cudaFuncSetAttribute(genp_l21_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
-    configured = true;
-  }
+  static const cudaError_t configured = [] {
+    const cudaError_t e = cudaFuncSetAttribute(genp_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
+    return e != cudaSuccess ? e
+                            : cudaFuncSetAttribute(genp_l21_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   120 * 1024);
+  }();
+  ALG_CUDA_TRY(configured);
   for (int k0 = 0; k0 < n; k0 += nb) {
     const int kb = std::min(nb, n - k0);
     const int kr = k0 + kb;

@@ -562,12 +562,14 @@ namespace {
 
 template <int W>
 int launch_fused(alg_ctx* ctx, const TsluArgs& p, int groups0, int side_blocks, TsluScratch* ws, bool* done) {
-  static int max_ctas = -1;
-  if (max_ctas < 0) {
+  // co-resident CTAs of the single launch, computed once per process (a
+  // thread-safe static initializer; 0 when the query fails)
+  static const int max_ctas = [ctx] {
     int per_sm = 0;
-    ALG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tslu_fused_kernel<W>, kRows, 0));
-    max_ctas = per_sm * ctx->sm_count;
-  }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tslu_fused_kernel<W>, kRows, 0) == cudaSuccess
+               ? per_sm * ctx->sm_count
+               : 0;
+  }();
   *done = false;
   const int grid = std::max(groups0, side_blocks);
   // the waiting CTAs hold their SMs until the root is done, which the
