@@ -45,6 +45,22 @@ def test_python_signatures_cover_the_header():
     assert set(declared_symbols()) <= bound
 
 
+def test_python_argument_counts_match_the_header():
+    # every prototype's parameter count equals the ctypes binding's, so a
+    # changed C signature cannot be called with a stale argument list
+    from algebra_linear_b200 import _lib
+
+    protos = {}
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(alg_[a-z0-9_]+)\s*\(([^;{}]*?)\)\s*;", text, flags=re.S):
+            params = m.group(2).strip()
+            protos[m.group(1)] = 0 if params in ("", "void") else len(params.split(","))
+    bound = {name: len(args) for name, _, args in _lib.SIGNATURES}
+    assert protos and {k: v for k, v in protos.items() if bound.get(k) != v} == {}
+
+
 def test_status_strings_are_the_reference_messages():
     # src/sparse/faer/error.rs:52-64 (display_messages_are_exact)
     from algebra_linear_b200 import _lib
