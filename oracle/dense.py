@@ -45,6 +45,8 @@ def load() -> C.CDLL:
         lib.oracle_backward_error.restype = C.c_double
         lib.oracle_get01.argtypes = [P, P, P, SZ, SZ]
         lib.oracle_get01.restype = C.c_double
+        lib.oracle_latm1.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, P, SZ, P]
+        lib.oracle_dlatms_general.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, SZ, SZ, P, P, P]
         _lib = lib
     return _lib
 
@@ -124,3 +126,15 @@ def c1_system(n: int, seed=(1988, 1989, 1990, 1991)):
     x, _ = larnv("Symmetric", s, n)
     b = dgemv(a, x, n, n)
     return a, x, b
+
+
+def dlatms_general(dist: str, mode: int, cond: float, dmax: float, m: int, n: int, seed, d=None):
+    """families.rs:903-1078 (DLATMS, nonsymmetric, full storage): returns
+    (info, a column-major m*n, d, seed_after)."""
+    s = (C.c_uint32 * 4)(*seed)
+    a = np.zeros(max(m * n, 1), dtype=np.float64)
+    dv = np.zeros(max(min(m, n), 1), dtype=np.float64)
+    if d is not None:
+        dv[: len(d)] = d
+    info = load().oracle_dlatms_general(DIST[dist], mode, cond, dmax, m, n, _p(a), _p(dv), s)
+    return info, a[: m * n], dv[: min(m, n)], list(s)

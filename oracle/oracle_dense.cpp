@@ -365,3 +365,174 @@ double oracle_get01(const double* a, const double* lu, const size_t* ipiv, size_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// DLATMS for general (nonsymmetric, full) matrices — families.rs:255-370 and
+// 903-1078: the spectrum from latm1, scaled to dmax, then A = U D V with U
+// and V built one Householder reflection at a time from both sides (dlagge),
+// every reflector drawn from the Normal larnv stream and normed by the
+// reference BLAS's running-scale dnrm2. The test matrices of the sparse
+// accuracy tests (accuracy_tests.rs:15-30) come from here.
+// ---------------------------------------------------------------------------
+namespace {
+
+// x^i for i >= 0 by binary exponentiation, the algorithm of the __powidf2
+// runtime routine that rustc's f64::powi lowers to for a variable exponent
+double powi_binary(double a, int b) {
+  const bool recip = b < 0;
+  unsigned p = recip ? 0u - (unsigned)b : (unsigned)b;
+  double r = 1.0;
+  for (;;) {
+    if (p & 1u) r *= a;
+    p >>= 1;
+    if (p == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0 / r : r;
+}
+
+double laran(uint32_t seed[4]) {
+  double x[1];
+  laruv(seed, 1, x);
+  return x[0];
+}
+
+double dnrm2_reference(const double* x, size_t n) {
+  double scale = 0.0, ssq = 1.0;
+  for (size_t i = 0; i < n; ++i) {
+    const double absxi = std::fabs(x[i]);
+    if (absxi > 0.0) {
+      if (scale < absxi) {
+        const double r = scale / absxi;
+        ssq = 1.0 + ssq * r * r;
+        scale = absxi;
+      } else {
+        const double r = absxi / scale;
+        ssq += r * r;
+      }
+    }
+  }
+  return scale * std::sqrt(ssq);
+}
+
+}  // namespace
+
+extern "C" {
+
+// families.rs:280-356 (latm1). dist as oracle_larnv. Returns INFO.
+int oracle_latm1(int mode, double cond, int irsign, int dist, uint32_t seed[4], size_t n, double* d) {
+  const bool ordinary = mode != -6 && mode != 0 && mode != 6;
+  if (mode < -6 || mode > 6) return -1;
+  if (ordinary && irsign != 0 && irsign != 1) return -2;
+  if (ordinary && cond < 1.0) return -3;
+  if (n == 0 || mode == 0) return 0;
+  switch (mode < 0 ? -mode : mode) {
+    case 1:
+      for (size_t i = 0; i < n; ++i) d[i] = 1.0 / cond;
+      d[0] = 1.0;
+      break;
+    case 2:
+      for (size_t i = 0; i < n; ++i) d[i] = 1.0;
+      d[n - 1] = 1.0 / cond;
+      break;
+    case 3:
+      d[0] = 1.0;
+      if (n > 1) {
+        const double alpha = std::pow(cond, -1.0 / (double)(n - 1));
+        for (size_t i = 1; i < n; ++i) d[i] = powi_binary(alpha, (int)i);
+      }
+      break;
+    case 4:
+      d[0] = 1.0;
+      if (n > 1) {
+        const double temp = 1.0 / cond;
+        const double alpha = (1.0 - temp) / (double)(n - 1);
+        for (size_t i = 1; i < n; ++i) d[i] = (double)(n - i - 1) * alpha + temp;
+      }
+      break;
+    case 5: {
+      const double alpha = std::log(1.0 / cond);
+      for (size_t i = 0; i < n; ++i) d[i] = std::exp(alpha * laran(seed));
+      break;
+    }
+    default:
+      oracle_larnv(dist, seed, n, d);
+  }
+  if (ordinary && irsign == 1)
+    for (size_t i = 0; i < n; ++i)
+      if (laran(seed) > 0.5) d[i] = -d[i];
+  if (mode < 0)
+    for (size_t i = 0, j = n - 1; i < j; ++i, --j) std::swap(d[i], d[j]);
+  return 0;
+}
+
+// families.rs:903-992 (dlatms) for SYM = nonsymmetric, PACK = full, and
+// 994-1078 (dlagge). a is m x n column-major, d min(m, n) entries (read when
+// mode == 0). Returns INFO (the reference's codes that apply to this form).
+int oracle_dlatms_general(int dist, int mode, double cond, double dmax, size_t m, size_t n, double* a, double* d,
+                          uint32_t seed[4]) {
+  const size_t mnmin = m < n ? m : n;
+  if (m == 0 || n == 0) return 0;
+  if (mode < -6 || mode > 6) return -7;
+  if (mode != 0 && mode != 6 && mode != -6 && cond < 1.0) return -8;
+  for (int k = 0; k < 4; ++k) seed[k] %= 4096;
+  if (seed[3] % 2 != 1) seed[3] += 1;
+  if (oracle_latm1(mode, cond, 0, dist, seed, mnmin, d) != 0) return 1;
+  if (mode != 0 && mode != 6 && mode != -6) {
+    double temp = 0.0;
+    for (size_t i = 0; i < mnmin; ++i) temp = std::max(temp, std::fabs(d[i]));
+    if (!(temp > 0.0)) return 2;
+    const double alpha = dmax / temp;
+    for (size_t i = 0; i < mnmin; ++i) d[i] *= alpha;
+  }
+  for (size_t k = 0; k < m * n; ++k) a[k] = 0.0;
+  for (size_t i = 0; i < mnmin; ++i) a[i + i * m] = d[i];
+  if (m == 1 && n == 1) return 0;
+  const size_t lw = m > n ? m : n;
+  std::vector<double> w(lw), y(lw);
+  auto reflector = [&](size_t len) -> double {  // w <- the reflector, returns tau
+    oracle_larnv(3, seed, len, w.data());
+    const double wn = dnrm2_reference(w.data(), len);
+    const double wa = w[0] < 0.0 ? -wn : wn;
+    if (wn == 0.0) return 0.0;
+    const double wb = w[0] + wa;
+    const double inv = 1.0 / wb;
+    for (size_t k = 1; k < len; ++k) w[k] *= inv;
+    w[0] = 1.0;
+    return wb / wa;
+  };
+  for (size_t i = mnmin; i-- > 0;) {
+    if (i + 1 < m) {  // A(i:m, i:n) -= tau w (w^T A(i:m, i:n))
+      const size_t len = m - i;
+      const double tau = reflector(len);
+      if (tau != 0.0) {
+        const size_t ncols = n - i;
+        for (size_t j = 0; j < ncols; ++j) {
+          double sum = 0.0;
+          for (size_t k = 0; k < len; ++k) sum += a[(i + k) + (i + j) * m] * w[k];
+          y[j] = sum;
+        }
+        for (size_t j = 0; j < ncols; ++j)
+          for (size_t k = 0; k < len; ++k) a[(i + k) + (i + j) * m] -= tau * w[k] * y[j];
+      }
+    }
+    if (i + 1 < n) {  // A(i:m, i:n) -= tau (A(i:m, i:n) w) w^T
+      const size_t len = n - i;
+      const double tau = reflector(len);
+      if (tau != 0.0) {
+        const size_t nrows = m - i;
+        for (size_t k = 0; k < nrows; ++k) {
+          double sum = 0.0;
+          for (size_t j = 0; j < len; ++j) sum += a[(i + k) + (i + j) * m] * w[j];
+          y[k] = sum;
+        }
+        for (size_t j = 0; j < len; ++j)
+          for (size_t k = 0; k < nrows; ++k) a[(i + k) + (i + j) * m] -= tau * y[k] * w[j];
+      }
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"
+

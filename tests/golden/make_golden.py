@@ -11,6 +11,11 @@ whose values the reference captured from LAPACK 3.12.1's libtmglib (`dlarnv_`)
 for seed [1988, 1989, 1990, 1991], n = 200: x[0..12], x[198..200] and the seed
 after the call, for the Uniform, Symmetric and Normal distributions.
 
+Writes tests/golden/dlatms_kat.json from the test
+`dlatms_matches_the_reference_matrices` in src/lapack/families.rs:2014-2470
+(twelve DLATMS calls whose spectra, matrices and final seeds the reference
+captured from LAPACK 3.12.1's libtmglib).
+
 Writes tests/golden/colamd_kat.json from the test `matches_faer_on_fixtures`
 in src/sparse/faer/colamd.rs:886-918 (permutations the reference captured from
 faer's colamd::order): each fixture's CSC pattern, built here from the
@@ -111,11 +116,39 @@ def extract_colamd(src: str) -> dict:
     return {"source": "src/sparse/faer/colamd.rs:886-918 (matches_faer_on_fixtures)", "cases": cases}
 
 
+def extract_dlatms(src: str) -> dict:
+    """families.rs:2014-2470 (dlatms_matches_the_reference_matrices): twelve
+    DLATMS calls from seed SEEDY with the spectrum, the matrix and the seed
+    after the call that the reference captured from LAPACK's libtmglib."""
+    start = src.index("fn dlatms_matches_the_reference_matrices")
+    body = src[start:src.index("fn dlatms_reports_what_the_reference_reports", start)]
+    arrays = {}
+    for m in re.finditer(r"let ([ad]\d+): \[f64; \d+\] = \[(.*?)\];", body, flags=re.S):
+        text = re.sub(r"//[^\n]*", "", m.group(2))
+        arrays[m.group(1)] = [v.strip() for v in text.split(",") if v.strip()]
+    cases = []
+    pat = (r"Dlatms \{\s*dist: Dist::(\w+),\s*sym: DlatmsSym::(\w+),\s*mode: (-?\d+),\s*cond: ([^,]+),"
+           r"\s*dmax: ([^,]+),\s*pack: DlatmsPack::(\w+),\s*\},\s*(\d+),\s*(\d+),\s*\[([^\]]+)\],"
+           r"\s*&(d\d+),\s*&(a\d+),")
+    for m in re.finditer(pat, body):
+        dist, sym, mode, cond, dmax, pack, mm, nn, seed, dn, an = m.groups()
+        cases.append({"dist": dist, "sym": sym, "mode": int(mode), "cond": cond.strip(), "dmax": dmax.strip(),
+                      "pack": pack, "m": int(mm), "n": int(nn), "seed_after": [int(v) for v in seed.split(",")],
+                      "d": arrays[dn], "a": arrays[an]})
+    assert len(cases) == 12, len(cases)
+    seedy = re.search(r"const SEEDY: \[u32; 4\] = \[([^\]]+)\]", src)
+    return {"source": "src/lapack/families.rs:2014-2470 (dlatms_matches_the_reference_matrices)",
+            "seed": [int(v) for v in seedy.group(1).split(",")], "cases": cases}
+
+
 def main() -> None:
     root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     fam = (root / "src/lapack/families.rs").read_text()
     out = HERE / "larnv_kat.json"
     out.write_text(json.dumps(extract_larnv(fam), indent=1) + "\n")
+    print("wrote", out)
+    out = HERE / "dlatms_kat.json"
+    out.write_text(json.dumps(extract_dlatms(fam), indent=1) + "\n")
     print("wrote", out)
     col = (root / "src/sparse/faer/colamd.rs").read_text()
     out = HERE / "colamd_kat.json"

@@ -235,3 +235,26 @@ def test_oracle_agrees_with_an_independent_lu(oracle):
     assert rc == 0
     assert list(piv) == ipiv
     assert np.max(np.abs(bw - xs)) / np.max(np.abs(xs)) < 1e-12
+
+
+def _dlatms_general_cases():
+    kat = json.loads((GOLDEN / "dlatms_kat.json").read_text())
+    return [(kat["seed"], c) for c in kat["cases"] if c["sym"] == "NonSymmetric" and c["pack"] == "Full"]
+
+
+@pytest.mark.parametrize("seed,case", _dlatms_general_cases(),
+                         ids=lambda v: f"mode{v['mode']}_{v['m']}x{v['n']}" if isinstance(v, dict) else "")
+def test_dlatms_matches_the_reference_matrices(oracle, seed, case):
+    # families.rs:2014-2470: the seed after the call exactly, spectrum and
+    # matrix to the reference's own 1e-13 relative (its values come from
+    # LAPACK's libtmglib, whose BLAS sums in another order)
+    want_d = np.array([float(v) for v in case["d"]])
+    want_a = np.array([float(v) for v in case["a"]])
+    info, a, d, seed_after = oracle.dlatms_general(case["dist"], case["mode"], float(case["cond"]),
+                                                   float(case["dmax"]), case["m"], case["n"], seed, want_d)
+    assert info == 0
+    assert seed_after == case["seed_after"]
+    for got, want in ((d, want_d), (a, want_a)):
+        zero = want == 0.0
+        assert np.all(got[zero] == 0.0)
+        assert np.all(np.abs(got[~zero] - want[~zero]) <= 1e-13 * np.abs(want[~zero]))

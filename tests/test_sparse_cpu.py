@@ -330,3 +330,37 @@ def test_simplicial_and_supernodal_oracles_agree(oracle_sparse, dims):
     xs, x = fs.solve(b), f.solve(b)
     assert np.max(np.abs(xs - x)) / np.max(np.abs(x)) <= 1e-12
     assert fs.nnz_l >= f.nnz_l and fs.nnz_u >= f.nnz_u, (fs.nnz_l, f.nnz_l, fs.nnz_u, f.nnz_u)
+
+
+@pytest.mark.parametrize("case,n", list(enumerate([4, 8, 16, 32])), ids=lambda v: str(v))
+def test_accuracy_on_lapack_random_matrices(oracle_sparse, case, n):
+    """accuracy_tests.rs:74-116: DLATMS matrices (mode 3, cond 1e2 and 1e4)
+    stored densely as CSC, solved by the simplicial and supernodal
+    restatements and by the path Auto(1.0) picks (supernodal from n = 16):
+    forward error <= 1e-9 cond, scaled residual <= 1e-13 cond."""
+    dense = oracle_sparse.dense
+    for ci, cond in enumerate([1e2, 1e4]):
+        seed = [1234 + case * 17, 2345 + ci, 3456 + case, 4567]
+        info, a, _, _ = dense.dlatms_general("Uniform", 3, cond, 1.0, n, n, seed)
+        assert info == 0
+        A = a.reshape(n, n).T
+        x_exact = 1.0 + (np.arange(n) % 7) * 0.25
+        b = A @ x_exact
+        cp = list(range(0, n * n + 1, n))
+        ri = [i for _ in range(n) for i in range(n)]
+        xs = {}
+        f, _ = _simplicial(oracle_sparse, cp, ri, a)
+        xs["simplicial"] = f.solve(b)
+        sup = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
+        f = oracle_sparse.Factors(n, cp, ri, a, sup["col_perm"], sup["col_perm_inv"], sup["supernode_ptr"])
+        xs["supernodal"] = f.solve(b)
+        auto = SparseLu.analyze(cp, ri, LuMethod.auto(1.0))
+        xs["auto"] = xs["supernodal"] if auto.effective_method() == "Supernodal" else xs["simplicial"]
+        if n >= 16:
+            assert auto.effective_method() == "Supernodal", n
+        anorm = np.max(np.abs(A).sum(axis=1))
+        for name, x in xs.items():
+            err = np.max(np.abs(x - x_exact)) / max(np.max(np.abs(x_exact)), 1.0)
+            res = np.max(np.abs(A @ x - b)) / (anorm * np.max(np.abs(x)) + np.max(np.abs(b)))
+            assert err <= 1e-9 * cond, (name, n, cond, err)
+            assert res <= 1e-13 * cond, (name, n, cond, res)
