@@ -209,3 +209,31 @@ def test_simplicial_request_matches_the_simplicial_oracle(gpu, osp, dims):
     if dims != (9, 8, 7):
         s = lu.stats()
         assert (s["nnz_l"], s["nnz_u"]) == (ref.nnz_l, ref.nnz_u)
+
+
+@pytest.mark.parametrize("case,n", list(enumerate([4, 8, 16, 32])), ids=lambda v: str(v))
+def test_accuracy_on_lapack_random_matrices(gpu, osp, case, n):
+    """accuracy_tests.rs:74-116 on the GPU: DLATMS matrices (mode 3, cond 1e2
+    and 1e4) stored densely, every method: forward error <= 1e-9 cond and
+    scaled residual <= 1e-13 cond; Auto(1.0) picks the supernodal path from
+    n = 16."""
+    for ci, cond in enumerate([1e2, 1e4]):
+        seed = [1234 + case * 17, 2345 + ci, 3456 + case, 4567]
+        info, a, _, _ = osp.dense.dlatms_general("Uniform", 3, cond, 1.0, n, n, seed)
+        assert info == 0
+        A = a.reshape(n, n).T
+        x_exact = 1.0 + (np.arange(n) % 7) * 0.25
+        b = A @ x_exact
+        cp = list(range(0, n * n + 1, n))
+        ri = [i for _ in range(n) for i in range(n)]
+        anorm = np.max(np.abs(A).sum(axis=1))
+        for method in (LuMethod.simplicial(), LuMethod.supernodal(), LuMethod.auto(1.0)):
+            lu = SparseLu.analyze(cp, ri, method)
+            if method.kind == LuMethod.auto(1.0).kind and n >= 16:
+                assert lu.effective_method() == "Supernodal"
+            lu.factorize(cp, ri, a)
+            x = b.copy()
+            lu.solve(x)
+            err = np.max(np.abs(x - x_exact)) / max(np.max(np.abs(x_exact)), 1.0)
+            res = np.max(np.abs(A @ x - b)) / (anorm * np.max(np.abs(x)) + np.max(np.abs(b)))
+            assert err <= 1e-9 * cond and res <= 1e-13 * cond, (n, cond, err, res)
