@@ -31,11 +31,55 @@ namespace {
 
 constexpr size_t kNone = (size_t)-1;
 
-struct Factors {
+// The scalar operations of the reference's SparseScalar (lu.rs:25-82) for
+// f64 and for Complex64 = num_complex::Complex<f64> (num-complex 0.4, not
+// vendored): |x| is the modulus hypot(re, im) for a complex entry, recip is
+// num-complex's inv() = (re / (re^2 + im^2), -im / (re^2 + im^2)), products
+// (ac - bd) + i(ad + bc), sums and differences component-wise.
+struct zc {
+  double re, im;
+};
+inline double s_abs(double v) { return std::fabs(v); }
+inline double s_abs(zc v) { return std::hypot(v.re, v.im); }
+inline double s_recip(double v) { return 1.0 / v; }
+inline zc s_recip(zc v) {
+  const double ns = v.re * v.re + v.im * v.im;
+  return {v.re / ns, -v.im / ns};
+}
+inline double s_mul(double a, double b) { return a * b; }
+inline zc s_mul(zc a, zc b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline void s_add(double& a, double b) { a += b; }
+inline void s_add(zc& a, zc b) {
+  a.re += b.re;
+  a.im += b.im;
+}
+inline void s_sub(double& a, double b) { a -= b; }
+inline void s_sub(zc& a, zc b) {
+  a.re -= b.re;
+  a.im -= b.im;
+}
+inline bool s_finite(double v) { return std::isfinite(v); }
+inline bool s_finite(zc v) { return std::isfinite(v.re) && std::isfinite(v.im); }
+template <typename T>
+T s_zero();
+template <>
+double s_zero<double>() { return 0.0; }
+template <>
+zc s_zero<zc>() { return {0.0, 0.0}; }
+template <typename T>
+T s_one();
+template <>
+double s_one<double>() { return 1.0; }
+template <>
+zc s_one<zc>() { return {1.0, 0.0}; }
+
+template <typename T>
+struct FactorsT {
   size_t n = 0;
   std::vector<size_t> lp, li, up, ui, row_perm, col_perm_inv;
-  std::vector<double> lv, uv;
+  std::vector<T> lv, uv;
 };
+using Factors = FactorsT<double>;
 
 size_t owner_of(const std::vector<size_t>& ptr, size_t col) {
   // the supernode whose column range holds col
@@ -44,12 +88,13 @@ size_t owner_of(const std::vector<size_t>& ptr, size_t col) {
 
 // Partial-pivoting LU of the nfac leading columns of an nrows x ncols
 // column-major front (supernodal_lu.rs:490-533). Returns false if singular.
-bool factor_front(std::vector<double>& a, size_t nrows, size_t nfac, size_t ncols, std::vector<size_t>& piv) {
+template <typename T>
+bool factor_front(std::vector<T>& a, size_t nrows, size_t nfac, size_t ncols, std::vector<size_t>& piv) {
   for (size_t k = 0; k < nfac; ++k) {
     size_t p = k;
-    double best = std::fabs(a[k + k * nrows]);
+    double best = s_abs(a[k + k * nrows]);
     for (size_t i = k + 1; i < nrows; ++i) {
-      const double v = std::fabs(a[i + k * nrows]);
+      const double v = s_abs(a[i + k * nrows]);
       if (v > best) {
         best = v;
         p = i;
@@ -59,34 +104,29 @@ bool factor_front(std::vector<double>& a, size_t nrows, size_t nfac, size_t ncol
     if (p != k)
       for (size_t j = 0; j < ncols; ++j) std::swap(a[j * nrows + k], a[j * nrows + p]);
     piv[k] = p;
-    const double inv = 1.0 / a[k + k * nrows];
-    for (size_t i = k + 1; i < nrows; ++i) a[i + k * nrows] = a[i + k * nrows] * inv;
+    const T inv = s_recip(a[k + k * nrows]);
+    for (size_t i = k + 1; i < nrows; ++i) a[i + k * nrows] = s_mul(a[i + k * nrows], inv);
     for (size_t j = k + 1; j < ncols; ++j) {
-      const double akj = a[k + j * nrows];
-      for (size_t i = k + 1; i < nrows; ++i) a[i + j * nrows] -= akj * a[i + k * nrows];
+      const T akj = a[k + j * nrows];
+      for (size_t i = k + 1; i < nrows; ++i) s_sub(a[i + j * nrows], s_mul(akj, a[i + k * nrows]));
     }
   }
   return true;
 }
 
-}  // namespace
-
-extern "C" {
-
-// Status: 0 ok, 104 singular (the reference's Error::Singular), 101 invalid
-// structure (a factor lost its diagonal), 107 a non-finite value.
-int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val, const size_t* col_perm,
-                          const size_t* col_perm_inv, const size_t* sn_ptr, size_t n_sn, void** out) {
+template <typename T>
+int splu_factorize_t(size_t n, const size_t* cp, const size_t* ri, const T* val, const size_t* col_perm,
+                     const size_t* col_perm_inv, const size_t* sn_ptr, size_t n_sn, void** out) {
   *out = nullptr;
   const size_t nnz = cp[n];
   for (size_t q = 0; q < nnz; ++q)
-    if (!std::isfinite(val[q])) return 107;
+    if (!s_finite(val[q])) return 107;
   std::vector<size_t> ptr(sn_ptr, sn_ptr + n_sn + 1);
   const size_t ns = n_sn;
 
   // A transposed, each entry's column replaced by its new position
   std::vector<size_t> tp(n + 1, 0), tcol(nnz);
-  std::vector<double> tval(nnz);
+  std::vector<T> tval(nnz);
   for (size_t q = 0; q < nnz; ++q) tp[ri[q] + 1] += 1;
   for (size_t r = 0; r < n; ++r) tp[r + 1] += tp[r];
   {
@@ -101,7 +141,7 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
 
   std::vector<size_t> rperm(n), rpos(n);  // position -> row, row -> position
   for (size_t i = 0; i < n; ++i) rperm[i] = rpos[i] = i;
-  std::vector<std::vector<std::pair<size_t, double>>> lcol(n), ucol(n);
+  std::vector<std::vector<std::pair<size_t, T>>> lcol(n), ucol(n);
   std::vector<std::vector<size_t>> l_rows_to_sn(n);  // row -> supernodes whose L panel holds it
   std::vector<std::vector<size_t>> u_reach(ns);      // supernode -> earlier supernodes whose U reaches it
   std::vector<std::vector<size_t>> panel_cols(ns);   // supernode -> its C_s
@@ -157,18 +197,18 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
     for (size_t t = 0; t < nr; ++t) rloc[R[t]] = t;
 
     // L front: A, then every earlier (k, u) stored for each column
-    std::vector<double> F(nr * w, 0.0);
+    std::vector<T> F(nr * w, s_zero<T>());
     for (size_t jj = 0; jj < w; ++jj) {
       const size_t pj = col_perm[sb + jj];
       for (size_t q = cp[pj]; q < cp[pj + 1]; ++q) {
         const size_t li = rloc[ri[q]];
-        if (li != kNone) F[li + jj * nr] += val[q];
+        if (li != kNone) s_add(F[li + jj * nr], val[q]);
       }
       for (const auto& ku : ucol[sb + jj]) {
         if (ku.first >= sb) continue;
         for (const auto& rl : lcol[ku.first]) {
           const size_t li = rloc[rl.first];
-          if (li != kNone) F[li + jj * nr] -= rl.second * ku.second;
+          if (li != kNone) s_sub(F[li + jj * nr], s_mul(rl.second, ku.second));
         }
       }
     }
@@ -193,12 +233,12 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
     build_cols(sb, se);
     for (size_t t = 0; t < C.size(); ++t) cloc[C[t]] = t;
     const size_t nc = C.size();
-    std::vector<double> U(nr * nc, 0.0);
+    std::vector<T> U(nr * nc, s_zero<T>());
     for (size_t li = 0; li < nr; ++li) {
       const size_t row = R[li];
       for (size_t t = tp[row]; t < tp[row + 1]; ++t) {
         const size_t c = tcol[t];
-        if (c >= se && cloc[c] != kNone) U[li + cloc[c] * nr] += tval[t];
+        if (c >= se && cloc[c] != kNone) s_add(U[li + cloc[c] * nr], tval[t]);
       }
     }
     for (size_t ci = 0; ci < nc; ++ci)
@@ -206,30 +246,30 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
         if (ku.first >= sb) continue;
         for (const auto& rl : lcol[ku.first]) {
           const size_t li = rloc[rl.first];
-          if (li != kNone) U[li + ci * nr] -= rl.second * ku.second;
+          if (li != kNone) s_sub(U[li + ci * nr], s_mul(rl.second, ku.second));
         }
       }
     for (size_t jj = 0; jj < w; ++jj)
       for (size_t ii = jj + 1; ii < w; ++ii) {
-        const double l = F[ii + jj * nr];
-        for (size_t ci = 0; ci < nc; ++ci) U[ii + ci * nr] -= l * U[jj + ci * nr];
+        const T l = F[ii + jj * nr];
+        for (size_t ci = 0; ci < nc; ++ci) s_sub(U[ii + ci * nr], s_mul(l, U[jj + ci * nr]));
       }
     // store, dropping exact zeros
     for (size_t jj = 0; jj < w; ++jj)
       for (size_t li = jj; li < nr; ++li) {
-        const double v = li == jj ? 1.0 : F[li + jj * nr];
-        if (li == jj || std::fabs(v) != 0.0) lcol[sb + jj].push_back({R[li], v});
+        const T v = li == jj ? s_one<T>() : F[li + jj * nr];
+        if (li == jj || s_abs(v) != 0.0) lcol[sb + jj].push_back({R[li], v});
       }
     for (size_t jj = 0; jj < w; ++jj)
       for (size_t ii = 0; ii <= jj; ++ii) {
-        const double v = F[ii + jj * nr];
-        if (ii == jj || std::fabs(v) != 0.0) ucol[sb + jj].push_back({sb + ii, v});
+        const T v = F[ii + jj * nr];
+        if (ii == jj || s_abs(v) != 0.0) ucol[sb + jj].push_back({sb + ii, v});
       }
     for (size_t ci = 0; ci < nc; ++ci) {
       const size_t c = C[ci];
       for (size_t ii = 0; ii < w; ++ii) {
-        const double v = U[ii + ci * nr];
-        if (std::fabs(v) != 0.0) ucol[c].push_back({sb + ii, v});
+        const T v = U[ii + ci * nr];
+        if (s_abs(v) != 0.0) ucol[c].push_back({sb + ii, v});
       }
       const size_t node = owner_of(ptr, c);
       if (node > s && (u_reach[node].empty() || u_reach[node].back() != s)) u_reach[node].push_back(s);
@@ -241,14 +281,14 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
     panel_cols[s] = C;
   }
 
-  auto* f = new Factors();
+  auto* f = new FactorsT<T>();
   f->n = n;
   f->lp.assign(n + 1, 0);
   f->up.assign(n + 1, 0);
   for (size_t j = 0; j < n; ++j) {
     for (auto& e : lcol[j]) e.first = rpos[e.first];
     std::stable_sort(lcol[j].begin(), lcol[j].end(),
-                     [](const std::pair<size_t, double>& x, const std::pair<size_t, double>& y) { return x.first < y.first; });
+                     [](const std::pair<size_t, T>& x, const std::pair<size_t, T>& y) { return x.first < y.first; });
     if (lcol[j].empty() || lcol[j].front().first != j) {
       delete f;
       return 101;
@@ -256,7 +296,7 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
   }
   for (size_t c = 0; c < n; ++c) {
     std::stable_sort(ucol[c].begin(), ucol[c].end(),
-                     [](const std::pair<size_t, double>& x, const std::pair<size_t, double>& y) { return x.first < y.first; });
+                     [](const std::pair<size_t, T>& x, const std::pair<size_t, T>& y) { return x.first < y.first; });
     if (ucol[c].empty() || ucol[c].back().first != c) {
       delete f;
       return 101;
@@ -280,51 +320,6 @@ int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const do
   return 0;
 }
 
-void oracle_splu_sizes(const void* h, size_t* nnz_l, size_t* nnz_u) {
-  const auto* f = static_cast<const Factors*>(h);
-  *nnz_l = f->lp[f->n];
-  *nnz_u = f->up[f->n];
-}
-
-void oracle_splu_get(const void* h, size_t* lp, size_t* li, double* lv, size_t* up, size_t* ui, double* uv,
-                     size_t* row_perm) {
-  const auto* f = static_cast<const Factors*>(h);
-  std::memcpy(lp, f->lp.data(), sizeof(size_t) * (f->n + 1));
-  std::memcpy(up, f->up.data(), sizeof(size_t) * (f->n + 1));
-  if (!f->li.empty()) {
-    std::memcpy(li, f->li.data(), sizeof(size_t) * f->li.size());
-    std::memcpy(lv, f->lv.data(), sizeof(double) * f->lv.size());
-  }
-  if (!f->ui.empty()) {
-    std::memcpy(ui, f->ui.data(), sizeof(size_t) * f->ui.size());
-    std::memcpy(uv, f->uv.data(), sizeof(double) * f->uv.size());
-  }
-  std::memcpy(row_perm, f->row_perm.data(), sizeof(size_t) * f->n);
-}
-
-// SupernodalLu::solve (supernodal_lu.rs:118-133) with the sweeps of
-// lu.rs:440-464: permute by rows, unit lower sweep by columns, upper sweep
-// from the last column (x_j times the reciprocal of the diagonal), permute back.
-void oracle_splu_solve(const void* h, double* b) {
-  const auto* f = static_cast<const Factors*>(h);
-  const size_t n = f->n;
-  std::vector<double> x(n);
-  for (size_t i = 0; i < n; ++i) x[i] = b[f->row_perm[i]];
-  for (size_t j = 0; j < n; ++j) {
-    const double xj = x[j];
-    for (size_t k = f->lp[j] + 1; k < f->lp[j + 1]; ++k) x[f->li[k]] -= f->lv[k] * xj;
-  }
-  for (size_t j = n; j-- > 0;) {
-    const size_t end = f->up[j + 1];
-    const double xj = x[j] * (1.0 / f->uv[end - 1]);
-    x[j] = xj;
-    for (size_t k = f->up[j]; k + 1 < end; ++k) x[f->ui[k]] -= f->uv[k] * xj;
-  }
-  for (size_t i = 0; i < n; ++i) b[i] = x[f->col_perm_inv[i]];
-}
-
-void oracle_splu_free(void* h) { delete static_cast<Factors*>(h); }
-
 // The simplicial path, lu.rs:209-327 (SymbolicLu::factorize) with
 // l_incomplete_solve_sparse, reach and depth_first_search (:349-436), over
 // the same column order: for the j-th column, the rows reachable from A's
@@ -337,16 +332,17 @@ void oracle_splu_free(void* h) { delete static_cast<Factors*>(h); }
 // for every other unpivoted row of the reach, zeros included. L's rows
 // become positions at the end; no sorting (L's pivot first, U's diagonal
 // last, as the sweeps expect). Same status codes as oracle_splu_factorize.
-int oracle_simplicial_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val,
-                                const size_t* col_perm, const size_t* col_perm_inv, void** out) {
+template <typename T>
+int simplicial_factorize_t(size_t n, const size_t* cp, const size_t* ri, const T* val, const size_t* col_perm,
+                           const size_t* col_perm_inv, void** out) {
   *out = nullptr;
   for (size_t q = 0; q < cp[n]; ++q)
-    if (!std::isfinite(val[q])) return 107;
-  auto* f = new Factors;
+    if (!s_finite(val[q])) return 107;
+  auto* f = new FactorsT<T>;
   f->n = n;
   f->lp.assign(n + 1, 0);
   f->up.assign(n + 1, 0);
-  std::vector<double> x(n, 0.0);
+  std::vector<T> x(n, s_zero<T>());
   std::vector<size_t> marked(n, 0), reach(n), stack(n), rpi(n, n);
   for (size_t j = 0; j < n; ++j) {
     const size_t pj = col_perm[j], mark = j + 1;
@@ -382,19 +378,19 @@ int oracle_simplicial_factorize(size_t n, const size_t* cp, const size_t* ri, co
     size_t tail = n;
     for (size_t q = cp[pj]; q < cp[pj + 1]; ++q)
       if (marked[ri[q]] < mark) tail = dfs(ri[q], tail);
-    for (size_t q = cp[pj]; q < cp[pj + 1]; ++q) x[ri[q]] += val[q];
+    for (size_t q = cp[pj]; q < cp[pj + 1]; ++q) s_add(x[ri[q]], val[q]);
     for (size_t t = tail; t < n; ++t) {
       const size_t i = reach[t], pi = rpi[i];
       if (pi >= j) continue;
-      const double xi = x[i];
-      for (size_t k = f->lp[pi] + 1; k < f->lp[pi + 1]; ++k) x[f->li[k]] -= f->lv[k] * xi;
+      const T xi = x[i];
+      for (size_t k = f->lp[pi] + 1; k < f->lp[pi + 1]; ++k) s_sub(x[f->li[k]], s_mul(f->lv[k], xi));
     }
     size_t piv = n;
     double pval = -1.0;
     for (size_t t = tail; t < n; ++t) {
       const size_t i = reach[t];
       if (rpi[i] == n) {
-        const double v = std::fabs(x[i]);
+        const double v = s_abs(x[i]);
         if (std::isnan(v) || std::isnan(pval) || v > pval) {
           piv = i;
           pval = v;
@@ -408,20 +404,20 @@ int oracle_simplicial_factorize(size_t n, const size_t* cp, const size_t* ri, co
       delete f;
       return 104;
     }
-    const double xp = x[piv], xp_inv = 1.0 / xp;
+    const T xp = x[piv], xp_inv = s_recip(xp);
     rpi[piv] = j;
     f->ui.push_back(j);
     f->uv.push_back(xp);
     f->up[j + 1] = f->ui.size();
     f->li.push_back(piv);
-    f->lv.push_back(1.0);
+    f->lv.push_back(s_one<T>());
     for (size_t t = tail; t < n; ++t) {
       const size_t i = reach[t];
       if (rpi[i] == n) {
         f->li.push_back(i);
-        f->lv.push_back(x[i] * xp_inv);
+        f->lv.push_back(s_mul(x[i], xp_inv));
       }
-      x[i] = 0.0;
+      x[i] = s_zero<T>();
     }
     f->lp[j + 1] = f->li.size();
   }
@@ -432,5 +428,97 @@ int oracle_simplicial_factorize(size_t n, const size_t* cp, const size_t* ri, co
   *out = f;
   return 0;
 }
+
+template <typename T>
+void splu_get_t(const void* h, size_t* lp, size_t* li, void* lv, size_t* up, size_t* ui, void* uv,
+                size_t* row_perm) {
+  const auto* f = static_cast<const FactorsT<T>*>(h);
+  std::memcpy(lp, f->lp.data(), sizeof(size_t) * (f->n + 1));
+  std::memcpy(up, f->up.data(), sizeof(size_t) * (f->n + 1));
+  if (!f->li.empty()) {
+    std::memcpy(li, f->li.data(), sizeof(size_t) * f->li.size());
+    std::memcpy(lv, f->lv.data(), sizeof(T) * f->lv.size());
+  }
+  if (!f->ui.empty()) {
+    std::memcpy(ui, f->ui.data(), sizeof(size_t) * f->ui.size());
+    std::memcpy(uv, f->uv.data(), sizeof(T) * f->uv.size());
+  }
+  std::memcpy(row_perm, f->row_perm.data(), sizeof(size_t) * f->n);
+}
+
+// SupernodalLu::solve (supernodal_lu.rs:118-133), the same as LuFactors::solve
+// (lu.rs:177-198), with the sweeps of lu.rs:440-464: permute by rows, unit
+// lower sweep by columns, upper sweep from the last column (x_j times the
+// reciprocal of the diagonal), permute back.
+template <typename T>
+void splu_solve_t(const void* h, T* b) {
+  const auto* f = static_cast<const FactorsT<T>*>(h);
+  const size_t n = f->n;
+  std::vector<T> x(n);
+  for (size_t i = 0; i < n; ++i) x[i] = b[f->row_perm[i]];
+  for (size_t j = 0; j < n; ++j) {
+    const T xj = x[j];
+    for (size_t k = f->lp[j] + 1; k < f->lp[j + 1]; ++k) s_sub(x[f->li[k]], s_mul(f->lv[k], xj));
+  }
+  for (size_t j = n; j-- > 0;) {
+    const size_t end = f->up[j + 1];
+    const T xj = s_mul(x[j], s_recip(f->uv[end - 1]));
+    x[j] = xj;
+    for (size_t k = f->up[j]; k + 1 < end; ++k) s_sub(x[f->ui[k]], s_mul(f->uv[k], xj));
+  }
+  for (size_t i = 0; i < n; ++i) b[i] = x[f->col_perm_inv[i]];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Status: 0 ok, 104 singular (the reference's Error::Singular), 101 invalid
+// structure (a factor lost its diagonal), 107 a non-finite value. The z
+// entry points take and return complex values as interleaved (re, im)
+// doubles; a handle is used with the entry points of its own scalar type.
+int oracle_splu_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val, const size_t* col_perm,
+                          const size_t* col_perm_inv, const size_t* sn_ptr, size_t n_sn, void** out) {
+  return splu_factorize_t<double>(n, cp, ri, val, col_perm, col_perm_inv, sn_ptr, n_sn, out);
+}
+int oracle_zsplu_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val, const size_t* col_perm,
+                           const size_t* col_perm_inv, const size_t* sn_ptr, size_t n_sn, void** out) {
+  return splu_factorize_t<zc>(n, cp, ri, reinterpret_cast<const zc*>(val), col_perm, col_perm_inv, sn_ptr, n_sn,
+                              out);
+}
+int oracle_simplicial_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val,
+                                const size_t* col_perm, const size_t* col_perm_inv, void** out) {
+  return simplicial_factorize_t<double>(n, cp, ri, val, col_perm, col_perm_inv, out);
+}
+int oracle_zsimplicial_factorize(size_t n, const size_t* cp, const size_t* ri, const double* val,
+                                 const size_t* col_perm, const size_t* col_perm_inv, void** out) {
+  return simplicial_factorize_t<zc>(n, cp, ri, reinterpret_cast<const zc*>(val), col_perm, col_perm_inv, out);
+}
+
+void oracle_splu_sizes(const void* h, size_t* nnz_l, size_t* nnz_u) {
+  const auto* f = static_cast<const Factors*>(h);
+  *nnz_l = f->lp[f->n];
+  *nnz_u = f->up[f->n];
+}
+void oracle_zsplu_sizes(const void* h, size_t* nnz_l, size_t* nnz_u) {
+  const auto* f = static_cast<const FactorsT<zc>*>(h);
+  *nnz_l = f->lp[f->n];
+  *nnz_u = f->up[f->n];
+}
+
+void oracle_splu_get(const void* h, size_t* lp, size_t* li, double* lv, size_t* up, size_t* ui, double* uv,
+                     size_t* row_perm) {
+  splu_get_t<double>(h, lp, li, lv, up, ui, uv, row_perm);
+}
+void oracle_zsplu_get(const void* h, size_t* lp, size_t* li, double* lv, size_t* up, size_t* ui, double* uv,
+                      size_t* row_perm) {
+  splu_get_t<zc>(h, lp, li, lv, up, ui, uv, row_perm);
+}
+
+void oracle_splu_solve(const void* h, double* b) { splu_solve_t<double>(h, b); }
+void oracle_zsplu_solve(const void* h, double* b) { splu_solve_t<zc>(h, reinterpret_cast<zc*>(b)); }
+
+void oracle_splu_free(void* h) { delete static_cast<Factors*>(h); }
+void oracle_zsplu_free(void* h) { delete static_cast<FactorsT<zc>*>(h); }
 
 }  // extern "C"

@@ -25,6 +25,12 @@ def _lib():
         lib.oracle_splu_solve.argtypes = [P, P]
         lib.oracle_splu_free.argtypes = [P]
         lib.oracle_simplicial_factorize.argtypes = [SZ, P, P, P, P, P, C.POINTER(C.c_void_p)]
+        lib.oracle_zsplu_factorize.argtypes = [SZ, P, P, P, P, P, P, SZ, C.POINTER(C.c_void_p)]
+        lib.oracle_zsimplicial_factorize.argtypes = [SZ, P, P, P, P, P, C.POINTER(C.c_void_p)]
+        lib.oracle_zsplu_sizes.argtypes = [P, C.POINTER(SZ), C.POINTER(SZ)]
+        lib.oracle_zsplu_get.argtypes = [P, P, P, P, P, P, P, P]
+        lib.oracle_zsplu_solve.argtypes = [P, P]
+        lib.oracle_zsplu_free.argtypes = [P]
         lib._sparse_bound = True
     return lib
 
@@ -35,43 +41,48 @@ def _u(a) -> np.ndarray:
 
 class Factors:
     """The reference's supernodal factors of one matrix (positions, CSC);
-    with supernode_ptr None, its simplicial factors (lu.rs:209-327)."""
+    with supernode_ptr None, its simplicial factors (lu.rs:209-327). Complex
+    values (numpy complex128) give the SparseLu<Complex64> factors."""
 
     def __init__(self, n, col_ptr, row_idx, values, col_perm, col_perm_inv, supernode_ptr):
         lib = _lib()
         self.n = int(n)
+        self.complex = np.iscomplexobj(values)
+        dt = np.complex128 if self.complex else np.float64
+        z = "z" if self.complex else ""
+        self._fn = {k: getattr(lib, f"oracle_{z}splu_{k}") for k in ("sizes", "get", "solve", "free")}
         cp, ri = _u(col_ptr), _u(row_idx)
-        v = np.ascontiguousarray(values, dtype=np.float64)
+        v = np.ascontiguousarray(values, dtype=dt)
         cpm, cpi = _u(col_perm), _u(col_perm_inv)
         snp = _u(supernode_ptr) if supernode_ptr is not None else None
         h = C.c_void_p()
         if supernode_ptr is None:  # the simplicial path
-            self.status = lib.oracle_simplicial_factorize(self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data,
-                                                          cpm.ctypes.data, cpi.ctypes.data, C.byref(h))
+            self.status = getattr(lib, f"oracle_{z}simplicial_factorize")(
+                self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data, cpm.ctypes.data, cpi.ctypes.data, C.byref(h))
         else:
-            self.status = lib.oracle_splu_factorize(self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data,
-                                                    cpm.ctypes.data, cpi.ctypes.data, snp.ctypes.data,
-                                                    len(snp) - 1, C.byref(h))
+            self.status = getattr(lib, f"oracle_{z}splu_factorize")(
+                self.n, cp.ctypes.data, ri.ctypes.data, v.ctypes.data, cpm.ctypes.data, cpi.ctypes.data,
+                snp.ctypes.data, len(snp) - 1, C.byref(h))
         self.h = h if self.status == 0 else None
         if self.h is None:
             return
         nl, nu = C.c_size_t(), C.c_size_t()
-        lib.oracle_splu_sizes(h, C.byref(nl), C.byref(nu))
+        self._fn["sizes"](h, C.byref(nl), C.byref(nu))
         self.l_col_ptr = np.zeros(self.n + 1, np.uint64)
         self.u_col_ptr = np.zeros(self.n + 1, np.uint64)
         self.l_row_idx = np.zeros(max(nl.value, 1), np.uint64)
         self.u_row_idx = np.zeros(max(nu.value, 1), np.uint64)
-        self.l_val = np.zeros(max(nl.value, 1))
-        self.u_val = np.zeros(max(nu.value, 1))
+        self.l_val = np.zeros(max(nl.value, 1), dtype=dt)
+        self.u_val = np.zeros(max(nu.value, 1), dtype=dt)
         self.row_perm = np.zeros(max(self.n, 1), np.uint64)
-        lib.oracle_splu_get(h, self.l_col_ptr.ctypes.data, self.l_row_idx.ctypes.data, self.l_val.ctypes.data,
-                            self.u_col_ptr.ctypes.data, self.u_row_idx.ctypes.data, self.u_val.ctypes.data,
-                            self.row_perm.ctypes.data)
+        self._fn["get"](h, self.l_col_ptr.ctypes.data, self.l_row_idx.ctypes.data, self.l_val.ctypes.data,
+                        self.u_col_ptr.ctypes.data, self.u_row_idx.ctypes.data, self.u_val.ctypes.data,
+                        self.row_perm.ctypes.data)
         self.nnz_l, self.nnz_u = nl.value, nu.value
 
     def solve(self, b) -> np.ndarray:
-        x = np.array(b, dtype=np.float64, copy=True)
-        _lib().oracle_splu_solve(self.h, x.ctypes.data)
+        x = np.array(b, dtype=np.complex128 if self.complex else np.float64, copy=True)
+        self._fn["solve"](self.h, x.ctypes.data)
         return x
 
     def flops_estimate(self) -> int:
@@ -82,7 +93,7 @@ class Factors:
 
     def __del__(self):
         if getattr(self, "h", None):
-            _lib().oracle_splu_free(self.h)
+            self._fn["free"](self.h)
             self.h = None
 
 

@@ -364,3 +364,68 @@ def test_accuracy_on_lapack_random_matrices(oracle_sparse, case, n):
             res = np.max(np.abs(A @ x - b)) / (anorm * np.max(np.abs(x)) + np.max(np.abs(b)))
             assert err <= 1e-9 * cond, (name, n, cond, err)
             assert res <= 1e-13 * cond, (name, n, cond, res)
+
+
+def _complex_factors(osp, cp, ri, v, method):
+    lu = SparseLu.analyze(cp, ri, method)
+    sym = lu.symbolic()
+    snp = sym["supernode_ptr"] if lu.effective_method() == "Supernodal" else None
+    return osp.Factors(len(cp) - 1, cp, ri, np.asarray(v, dtype=np.complex128), sym["col_perm"],
+                       sym["col_perm_inv"], snp)
+
+
+def test_complex_oracle_pins(oracle_sparse):
+    """SparseLu<Complex64> restated (the same loops over num-complex
+    arithmetic): sparse_lu.rs:279-295, supernodal_lu.rs:763-805 and
+    accuracy_tests.rs:120-150."""
+    # sparse_lu.rs:279-295: [4 1; 1 3] as complex values, Auto
+    for method in (LuMethod.auto(), LuMethod.supernodal(), LuMethod.simplicial()):
+        f = _complex_factors(oracle_sparse, COL_PTR, ROW_IDX, [4, 1, 1, 3], method)
+        x = f.solve([1.0, 2.0])
+        assert np.all(np.abs(x - np.array([1 / 11, 7 / 11])) < 1e-14)
+    # supernodal_lu.rs:763-805: tridiagonal, diagonal 6 + i, off-diagonals 0.5 - 0.25 i
+    n = 12
+    cp, ri = [0], []
+    for j in range(n):
+        ri.extend(sorted({j, max(j - 1, 0), min(j + 1, n - 1)}))
+        cp.append(len(ri))
+    v = np.array([6 + 1j if ri[k] == j else 0.5 - 0.25j for j in range(n) for k in range(cp[j], cp[j + 1])])
+    x_true = np.arange(n) + 1.0 - 0.5j
+    b = np.zeros(n, dtype=np.complex128)
+    for j in range(n):
+        for k in range(cp[j], cp[j + 1]):
+            b[ri[k]] += v[k] * x_true[j]
+    for method in (LuMethod.supernodal(), LuMethod.simplicial()):
+        x = _complex_factors(oracle_sparse, cp, ri, v, method).solve(b)
+        assert np.all(np.abs(x - x_true) < 1e-12)
+    # accuracy_tests.rs:120-150: A = Re + 0.25 i Im from two DLATMS matrices, n = 8
+    n = 8
+    _, re, _, _ = oracle_sparse.dense.dlatms_general("Uniform", 3, 1e2, 1.0, n, n, [11, 22, 33, 44])
+    _, im, _, _ = oracle_sparse.dense.dlatms_general("Uniform", 3, 1e2, 1.0, n, n, [55, 66, 77, 88])
+    a = re + 0.25j * im
+    x_exact = np.array([complex(1.0 + i % 5, -0.5) for i in range(n)])
+    b = a.reshape(n, n).T @ x_exact
+    cp = list(range(0, n * n + 1, n))
+    ri = [i for _ in range(n) for i in range(n)]
+    for method in (LuMethod.auto(), LuMethod.supernodal(), LuMethod.simplicial()):
+        x = _complex_factors(oracle_sparse, cp, ri, a, method).solve(b)
+        err = np.max(np.abs(x - x_exact)) / np.max(np.abs(x_exact))
+        assert err < 1e-9, err
+
+
+def test_complex_oracle_on_real_values_follows_the_real_oracle(oracle_sparse):
+    """With zero imaginary parts the complex restatement takes the real one's
+    pivots and structure and keeps every imaginary part zero; its values agree
+    to rounding only, since num-complex's reciprocal is re / (re^2 + im^2),
+    not 1 / re."""
+    cp, ri, kind = oracle_sparse.grid_pattern(7, 6, 5)
+    v, _ = oracle_sparse.convection_diffusion_values(kind, [2, 4, 6, 9])
+    n = len(cp) - 1
+    sym = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
+    for snp in (sym["supernode_ptr"], None):
+        fr = oracle_sparse.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], snp)
+        fz = oracle_sparse.Factors(n, cp, ri, v.astype(np.complex128), sym["col_perm"], sym["col_perm_inv"], snp)
+        assert np.array_equal(fr.row_perm, fz.row_perm) and fr.nnz_l == fz.nnz_l and fr.nnz_u == fz.nnz_u
+        np.testing.assert_allclose(fz.l_val[:fz.nnz_l].real, fr.l_val[:fr.nnz_l], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(fz.u_val[:fz.nnz_u].real, fr.u_val[:fr.nnz_u], rtol=1e-12, atol=1e-15)
+        assert not np.any(fz.l_val[:fz.nnz_l].imag) and not np.any(fz.u_val[:fz.nnz_u].imag)
