@@ -78,7 +78,10 @@ SIGNATURES = [
     ("alg_batch_solve_graph", _I, [_P, _P, _P, _P]),
     ("alg_batch_autotune", _I, [_P, _P, _P, _P, _P, _P, _P]),
     ("alg_batch_info", _I, [_P, _P, _P, _P, _P, _P]),
+    ("alg_batch_panels", _I, [_P, _P]),
+    ("alg_batch_set_config", _I, [_P, _I, _I, _I]),
     ("alg_batch_eta", _I, [_P, _P]),
+    ("alg_batch_ipiv", _I, [_P, _P]),
     ("alg_batch_destroy", None, [_P]),
     ("alg_gemm_tc_sub_dev", _I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I]),
     ("alg_gemm_dmma_sub_dev", _I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I]),

@@ -8,6 +8,8 @@ float64 CUDA tensors at the offsets the plan reports.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import pathlib
 
 import numpy as np
 import torch
@@ -27,6 +29,7 @@ class BatchPlan:
         self.ctx = ctx
         self.orders = np.asarray(orders, dtype=np.int32)
         self.count = int(self.orders.size)
+        self.mixed = bool(mixed)
         h = C.c_void_p()
         _check(self._lib.alg_batch_create(ctx.handle, self.count, self.orders.ctypes.data, 1 if mixed else 0,
                                           C.byref(h)))
@@ -53,11 +56,38 @@ class BatchPlan:
         fn = self._lib.alg_batch_solve_graph if graph else self._lib.alg_batch_solve
         _check(fn(self.handle, a.data_ptr(), b.data_ptr(), info.data_ptr()))
 
-    def autotune(self, a, b, info, a_src, b_src):
-        out = np.zeros(8, dtype=np.int32)
+    def autotune(self, a, b, info, a_src, b_src, cache: str | None = None) -> dict:
+        """Picks each size bucket's launch shape (CTA size x panel width) by
+        timing them on this batch (a, b are scratch: restored from a_src,
+        b_src before every trial). With `cache` (a JSON file), shapes already
+        chosen for the same bucket (its cap, the form and the device name) are
+        reused without timing, and new choices are added to the file."""
+        key = None
+        entries = {}
+        if cache:
+            path = pathlib.Path(cache)
+            if path.exists():
+                entries = json.loads(path.read_text())
+            dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "none"
+            key = lambda cap: f"{dev}|{'mixed' if self.mixed else 'fp64'}|cap{cap}"  # noqa: E731
+            buckets = self.info()["buckets"]
+            if all(key(bk["cap"]) in entries for bk in buckets):
+                for i, bk in enumerate(buckets):
+                    e = entries[key(bk["cap"])]
+                    _check(self._lib.alg_batch_set_config(self.handle, i, int(e["threads"]), int(e["panel"])))
+                out = self.info()
+                out["tuned"] = "cache"
+                return out
+        th = np.zeros(8, dtype=np.int32)
         _check(self._lib.alg_batch_autotune(self.handle, a.data_ptr(), b.data_ptr(), info.data_ptr(),
-                                            a_src.data_ptr(), b_src.data_ptr(), out.ctypes.data))
-        return self.info()
+                                            a_src.data_ptr(), b_src.data_ptr(), th.ctypes.data))
+        out = self.info()
+        out["tuned"] = "timed"
+        if key is not None:
+            for bk in out["buckets"]:
+                entries[key(bk["cap"])] = {"threads": bk["threads"], "panel": bk["panel"]}
+            pathlib.Path(cache).write_text(json.dumps(entries, indent=1, sort_keys=True) + "\n")
+        return out
 
     def info(self) -> dict:
         nb = C.c_int()
@@ -68,10 +98,18 @@ class BatchPlan:
         _check(self._lib.alg_batch_info(self.handle, C.byref(nb), caps.ctypes.data, thr.ctypes.data,
                                         cnt.ctypes.data, C.byref(fl)))
         k = nb.value
-        return {"buckets": [{"cap": int(caps[i]), "threads": int(thr[i]), "count": int(cnt[i])} for i in range(k)],
-                "flops": fl.value}
+        pan = np.zeros(8, dtype=np.int32)
+        _check(self._lib.alg_batch_panels(self.handle, pan.ctypes.data))
+        return {"buckets": [{"cap": int(caps[i]), "threads": int(thr[i]), "panel": int(pan[i]), "count": int(cnt[i])}
+                            for i in range(k)], "flops": fl.value}
 
     def eta(self) -> np.ndarray:
         out = np.zeros(max(self.count, 1))
         _check(self._lib.alg_batch_eta(self.handle, out.ctypes.data))
         return out[: self.count]
+
+    def ipiv(self) -> np.ndarray:
+        """Pivots of the last solve (0-based pivot rows), packed at the b offsets."""
+        out = np.zeros(max(self.b_total, 1), dtype=np.int32)
+        _check(self._lib.alg_batch_ipiv(self.handle, out.ctypes.data))
+        return out[: self.b_total]

@@ -6,10 +6,10 @@
 // multipliers by division, then the forward/back sweeps. A CTA pulls systems
 // from a queue ordered by decreasing order n (largest first, for balance) and
 // factorizes each one in place in its global buffer with a right-looking
-// blocked schedule: a kPB-column panel factored in shared memory, its row
+// blocked schedule: a 16- or 32-column panel factored in shared memory, its row
 // interchanges applied to the other columns by one gather, U12 by a
-// row-block triangular solve, and the trailing update in 64 x 64 tiles staged
-// through shared memory. The mixed form factorizes an FP32 copy and refines
+// row-block triangular solve, and the trailing update in 64 x 64 tiles (U12
+// staged in shared memory, a register micro-tile per thread). The mixed form factorizes an FP32 copy and refines
 // x in FP64 against the FP64 matrix until the system's normwise backward
 // error is within tol.
 #include <algorithm>
@@ -21,6 +21,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <math_constants.h>
 
 #include "batched.cuh"
@@ -28,9 +30,9 @@
 namespace alg {
 namespace {
 
-constexpr int kPB = 32;       // panel width
 constexpr int kMaxN = 512;    // largest order a CTA handles
 constexpr int kT = 64;        // trailing-update tile
+constexpr int kTR = 4;        // rows of a thread's micro-tile in the trailing update
 
 template <typename T>
 __device__ __forceinline__ T fma_t(T a, T b, T c);
@@ -72,11 +74,12 @@ __device__ int block_argmax(double key, int idx, double* red_k, int* red_i) {
 // in place; ipiv (global, n ints); returns 0 or 1 + the first singular column.
 // Shared memory of cta_getrf for panels of up to `cap` rows.
 template <typename T>
-__host__ __device__ constexpr size_t getrf_smem(int cap) {
-  return sizeof(T) * ((size_t)cap * kPB + 2 * kPB * kT) + 32 * 8 + 32 * 4 + (4 * kPB + 4) * 4;
+__host__ __device__ constexpr size_t getrf_smem(int cap, int pb) {
+  return sizeof(T) * ((size_t)cap * pb + 2 * pb * kT) + 32 * 8 + 32 * 4 + (4 * pb + 4) * 4;
 }
 
-template <typename T>
+// NT: threads of the CTA; kPB: panel width (16 or 32, the autotuner's choice).
+template <typename T, int NT, int kPB>
 __device__ int cta_getrf(T* a, int n, int* ipiv, unsigned char* smem, int cap) {
   const int kMaxN = cap;                                   // panel stride (rows)
   T* panel = reinterpret_cast<T*>(smem);                   // cap x kPB, [col][row]
@@ -200,18 +203,44 @@ __device__ int cta_getrf(T* a, int n, int* ipiv, unsigned char* smem, int cap) {
           if (kk < w) ut[c * kPB + kk] = c < cw ? a[(size_t)(k0 + kk) + (size_t)(c0 + c) * n] : T(0);
         }
         __syncthreads();
+        // register micro-tile per thread: kTR rows (tr + 16 i) x kTC columns
+        // (tc + kCG j) of the 64 x 64 tile; each entry's terms are still
+        // accumulated in increasing kk, one fused multiply-add each
+        constexpr int kRG = kT / kTR, kCG = NT / kRG, kTC = kT / kCG;
+        static_assert(kRG * kCG == NT && kCG * kTC == kT, "micro-tile covers the tile");
+        const int tr = threadIdx.x % kRG, tc = threadIdx.x / kRG;
         for (int ti = 0; ti < tiles; ++ti) {
           const int r0 = kr + ti * kT, rw = min(kT, n - r0);
-          // each thread: rows r, columns c, c + step, ...
-          for (int e = threadIdx.x; e < kT * kT; e += blockDim.x) {
-            const int r = e % kT, c = e / kT;
-            if (r < rw && c < cw) {
-              const T* lrow = panel + (r0 - k0 + r);
-              T acc = a[(size_t)(r0 + r) + (size_t)(c0 + c) * n];
-              for (int kk = 0; kk < w; ++kk) acc = fma_t<T>(-lrow[kk * kMaxN], ut[c * kPB + kk], acc);
-              a[(size_t)(r0 + r) + (size_t)(c0 + c) * n] = acc;
+          T acc[kTR][kTC];
+#pragma unroll
+          for (int i = 0; i < kTR; ++i)
+#pragma unroll
+            for (int j = 0; j < kTC; ++j) {
+              const int r = tr + kRG * i, c = tc + kCG * j;
+              acc[i][j] = (r < rw && c < cw) ? a[(size_t)(r0 + r) + (size_t)(c0 + c) * n] : T(0);
             }
+          const T* lcol = panel + (r0 - k0);
+          for (int kk = 0; kk < w; ++kk) {
+            T l[kTR], u[kTC];
+#pragma unroll
+            for (int i = 0; i < kTR; ++i) {
+              const int r = tr + kRG * i;
+              l[i] = r < rw ? lcol[kk * kMaxN + r] : T(0);
+            }
+#pragma unroll
+            for (int j = 0; j < kTC; ++j) u[j] = ut[(tc + kCG * j) * kPB + kk];
+#pragma unroll
+            for (int i = 0; i < kTR; ++i)
+#pragma unroll
+              for (int j = 0; j < kTC; ++j) acc[i][j] = fma_t<T>(-l[i], u[j], acc[i][j]);
           }
+#pragma unroll
+          for (int i = 0; i < kTR; ++i)
+#pragma unroll
+            for (int j = 0; j < kTC; ++j) {
+              const int r = tr + kRG * i, c = tc + kCG * j;
+              if (r < rw && c < cw) a[(size_t)(r0 + r) + (size_t)(c0 + c) * n] = acc[i][j];
+            }
         }
         __syncthreads();
       }
@@ -315,7 +344,7 @@ struct BatchArgs {
   double tol_scale;        // tol = tol_scale * n * 2^-53
 };
 
-template <int NT>
+template <int NT, int PB>
 __global__ void __launch_bounds__(NT) batched_gesv_kernel(BatchArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int next;
@@ -334,7 +363,7 @@ __global__ void __launch_bounds__(NT) batched_gesv_kernel(BatchArgs p) {
     double* b = p.b + p.b_off[s];
     int* ipiv = p.ipiv + p.b_off[s];
     if (!p.mixed) {
-      const int info = cta_getrf<double>(a, n, ipiv, lus, p.cap);
+      const int info = cta_getrf<double, NT, PB>(a, n, ipiv, lus, p.cap);
       if (threadIdx.x == 0) p.info[s] = info;
       if (info == 0) cta_getrs<double, double>(a, n, ipiv, b, vs);
       continue;
@@ -343,7 +372,7 @@ __global__ void __launch_bounds__(NT) batched_gesv_kernel(BatchArgs p) {
     float* a32 = p.a32 + p.a_off[s];
     for (size_t e = threadIdx.x; e < (size_t)n * n; e += NT) a32[e] = __double2float_rn(a[e]);
     __syncthreads();
-    const int info = cta_getrf<float>(a32, n, ipiv, lus, p.cap);
+    const int info = cta_getrf<float, NT, PB>(a32, n, ipiv, lus, p.cap);
     if (info != 0) {
       if (threadIdx.x == 0) p.info[s] = info;
       continue;
@@ -376,29 +405,31 @@ __global__ void __launch_bounds__(NT) batched_gesv_kernel(BatchArgs p) {
   }
 }
 
-size_t kernel_smem(int cap, bool mixed) {
-  const size_t g = mixed ? getrf_smem<float>(cap) : getrf_smem<double>(cap);
+size_t kernel_smem(int cap, bool mixed, int pb) {
+  const size_t g = mixed ? getrf_smem<float>(cap, pb) : getrf_smem<double>(cap, pb);
   return sizeof(double) * (size_t)cap + std::max(g, sizeof(double) * (size_t)cap) + 64;
+}
+// one limit for every bucket sharing an instantiation: the largest any asks for
+size_t kernel_smem_max() {
+  return std::max(kernel_smem(kMaxN, false, 32), kernel_smem(kMaxN, true, 32));
 }
 
 // Host-side configuration (not stream work, so never inside a graph capture).
-template <int NT>
+template <int NT, int PB>
 int configure_bucket(alg_ctx* ctx, int cap, bool mixed, int count, int* grid) {
-  const size_t smem = kernel_smem(cap, mixed);
-  // one limit for every bucket sharing this instantiation: the largest any asks for
-  const size_t smem_max = std::max(kernel_smem(kMaxN, false), kernel_smem(kMaxN, true));
-  ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_max));
+  const size_t smem = kernel_smem(cap, mixed, PB);
+  ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<NT, PB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kernel_smem_max()));
   int per_sm = 0;
-  ALG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_gesv_kernel<NT>, NT, smem));
+  ALG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_gesv_kernel<NT, PB>, NT, smem));
   *grid = std::max(1, std::min(std::max(1, per_sm) * ctx->sm_count, count));
   return ALG_OK;
 }
 
-template <int NT>
+template <int NT, int PB>
 int launch_bucket(alg_ctx* ctx, const BatchArgs& p, int grid) {
-  const size_t smem = kernel_smem(p.cap, p.mixed != 0);
-  batched_gesv_kernel<NT><<<grid, NT, smem, ctx->stream>>>(p);
+  const size_t smem = kernel_smem(p.cap, p.mixed != 0, PB);
+  batched_gesv_kernel<NT, PB><<<grid, NT, smem, ctx->stream>>>(p);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
@@ -426,18 +457,28 @@ int batch_launch_bucket(alg_ctx* ctx, const BatchSpec& sp, const BucketLaunch& b
   p.max_ir = sp.max_ir > 0 ? sp.max_ir : 10;
   p.tol_scale = sp.tol_scale > 0 ? sp.tol_scale : 10.0;
   ALG_CUDA_TRY(cudaMemsetAsync(bl.d_queue, 0, sizeof(int), ctx->stream));
+  const bool narrow = bl.panel == 16;
   switch (bl.threads) {
-    case 128: return launch_bucket<128>(ctx, p, bl.grid);
-    case 512: return launch_bucket<512>(ctx, p, bl.grid);
-    default: return launch_bucket<256>(ctx, p, bl.grid);
+    case 128: return narrow ? launch_bucket<128, 16>(ctx, p, bl.grid) : launch_bucket<128, 32>(ctx, p, bl.grid);
+    case 512: return narrow ? launch_bucket<512, 16>(ctx, p, bl.grid) : launch_bucket<512, 32>(ctx, p, bl.grid);
+    default: return narrow ? launch_bucket<256, 16>(ctx, p, bl.grid) : launch_bucket<256, 32>(ctx, p, bl.grid);
   }
 }
 
 int batch_configure_bucket(alg_ctx* ctx, bool mixed, BucketLaunch* bl) {
+  if (bl->panel != 16) bl->panel = 32;
+  const bool narrow = bl->panel == 16;
   switch (bl->threads) {
-    case 128: return configure_bucket<128>(ctx, bl->cap, mixed, bl->count, &bl->grid);
-    case 512: return configure_bucket<512>(ctx, bl->cap, mixed, bl->count, &bl->grid);
-    default: return configure_bucket<256>(ctx, bl->cap, mixed, bl->count, &bl->grid);
+    case 128:
+      return narrow ? configure_bucket<128, 16>(ctx, bl->cap, mixed, bl->count, &bl->grid)
+                    : configure_bucket<128, 32>(ctx, bl->cap, mixed, bl->count, &bl->grid);
+    case 512:
+      return narrow ? configure_bucket<512, 16>(ctx, bl->cap, mixed, bl->count, &bl->grid)
+                    : configure_bucket<512, 32>(ctx, bl->cap, mixed, bl->count, &bl->grid);
+    default:
+      bl->threads = 256;
+      return narrow ? configure_bucket<256, 16>(ctx, bl->cap, mixed, bl->count, &bl->grid)
+                    : configure_bucket<256, 32>(ctx, bl->cap, mixed, bl->count, &bl->grid);
   }
 }
 
@@ -632,8 +673,11 @@ int alg_batch_solve_graph(alg_batch* b, double* d_a, double* d_b, int* d_info) {
   return ALG_OK;
 }
 
-// Tries 128 / 256 / 512 threads per CTA for each bucket on the given batch
-// (which it solves several times: pass scratch copies) and keeps the fastest.
+// Tries every launch shape for each bucket on the given batch (which it
+// solves several times: pass scratch copies) and keeps the fastest: 128 / 256
+// / 512 threads per CTA (with the trailing update's micro-tile 4 x 8, 4 x 4
+// or 4 x 2 per thread) times a 16- or 32-column panel (the split between the
+// column-serial panel and the register-tiled update).
 int alg_batch_autotune(alg_batch* b, double* d_a, double* d_b, int* d_info, const double* d_a_src,
                        const double* d_b_src, int* threads_out) {
   if (b == nullptr) return ALG_INVALID_ARGUMENT;
@@ -657,10 +701,12 @@ int alg_batch_autotune(alg_batch* b, double* d_a, double* d_b, int* d_info, cons
   for (size_t k = 0; k < b->buckets.size(); ++k) {
     auto& bl = b->buckets[k];
     float best = 1e30f;
-    int best_t = bl.threads;
-    for (int t : {128, 256, 512}) {
+    int best_t = bl.threads, best_p = bl.panel;
+    for (int cfg = 0; cfg < 6; ++cfg) {
+      const int t = 128 << (cfg >> 1), pb = (cfg & 1) ? 32 : 16;
       alg::BucketLaunch trial = bl;
       trial.threads = t;
+      trial.panel = pb;
       ALG_TRY(alg::batch_configure_bucket(ctx, b->mixed != 0, &trial));
       for (int rep = 0; rep < 2; ++rep) {
         ALG_CUDA_TRY(cudaMemcpyAsync(d_a, d_a_src, 8 * (size_t)b->a_total, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -674,10 +720,12 @@ int alg_batch_autotune(alg_batch* b, double* d_a, double* d_b, int* d_info, cons
         if (rep == 1 && ms < best) {
           best = ms;
           best_t = t;
+          best_p = pb;
         }
       }
     }
     bl.threads = best_t;
+    bl.panel = best_p;
     ALG_TRY(alg::batch_configure_bucket(ctx, b->mixed != 0, &bl));
     if (threads_out) threads_out[k] = best_t;
   }
@@ -702,9 +750,37 @@ int alg_batch_info(const alg_batch* b, int* n_buckets, int* caps, int* threads, 
   return ALG_OK;
 }
 
+int alg_batch_panels(const alg_batch* b, int* panels) {
+  if (b == nullptr || panels == nullptr) return ALG_INVALID_ARGUMENT;
+  for (size_t k = 0; k < b->buckets.size(); ++k) panels[k] = b->buckets[k].panel;
+  return ALG_OK;
+}
+
+int alg_batch_set_config(alg_batch* b, int bucket, int threads, int panel) {
+  if (b == nullptr || bucket < 0 || bucket >= (int)b->buckets.size()) return ALG_INVALID_ARGUMENT;
+  if ((threads != 128 && threads != 256 && threads != 512) || (panel != 16 && panel != 32))
+    return ALG_INVALID_ARGUMENT;
+  alg::BucketLaunch& bl = b->buckets[bucket];
+  bl.threads = threads;
+  bl.panel = panel;
+  ALG_TRY(alg::batch_configure_bucket(b->ctx, b->mixed != 0, &bl));
+  if (b->graph) {  // the captured launches used the old shape
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return ALG_OK;
+}
+
 int alg_batch_eta(const alg_batch* b, double* eta_host) {
   if (b == nullptr || eta_host == nullptr) return ALG_INVALID_ARGUMENT;
   ALG_CUDA_TRY(cudaMemcpy(eta_host, b->d_eta, sizeof(double) * b->count, cudaMemcpyDeviceToHost));
+  return ALG_OK;
+}
+
+int alg_batch_ipiv(const alg_batch* b, int* ipiv_host) {
+  if (b == nullptr || ipiv_host == nullptr) return ALG_INVALID_ARGUMENT;
+  if (b->b_total == 0) return ALG_OK;
+  ALG_CUDA_TRY(cudaMemcpy(ipiv_host, b->d_ipiv, sizeof(int) * b->b_total, cudaMemcpyDeviceToHost));
   return ALG_OK;
 }
 
@@ -729,11 +805,12 @@ void alg_batch_destroy(alg_batch* b) {
 // batched kernel above (FP32 LU with partial pivoting, FP64 refinement) on
 // one system, and takes its working memory (the FP32 copy of A, the residual
 // vector, the work counter) from the file-scope array below instead of from
-// an allocation. Set-up per device (the array's address and the kernel's
-// shared-memory limit) is host-side work done by the first call on that
-// device. Every call on a device shares the one array, so calls that overlap
-// on the GPU (different streams, or different host threads) race on it;
-// calls on one stream are ordered and safe.
+// an allocation. Set-up per device (the array's address, the kernels' load
+// and the shared-memory limit) is host-side work done by the first call in
+// each CUDA context; a call with n = 0 does only the set-up. Every call on a
+// device shares the one array, so calls that overlap on the GPU (different
+// streams, or different host threads) race on it; calls on one stream are
+// ordered and safe.
 namespace alg {
 namespace {
 
@@ -774,24 +851,61 @@ __global__ void noalloc_header_kernel(NoAllocHeader* h, int n) {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
+// Per device: the array's address and the unique id (cuCtxGetId) of the CUDA
+// context it was looked up in. A __device__ symbol's address belongs to one
+// context; after cudaDeviceReset, or when the caller makes another context
+// current, the id differs and the set-up runs again.
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kNoAllocMaxDevices] = {};
 
-// Per-device set-up (host side, not stream work), with `dev` current: the
-// scratch array's device address and the dynamic shared-memory limit of each
-// kernel instantiation used below.
+// The two driver calls are reached through the runtime's entry-point table,
+// so the library does not link libcuda (it stays loadable on hosts without
+// a driver, where every call reports ALG_NO_DEVICE).
+int current_context_id(unsigned long long* id) {
+  static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  if (get_current == nullptr || get_id == nullptr) {
+    cudaDriverEntryPointQueryResult q1, q2;
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      cudaGetLastError();
+      return ALG_CUDA_ERROR;
+    }
+    get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f1);
+    get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f2);
+  }
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS || c == nullptr) return ALG_CUDA_ERROR;
+  if (get_id(c, id) != CUDA_SUCCESS) return ALG_CUDA_ERROR;
+  return ALG_OK;
+}
+
+// Set-up (host side, not stream work), with `dev` current. cudaGetSymbolAddress
+// loads this file's module if lazy loading (the CUDA 12 default) has not
+// yet, which is when the static array comes into being on the device; the
+// kernels are loaded here too (cudaFuncGetAttributes / cudaFuncSetAttribute),
+// so no later call loads code or data.
 int noalloc_setup(int dev, unsigned char** out) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (g_noalloc_ptr[dev] == nullptr) {
+  unsigned long long id = 0;
+  if (g_noalloc_ptr[dev] == nullptr || current_context_id(&id) != ALG_OK || id != g_noalloc_ctx[dev]) {
     void* p = nullptr;
-    ALG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    const size_t smem_max = std::max(kernel_smem(kMaxN, false), kernel_smem(kMaxN, true));
-    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_max));
-    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_max));
-    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_max));
+    ALG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));  // also makes the primary context current
+    ALG_TRY(current_context_id(&id));
+    cudaFuncAttributes fa;
+    ALG_CUDA_TRY(cudaFuncGetAttributes(&fa, noalloc_header_kernel));
+    const int smem_max = (int)kernel_smem_max();
+    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<128, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem_max));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<256, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem_max));
+    ALG_CUDA_TRY(cudaFuncSetAttribute(batched_gesv_kernel<512, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem_max));
     g_noalloc_ptr[dev] = p;
+    g_noalloc_ctx[dev] = id;
   }
   *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
   return ALG_OK;
@@ -799,7 +913,7 @@ int noalloc_setup(int dev, unsigned char** out) {
 
 template <int NT>
 int noalloc_launch(cudaStream_t s, const BatchArgs& p) {
-  batched_gesv_kernel<NT><<<1, NT, kernel_smem(p.cap, true), s>>>(p);
+  batched_gesv_kernel<NT, 32><<<1, NT, kernel_smem(p.cap, true, 32), s>>>(p);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   return ALG_OK;
@@ -817,8 +931,7 @@ extern "C" int alg_dgesv_mixed_noalloc(void* stream, const double* d_a, double* 
                    kNoAllocMaxN);
     return ALG_BAD_SHAPE;
   }
-  if (n == 0) return ALG_OK;
-  if (d_a == nullptr || d_b == nullptr || d_info == nullptr) return ALG_INVALID_ARGUMENT;
+  if (n > 0 && (d_a == nullptr || d_b == nullptr || d_info == nullptr)) return ALG_INVALID_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -829,6 +942,7 @@ extern "C" int alg_dgesv_mixed_noalloc(void* stream, const double* d_a, double* 
   if (dev < 0 || dev >= kNoAllocMaxDevices) return ALG_INVALID_ARGUMENT;
   unsigned char* base = nullptr;
   ALG_TRY(noalloc_setup(dev, &base));
+  if (n == 0) return ALG_OK;  // the set-up call: nothing is queued
   auto* hdr = reinterpret_cast<NoAllocHeader*>(base + kNoAllocA32 + kNoAllocWork + kNoAllocIpiv);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the size bucket and CTA size a one-system plan of this order uses

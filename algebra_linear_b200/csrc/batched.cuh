@@ -27,6 +27,7 @@ struct BucketLaunch {
   int count = 0;
   int cap = 0;          // largest order in the bucket
   int threads = 256;    // CTA size chosen by the autotuner
+  int panel = 32;       // panel width (16 or 32) chosen by the autotuner
   int grid = 1;         // persistent CTAs (resident on the device at once)
   const int* d_order = nullptr;
   int* d_queue = nullptr;

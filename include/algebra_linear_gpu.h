@@ -285,14 +285,23 @@ int alg_batch_solve(alg_batch* batch, double* d_a, double* d_b, int* d_info);
 /* The same launch sequence captured once in a CUDA graph (per buffer set) and
  * replayed; the capturing call solves the batch too. */
 int alg_batch_solve_graph(alg_batch* batch, double* d_a, double* d_b, int* d_info);
-/* Autotuner: times 128/256/512 threads per CTA for every size bucket on this
- * batch (restoring the inputs from d_a_src/d_b_src before each trial) and
- * keeps the fastest; threads_out (may be NULL) receives one value per bucket. */
+/* Autotuner: for every size bucket, times each launch shape on this batch
+ * (restoring the inputs from d_a_src/d_b_src before each trial): 128, 256 or
+ * 512 threads per CTA (the trailing update's register micro-tile 4 x 8, 4 x 4
+ * or 4 x 2 per thread) times a 16- or 32-column panel, and keeps the fastest;
+ * threads_out (may be NULL) receives one value per bucket, alg_batch_panels
+ * the panel widths. Shapes from an earlier run can be set directly with
+ * alg_batch_set_config (host-side; not inside a stream capture). */
 int alg_batch_autotune(alg_batch* batch, double* d_a, double* d_b, int* d_info, const double* d_a_src,
                        const double* d_b_src, int* threads_out);
 int alg_batch_info(const alg_batch* batch, int* n_buckets, int* caps, int* threads, int* counts,
                    double* flops);
+int alg_batch_panels(const alg_batch* batch, int* panels);
+int alg_batch_set_config(alg_batch* batch, int bucket, int threads, int panel);
 int alg_batch_eta(const alg_batch* batch, double* eta_host);
+/* Copies the pivots of the last solve (0-based pivot rows of each system's
+ * LU, FP64 or FP32, at the b offsets) to ipiv_host (sum of the orders ints). */
+int alg_batch_ipiv(const alg_batch* batch, int* ipiv_host);
 void alg_batch_destroy(alg_batch* batch);
 
 /* The tensor-core trailing update of the low-precision LU on device buffers:
@@ -481,23 +490,35 @@ void alg_server_destroy(alg_server* server);
  * d_b (n) becomes x; *d_info receives 0, 1 + the first zero pivot's column,
  * or -(iterations + 1) when refinement missed the target. d_ipiv (n ints,
  * the FP32 LU's 0-based pivot rows) and d_eta (the backward error) may be
- * NULL. All pointers are device pointers; the work is queued on `stream` (a
- * cudaStream_t; NULL is the default stream) and the call returns without
- * synchronising.
+ * NULL. When *d_info > 0 (a zero pivot) neither d_b nor *d_eta is written.
+ * All pointers are device pointers; the work is queued on `stream` (a
+ * cudaStream_t of the current context; NULL is the default stream) and the
+ * call returns without synchronising.
  *
- * Working memory: one static device array of ALG_NOALLOC_SCRATCH_BYTES,
- * which every GPU that loads the library holds until exit (the FP32 copy of
- * A, a residual vector, pivots, a work counter). n > ALG_NOALLOC_MAX_N (or
- * n < 0) returns ALG_BAD_SHAPE and queues nothing; n = 0 returns ALG_OK.
+ * Set-up: a call with n = 0 (the pointers are then ignored and may be NULL)
+ * queues nothing and only does the host-side set-up for the current device
+ * and CUDA context: it loads the library's device code for this entry point,
+ * looks up the static array's device address and sets the kernel's
+ * shared-memory limit. It returns ALG_OK, or ALG_NO_DEVICE without a GPU.
+ * The first call with n > 0 does the same set-up if no call has done it yet
+ * in the current context. Make the set-up call at start-up, before any
+ * stream capture: it is the only call that can meet out-of-memory.
+ *
+ * Working memory: one static device array of ALG_NOALLOC_SCRATCH_BYTES (the
+ * FP32 copy of A, a residual vector, pivots, a work counter). It comes into
+ * being on a device when the library's device code is loaded there: at the
+ * set-up call under CUDA's default lazy module loading, or when the context
+ * is created under CUDA_MODULE_LOADING=EAGER. From then on that GPU holds it
+ * until the context is destroyed (process exit or cudaDeviceReset); after a
+ * reset, or in another context, the next call repeats the set-up. Do not
+ * pass a stream of one context while another is current.
+ * n > ALG_NOALLOC_MAX_N (or n < 0) returns ALG_BAD_SHAPE and queues nothing.
  * The array keeps the previous call's contents; the work counter must be 0
  * when the kernel starts, and each call resets it itself, in stream order,
  * so the caller clears nothing. All calls on one device share the array:
  * calls that overlap on the GPU (on different streams, or from different
  * host threads without ordering) race on it and give wrong results; calls
- * queued on one stream are safe. The first call on each device does
- * host-side set-up (looks up the array's device address and sets the
- * kernel's shared-memory limit); make that first call before beginning any
- * stream capture. */
+ * queued on one stream are safe. */
 #define ALG_NOALLOC_MAX_N 512
 #define ALG_NOALLOC_SCRATCH_BYTES 1054976
 int alg_dgesv_mixed_noalloc(void* stream, const double* d_a, double* d_b, int n, int* d_ipiv, int* d_info,

@@ -5,9 +5,11 @@ pool, serving loops that must not synchronise the device, callers that must
 not meet out-of-memory after start-up): it runs the mixed form of the
 batched dgesv kernel on one system with its working memory in a static
 device array. On the GPU it must agree bit for bit with a one-system
-alg_batch plan (mixed = 1) on the same input, call after call while the
-static array is reused. This file is named to be collected last, so the
-calls also run after everything the other test files left on the device."""
+alg_batch plan (mixed = 1) on the same input (solution, backward error and
+pivots), call after call while the static array is reused, and the device's
+free memory must not change across the calls after the first. This file is
+named to be collected last, so the calls also run after everything the other
+test files left on the device."""
 
 import ctypes as C
 
@@ -30,8 +32,9 @@ def test_noalloc_rejects_orders_beyond_its_scratch():
     lib = _lib.load()
     assert lib.alg_dgesv_mixed_noalloc(None, None, None, MAX_N + 1, None, None, None) == _lib.BAD_SHAPE
     assert lib.alg_dgesv_mixed_noalloc(None, None, None, -1, None, None, None) == _lib.BAD_SHAPE
-    assert lib.alg_dgesv_mixed_noalloc(None, None, None, 0, None, None, None) == _lib.OK
     assert lib.alg_dgesv_mixed_noalloc(None, None, None, 4, None, None, None) == _lib.INVALID_ARGUMENT
+    # n = 0 is the set-up call: Ok on a GPU, no-device without one
+    assert lib.alg_dgesv_mixed_noalloc(None, None, None, 0, None, None, None) in (_lib.OK, _lib.NO_DEVICE)
 
 
 def _batched_reference(ctx, a, b, n):
@@ -46,7 +49,7 @@ def _batched_reference(ctx, a, b, n):
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
     plan.solve(A, B, info)
     torch.cuda.synchronize()
-    out = B.cpu().numpy(), int(info.cpu()[0]), float(plan.eta()[0])
+    out = B.cpu().numpy(), int(info.cpu()[0]), float(plan.eta()[0]), plan.ipiv().copy()
     plan.close()
     return out
 
@@ -58,30 +61,40 @@ def test_noalloc_matches_the_batched_entry_point_call_after_call(gpu, oracle):
     from algebra_linear_b200 import _lib, device
 
     lib = gpu
+    assert lib.alg_dgesv_mixed_noalloc(None, None, None, 0, None, None, None) == _lib.OK  # set-up call
     orders = [300, 512, 37]  # the second call reuses the array at full size, the third after it
-    results = []
+    # every device buffer of the three calls exists before the first, so that
+    # nothing but the entry point could change the device's free memory
+    calls = []
     for k, n in enumerate(orders):
         a, b = _system(oracle, n, seed=5 + k)
-        A = torch.from_numpy(a.copy()).cuda()
-        B = torch.from_numpy(b.copy()).cuda()
-        ipiv = torch.full((n,), -1, dtype=torch.int32, device="cuda")
-        info = torch.full((1,), 99, dtype=torch.int32, device="cuda")
-        eta = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
-        stream = torch.cuda.current_stream().cuda_stream
+        calls.append((n, a, b, torch.from_numpy(a.copy()).cuda(), torch.from_numpy(b.copy()).cuda(),
+                      torch.full((n,), -1, dtype=torch.int32, device="cuda"),
+                      torch.full((1,), 99, dtype=torch.int32, device="cuda"),
+                      torch.full((1,), -1.0, dtype=torch.float64, device="cuda")))
+    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    free_after = []
+    for n, a, b, A, B, ipiv, info, eta in calls:
         rc = lib.alg_dgesv_mixed_noalloc(C.c_void_p(stream), A.data_ptr(), B.data_ptr(), n, ipiv.data_ptr(),
                                          info.data_ptr(), eta.data_ptr())
         assert rc == _lib.OK, _lib.status_string(rc)
         torch.cuda.synchronize()
-        results.append((n, a, b, B.cpu().numpy(), int(info.cpu()[0]), float(eta.cpu()[0]), ipiv.cpu().numpy()))
+        free_after.append(torch.cuda.mem_get_info()[0])
+    # calls 2 and 3 allocated nothing on the device
+    assert free_after[1] == free_after[0] and free_after[2] == free_after[0], free_after
+    results = [(n, a, b, B.cpu().numpy(), int(info.cpu()[0]), float(eta.cpu()[0]), ipiv.cpu().numpy())
+               for n, a, b, A, B, ipiv, info, eta in calls]
+    for n, a, b, A, *_ in calls:
         assert np.array_equal(A.cpu().numpy(), a)  # A is only read
     with device.Context() as ctx:
         for n, a, b, x, info, eta, ipiv in results:
-            xr, info_r, eta_r = _batched_reference(ctx, a, b, n)
+            xr, info_r, eta_r, ipiv_r = _batched_reference(ctx, a, b, n)
             assert info == info_r == 0, (n, info, info_r)
             assert np.array_equal(x, xr), n
             assert eta == eta_r, (n, eta, eta_r)
+            assert np.array_equal(ipiv, ipiv_r), n
             assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53
-            assert np.all(ipiv >= np.arange(n)) and ipiv.max() < n  # row k's pivot comes from rows k..n-1
 
 
 @pytest.mark.gpu
@@ -97,9 +110,13 @@ def test_noalloc_reports_a_zero_pivot_like_the_batched_entry_point(gpu, oracle):
     A = torch.from_numpy(a.copy()).cuda()
     B = torch.from_numpy(b.copy()).cuda()
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
-    rc = lib.alg_dgesv_mixed_noalloc(None, A.data_ptr(), B.data_ptr(), n, None, info.data_ptr(), None)
+    eta = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    rc = lib.alg_dgesv_mixed_noalloc(None, A.data_ptr(), B.data_ptr(), n, None, info.data_ptr(), eta.data_ptr())
     assert rc == _lib.OK
     torch.cuda.synchronize()
     with device.Context() as ctx:
-        _, info_r, _ = _batched_reference(ctx, a, b, n)
+        _, info_r, _, _ = _batched_reference(ctx, a, b, n)
     assert int(info.cpu()[0]) == info_r > 0
+    # on a zero pivot neither b nor the backward error is written
+    assert float(eta.cpu()[0]) == -1.0
+    assert np.array_equal(B.cpu().numpy(), b)
