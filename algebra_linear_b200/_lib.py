@@ -63,6 +63,8 @@ SIGNATURES = [
     ("alg_ctx_create", _I, [_P, C.POINTER(_P)]),
     ("alg_ctx_destroy", None, [_P]),
     ("alg_ctx_set_stream", _I, [_P, _P]),
+    ("alg_ctx_set_wait_limit", _I, [_P, C.c_ulonglong]),
+    ("alg_ctx_inject_stuck_wait", _I, [_P, _I]),
     ("alg_dgetrf_dev", _I, [_P, _I, _P, _I, _I, _P, _P]),
     ("alg_dgetrf_rect_dev", _I, [_P, _I, _P, _I, _I, _I, _P]),
     ("alg_dgetrs_dev", _I, [_P, _P, _I, _I, _P, _P, _I, _I]),

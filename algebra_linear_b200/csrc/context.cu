@@ -249,6 +249,18 @@ void alg_ctx_destroy(alg_ctx* ctx) {
   delete ctx;
 }
 
+int alg_ctx_set_wait_limit(alg_ctx* ctx, unsigned long long limit_ns) {
+  if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
+  ctx->wait_limit_ns = limit_ns;
+  return ALG_OK;
+}
+
+int alg_ctx_inject_stuck_wait(alg_ctx* ctx, int count) {
+  if (ctx == nullptr || count < 0) return ALG_INVALID_ARGUMENT;
+  ctx->stuck_waits = count;
+  return ALG_OK;
+}
+
 int alg_ctx_set_stream(alg_ctx* ctx, void* cuda_stream) {
   if (ctx == nullptr) return ALG_INVALID_ARGUMENT;
   if (ctx->own_stream && ctx->stream) {

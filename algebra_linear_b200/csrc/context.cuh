@@ -61,6 +61,11 @@ struct alg_ctx {
   // low-priority one for the rest of each trailing update (created on use)
   cudaStream_t la_stream[2] = {nullptr, nullptr};
   cudaEvent_t la_event[4] = {nullptr, nullptr, nullptr, nullptr};
+  // bounded device waits of the dataflow solves: the limit (alg_ctx_set_wait_limit)
+  // and the number of coming solves whose first block waits on a flag that
+  // nothing sets (alg_ctx_inject_stuck_wait: tests of the timeout path)
+  unsigned long long wait_limit_ns = 0;  // 0: the library default (2 s)
+  int stuck_waits = 0;
 };
 
 namespace alg {

@@ -212,6 +212,16 @@ bool dmma_disabled() {
   return off;
 }
 
+// ALG_GEMM_WIDE=1: the CUDA-core update's former 128 x 128 tiles (one CTA
+// per SM) instead of 128 x 64 tiles two to an SM (for comparison).
+bool gemm_wide_tiles() {
+  static const bool v = [] {
+    const char* e = std::getenv("ALG_GEMM_WIDE");
+    return e != nullptr && e[0] == '1';
+  }();
+  return v;
+}
+
 template <typename T, bool EXACT>
 int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T* B, int ldb,
                  T* C, int ldc) {
@@ -220,9 +230,14 @@ int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T
     // the fused FP64 form runs on the FP64 tensor cores
     if (!dmma_disabled()) return gemm_dmma_sub_dev(ctx, M, N, K, A, lda, B, ldb, C, ldc);
   }
-  dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + kGemmBN - 1) / kGemmBN);
   const int tok = prof_begin(ctx, ALG_K_GEMM);
-  gemm_sub_kernel<T, EXACT><<<grid, kGemmThreads, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  if (gemm_wide_tiles()) {
+    dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + 127) / 128);
+    gemm_sub_kernel<T, EXACT, 128><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  } else {
+    dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + 63) / 64);
+    gemm_sub_kernel<T, EXACT, 64><<<grid, 128, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  }
   count_launches();
   prof_end(ctx, tok, 2.0 * M * N * K, sizeof(T) * (2.0 * M * N + double(M) * K + double(K) * N));
   ALG_CUDA_TRY(cudaGetLastError());
@@ -490,6 +505,7 @@ int host_lu(int update, double* a, size_t m, size_t nc, size_t* ipiv, double* de
   const bool singular = ctx->h_status->singular_col != INT_MAX;
   if (!singular && d_b) {
     ALG_TRY(solve_any(ctx, update, d_a, M, M, d_perm, d_b, R, M));
+    ALG_TRY(alg::status_fetch(ctx));  // a timed-out sweep is an error, not a result
     ALG_CUDA_TRY(cudaMemcpyAsync(b, d_b, sizeof(double) * m * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
   }
   ALG_CUDA_TRY(cudaMemcpyAsync(a, d_a, sizeof(double) * m * nc, cudaMemcpyDeviceToHost, ctx->stream));
@@ -678,9 +694,9 @@ int alg_dgetrs_dev(alg_ctx* ctx, const double* d_lu, int n, int lda, const int32
                    double* d_b, int nrhs, int ldb) {
   if (ctx == nullptr || d_perm == nullptr) return ALG_INVALID_ARGUMENT;
   if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n)) return ALG_BAD_SHAPE;
+  ALG_TRY(alg::status_reset(ctx));
   ALG_TRY(solve_any(ctx, ALG_UPDATE_EXACT, d_lu, n, lda, d_perm, d_b, nrhs, ldb));
-  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return ALG_OK;
+  return alg::status_fetch(ctx);  // synchronises; reports a timed-out sweep
 }
 
 int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda, double* d_b, int nrhs,
@@ -698,8 +714,7 @@ int alg_dgesv_dev(alg_ctx* ctx, int update, double* d_a, int n, int lda, double*
   ALG_TRY(alg::status_fetch(ctx));
   if (ctx->h_status->singular_col != INT_MAX) return ALG_SINGULAR;
   ALG_TRY(solve_any(ctx, update, d_a, n, lda, perm, d_b, nrhs, ldb));
-  ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return ALG_OK;
+  return alg::status_fetch(ctx);  // synchronises; reports a timed-out sweep
 }
 
 }  // extern "C"

@@ -961,21 +961,25 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T*
 // column-major. Each thread owns an 8 x 8 block of C in registers, loads it
 // once, applies the K terms in increasing k (EXACT: rounded product then
 // rounded difference, the reference's per-entry sequence), and stores it once.
-// 128 x 128 CTA tile, K staged through shared memory 8 at a time with
+// 128 x BN CTA tile (BN = 128: 256 threads, one CTA per SM; BN = 64: 128
+// threads, two CTAs per SM, so one tile's C load and store overlap the
+// other's arithmetic), K staged through shared memory 8 at a time with
 // register double buffering. Out-of-range A rows / B columns / k are zero,
 // which leaves every in-range entry unchanged bit for bit (x - 0*0 = x).
 // ---------------------------------------------------------------------------
-constexpr int kGemmBM = 128, kGemmBN = 128, kGemmBK = 8, kGemmThreads = 256;
+constexpr int kGemmBM = 128, kGemmBK = 8;
 
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kGemmThreads, 1) gemm_sub_kernel(
+template <typename T, bool EXACT, int BN>
+__global__ void __launch_bounds__(2 * BN, BN == 64 ? 2 : 1) gemm_sub_kernel(
     int M, int N, int K, const T* __restrict__ A, int lda, const T* __restrict__ B, int ldb,
     T* __restrict__ Cm, int ldc) {
+  constexpr int kThreads = 2 * BN, kHalf = BN / 2, kAPer = kGemmBK * kGemmBM / kThreads,
+                kBPer = kGemmBK * BN / kThreads;
   __shared__ __align__(16) T As[2][kGemmBK][kGemmBM];
-  __shared__ __align__(16) T Bs[2][kGemmBK][kGemmBN + 2];
+  __shared__ __align__(16) T Bs[2][kGemmBK][BN + 2];
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
-  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * kGemmBN;
+  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
 
   T acc[8][8];
 #pragma unroll
@@ -983,21 +987,25 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_sub_kernel(
     const int mi = m0 + (r >> 2) * 64 + tx * 4 + (r & 3);
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      const int nj = n0 + (c >> 2) * 64 + ty * 4 + (c & 3);
+      const int nj = n0 + (c >> 2) * kHalf + ty * 4 + (c & 3);
       acc[r][c] = (mi < M && nj < N) ? Cm[(size_t)mi + (size_t)nj * ldc] : T(0);
     }
   }
 
-  // loader mapping: A chunk is kGemmBK x 128 (k-major in smem): 4 per thread
-  // B chunk is kGemmBK x 128: 4 per thread
-  T ra[4], rb[4];
+  // loader mapping: the A chunk is kGemmBK x 128 (k-major in smem), the B
+  // chunk kGemmBK x BN
+  T ra[kAPer], rb[kBPer];
   auto load_chunk = [&](int k0) {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int idx = tid + t * kGemmThreads;
+    for (int t = 0; t < kAPer; ++t) {
+      const int idx = tid + t * kThreads;
       const int mm = idx & 127, kk = idx >> 7;
       const int gm = m0 + mm, gk = k0 + kk;
       ra[t] = (gm < M && gk < K) ? A[(size_t)gm + (size_t)gk * lda] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < kBPer; ++t) {
+      const int idx = tid + t * kThreads;
       const int bk = idx & 7, bn = idx >> 3;
       const int gn = n0 + bn, gk2 = k0 + bk;
       rb[t] = (gn < N && gk2 < K) ? B[(size_t)gk2 + (size_t)gn * ldb] : T(0);
@@ -1005,9 +1013,13 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_sub_kernel(
   };
   auto store_chunk = [&](int buf) {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int idx = tid + t * kGemmThreads;
+    for (int t = 0; t < kAPer; ++t) {
+      const int idx = tid + t * kThreads;
       As[buf][idx >> 7][idx & 127] = ra[t];
+    }
+#pragma unroll
+    for (int t = 0; t < kBPer; ++t) {
+      const int idx = tid + t * kThreads;
       Bs[buf][idx & 7][idx >> 3] = rb[t];
     }
   };
@@ -1027,7 +1039,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_sub_kernel(
 #pragma unroll
       for (int r = 0; r < 8; ++r) af[r] = As[buf][kk][(r >> 2) * 64 + tx * 4 + (r & 3)];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) bf[c] = Bs[buf][kk][(c >> 2) * 64 + ty * 4 + (c & 3)];
+      for (int c = 0; c < 8; ++c) bf[c] = Bs[buf][kk][(c >> 2) * kHalf + ty * 4 + (c & 3)];
 #pragma unroll
       for (int r = 0; r < 8; ++r)
 #pragma unroll
@@ -1042,7 +1054,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_sub_kernel(
     const int mi = m0 + (r >> 2) * 64 + tx * 4 + (r & 3);
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      const int nj = n0 + (c >> 2) * 64 + ty * 4 + (c & 3);
+      const int nj = n0 + (c >> 2) * kHalf + ty * 4 + (c & 3);
       if (mi < M && nj < N) Cm[(size_t)mi + (size_t)nj * ldc] = acc[r][c];
     }
   }

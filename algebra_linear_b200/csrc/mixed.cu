@@ -424,7 +424,7 @@ int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, i
   if (converged) {
     ALG_CUDA_TRY(cudaMemcpy2DAsync(d_b, sizeof(double) * ldb, x, sizeof(double) * n, sizeof(double) * n, nrhs,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
-    ALG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ALG_TRY(status_fetch(ctx));  // synchronises; a timed-out sweep of the refinement is an error
     if (R.path != ALG_MIXED_PATH_GMRES) R.path = ALG_MIXED_PATH_IR;
     return ALG_OK;
   }

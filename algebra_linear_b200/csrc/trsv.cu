@@ -62,10 +62,35 @@ __device__ __forceinline__ void prefetch_tile(T* tile, const T* lu, int lda, int
   }
 }
 
+// Thread 0's bounded wait for a block's ready flag: 1 when it is set, 0 when
+// another CTA aborted or the limit ran out (then this CTA raises the abort
+// flag and the status block's timeout, so every CTA of the launch returns).
+__device__ __forceinline__ int wait_ready(const int* flag, int* abort_flag, DevStatus* status, uint64_t limit_ns) {
+  uint64_t t0 = 0;
+  for (int it = 0;; ++it) {
+    if (ld_acquire(flag) != 0) return 1;
+    if (ld_acquire(abort_flag) != 0) return 0;
+    if ((it & 255) == 0) {
+      const uint64_t now = global_timer_ns();
+      if (it == 0) {
+        t0 = now;
+      } else if (now - t0 > limit_ns) {
+        atomicExch(abort_flag, 1);
+        atomicExch(&status->timeout, 1);
+        return 0;
+      }
+    }
+  }
+}
+
+// stuck_wait != 0: the CTA of the sweep's first block waits on flags[nb], a
+// slot cleared before the launch that nothing sets, so the wait runs out
+// (the timeout path, exercised by tests without any fault).
 template <typename T, bool EXACT, bool UPPER>
 __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __restrict__ lu, int lda, int n, T* x,
                                                                   int ldx, int nrhs, int* flags, int* abort_flag,
-                                                                  DevStatus* status) {
+                                                                  DevStatus* status, uint64_t wait_limit_ns,
+                                                                  int stuck_wait) {
   extern __shared__ __align__(16) unsigned char tsm[];
   T* tiles = reinterpret_cast<T*>(tsm);                 // [2][kTB*kTB] factor tiles, [col][row]
   T* dtile = tiles + 2 * kTB * kTB;                      // diagonal block, [col][row]
@@ -77,6 +102,11 @@ __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __res
   const int nb = (n + kTB - 1) / kTB;
   const int r = threadIdx.x & (kTB - 1);  // row within the block
   const int qt = threadIdx.x >> 6;        // column quarter
+  if (stuck_wait && blockIdx.x == 0) {
+    if (threadIdx.x == 0) stop = !wait_ready(&flags[nb], abort_flag, status, wait_limit_ns);
+    __syncthreads();
+    if (stop) return;
+  }
   for (int s = blockIdx.x; s < nb; s += gridDim.x) {
     // sweep position s -> block index (forward: ascending, backward: descending)
     const int bi = UPPER ? nb - 1 - s : s;
@@ -133,24 +163,7 @@ __global__ void __launch_bounds__(kTThreads) trsv_dataflow_kernel(const T* __res
       }
       cp_async_commit();
       // wait for block bj (bounded); a failure anywhere stops every CTA
-      if (threadIdx.x == 0) {
-        int ok = 0;
-        uint64_t t0 = 0;
-        for (int it = 0;; ++it) {
-          if (ld_acquire(&flags[bj]) != 0) { ok = 1; break; }
-          if (ld_acquire(abort_flag) != 0) break;
-          if ((it & 255) == 0) {
-            const uint64_t now = global_timer_ns();
-            if (it == 0) t0 = now;
-            else if (now - t0 > kWaitLimitNs) {
-              atomicExch(abort_flag, 1);
-              atomicExch(&status->timeout, 1);
-              break;
-            }
-          }
-        }
-        stop = !ok;
-      }
+      if (threadIdx.x == 0) stop = !wait_ready(&flags[bj], abort_flag, status, wait_limit_ns);
       __syncthreads();
       if (stop) {
         cp_async_wait<0>();
@@ -251,8 +264,14 @@ int launch_trsv(alg_ctx* ctx, const T* lu, int lda, int n, T* x, int ldx, int nr
   }
   int grid = std::min(nb, max_blocks);
   ALG_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int) * (nb + 1), ctx->stream));
+  uint64_t limit = ctx->wait_limit_ns ? ctx->wait_limit_ns : kWaitLimitNs;
+  int stuck = 0;
+  if (ctx->stuck_waits > 0) {
+    --ctx->stuck_waits;
+    stuck = 1;
+  }
   void* args[] = {(void*)&lu, (void*)&lda, (void*)&n, (void*)&x, (void*)&ldx, (void*)&nrhs,
-                  (void*)&flags, (void*)&abort_flag, (void*)&ctx->d_status};
+                  (void*)&flags, (void*)&abort_flag, (void*)&ctx->d_status, (void*)&limit, (void*)&stuck};
   ALG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)trsv_dataflow_kernel<T, EXACT, UPPER>, dim3(grid),
                                            dim3(kTThreads), args, kTSmem<T>, ctx->stream));
   count_launches();

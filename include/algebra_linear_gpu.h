@@ -154,6 +154,17 @@ int alg_ctx_create(void* cuda_stream, alg_ctx** out);
 void alg_ctx_destroy(alg_ctx* ctx);
 /* Rebinds the stream (e.g. to the caller framework's current stream). */
 int alg_ctx_set_stream(alg_ctx* ctx, void* cuda_stream);
+/* Every device-side wait of the triangular solves (the dataflow sweeps of
+ * alg_dgetrs_dev, alg_dgesv_dev, the host drop-ins and the mixed form's
+ * refinement) gives up after limit_ns nanoseconds (0: the default, 2 s):
+ * the kernel raises an abort flag, every CTA returns, and the call reports
+ * ALG_TIMEOUT; the context stays usable. No counterpart in the reference. */
+int alg_ctx_set_wait_limit(alg_ctx* ctx, unsigned long long limit_ns);
+/* Failure injection for tests of that path (no counterpart in the
+ * reference): the next `count` triangular sweeps on this context start with
+ * a wait on a flag that nothing sets, so the wait runs out after the limit
+ * and the call reports ALG_TIMEOUT; nothing faults or hangs. */
+int alg_ctx_inject_stuck_wait(alg_ctx* ctx, int count);
 
 /* In-place LU of the n x n device matrix d_a (leading dimension lda >= n).
  * d_ipiv: n int32, LAPACK-style sequential interchanges (0-based).

@@ -196,3 +196,57 @@ def test_tournament_single_launch_matches_level_launches(gpu, oracle, monkeypatc
             assert rep["tournament"] and rep["path"] == "ir", rep
             xs.append(B.cpu().numpy())
     assert np.array_equal(xs[0], xs[1])
+
+
+def _c2_system(ctx, n, nrhs, seed):
+    """The dense workload at a C2 order, generated on the device by the
+    reference's DLARNV stream: A iid U(-1,1) (no shift), x_true continuing
+    the stream, b = A x_true."""
+    A, s = ctx.larnv(2, seed, n * n)
+    xt, _ = ctx.larnv(2, s, n * nrhs)
+    b = (A.view(n, n).t() @ xt.view(nrhs, n).t()).t().contiguous().view(-1)
+    return A.clone(), b
+
+
+def _eta(A, x, b, n, nrhs):
+    Am = A.view(n, n).t()
+    X, B = x.view(nrhs, n).t(), b.view(nrhs, n).t()
+    r = (B - Am @ X).abs().amax(dim=0)
+    den = Am.abs().sum(dim=1).max() * X.abs().amax(dim=0) + B.abs().amax(dim=0)
+    return float((r / den).max())
+
+
+@pytest.mark.parametrize("nrhs", [1, 64])
+def test_c2_order_mixed_forms_reach_fp64_backward_error(gpu, nrhs):
+    """C2 at n = 8192: the TF32x3 and FP32 mixed forms (tournament pivoting,
+    FP64 refinement) reach eta <= 10 n 2^-53, and their x agrees with the
+    FP64 solution of the bit-exact GPU form (which reproduces the oracle's
+    LU bit for bit, tests/test_dense_gpu.py) to within cond_inf(A) times
+    that backward error. The FP64 refinement path, not the fallback, must
+    deliver it."""
+    import torch
+
+    from algebra_linear_b200 import _lib, device, mixed
+
+    n = 8192
+    tol = 10 * n * 2.0**-53
+    with device.Context() as ctx:
+        A0, b0 = _c2_system(ctx, n, nrhs, [1988, 1989, 1990, 1991])
+        A, x64 = A0.clone(), b0.clone()
+        ctx.dgesv(A, x64, n, nrhs, update=_lib.UPDATE_EXACT)
+        del A
+        eta64 = _eta(A0, x64, b0, n, nrhs)
+        assert eta64 <= tol, eta64
+        Am = A0.view(n, n).t()
+        cond = float(Am.abs().sum(dim=1).max() * torch.linalg.inv(Am).abs().sum(dim=1).max())
+        for prec in ("tf32x3", "fp32"):
+            x = b0.clone()
+            rep = mixed.dgesv_mixed_dev(ctx, A0, x, n, nrhs, precision=prec, no_fallback=True)
+            assert rep["path"] in ("ir", "gmres") and rep["tournament"], (prec, rep)
+            eta = _eta(A0, x, b0, n, nrhs)
+            assert eta <= tol, (prec, eta, rep)
+            X, X64 = x.view(nrhs, n), x64.view(nrhs, n)
+            fwd = float(((X - X64).abs().amax(dim=1) / X64.abs().amax(dim=1)).max())
+            assert fwd <= 2 * cond * tol, (prec, fwd, cond)
+            print(f"n={n} nrhs={nrhs} {prec}: eta {eta:.2e} (fp64 exact {eta64:.2e}), forward error vs the "
+                  f"FP64 solution {fwd:.2e}, cond_inf {cond:.3g}, {rep}")

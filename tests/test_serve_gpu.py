@@ -84,3 +84,32 @@ def test_admission_respects_the_budget(gpu, oracle):
     for (s0, e0), (s1, e1) in zip(spans, spans[1:]):
         assert s1 >= e0  # no two were admitted at once
     assert all(r.status == 0 for r in reqs)
+
+
+def test_reported_backward_error_matches_the_host(gpu, oracle):
+    """A mixed dense request reports the refinement's final normwise
+    backward error; it must agree with the error of the returned x computed
+    on the host (within a factor of 4: the residual is summed in another
+    order) and be within 10 n 2^-53. Plain FP64 requests report -1."""
+    from algebra_linear_b200.serve import Request, Server
+
+    reqs, systems = [], []
+    for k, n in enumerate([64, 257, 1000, 3000]):
+        a, b = _dense_system(oracle, n, 60 + k)
+        systems.append((a, b, n))
+        reqs.append(Request.dense(a, b, mixed=True))
+    reqs.append(Request.dense(*_dense_system(oracle, 100, 70), mixed=False))
+    with Server(workers=2, hbm_budget=8 << 30, max_dense_n=3000) as srv:
+        for r in reqs:
+            srv.submit(r)
+        srv.drain()
+    assert all(r.status == 0 for r in reqs)
+    assert reqs[-1].backward_error == -1.0
+    for r, (a, b, n) in zip(reqs, systems):
+        host = oracle.backward_error(a, r.solution, b, n)
+        rep = r.backward_error
+        print(f"n={n}: reported eta {rep:.3e}, host eta {host:.3e}")
+        assert host <= 10 * n * 2.0**-53, (n, host)
+        assert rep <= 10 * n * 2.0**-53, (n, rep)
+        if host > 0:
+            assert host / 4 <= rep <= 4 * host, (n, rep, host)
