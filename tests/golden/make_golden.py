@@ -142,7 +142,9 @@ def extract_dlatms(src: str) -> dict:
 
 
 def main() -> None:
-    root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/algebra_linear")
+    root = pathlib.Path(sys.argv[1])
     fam = (root / "src/lapack/families.rs").read_text()
     out = HERE / "larnv_kat.json"
     out.write_text(json.dumps(extract_larnv(fam), indent=1) + "\n")
