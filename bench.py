@@ -60,7 +60,6 @@ def parse_args():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--forms", default="")
-    ap.add_argument("--cpu-n", type=int, default=1024, help="order of the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["dense", "sparse", "serve", "batched"], default="dense",
@@ -431,24 +430,19 @@ class _OneCore:
         return {"cpu_model": _cpu_model(), "pinned_core": self.core}
 
 
-def cpu_baseline(n_cpu: int, reps: int = 3):
-    """The oracle (C++ restatement of lapack::dgesv, mod.rs:309-354) on one
-    host core, dgesv at order n_cpu, median of reps."""
-    from oracle import dense as oracle
-
-    a, _, b = oracle.c1_system(n_cpu)
-    ts = []
+def cpu_baseline(n: int, cols: int = 2):
+    """The reference's path on this workload on one host core: `cols`
+    leading columns of its kij LU on the full n x n matrix (ReferenceSample)."""
     with _OneCore() as pin:
-        for _ in range(reps):
-            aw, bw = a.copy(), b.copy()
-            t0 = time.perf_counter()
-            rc, _ = oracle.dgesv(aw, bw, n_cpu)
-            ts.append(time.perf_counter() - t0)
-            assert rc == 0
-    t = statistics.median(ts)
-    return {"value": flops_dgesv(n_cpu, 1) / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
-            "sample": f"dgesv n={n_cpu}, 1 RHS, same larnv workload, median of {reps} "
-                      f"({t:.2f} s each); the reference path is single-threaded", **pin.info()}
+        ref = ReferenceSample(n)
+        t, fl = 0.0, 0.0
+        for _ in range(cols):
+            dt, f = ref.columns(1)
+            t += dt
+            fl += f
+    return {"value": fl / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
+            "sample": f"the first {cols} columns of the reference's kij LU loop on the n={n} matrix of the "
+                      f"workload ({t:.1f} s); the reference path is single-threaded", **pin.info()}
 
 
 
@@ -964,33 +958,74 @@ def run_serve(args, world, rank, local, pg):
     lu.close()
 
 # --------------------------------------------------------------------------- arms
+def dense_config(n: int, nrhs: int, world: int) -> dict:
+    """The workload both arms report (the same dict, so they compare)."""
+    return {"workload": f"dense dgesv n={n}, {nrhs} RHS, A iid U(-1,1) no shift, b = A x_true",
+            "n": n, "nrhs": nrhs, "parallelism": f"replicas x{world}",
+            "l2": "inputs (8 n^2 B) larger than L2; no flush"}
+
+
+class ReferenceSample:
+    """The reference's dgesv path on this workload, timed in bounded samples:
+    the oracle's restatement of dgetrf_with_pivots (mod.rs:112-163) run on
+    the full n x n matrix of the workload (generated by the same DLARNV
+    stream), some columns of the kij loop per sample, continuing where the
+    previous sample stopped. A whole factorization at n = 16384 would take
+    hours on one core (each column's rank-1 update streams the trailing
+    matrix with the reference's stride-n inner loop), so its rate is measured
+    on its leading columns, which carry the most work per column. GFLOP/s
+    counts the loop's divisions, multiplies and subtractions."""
+
+    def __init__(self, n: int, seed=SEEDY):
+        import numpy as np
+
+        from oracle import dense as oracle
+
+        self.oracle = oracle
+        self.n = n
+        self.a, _ = oracle.larnv("Symmetric", list(seed), n * n)
+        self.ipiv = np.zeros(n, dtype=np.uint64)
+        self.k = 0
+
+    def columns(self, cols: int):
+        """Runs the next `cols` columns; returns (seconds, flops)."""
+        n, k0 = self.n, self.k
+        k1 = min(n, k0 + cols)
+        t0 = time.perf_counter()
+        rc = self.oracle.dgetrf_range(self.a, n, k0, k1, self.ipiv)
+        dt = time.perf_counter() - t0
+        assert rc == 0
+        self.k = k1
+        fl = sum(float(n - k - 1) * (1.0 + 2.0 * (n - k - 1)) for k in range(k0, k1))
+        return dt, fl
+
+
 def run_reference(args, world, rank, pg):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", "1")
-    from oracle import dense as oracle
-
-    n_cpu = args.cpu_n
-    a, _, b = oracle.c1_system(n_cpu)
+    n, nrhs = args.n, args.nrhs
     with _OneCore() as pin:
+        ref = ReferenceSample(n)
         for _ in range(args.warmup):
-            oracle.dgesv(a.copy(), b.copy(), n_cpu)
-        t0 = time.perf_counter()
+            ref.columns(1)
+        t, fl = 0.0, 0.0
         for _ in range(args.steps):
-            oracle.dgesv(a.copy(), b.copy(), n_cpu)
-        dt = (time.perf_counter() - t0) / args.steps
-    v = flops_dgesv(n_cpu, 1) / dt / 1e9
+            dt, f = ref.columns(1)
+            t += dt
+            fl += f
+    v = fl / t / 1e9
+    sample = (f"one column of the reference's kij LU loop per step on the n={n} matrix of the workload "
+              f"(columns {args.warmup}..{args.warmup + args.steps - 1} timed after {args.warmup} warm-up columns; "
+              f"{t / args.steps:.1f} s each); the reference path is single-threaded and its Rust crate cannot be "
+              "built in this image, so the oracle's C++ restatement of it runs")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (larnv Symmetric, seed "
-        f"{SEEDY})",
-        "config": {"workload": f"dense dgesv, A iid U(-1,1), 1 RHS; reference CPU path sampled at n={n_cpu}",
-                   "n": n_cpu, "nrhs": 1, "parallelism": "1 host core"},
-        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": 1, "kind": "port",
-                         "sample": f"one dgesv of order {n_cpu} per step (the reference is single-threaded; "
-                                   "its Rust crate cannot be built here, so the oracle's C++ restatement runs)",
-                         **pin.info()},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic: larnv Symmetric U(-1,1) stream, seed {SEEDY} (rank r: word 4 = 1991+2r)",
+        "config": dense_config(n, nrhs, world),
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": 1, "kind": "port", "sample": sample, **pin.info()},
         "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -1039,9 +1074,8 @@ def run_ours(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "f64" if head.startswith("fp64") else "f32/" + head.split("_")[1] + "+f64",
         "data": f"synthetic: larnv Symmetric U(-1,1) stream, seed {seed} (rank r: word 4 = 1991+2r)",
-        "config": {"workload": f"dense dgesv n={n}, {nrhs} RHS, A iid U(-1,1) no shift, b = A x_true",
-                   "n": n, "nrhs": nrhs, "form": head, "parallelism": f"replicas x{world}",
-                   "l2": "inputs (8 n^2 B) larger than L2; no flush"},
+        "config": dense_config(n, nrhs, world),
+        "form": head,
         "forms": {k: {**{kk: vv for kk, vv in v.items() if kk != "profile"},
                       "kernel_ms_per_step": {c: r["ms"] for c, r in (v["profile"] or {}).items()}}
                   for k, v in results.items()},
@@ -1056,7 +1090,7 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_e2e:
         line["e2e"] = e2e_run(head, A0, b0, n, nrhs, steps=max(2, min(args.steps, 3)))
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_n)
+        line["cpu_baseline"] = cpu_baseline(n)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

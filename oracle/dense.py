@@ -33,6 +33,7 @@ def load() -> C.CDLL:
         P, SZ = C.c_void_p, C.c_size_t
         lib.oracle_larnv.argtypes = [C.c_int, P, SZ, P]
         lib.oracle_dgetrf.argtypes = [P, SZ, P, P, P]
+        lib.oracle_dgetrf_range.argtypes = [P, SZ, SZ, SZ, P]
         lib.oracle_dgetrf_rect.argtypes = [P, SZ, SZ, P]
         lib.oracle_dgetrs.argtypes = [P, P, P, SZ, SZ]
         lib.oracle_dgesv.argtypes = [P, P, SZ, SZ, P]
@@ -70,6 +71,12 @@ def dgetrf(a: np.ndarray, n: int):
     bad = np.zeros(1, dtype=np.uint64)
     rc = load().oracle_dgetrf(_p(a), n, _p(ipiv), _p(det), _p(bad))
     return rc, [int(v) for v in ipiv[:n]], float(det[0]), int(bad[0])
+
+
+def dgetrf_range(a: np.ndarray, n: int, k0: int, k1: int, ipiv: np.ndarray) -> int:
+    """Steps k0 <= k < k1 of dgetrf (mod.rs:112-163) on a (n x n, in place),
+    continuing an earlier call; ipiv: a uint64 array of n entries."""
+    return load().oracle_dgetrf_range(_p(a), n, k0, k1, _p(ipiv))
 
 
 def dgetrf_rect(a: np.ndarray, nrows: int, ncols: int):

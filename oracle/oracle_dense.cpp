@@ -120,36 +120,31 @@ void oracle_larnv(int dist, uint32_t seed[4], size_t n, double* x) {
   }
 }
 
-// mod.rs:112-163 (dgetrf_with_pivots). Unblocked right-looking LU with
-// partial pivoting; ipiv 0-based sequential interchanges; det = ±prod(u_kk).
-// On a zero pivot returns OR_SINGULAR with `a` partially factored, and
-// *bad_col (if given) names the column.
-int oracle_dgetrf(double* a, size_t n, size_t* ipiv, double* det, size_t* bad_col) {
-  if (det) *det = 1.0;
-  if (n == 0) return OR_OK;
-  double d_acc = 1.0;
-  for (size_t k = 0; k < n; ++k) {
+// mod.rs:112-163 (dgetrf_with_pivots), steps k0 <= k < k1 of the unblocked
+// right-looking LU with partial pivoting: pivot search, whole-row swap,
+// multipliers by division, rank-1 update. d_acc follows the determinant
+// (sign flip per interchange, times the pivot). Returns the first column
+// with a zero pivot, or n.
+static size_t getrf_steps(double* a, size_t n, size_t k0, size_t k1, size_t* ipiv, double* d_acc) {
+  for (size_t k = k0; k < k1; ++k) {
     size_t pivot = k;
     double best = std::fabs(a[k + k * n]);
     for (size_t i = k + 1; i < n; ++i) {
       const double cand = std::fabs(a[i + k * n]);
       if (cand > best) { best = cand; pivot = i; }
     }
-    if (best <= 0.0) {
-      if (bad_col) *bad_col = k;
-      return OR_SINGULAR;
-    }
+    if (best <= 0.0) return k;
     if (pivot != k) {
       for (size_t j = 0; j < n; ++j) {
         const double t = a[j * n + k];
         a[j * n + k] = a[j * n + pivot];
         a[j * n + pivot] = t;
       }
-      d_acc = -d_acc;
+      *d_acc = -*d_acc;
     }
     ipiv[k] = pivot;
     const double d = a[k + k * n];
-    d_acc *= d;
+    *d_acc *= d;
     for (size_t i = k + 1; i < n; ++i) {
       const double factor = a[i + k * n] / d;
       a[i + k * n] = factor;
@@ -158,8 +153,33 @@ int oracle_dgetrf(double* a, size_t n, size_t* ipiv, double* det, size_t* bad_co
       }
     }
   }
+  return n;
+}
+
+// mod.rs:112-163 (dgetrf_with_pivots). Unblocked right-looking LU with
+// partial pivoting; ipiv 0-based sequential interchanges; det = ±prod(u_kk).
+// On a zero pivot returns OR_SINGULAR with `a` partially factored, and
+// *bad_col (if given) names the column.
+int oracle_dgetrf(double* a, size_t n, size_t* ipiv, double* det, size_t* bad_col) {
+  if (det) *det = 1.0;
+  if (n == 0) return OR_OK;
+  double d_acc = 1.0;
+  const size_t bad = getrf_steps(a, n, 0, n, ipiv, &d_acc);
+  if (bad < n) {
+    if (bad_col) *bad_col = bad;
+    return OR_SINGULAR;
+  }
   if (det) *det = d_acc;
   return OR_OK;
+}
+
+// Steps k0 <= k < k1 of the same factorization, continuing where an earlier
+// call stopped (a bounded sample of a large LU for timing the reference's
+// path); OR_SINGULAR on a zero pivot.
+int oracle_dgetrf_range(double* a, size_t n, size_t k0, size_t k1, size_t* ipiv) {
+  double d_acc = 1.0;
+  if (k1 > n) k1 = n;
+  return getrf_steps(a, n, k0, k1, ipiv, &d_acc) < n ? OR_SINGULAR : OR_OK;
 }
 
 // mod.rs:202-238 (dgetrf_rect): the same loop on an nrows x ncols panel,
