@@ -271,6 +271,27 @@ int tc_reserve_sms() {
   return v;
 }
 
+// ALG_INBLOCK_TC=0: the in-block updates of the low-precision LU on the CUDA
+// cores (FP32) instead of the tensor cores (for comparison).
+bool inblock_tc_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("ALG_INBLOCK_TC");
+    return !(e != nullptr && e[0] == '0');
+  }();
+  return on;
+}
+
+// Cap of the chain's persistent tensor-core grids under the look-ahead:
+// the SMs the wide update leaves free. ALG_TC_CHAIN_CTAS overrides it (0:
+// no cap, every SM).
+int tc_chain_ctas() {
+  static const int v = [] {
+    const char* e = std::getenv("ALG_TC_CHAIN_CTAS");
+    return e ? std::max(0, std::atoi(e)) : tc_reserve_sms();
+  }();
+  return v;
+}
+
 template <typename T, bool EXACT>
 int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, int* ipiv, int* perm,
                           const LuPlan& plan) {
@@ -292,6 +313,10 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   }
   const int nb = std::max(1, plan.nb);
   const int nbl = std::max(1, std::min(plan.nbl, kPanelMaxW));
+  // persistent tensor-core grids: the wide update's cap (0: every SM) and the
+  // look-ahead chain's (its launches must fit on the SMs the wide update
+  // leaves free, or their extra CTAs wait for the wide update to retire)
+  int wide_ctas = 0, chain_ctas = 0;
 
   // the leaf panels of block [k0, k0 + kb), with their in-block updates
   auto factor_block = [&](int k0, int kb, int* lb) -> int {
@@ -323,9 +348,21 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
       const int cr = c0 + w;  // first column right of the leaf
       if (cr < k0 + kb) {
         if (!u12_done) ALG_TRY((launch_trsm<T, EXACT>(ctx, a, lda, c0, w, cr, k0 + kb)));
-        ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - cr, k0 + kb - cr, w, a + (size_t)cr + (size_t)c0 * lda, lda,
-                                        a + (size_t)c0 + (size_t)cr * lda, lda,
-                                        a + (size_t)cr + (size_t)cr * lda, lda)));
+        bool tc_done = false;
+        if constexpr (std::is_same<T, float>::value) {
+          // the in-block update on the tensor cores too when their operands
+          // keep FP32 accuracy (TF32x3; whole 128-byte K slices only)
+          if (plan.tc_prec == ALG_PREC_TF32X3 && inblock_tc_enabled() && w % 32 == 0) {
+            ALG_TRY(gemm_tc_sub_dev(ctx, plan.tc_prec, m - cr, k0 + kb - cr, w, a + (size_t)cr + (size_t)c0 * lda,
+                                    lda, a + (size_t)c0 + (size_t)cr * lda, lda, a + (size_t)cr + (size_t)cr * lda,
+                                    lda, WS_TC_CHAIN, chain_ctas));
+            tc_done = true;
+          }
+        }
+        if (!tc_done)
+          ALG_TRY((gemm_sub_dev<T, EXACT>(ctx, m - cr, k0 + kb - cr, w, a + (size_t)cr + (size_t)c0 * lda, lda,
+                                          a + (size_t)c0 + (size_t)cr * lda, lda,
+                                          a + (size_t)cr + (size_t)cr * lda, lda)));
       }
     }
     return ALG_OK;
@@ -346,7 +383,6 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   // wide: the update of the rest of the matrix (off the look-ahead chain);
   // the chain's narrow update converts its tensor-core operands in a
   // workspace of its own, since both can be in flight at once
-  int wide_ctas = 0;  // cap of the wide update's persistent grid (0: every SM)
   auto update = [&](int k0, int kb, int cb, int ce, bool wide) -> int {
     if (ce <= cb) return ALG_OK;
     const int kr = k0 + kb;
@@ -357,7 +393,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
       if (plan.tc_prec >= 0 && kb % (plan.tc_prec == ALG_PREC_BF16 ? 64 : 32) == 0)
         return gemm_tc_sub_dev(ctx, plan.tc_prec, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda,
-                               wide ? WS_KRYLOV : WS_TC_CHAIN, wide ? wide_ctas : 0);
+                               wide ? WS_KRYLOV : WS_TC_CHAIN, wide ? wide_ctas : chain_ctas);
     }
     return gemm_sub_dev<T, EXACT>(ctx, m - kr, ce - cb, kb, a + (size_t)kr + (size_t)k0 * lda, lda,
                                   a + (size_t)k0 + (size_t)cb * lda, lda, a + (size_t)kr + (size_t)cb * lda, lda);
@@ -380,6 +416,7 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   // block k to everything else; the two meet once per block.
   ALG_TRY(ctx_lookahead_streams(ctx));
   wide_ctas = std::max(1, ctx->sm_count - tc_reserve_sms());
+  chain_ctas = tc_chain_ctas();
   cudaStream_t user = ctx->stream, sa = ctx->la_stream[0], sb = ctx->la_stream[1];
   cudaEvent_t ev_a = ctx->la_event[0], ev_b = ctx->la_event[1], ev_in = ctx->la_event[2];
   ALG_CUDA_TRY(cudaEventRecord(ev_in, user));
