@@ -254,8 +254,10 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
     return;
   }
   // ---- root: winners, L11 \ U11, the top rows' original values ------------
+  __shared__ int win_s[kW];  // the winners, for the serial steps below (shared, not global, latency)
   if (step >= 0) {
     ws->win[step] = row;
+    win_s[step] = row;
 #pragma unroll
     for (int c = 0; c < W; ++c)
       if (c < w) ws->top_lu[c * kW + step] = v[c];
@@ -281,16 +283,15 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
     if (lane < w) {
       occ_top[lane] = c0 + lane;
       loc_top[lane] = lane;
-      const int gr = ws->win[lane];
-      occ_out[lane] = gr;
+      occ_out[lane] = win_s[lane];
     }
     __syncwarp();
     if (lane == 0) {
       for (int j = 0; j < w; ++j) {
-        const int gr = ws->win[j];
+        const int gr = win_s[j];
         const bool g_top = gr < c0 + w;  // candidates are rows >= c0
         const int cur = g_top ? loc_top[gr - c0] : kW + j;
-        const int pr = cur < kW ? c0 + cur : ws->win[cur - kW];
+        const int pr = cur < kW ? c0 + cur : win_s[cur - kW];
         ipiv[c0 + j] = pr;
         const int h = occ_top[j];  // the row at c0 + j goes where gr was
         occ_top[j] = gr;
@@ -305,27 +306,28 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
     }
     __syncwarp();
     // the moved rows: top positions and the below-top winners' positions
-    // whose occupant changed (a set; the apply step's order does not matter)
-    if (lane == 0) {
-      int nm = 0;
-      for (int i = 0; i < w; ++i)
-        if (occ_top[i] != c0 + i) {
-          ws->move_pos[nm] = c0 + i;
-          ws->move_src[nm] = occ_top[i];
-          ws->move_lab[nm] = first_leaf ? occ_top[i] : lab[occ_top[i]];
-          ++nm;
-        }
-      for (int j = 0; j < w; ++j) {
-        const int gr = ws->win[j];
-        if (gr >= c0 + w && occ_out[j] != gr) {
-          ws->move_pos[nm] = gr;
-          ws->move_src[nm] = occ_out[j];
-          ws->move_lab[nm] = first_leaf ? occ_out[j] : lab[occ_out[j]];
-          ++nm;
-        }
-      }
-      ws->nmoves = nm;
+    // whose occupant changed (a set; the apply step's order does not
+    // matter), one lane per position, slots by a ballot prefix count
+    const unsigned below = (1u << lane) - 1u;
+    const bool mt = lane < w && occ_top[lane] != c0 + lane;
+    const unsigned bt = __ballot_sync(0xffffffffu, mt);
+    const int nt = __popc(bt);
+    if (mt) {
+      const int slot = __popc(bt & below), src = occ_top[lane];
+      ws->move_pos[slot] = c0 + lane;
+      ws->move_src[slot] = src;
+      ws->move_lab[slot] = first_leaf ? src : lab[src];
     }
+    const int gw = lane < w ? win_s[lane] : 0;
+    const bool mo = lane < w && gw >= c0 + w && occ_out[lane] != gw;
+    const unsigned bo = __ballot_sync(0xffffffffu, mo);
+    if (mo) {
+      const int slot = nt + __popc(bo & below), src = occ_out[lane];
+      ws->move_pos[slot] = gw;
+      ws->move_src[slot] = src;
+      ws->move_lab[slot] = first_leaf ? src : lab[src];
+    }
+    if (lane == 0) ws->nmoves = nt + __popc(bo);
   }
   __syncthreads();
 }
