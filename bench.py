@@ -41,10 +41,15 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "dgesv GFLOP/s, FP64 vs mixed-precision+IR at equal backward error; p99 latency"
 SEEDY = [1988, 1989, 1990, 1991]
-# DRAM bytes per algorithmic flop of the CUDA-core trailing-update kernel, per
-# form, from ncu captures of its largest launch at n = 4096 (profiles/); a
-# form without a capture reports traffic null.
-GEMM_TRAFFIC_PER_FLOP = {}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
+# byte of a kernel class, from single-launch ncu captures at n = 8192; a
+# launch's traffic is this ratio times its algorithmic bytes (the panel:
+# 2 x 4 B x rows x 32 per leaf; the tensor-core update: 4 B x (2 M N + M K +
+# K N)), i.e. the capture scaled by the units the launch processes.
+TRAFFIC_PER_ALG_BYTE = {
+    "panel": (2.08 / 2.10, "profiles/tslu_fused_kernel_n8192.md"),
+    "gemm_tc": ((45.37 + 0.17) / 63.1, "profiles/gemm_tc_kernel_n8192.md"),
+}
 
 
 def flops_dgesv(n: int, nrhs: int) -> float:
@@ -340,11 +345,12 @@ def roofline(res, form, peaks, gemm_peaks, cls=None):
             peak, src = gemm_peaks["f64"], "cuBLAS DGEMM measured in this run"
         else:
             peak, src = gemm_peaks["f32"], "cuBLAS SGEMM (CUDA cores, TF32 off) measured in this run"
-        traffic = None
-        if cls == "gemm" and GEMM_TRAFFIC_PER_FLOP.get(form) is not None:
-            traffic = GEMM_TRAFFIC_PER_FLOP[form] * rec["flops"] / max(rec["launches"], 1)
+        traffic, tsrc = None, None
+        if cls in TRAFFIC_PER_ALG_BYTE:
+            ratio, tsrc = TRAFFIC_PER_ALG_BYTE[cls]
+            traffic = ratio * rec["bytes"] / max(rec["launches"], 1)
         return {"kernel": cls, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": src,
+                "frac": achieved / peak, "traffic": traffic, "traffic_source": tsrc, "peak_source": src,
                 "launches": rec["launches"], "avg_launch_ms": per_launch_ms, "share_of_step":
                 rec["ms"] / sum(v["ms"] for v in prof.values())}
     achieved = rec["bytes"] / rec["ms"] / 1e6  # GB/s
@@ -353,8 +359,13 @@ def roofline(res, form, peaks, gemm_peaks, cls=None):
            "frac": achieved / peak, "traffic": None, "launches": rec["launches"],
            "avg_launch_ms": per_launch_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
            else "fallback 6650", "share_of_step": rec["ms"] / sum(v["ms"] for v in prof.values())}
+    if cls in TRAFFIC_PER_ALG_BYTE and form.startswith("mixed"):
+        ratio, out["traffic_source"] = TRAFFIC_PER_ALG_BYTE[cls]
+        out["traffic"] = ratio * rec["bytes"] / max(rec["launches"], 1)
     if cls == "panel":
         out["note"] = "latency-bound column chain (pivot search per column); bytes = the panel read and written once"
+        # per column of the leaf chain: what a latency-bound panel is judged by
+        out["ns_per_column"] = 1e6 * rec["ms"] / max(rec["launches"], 1) / (32 if form.startswith("mixed") else 16)
     return out
 
 
