@@ -271,23 +271,26 @@ int tc_reserve_sms() {
   return v;
 }
 
-// ALG_INBLOCK_TC=0: the in-block updates of the low-precision LU on the CUDA
-// cores (FP32) instead of the tensor cores (for comparison).
+// ALG_INBLOCK_TC=1: the TF32x3 LU's in-block updates on the tensor cores
+// instead of the FP32 CUDA cores. Measured slower at n = 16384 (72.4 vs 70.7
+// ms per solve: the operand conversion and the persistent launch cost more
+// than the narrow K = 32 update saves), so off by default.
 bool inblock_tc_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("ALG_INBLOCK_TC");
-    return !(e != nullptr && e[0] == '0');
+    return e != nullptr && e[0] == '1';
   }();
   return on;
 }
 
-// Cap of the chain's persistent tensor-core grids under the look-ahead:
-// the SMs the wide update leaves free. ALG_TC_CHAIN_CTAS overrides it (0:
-// no cap, every SM).
+// Cap of the look-ahead chain's persistent tensor-core grids (0: none, every
+// SM). Capping them at the SMs the wide update leaves free measured no
+// better (72.4 vs 71.9 ms at n = 16384), so off by default; ALG_TC_CHAIN_CTAS
+// sets it.
 int tc_chain_ctas() {
   static const int v = [] {
     const char* e = std::getenv("ALG_TC_CHAIN_CTAS");
-    return e ? std::max(0, std::atoi(e)) : tc_reserve_sms();
+    return e ? std::max(0, std::atoi(e)) : 0;
   }();
   return v;
 }

@@ -262,9 +262,19 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
     for (int c = 0; c < W; ++c)
       if (c < w) ws->top_lu[c * kW + step] = v[c];
   }
-  for (int e = t; e < w * w; e += kRows) {
-    const int r = e % w, c = e / w;
-    ws->top_orig[c * kW + r] = a[(size_t)(c0 + r) + (size_t)(c0 + c) * lda];
+  {  // every load first, then the stores (kept in flight together)
+    constexpr int kPer = (kW * kW + kRows - 1) / kRows;
+    float tv[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = t + u * kRows;
+      tv[u] = e < w * w ? a[(size_t)(c0 + e % w) + (size_t)(c0 + e / w) * lda] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = t + u * kRows;
+      if (e < w * w) ws->top_orig[(e / w) * kW + e % w] = tv[u];
+    }
   }
   if (t == 0 && zero_col >= 0) atomicMin(&in.status->singular_col, c0 + zero_col);
   __syncthreads();
@@ -352,6 +362,7 @@ template <int W>
 __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab, int first_leaf,
                            int cta, int ncta, int side_blocks, int row_cta0, const TsluScratch* ws) {
   __shared__ float U[kW * kW];
+  __shared__ float Uinv[kW * kW];
   __shared__ int mpos[kMaxMoves], msrc[kMaxMoves], mlab[kMaxMoves];
   __shared__ int nm_s;
   if (threadIdx.x == 0) nm_s = __ldcg(&ws->nmoves);
@@ -418,6 +429,22 @@ __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int
   if (cta < row_cta0) return;
   for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = __ldcg(&ws->top_lu[e]);
   __syncthreads();
+  // U11^-1 (upper triangular, [col][k] like U), so that each row's
+  // multipliers are a product with it instead of a dependent chain of
+  // divisions: column j by back substitution in thread j
+  if (threadIdx.x < w) {
+    const int j = threadIdx.x;
+    // a zero pivot (the factorization reports it) gives zero multipliers
+    const float dj = U[j + j * kW];
+    Uinv[j + j * kW] = dj != 0.0f ? 1.0f / dj : 0.0f;
+    for (int i = j - 1; i >= 0; --i) {
+      float s = 0.0f;
+      for (int k = i + 1; k <= j; ++k) s = fmaf(U[i + k * kW], Uinv[k + j * kW], s);
+      const float di = U[i + i * kW];
+      Uinv[i + j * kW] = di != 0.0f ? -s / di : 0.0f;
+    }
+  }
+  __syncthreads();
   const int nm = nm_s;
   const int gtid = (cta - row_cta0) * blockDim.x + threadIdx.x;
   const int nth = (ncta - row_cta0) * blockDim.x;
@@ -434,19 +461,18 @@ __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int
     for (int j = 0; j < W; ++j)
       x[j] = j < w ? (from_top ? __ldcg(&ws->top_orig[j * kW + (src - c0)]) : a[(size_t)src + (size_t)(c0 + j) * lda])
                     : 0.0f;
+    // l = a U11^-1: 32 independent dot products (no division on the chain)
+    float y[W];
 #pragma unroll
     for (int j = 0; j < W; ++j) {
-      if (j < w) {
-        float s = x[j];
+      float s = 0.0f;
 #pragma unroll
-        for (int i = 0; i < j; ++i) s = fmaf(-x[i], U[i + j * kW], s);
-        const float d = U[j + j * kW];
-        x[j] = d != 0.0f ? s / d : 0.0f;
-      }
+      for (int i = 0; i <= j; ++i) s = fmaf(x[i], Uinv[i + j * kW], s);
+      y[j] = s;
     }
 #pragma unroll
     for (int j = 0; j < W; ++j)
-      if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = x[j];
+      if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = y[j];
     if (hit >= 0)
       lab[r] = mlab[hit];
     else if (first_leaf)
