@@ -192,8 +192,12 @@ struct LevelIn {
 
 // Proposals written by other CTAs are read through L2 (__ldcg): in the
 // single-launch form they were written during this launch by other SMs.
+// keep: at level 0 (src < 0), receives this thread's row's original values
+// (the single-launch form's apply step reuses them instead of reading the
+// panel again).
 template <int W>
-__device__ void level_body(const LevelIn& in, int g, int src, int nchild, int dst, bool root, TsluScratch* ws) {
+__device__ __forceinline__ void level_body(const LevelIn& in, int g, int src, int nchild, int dst, bool root,
+                                           TsluScratch* ws, float (&keep)[W]) {
   __shared__ GeppShared box;
   __shared__ int zero_col;
   __shared__ int coff[kFan + 1];
@@ -238,6 +242,10 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
   float v[W];
 #pragma unroll
   for (int c = 0; c < W; ++c) v[c] = o[c];
+  if (src < 0) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) keep[c] = o[c];
+  }
   if (t == 0) zero_col = -1;
   __syncthreads();
   const int step = block_gepp<W>(v, nr, w, box, &zero_col);
@@ -290,10 +298,16 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
     __shared__ int occ_out[kW];  // row at the original position of winner j (a winner from below)
     __shared__ int loc_top[kW];  // where the row that started at c0 + i is: i' < kW top, kW + j outside
     const int lane = t;
+    __shared__ int lab_top[kW], lab_win[kW];  // labels of the top rows and of the winners
     if (lane < w) {
       occ_top[lane] = c0 + lane;
       loc_top[lane] = lane;
       occ_out[lane] = win_s[lane];
+      // issued before the serial steps, so their latency overlaps them
+      if (!first_leaf) {
+        lab_top[lane] = lab[c0 + lane];
+        lab_win[lane] = lab[win_s[lane]];
+      }
     }
     __syncwarp();
     if (lane == 0) {
@@ -318,6 +332,14 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
     // the moved rows: top positions and the below-top winners' positions
     // whose occupant changed (a set; the apply step's order does not
     // matter), one lane per position, slots by a ballot prefix count
+    // the label of a moved row (a top row or a winner)
+    auto label_of = [&](int row) {
+      if (first_leaf) return row;
+      if (row < c0 + w) return lab_top[row - c0];
+      int k = 0;
+      while (k + 1 < w && win_s[k] != row) ++k;
+      return lab_win[k];
+    };
     const unsigned below = (1u << lane) - 1u;
     const bool mt = lane < w && occ_top[lane] != c0 + lane;
     const unsigned bt = __ballot_sync(0xffffffffu, mt);
@@ -326,7 +348,7 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
       const int slot = __popc(bt & below), src = occ_top[lane];
       ws->move_pos[slot] = c0 + lane;
       ws->move_src[slot] = src;
-      ws->move_lab[slot] = first_leaf ? src : lab[src];
+      ws->move_lab[slot] = label_of(src);
     }
     const int gw = lane < w ? win_s[lane] : 0;
     const bool mo = lane < w && gw >= c0 + w && occ_out[lane] != gw;
@@ -335,7 +357,7 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
       const int slot = nt + __popc(bo & below), src = occ_out[lane];
       ws->move_pos[slot] = gw;
       ws->move_src[slot] = src;
-      ws->move_lab[slot] = first_leaf ? src : lab[src];
+      ws->move_lab[slot] = label_of(src);
     }
     if (lane == 0) ws->nmoves = nt + __popc(bo);
   }
@@ -346,7 +368,8 @@ __device__ void level_body(const LevelIn& in, int g, int src, int nchild, int ds
 template <int W>
 __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(LevelIn in, int src, int nchild, int dst, int root,
                                                            TsluScratch* ws) {
-  level_body<W>(in, blockIdx.x, src, nchild, dst, root != 0, ws);
+  float keep[W];
+  level_body<W>(in, blockIdx.x, src, nchild, dst, root != 0, ws, keep);
 }
 
 // 3. Blocks [0, side_blocks): the block panel's other columns follow the
@@ -358,11 +381,13 @@ constexpr int kSideCols = 8;
 // CTA `cta` of `ncta`: the first side_blocks CTAs permute the block panel's
 // other columns and turn the top rows of its trailing columns into U12; rows
 // are spread over the CTAs from row_cta0 on.
+// kept (the single-launch form, one row per thread): this thread's row's
+// original values from level 0, so that only moved rows read the panel.
 template <int W>
-__device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab, int first_leaf,
-                           int cta, int ncta, int side_blocks, int row_cta0, const TsluScratch* ws) {
+__device__ __forceinline__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab,
+                                           int first_leaf, int cta, int ncta, int side_blocks, int row_cta0,
+                                           const TsluScratch* ws, const float (&kept)[W], bool use_kept) {
   __shared__ float U[kW * kW];
-  __shared__ float Uinv[kW * kW];
   __shared__ int mpos[kMaxMoves], msrc[kMaxMoves], mlab[kMaxMoves];
   __shared__ int nm_s;
   if (threadIdx.x == 0) nm_s = __ldcg(&ws->nmoves);
@@ -429,27 +454,13 @@ __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int
   if (cta < row_cta0) return;
   for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = __ldcg(&ws->top_lu[e]);
   __syncthreads();
-  // U11^-1 (upper triangular, [col][k] like U), so that each row's
-  // multipliers are a product with it instead of a dependent chain of
-  // divisions: column j by back substitution in thread j
-  if (threadIdx.x < w) {
-    const int j = threadIdx.x;
-    // a zero pivot (the factorization reports it) gives zero multipliers
-    const float dj = U[j + j * kW];
-    Uinv[j + j * kW] = dj != 0.0f ? 1.0f / dj : 0.0f;
-    for (int i = j - 1; i >= 0; --i) {
-      float s = 0.0f;
-      for (int k = i + 1; k <= j; ++k) s = fmaf(U[i + k * kW], Uinv[k + j * kW], s);
-      const float di = U[i + i * kW];
-      Uinv[i + j * kW] = di != 0.0f ? -s / di : 0.0f;
-    }
-  }
-  __syncthreads();
   const int nm = nm_s;
   const int gtid = (cta - row_cta0) * blockDim.x + threadIdx.x;
   const int nth = (ncta - row_cta0) * blockDim.x;
-  // rows below the top
-  for (int r = c0 + w + gtid; r < n; r += nth) {
+  // rows below the top (with kept values: row c0 + gtid, the row this
+  // thread held at level 0)
+  for (int r = use_kept ? c0 + gtid : c0 + w + gtid; r < n; r += nth) {
+    if (r < c0 + w) continue;  // a top row (below)
     int src = r, hit = -1;
     for (int q = 0; q < nm; ++q)
       if (mpos[q] == r) hit = q;
@@ -457,22 +468,29 @@ __device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int
     // a row below the top either stays or is a row displaced from the top
     const bool from_top = src < c0 + w;
     float x[W];
+    if (use_kept && hit < 0) {
 #pragma unroll
-    for (int j = 0; j < W; ++j)
-      x[j] = j < w ? (from_top ? __ldcg(&ws->top_orig[j * kW + (src - c0)]) : a[(size_t)src + (size_t)(c0 + j) * lda])
-                    : 0.0f;
-    // l = a U11^-1: 32 independent dot products (no division on the chain)
-    float y[W];
+      for (int j = 0; j < W; ++j) x[j] = kept[j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < W; ++j)
+        x[j] = j < w ? (from_top ? __ldcg(&ws->top_orig[j * kW + (src - c0)])
+                                 : a[(size_t)src + (size_t)(c0 + j) * lda])
+                      : 0.0f;
+    }
 #pragma unroll
     for (int j = 0; j < W; ++j) {
-      float s = 0.0f;
+      if (j < w) {
+        float s = x[j];
 #pragma unroll
-      for (int i = 0; i <= j; ++i) s = fmaf(x[i], Uinv[i + j * kW], s);
-      y[j] = s;
+        for (int i = 0; i < j; ++i) s = fmaf(-x[i], U[i + j * kW], s);
+        const float d = U[j + j * kW];
+        x[j] = d != 0.0f ? s / d : 0.0f;
+      }
     }
 #pragma unroll
     for (int j = 0; j < W; ++j)
-      if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = y[j];
+      if (j < w) a[(size_t)r + (size_t)(c0 + j) * lda] = x[j];
     if (hit >= 0)
       lab[r] = mlab[hit];
     else if (first_leaf)
@@ -498,7 +516,9 @@ template <int W>
 __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int n, int c0, int w, int kb0, int kb1,
                                                          int* lab, int first_leaf, int side_blocks,
                                                          const TsluScratch* ws) {
-  apply_body<W>(a, lda, n, c0, w, kb0, kb1, lab, first_leaf, blockIdx.x, gridDim.x, side_blocks, side_blocks, ws);
+  float none[W];
+  apply_body<W>(a, lda, n, c0, w, kb0, kb1, lab, first_leaf, blockIdx.x, gridDim.x, side_blocks, side_blocks, ws,
+                none, false);
 }
 
 __device__ __forceinline__ uint64_t tslu_timer_ns() {
@@ -520,11 +540,14 @@ __global__ void __launch_bounds__(kRows, 1) tslu_fused_kernel(LevelIn in, int gr
   __shared__ int ok_s;
   int g = blockIdx.x, groups = groups0, src = -1, dst = 0, nchild = 0, level = 0;
   bool ran_root = false;
+  float kept[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) kept[c] = 0.0f;
   // CTAs beyond the level-0 blocks (there only for the side columns) take
   // no part in the tree
   for (; (int)blockIdx.x < groups0;) {
     const bool root = groups == 1;
-    level_body<W>(in, g, src, nchild, dst, root, ws);
+    level_body<W>(in, g, src, nchild, dst, root, ws, kept);
     if (root) {
       ran_root = true;
       break;
@@ -572,7 +595,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_fused_kernel(LevelIn in, int gr
   __syncthreads();
   if (!ok_s) return;
   apply_body<W>(const_cast<float*>(in.a), in.lda, in.n, in.c0, in.w, kb0, kb1, lab, in.first_leaf, blockIdx.x,
-                gridDim.x, side_blocks, 0, ws);
+                gridDim.x, side_blocks, 0, ws, kept, true);
 }
 
 }  // namespace
