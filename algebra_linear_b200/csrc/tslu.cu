@@ -192,12 +192,8 @@ struct LevelIn {
 
 // Proposals written by other CTAs are read through L2 (__ldcg): in the
 // single-launch form they were written during this launch by other SMs.
-// keep: at level 0 (src < 0), receives this thread's row's original values
-// (the single-launch form's apply step reuses them instead of reading the
-// panel again).
 template <int W>
-__device__ __forceinline__ void level_body(const LevelIn& in, int g, int src, int nchild, int dst, bool root,
-                                           TsluScratch* ws, float (&keep)[W]) {
+__device__ void level_body(const LevelIn& in, int g, int src, int nchild, int dst, bool root, TsluScratch* ws) {
   __shared__ GeppShared box;
   __shared__ int zero_col;
   __shared__ int coff[kFan + 1];
@@ -242,10 +238,7 @@ __device__ __forceinline__ void level_body(const LevelIn& in, int g, int src, in
   float v[W];
 #pragma unroll
   for (int c = 0; c < W; ++c) v[c] = o[c];
-  if (src < 0) {
-#pragma unroll
-    for (int c = 0; c < W; ++c) keep[c] = o[c];
-  }
+
   if (t == 0) zero_col = -1;
   __syncthreads();
   const int step = block_gepp<W>(v, nr, w, box, &zero_col);
@@ -368,8 +361,7 @@ __device__ __forceinline__ void level_body(const LevelIn& in, int g, int src, in
 template <int W>
 __global__ void __launch_bounds__(kRows, 1) tslu_level_kernel(LevelIn in, int src, int nchild, int dst, int root,
                                                            TsluScratch* ws) {
-  float keep[W];
-  level_body<W>(in, blockIdx.x, src, nchild, dst, root != 0, ws, keep);
+  level_body<W>(in, blockIdx.x, src, nchild, dst, root != 0, ws);
 }
 
 // 3. Blocks [0, side_blocks): the block panel's other columns follow the
@@ -381,12 +373,9 @@ constexpr int kSideCols = 8;
 // CTA `cta` of `ncta`: the first side_blocks CTAs permute the block panel's
 // other columns and turn the top rows of its trailing columns into U12; rows
 // are spread over the CTAs from row_cta0 on.
-// kept (the single-launch form, one row per thread): this thread's row's
-// original values from level 0, so that only moved rows read the panel.
 template <int W>
-__device__ __forceinline__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab,
-                                           int first_leaf, int cta, int ncta, int side_blocks, int row_cta0,
-                                           const TsluScratch* ws, const float (&kept)[W], bool use_kept) {
+__device__ void apply_body(float* a, int lda, int n, int c0, int w, int kb0, int kb1, int* lab, int first_leaf,
+                           int cta, int ncta, int side_blocks, int row_cta0, const TsluScratch* ws) {
   __shared__ float U[kW * kW];
   __shared__ int mpos[kMaxMoves], msrc[kMaxMoves], mlab[kMaxMoves];
   __shared__ int nm_s;
@@ -452,15 +441,18 @@ __device__ __forceinline__ void apply_body(float* a, int lda, int n, int c0, int
     }
   }
   if (cta < row_cta0) return;
+  __shared__ float rinv[kW];  // 1 / u_jj (0 for a zero pivot, which the factorization reports)
   for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) U[e] = __ldcg(&ws->top_lu[e]);
+  if (threadIdx.x < kW) {
+    const float d = __ldcg(&ws->top_lu[threadIdx.x * (kW + 1)]);
+    rinv[threadIdx.x] = d != 0.0f ? 1.0f / d : 0.0f;
+  }
   __syncthreads();
   const int nm = nm_s;
   const int gtid = (cta - row_cta0) * blockDim.x + threadIdx.x;
   const int nth = (ncta - row_cta0) * blockDim.x;
-  // rows below the top (with kept values: row c0 + gtid, the row this
-  // thread held at level 0)
-  for (int r = use_kept ? c0 + gtid : c0 + w + gtid; r < n; r += nth) {
-    if (r < c0 + w) continue;  // a top row (below)
+  // rows below the top
+  for (int r = c0 + w + gtid; r < n; r += nth) {
     int src = r, hit = -1;
     for (int q = 0; q < nm; ++q)
       if (mpos[q] == r) hit = q;
@@ -468,24 +460,20 @@ __device__ __forceinline__ void apply_body(float* a, int lda, int n, int c0, int
     // a row below the top either stays or is a row displaced from the top
     const bool from_top = src < c0 + w;
     float x[W];
-    if (use_kept && hit < 0) {
 #pragma unroll
-      for (int j = 0; j < W; ++j) x[j] = kept[j];
-    } else {
-#pragma unroll
-      for (int j = 0; j < W; ++j)
-        x[j] = j < w ? (from_top ? __ldcg(&ws->top_orig[j * kW + (src - c0)])
-                                 : a[(size_t)src + (size_t)(c0 + j) * lda])
-                      : 0.0f;
-    }
+    for (int j = 0; j < W; ++j)
+      x[j] = j < w ? (from_top ? __ldcg(&ws->top_orig[j * kW + (src - c0)]) : a[(size_t)src + (size_t)(c0 + j) * lda])
+                    : 0.0f;
+    // l = a U11^-1 by columns, right-looking: step j scales x_j and
+    // updates every later entry at once (independent FMAs, row j of U read
+    // as a batch), so the dependent chain is one product and one FMA per
+    // column instead of a division and a dot product
 #pragma unroll
     for (int j = 0; j < W; ++j) {
       if (j < w) {
-        float s = x[j];
+        x[j] *= rinv[j];
 #pragma unroll
-        for (int i = 0; i < j; ++i) s = fmaf(-x[i], U[i + j * kW], s);
-        const float d = U[j + j * kW];
-        x[j] = d != 0.0f ? s / d : 0.0f;
+        for (int k = j + 1; k < W; ++k) x[k] = fmaf(-x[j], U[j + k * kW], x[k]);
       }
     }
 #pragma unroll
@@ -516,9 +504,7 @@ template <int W>
 __global__ void __launch_bounds__(256) tslu_apply_kernel(float* a, int lda, int n, int c0, int w, int kb0, int kb1,
                                                          int* lab, int first_leaf, int side_blocks,
                                                          const TsluScratch* ws) {
-  float none[W];
-  apply_body<W>(a, lda, n, c0, w, kb0, kb1, lab, first_leaf, blockIdx.x, gridDim.x, side_blocks, side_blocks, ws,
-                none, false);
+  apply_body<W>(a, lda, n, c0, w, kb0, kb1, lab, first_leaf, blockIdx.x, gridDim.x, side_blocks, side_blocks, ws);
 }
 
 __device__ __forceinline__ uint64_t tslu_timer_ns() {
@@ -540,14 +526,11 @@ __global__ void __launch_bounds__(kRows, 1) tslu_fused_kernel(LevelIn in, int gr
   __shared__ int ok_s;
   int g = blockIdx.x, groups = groups0, src = -1, dst = 0, nchild = 0, level = 0;
   bool ran_root = false;
-  float kept[W];
-#pragma unroll
-  for (int c = 0; c < W; ++c) kept[c] = 0.0f;
   // CTAs beyond the level-0 blocks (there only for the side columns) take
   // no part in the tree
   for (; (int)blockIdx.x < groups0;) {
     const bool root = groups == 1;
-    level_body<W>(in, g, src, nchild, dst, root, ws, kept);
+    level_body<W>(in, g, src, nchild, dst, root, ws);
     if (root) {
       ran_root = true;
       break;
@@ -595,7 +578,7 @@ __global__ void __launch_bounds__(kRows, 1) tslu_fused_kernel(LevelIn in, int gr
   __syncthreads();
   if (!ok_s) return;
   apply_body<W>(const_cast<float*>(in.a), in.lda, in.n, in.c0, in.w, kb0, kb1, lab, in.first_leaf, blockIdx.x,
-                gridDim.x, side_blocks, 0, ws, kept, true);
+                gridDim.x, side_blocks, 0, ws);
 }
 
 }  // namespace
