@@ -47,27 +47,29 @@ __device__ __forceinline__ double pkey(double v, bool diag) {
   return a;
 }
 
-// Block-wide first-index argmax of keys; returns the winning index to all threads.
-__device__ int block_argmax(double key, int idx, double* red_k, int* red_i) {
+// Block-wide first-index argmax of keys (largest key, lowest index among
+// equals); returns the winning index to all threads. One barrier: each warp
+// posts its best in a mailbox slot double-buffered by `par` (the caller
+// alternates it per call, and its other barriers separate two calls with the
+// same parity), and every warp reduces the mailboxes itself.
+__device__ int block_argmax(double key, int idx, double* red_k, int* red_i, int par) {
   for (int off = 16; off > 0; off >>= 1) {
     const double ok = __shfl_down_sync(0xffffffffu, key, off);
     const int oi = __shfl_down_sync(0xffffffffu, idx, off);
     if (ok > key || (ok == key && oi < idx)) { key = ok; idx = oi; }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) { red_k[warp] = key; red_i[warp] = idx; }
+  if (lane == 0) { red_k[16 * par + warp] = key; red_i[16 * par + warp] = idx; }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double k = red_k[0];
-    int i = red_i[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-      if (red_k[w] > k || (red_k[w] == k && red_i[w] < i)) { k = red_k[w]; i = red_i[w]; }
-    red_i[0] = i;
+  const int nw = (int)(blockDim.x >> 5);
+  double k = lane < nw ? red_k[16 * par + lane] : -CUDART_INF;
+  int i = lane < nw ? red_i[16 * par + lane] : INT_MAX;
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ok = __shfl_xor_sync(0xffffffffu, k, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    if (ok > k || (ok == k && oi < i)) { k = ok; i = oi; }
   }
-  __syncthreads();
-  const int r = red_i[0];
-  __syncthreads();
-  return r;
+  return i;
 }
 
 // LU with partial pivoting of the n x n matrix a (global, leading dim n),
@@ -109,7 +111,7 @@ __device__ int cta_getrf(T* a, int n, int* ipiv, unsigned char* smem, int cap) {
         const double kk = pkey((double)panel[j * kMaxN + r], r == j);
         if (kk > key) { key = kk; idx = r; }
       }
-      const int p = block_argmax(key, idx, red_k, red_i);
+      const int p = block_argmax(key, idx, red_k, red_i, j & 1);
       const T d = panel[j * kMaxN + p];
       if (threadIdx.x == 0) {
         ipiv[k0 + j] = k0 + p;
@@ -128,14 +130,12 @@ __device__ int cta_getrf(T* a, int n, int* ipiv, unsigned char* smem, int cap) {
         }
       }
       __syncthreads();
-      for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) panel[j * kMaxN + r] = panel[j * kMaxN + r] / d;
-      __syncthreads();
-      const int wr = w - j - 1;
-      if (wr > 0) {
-        for (int idx2 = threadIdx.x; idx2 < (m - j - 1) * wr; idx2 += blockDim.x) {
-          const int r = j + 1 + idx2 % (m - j - 1), c = j + 1 + idx2 / (m - j - 1);
-          panel[c * kMaxN + r] = fma_t<T>(-panel[j * kMaxN + r], panel[c * kMaxN + j], panel[c * kMaxN + r]);
-        }
+      // each row's multiplier and its rank-1 update by the same thread (the
+      // pivot row, read here, is not written in this phase: no barrier between)
+      for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) {
+        const T l = panel[j * kMaxN + r] / d;
+        panel[j * kMaxN + r] = l;
+        for (int c = j + 1; c < w; ++c) panel[c * kMaxN + r] = fma_t<T>(-l, panel[c * kMaxN + j], panel[c * kMaxN + r]);
       }
       __syncthreads();
     }
