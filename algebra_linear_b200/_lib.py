@@ -91,6 +91,8 @@ SIGNATURES = [
     ("alg_splu_analyze", _I, [_P, _SZ, _P, _SZ, _I, C.c_double, _P]),
     ("alg_splu_factorize", _I, [_P, _P, _SZ, _P, _SZ, _P, _SZ]),
     ("alg_splu_solve", _I, [_P, _P, _SZ]),
+    ("alg_zsplu_factorize", _I, [_P, _P, _SZ, _P, _SZ, _P, _SZ]),
+    ("alg_zsplu_solve", _I, [_P, _P, _SZ]),
     ("alg_splu_effective_method", _I, [_P]),
     ("alg_splu_flop_ratio", _I, [_P, _P]),
     ("alg_splu_get_stats", _I, [_P, _P]),

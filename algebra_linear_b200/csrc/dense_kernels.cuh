@@ -526,8 +526,6 @@ __global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<
   __shared__ unsigned long long mbar[2];
   __shared__ __align__(16) unsigned long long rec[2][kPanelMaxC][Rec::kWords];
   __shared__ __align__(16) unsigned long long diag[2][Rec::kDiagWords];
-  __shared__ __align__(16) unsigned long long outbox[2][Rec::kWords];
-  __shared__ __align__(16) unsigned long long doutbox[2][Rec::kDiagWords];
   __shared__ double cand_key[2][NW];
   __shared__ int cand_idx[2][NW];
   __shared__ int cand_lab[2][NW][2];
@@ -640,35 +638,34 @@ __global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<
         const bool have = ci != INT_MAX;
         const T* crow = &stage[par][cw][0];
         const bool own_j = j >= rb && j < re;
-        // C == 1: the record goes straight into the CTA's own mailbox
-        unsigned long long* ob = C > 1 ? &outbox[par][0] : &rec[par][0][0];
-        unsigned long long* dob = C > 1 ? &doutbox[par][0] : &diag[par][0];
+        // lane kw builds word kw of the record in a register and stores it
+        // into slot q of every CTA's mailbox with st.async (each 8-byte store
+        // completes on that CTA's mbarrier); C == 1: straight into the own
+        // mailbox. No staging in shared memory, no proxy fence, no bulk copy.
+        const uint32_t bar_par = bar_base + 8u * par;
         for (int kw = lane; kw < Rec::kWords; kw += 32) {
           unsigned long long val = 0;
           if (kw == 0) val = (unsigned long long)__double_as_longlong(ck);
           else if (kw == 1) val = pack_ii(ci, have ? cand_lab[par][cw][0] : 0);
           else if (kw == 2) val = pack_ii(have ? cand_lab[par][cw][1] : 0, 0);
           else if (kw < 3 + Rec::kRowWords) val = row_word<T, W>(crow, kw - 3);
-          ob[kw] = val;
+          if (C > 1) {
+            const uint32_t la = rec_base + 8u * (uint32_t)((par * kPanelMaxC + q) * Rec::kWords + kw);
+            for (int t = 0; t < C; ++t) st_async_b64(mapa_u32(la, t), val, mapa_u32(bar_par, t));
+          } else {
+            rec[par][0][kw] = val;
+          }
         }
         if (own_j) {
           for (int kw = lane; kw < Rec::kDiagWords; kw += 32) {
             unsigned long long val = 0;
             if (kw == 0) val = pack_ii(dlab[par][0], dlab[par][1]);
             else if (kw < 1 + Rec::kRowWords) val = row_word<T, W>(&dstage[par][0], kw - 1);
-            dob[kw] = val;
-          }
-        }
-        if (C > 1) {
-          fence_proxy_async_smem();
-          __syncwarp();
-          if (lane < C) {
-            const uint32_t rbar = mapa_u32(bar_base + 8u * par, lane);
-            const uint32_t la = rec_base + 8u * (uint32_t)((par * kPanelMaxC + q) * Rec::kWords);
-            bulk_to_cta(mapa_u32(la, lane), smem_u32(ob), Rec::kBytes, rbar);
-            if (own_j) {
-              const uint32_t ld = diag_base + 8u * (uint32_t)(par * Rec::kDiagWords);
-              bulk_to_cta(mapa_u32(ld, lane), smem_u32(dob), Rec::kDiagBytes, rbar);
+            if (C > 1) {
+              const uint32_t ld = diag_base + 8u * (uint32_t)(par * Rec::kDiagWords + kw);
+              for (int t = 0; t < C; ++t) st_async_b64(mapa_u32(ld, t), val, mapa_u32(bar_par, t));
+            } else {
+              diag[par][kw] = val;
             }
           }
         }

@@ -76,9 +76,16 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, int 
 
 // A coarser partition for the GPU plan: chains of only-children merged into
 // their parents while the merged front's flops grow by at most tol.
-void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std::vector<idx>* ptr_out);
+void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, double traffic_scale,
+                       std::vector<idx>* ptr_out);
 // S with another supernode partition (same order, counts and column etree).
 void repartition(const Supernodal& S, const std::vector<idx>& ptr, Supernodal* out);
+// S's partition cut wherever a supernode's next column is not the etree
+// parent of the one before (the relaxation also merges a supernode into the
+// next one in the order when that one is not its parent): every front of the
+// GPU plan is then a chain of the column etree, so the unpivoted rows a front
+// passes up are those of its own subtree only.
+void split_at_etree_breaks(const Supernodal& S, Supernodal* out);
 
 }  // namespace sp
 }  // namespace alg

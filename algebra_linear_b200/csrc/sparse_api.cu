@@ -54,14 +54,17 @@ int check_view(const alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, co
   return ALG_OK;
 }
 
-int ensure_device(alg_splu* lu) {
-  if (lu->dev_ready) return ALG_OK;
+// Uploads the plan and allocates the arenas on first use; the first
+// factorization fixes the handle's scalar (words = 1 real, 2 complex) and a
+// later call with the other scalar is rejected (ALG_INVALID_ARGUMENT).
+int ensure_device(alg_splu* lu, int words = 1) {
+  if (lu->dev_ready) return lu->dev.words == words ? ALG_OK : ALG_INVALID_ARGUMENT;
   if (lu->ctx == nullptr) {
     const int rc = alg_ctx_create(nullptr, &lu->ctx);
     if (rc != ALG_OK) return rc;
     lu->own_ctx = true;
   }
-  const int rc = lu->dev.init(lu->ctx, &lu->plan);
+  const int rc = lu->dev.init(lu->ctx, &lu->plan, words);
   if (rc != ALG_OK) {
     lu->dev.release();
     return rc;
@@ -156,16 +159,28 @@ int alg_splu_analyze(const size_t* col_ptr, size_t col_ptr_len, const size_t* ro
   {
     int lanes = kLanes;
     if (const char* e = std::getenv("ALG_SPLU_LANES")) lanes = std::max(1, std::min(8, std::atoi(e)));
+    // the reference's partition cut at its etree breaks (ALG_SPLU_KEEP_GLUED=1:
+    // measurement switch that keeps it whole)
+    alg::sp::Supernodal chains;
+    if (std::getenv("ALG_SPLU_KEEP_GLUED"))
+      chains = lu->sym;
+    else
+      alg::sp::split_at_etree_breaks(lu->sym, &chains);
     alg::sp::FrontPlan first;
-    rc = alg::sp::build_front_plan(p, lu->sym, kSmallFrontRows, lanes, &first);
+    rc = alg::sp::build_front_plan(p, chains, kSmallFrontRows, lanes, &first);
     if (rc != ALG_OK) return rc;
     std::vector<idx> ptr;
-    alg::sp::amalgamate_chains(first, lu->sym, kChainTolerance, &ptr);
-    if (ptr.size() == lu->sym.supernode_ptr.size()) {
+    // the merge rules' tolerance and traffic weight (ALG_SPLU_CHAIN_TOL,
+    // ALG_SPLU_MERGE_TRAFFIC: measurement switches)
+    double tol = kChainTolerance, traffic = 1.0;
+    if (const char* e = std::getenv("ALG_SPLU_CHAIN_TOL")) tol = std::max(0.0, std::atof(e));
+    if (const char* e = std::getenv("ALG_SPLU_MERGE_TRAFFIC")) traffic = std::max(0.0, std::atof(e));
+    alg::sp::amalgamate_chains(first, chains, tol, traffic, &ptr);
+    if (ptr.size() == chains.supernode_ptr.size()) {
       lu->plan = std::move(first);
     } else {
       alg::sp::Supernodal coarse;
-      alg::sp::repartition(lu->sym, ptr, &coarse);
+      alg::sp::repartition(chains, ptr, &coarse);
       rc = alg::sp::build_front_plan(p, coarse, kSmallFrontRows, lanes, &lu->plan);
       if (rc != ALG_OK) return rc;
     }
@@ -203,20 +218,74 @@ int alg_splu_factorize(alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, 
   return factor_loaded(lu);
 }
 
-int alg_splu_solve(const alg_splu* lu_c, double* b, size_t b_len) {
-  if (lu_c == nullptr) return ALG_INVALID_ARGUMENT;
-  auto* lu = const_cast<alg_splu*>(lu_c);
+}  // extern "C"
+
+namespace {
+
+// solve with b of n values of `words` doubles each, from and to the host
+int solve_host(alg_splu* lu, double* b, size_t b_len, int words) {
   if (lu->cur < 0) return ALG_SP_NOT_FACTORIZED;
   if (b_len != lu->n || (b_len > 0 && b == nullptr)) return ALG_SP_BAD_SHAPE;
   if (lu->n == 0) return ALG_OK;
+  if (lu->dev.words != words) return ALG_INVALID_ARGUMENT;
   cudaStream_t st = lu->ctx->stream;
-  ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_rhs, b, sizeof(double) * lu->n, cudaMemcpyHostToDevice, st));
+  const size_t bytes = sizeof(double) * words * lu->n;
+  ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_rhs, b, bytes, cudaMemcpyHostToDevice, st));
   ALG_TRY(alg::status_reset(lu->ctx));
   ALG_TRY(lu->dev.solve(lu->cur));
-  ALG_CUDA_TRY(cudaMemcpyAsync(b, lu->dev.d_rhs, sizeof(double) * lu->n, cudaMemcpyDeviceToHost, st));
+  ALG_CUDA_TRY(cudaMemcpyAsync(b, lu->dev.d_rhs, bytes, cudaMemcpyDeviceToHost, st));
   ALG_TRY(alg::status_fetch(lu->ctx));  // synchronises
   if (lu->ctx->h_status->timeout) return ALG_TIMEOUT;
   return ALG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alg_splu_solve(const alg_splu* lu, double* b, size_t b_len) {
+  if (lu == nullptr) return ALG_INVALID_ARGUMENT;
+  return solve_host(const_cast<alg_splu*>(lu), b, b_len, 1);
+}
+
+// SparseLu<Complex64>::factorize (sparse_lu.rs:91-121 with T = Complex64):
+// values holds values_len complex entries as interleaved (re, im) doubles.
+int alg_zsplu_factorize(alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx,
+                        size_t row_idx_len, const double* values, size_t values_len) {
+  if (lu == nullptr) return ALG_INVALID_ARGUMENT;
+  int rc = check_view(lu, col_ptr, col_ptr_len, row_idx, row_idx_len, values_len);
+  if (rc != ALG_OK) return rc;
+  if (values_len > 0 && values == nullptr) return ALG_SP_BAD_SHAPE;
+  alg::sp::Pattern p;
+  p.n = (idx)lu->n;
+  p.col_ptr = col_ptr;
+  p.row_idx = row_idx;
+  if (row_idx_len != lu->nnz || alg::sp::fingerprint(p) != lu->fingerprint) return ALG_SP_STRUCTURE_MISMATCH;
+  for (size_t q = 0; q < 2 * values_len; ++q)
+    if (!std::isfinite(values[q])) return ALG_SP_NOT_FINITE;  // either part (lu.rs:79-81)
+  if (lu->dev_ready && lu->dev.words != 2) return ALG_INVALID_ARGUMENT;
+  if (lu->n == 0) {
+    lu->cur = 0;
+    lu->stats = alg_splu_stats{};
+    lu->stats.method = lu->effective;
+    lu->stats.has_flop_ratio = lu->has_ratio;
+    lu->stats.flop_ratio = lu->flop_ratio;
+    lu->stats.ordering_time = lu->ordering_time;
+    lu->has_stats = 1;
+    return ALG_OK;
+  }
+  if (lu->plan.structurally_singular) return ALG_SP_SINGULAR;
+  ALG_TRY(ensure_device(lu, 2));
+  ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_values, values, sizeof(double) * 2 * values_len, cudaMemcpyHostToDevice,
+                               lu->ctx->stream));
+  return factor_loaded(lu);
+}
+
+// SparseLu<Complex64>::solve (sparse_lu.rs:125-130): b holds n complex
+// entries as interleaved (re, im) doubles and becomes x.
+int alg_zsplu_solve(const alg_splu* lu, double* b, size_t b_len) {
+  if (lu == nullptr) return ALG_INVALID_ARGUMENT;
+  return solve_host(const_cast<alg_splu*>(lu), b, b_len, 2);
 }
 
 int alg_splu_effective_method(const alg_splu* lu) { return lu ? lu->effective : ALG_INVALID_ARGUMENT; }
@@ -317,7 +386,7 @@ int alg_splu_solve_dev(alg_splu* lu, double* d_b) {
   if (lu == nullptr) return ALG_INVALID_ARGUMENT;
   if (lu->cur < 0) return ALG_SP_NOT_FACTORIZED;
   if (lu->n == 0) return ALG_OK;
-  if (d_b == nullptr) return ALG_INVALID_ARGUMENT;
+  if (d_b == nullptr || lu->dev.words != 1) return ALG_INVALID_ARGUMENT;
   cudaStream_t st = lu->ctx->stream;
   ALG_CUDA_TRY(cudaMemcpyAsync(lu->dev.d_rhs, d_b, sizeof(double) * lu->n, cudaMemcpyDeviceToDevice, st));
   ALG_TRY(lu->dev.solve(lu->cur));

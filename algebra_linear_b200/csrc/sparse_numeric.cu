@@ -38,6 +38,66 @@ __device__ __forceinline__ double fma_t<double>(double a, double b, double c) { 
 template <>
 __device__ __forceinline__ float fma_t<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
+// The scalar of SparseLu<Complex64> (num_complex::Complex<f64>; lu.rs:61-82),
+// stored interleaved (re, im) as the host's arrays: num-complex's product
+// (ac - bd) + i(ad + bc), the pivot measure Complex::norm = hypot(re, im) and
+// the reciprocal Complex::inv = (re / |z|^2, -im / |z|^2). The factors equal
+// the reference's to rounding (the products may be fused here).
+struct zc {
+  double re, im;
+  zc() = default;
+  __host__ __device__ constexpr zc(double r, double i = 0.0) : re(r), im(i) {}
+};
+__device__ __forceinline__ zc operator+(zc a, zc b) { return zc(a.re + b.re, a.im + b.im); }
+__device__ __forceinline__ zc operator-(zc a, zc b) { return zc(a.re - b.re, a.im - b.im); }
+__device__ __forceinline__ zc operator-(zc a) { return zc(-a.re, -a.im); }
+__device__ __forceinline__ zc operator*(zc a, zc b) {
+  return zc(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+__device__ __forceinline__ zc& operator+=(zc& a, zc b) { return a = a + b; }
+__device__ __forceinline__ zc& operator-=(zc& a, zc b) { return a = a - b; }
+__device__ __forceinline__ zc& operator*=(zc& a, zc b) { return a = a * b; }
+__device__ __forceinline__ bool operator!=(zc a, zc b) { return a.re != b.re || a.im != b.im; }
+template <>
+__device__ __forceinline__ zc fma_t<zc>(zc a, zc b, zc c) {
+  return zc(__fma_rn(a.re, b.re, __fma_rn(-a.im, b.im, c.re)), __fma_rn(a.re, b.im, __fma_rn(a.im, b.re, c.im)));
+}
+
+// |x| as the pivot search compares it (SparseScalar::abs)
+template <typename T>
+__device__ __forceinline__ double pivot_key(T v) { return fabs((double)v); }
+template <>
+__device__ __forceinline__ double pivot_key<zc>(zc v) { return hypot(v.re, v.im); }
+
+// 1 / x (SparseScalar::recip)
+template <typename T>
+__device__ __forceinline__ T recip_t(T v) { return T(1) / v; }
+template <>
+__device__ __forceinline__ zc recip_t<zc>(zc v) {
+  const double ns = v.re * v.re + v.im * v.im;
+  return zc(v.re / ns, -v.im / ns);
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_t(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <>
+__device__ __forceinline__ zc shfl_t<zc>(zc v, int src) {
+  return zc(__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src));
+}
+
+// entry q of a host-layout value array (doubles; complex: interleaved pairs)
+template <typename T>
+__device__ __forceinline__ T load_value(const double* v, int64_t q) { return (T)v[q]; }
+template <>
+__device__ __forceinline__ zc load_value<zc>(const double* v, int64_t q) { return zc(v[2 * q], v[2 * q + 1]); }
+template <typename T>
+__device__ __forceinline__ void store_value(double* v, int64_t q, T x) { v[q] = (double)x; }
+template <>
+__device__ __forceinline__ void store_value<zc>(double* v, int64_t q, zc x) {
+  v[2 * q] = x.re;
+  v[2 * q + 1] = x.im;
+}
+
 template <typename T>
 struct SmallArgs {
   const FrontDesc* fronts;
@@ -57,49 +117,55 @@ struct SmallArgs {
   int* singular;
 };
 
-// C (mr x nc) -= A (mr x kd) B (kd x nc), all inside one front (column-major,
-// leading dimension ld), by one CTA of kSmallThreads: 64 x 64 tiles, each
-// thread a 4 x 4 register block, K staged through shared memory 16 at a time.
+// The 64 x 64 tile at (i0, j0) of C (mr x nc) -= A (mr x kd) B (kd x nc),
+// all inside one front (column-major, leading dimension ld), by one CTA of
+// kSmallThreads: each thread a 4 x 4 register block, K staged through shared
+// memory 16 at a time.
+template <typename T>
+__device__ __forceinline__ void cta_gemm_tile(T* C, const T* A, const T* B, int ld, int mr, int nc, int kd, int i0,
+                                              int j0, T* As, T* Bs) {
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = T(0);
+  for (int k0 = 0; k0 < kd; k0 += 16) {
+    __syncthreads();
+    for (int e = tid; e < 64 * 16; e += kSmallThreads) {
+      const int r = e & 63, k = e >> 6;  // A tile, rows contiguous
+      As[k * 64 + r] = (i0 + r < mr && k0 + k < kd) ? A[(i0 + r) + (int64_t)(k0 + k) * ld] : T(0);
+      const int kk = e & 15, c = e >> 4;  // B tile, k contiguous
+      Bs[kk * 64 + c] = (j0 + c < nc && k0 + kk < kd) ? B[(k0 + kk) + (int64_t)(j0 + c) * ld] : T(0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) av[r] = As[k * 64 + tx * 4 + r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) bv[c] = Bs[k * 64 + ty * 4 + c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma_t(av[r], bv[c], acc[r][c]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = i0 + tx * 4 + r, j = j0 + ty * 4 + c;
+      if (i < mr && j < nc) C[i + (int64_t)j * ld] -= acc[r][c];
+    }
+}
+
+// All tiles of it, by one CTA.
 template <typename T>
 __device__ void cta_gemm_sub(T* C, const T* A, const T* B, int ld, int mr, int nc, int kd, T* As, T* Bs) {
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   for (int i0 = 0; i0 < mr; i0 += 64)
-    for (int j0 = 0; j0 < nc; j0 += 64) {
-      T acc[4][4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = T(0);
-      for (int k0 = 0; k0 < kd; k0 += 16) {
-        __syncthreads();
-        for (int e = tid; e < 64 * 16; e += kSmallThreads) {
-          const int r = e & 63, k = e >> 6;  // A tile, rows contiguous
-          As[k * 64 + r] = (i0 + r < mr && k0 + k < kd) ? A[(i0 + r) + (int64_t)(k0 + k) * ld] : T(0);
-          const int kk = e & 15, c = e >> 4;  // B tile, k contiguous
-          Bs[kk * 64 + c] = (j0 + c < nc && k0 + kk < kd) ? B[(k0 + kk) + (int64_t)(j0 + c) * ld] : T(0);
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int k = 0; k < 16; ++k) {
-          T av[4], bv[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) av[r] = As[k * 64 + tx * 4 + r];
-#pragma unroll
-          for (int c = 0; c < 4; ++c) bv[c] = Bs[k * 64 + ty * 4 + c];
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[r][c] = fma_t(av[r], bv[c], acc[r][c]);
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int i = i0 + tx * 4 + r, j = j0 + ty * 4 + c;
-          if (i < mr && j < nc) C[i + (int64_t)j * ld] -= acc[r][c];
-        }
-    }
+    for (int j0 = 0; j0 < nc; j0 += 64) cta_gemm_tile(C, A, B, ld, mr, nc, kd, i0, j0, As, Bs);
   __syncthreads();
 }
 
@@ -125,7 +191,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
   }
   __syncthreads();
   for (int q = d.anew_begin + tid; q < d.anew_end; q += kSmallThreads)
-    f[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = (T)a.values[a.anew_q[q]];
+    f[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = load_value<T>(a.values, a.anew_q[q]);
   for (int k = d.child_begin; k < d.child_end; ++k) {
     const FrontDesc c = a.fronts[a.child_idx[k]];
     const int slot0 = a.child_slot[k];
@@ -155,7 +221,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
     double key = -1.0;
     int idx = INT_MAX;
     for (int i = k + tid; i < rows; i += kSmallThreads) {
-      const double v = fabs((double)f[i + (int64_t)k * rows]);
+      const double v = pivot_key(f[i + (int64_t)k * rows]);
       if (v > key) {
         key = v;
         idx = i;
@@ -199,7 +265,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_front_kernel(SmallArgs<T>
       }
     }
     __syncthreads();
-    const T inv = T(1) / f[k + (int64_t)k * rows];  // the pivot, swapped into row k
+    const T inv = recip_t(f[k + (int64_t)k * rows]);  // the pivot, swapped into row k
     // rank-1 update of the front's own columns, spread over all threads
     const int mr = rows - k - 1, mc = size - k - 1;
     for (int e = tid; e < mr * mc; e += kSmallThreads) {
@@ -271,7 +337,7 @@ __global__ void big_assemble_kernel(BigArgs<T> a) {
     for (int64_t i = tid; i < d.new_end - d.new_begin; i += nth) a.rowtmp[slotn + i] = a.new_rows[d.new_begin + i];
   }
   for (int64_t q = d.anew_begin + tid; q < d.anew_end; q += nth)
-    a.front[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = (T)a.values[a.anew_q[q]];
+    a.front[a.anew_slot[q] + (int64_t)a.anew_col[q] * rows] = load_value<T>(a.values, a.anew_q[q]);
   for (int k = d.child_begin; k < d.child_end; ++k) {
     const FrontDesc c = a.fronts[a.child_idx[k]];
     const int slot0 = a.child_slot[k];
@@ -307,6 +373,149 @@ __global__ void big_finalize_kernel(FrontDesc d, const T* front, const int* perm
       cb[i + (int64_t)t * d.cb_ld] = front[(size + i) + (int64_t)(size + t) * rows];
     }
   }
+}
+
+// ---- large complex fronts ----------------------------------------------------
+// The partial LU of a complex front (the contract of lu_factor_partial_dev:
+// the first `size` columns over all rows, interchanges across every column,
+// U12 and the Schur complement), blocked by kZnb columns, four launches per
+// block: the block's columns over all rows by one CTA (the reference's pivot
+// rule, lu_front supernodal_lu.rs:490-533: the first row of largest modulus,
+// multipliers by the reciprocal, the rank-1 updates inside the block); its
+// interchanges on the other columns; its rows of U12 by a unit-lower solve;
+// the trailing block by the tiled GEMM, one CTA per 64 x 64 tile.
+constexpr int kZnb = 32;
+constexpr int kZPanelThreads = 1024;
+
+__device__ __forceinline__ bool front_stopped(const DevStatus* st) {
+  return *reinterpret_cast<const volatile int*>(&st->singular_col) != INT_MAX;
+}
+
+__global__ void __launch_bounds__(kZPanelThreads) zfront_panel_kernel(zc* f, int rows, int k0, int k1, int* ipiv,
+                                                                      int* perm, DevStatus* st) {
+  __shared__ double mk[2][kZPanelThreads / 32];
+  __shared__ int mi[2][kZPanelThreads / 32];
+  if (front_stopped(st)) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (k0 == 0) {
+    for (int i = tid; i < rows; i += kZPanelThreads) perm[i] = i;
+    __syncthreads();
+  }
+  zc inv_prev(0.0);
+  for (int k = k0; k < k1; ++k) {
+    if (k > k0)
+      for (int i = k + tid; i < rows; i += kZPanelThreads) f[i + (int64_t)(k - 1) * rows] *= inv_prev;
+    double key = -1.0;
+    int idx = INT_MAX;
+    for (int i = k + tid; i < rows; i += kZPanelThreads) {
+      const double v = pivot_key(f[i + (int64_t)k * rows]);
+      if (v > key) {
+        key = v;
+        idx = i;
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ok = __shfl_down_sync(0xffffffffu, key, off);
+      const int oi = __shfl_down_sync(0xffffffffu, idx, off);
+      if (ok > key || (ok == key && oi < idx)) {
+        key = ok;
+        idx = oi;
+      }
+    }
+    const int par = k & 1;
+    if (lane == 0) {
+      mk[par][warp] = key;
+      mi[par][warp] = idx;
+    }
+    __syncthreads();
+    double bk = mk[par][0];
+    int p = mi[par][0];
+    for (int w = 1; w < kZPanelThreads / 32; ++w)
+      if (mk[par][w] > bk || (mk[par][w] == bk && mi[par][w] < p)) {
+        bk = mk[par][w];
+        p = mi[par][w];
+      }
+    if (!(bk > 0.0)) {
+      if (tid == 0) atomicMin(&st->singular_col, k);
+      return;  // uniform: every thread reduced the same mailboxes
+    }
+    if (p != k) {
+      for (int j = k0 + tid; j < k1; j += kZPanelThreads) {
+        const zc t = f[k + (int64_t)j * rows];
+        f[k + (int64_t)j * rows] = f[p + (int64_t)j * rows];
+        f[p + (int64_t)j * rows] = t;
+      }
+      if (tid == 0) {
+        const int t = perm[k];
+        perm[k] = perm[p];
+        perm[p] = t;
+      }
+    }
+    if (tid == 0) ipiv[k] = p;
+    __syncthreads();
+    const zc inv = recip_t(f[k + (int64_t)k * rows]);
+    const int mr = rows - k - 1, mc = k1 - k - 1;
+    for (int e = tid; e < mr * mc; e += kZPanelThreads) {
+      const int i = k + 1 + e % mr, j = k + 1 + e / mr;
+      f[i + (int64_t)j * rows] = fma_t(-f[k + (int64_t)j * rows], f[i + (int64_t)k * rows] * inv,
+                                       f[i + (int64_t)j * rows]);
+    }
+    inv_prev = inv;
+    __syncthreads();
+  }
+  for (int i = k1 + tid; i < rows; i += kZPanelThreads) f[i + (int64_t)(k1 - 1) * rows] *= inv_prev;
+}
+
+// The block's interchanges, in order, on every column outside it (a thread per column).
+__global__ void zfront_swap_kernel(zc* f, int rows, int cols, int k0, int k1, const int* ipiv, const DevStatus* st) {
+  if (front_stopped(st)) return;
+  const int w = k1 - k0, other = cols - w;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < other; t += gridDim.x * blockDim.x) {
+    zc* col = f + (int64_t)(t < k0 ? t : t + w) * rows;
+    for (int k = k0; k < k1; ++k) {
+      const int p = ipiv[k];
+      if (p != k) {
+        const zc v = col[k];
+        col[k] = col[p];
+        col[p] = v;
+      }
+    }
+  }
+}
+
+// U12 rows [k0, k1): x <- L11^-1 x for every column right of the block (a
+// thread per column; the unit-lower block in shared memory).
+__global__ void __launch_bounds__(256) zfront_trsm_kernel(zc* f, int rows, int cols, int k0, int k1,
+                                                          const DevStatus* st) {
+  __shared__ zc l11[kZnb][kZnb + 1];
+  if (front_stopped(st)) return;
+  const int w = k1 - k0;
+  for (int e = threadIdx.x; e < kZnb * kZnb; e += blockDim.x) {
+    const int r = e % kZnb, c = e / kZnb;
+    l11[c][r] = (r < w && c < w && r > c) ? f[(k0 + r) + (int64_t)(k0 + c) * rows] : zc(0.0);
+  }
+  __syncthreads();
+  for (int j = k1 + blockIdx.x * blockDim.x + threadIdx.x; j < cols; j += gridDim.x * blockDim.x) {
+    zc* col = f + k0 + (int64_t)j * rows;
+    zc x[kZnb];
+#pragma unroll
+    for (int r = 0; r < kZnb; ++r) x[r] = r < w ? col[r] : zc(0.0);
+#pragma unroll
+    for (int k = 0; k < kZnb; ++k)
+#pragma unroll
+      for (int i = k + 1; i < kZnb; ++i) x[i] = fma_t(-l11[k][i], x[k], x[i]);  // zero outside the block
+#pragma unroll
+    for (int r = 0; r < kZnb; ++r)
+      if (r < w) col[r] = x[r];
+  }
+}
+
+// Trailing block: C -= L21 U12, one 64 x 64 tile per CTA.
+__global__ void __launch_bounds__(kSmallThreads) zfront_gemm_kernel(zc* C, const zc* A, const zc* B, int ld, int mr,
+                                                                    int nc, int kd, const DevStatus* st) {
+  __shared__ zc As[64 * 16], Bs[16 * 64];
+  if (front_stopped(st)) return;
+  cta_gemm_tile(C, A, B, ld, mr, nc, kd, (int)blockIdx.x * 64, (int)blockIdx.y * 64, As, Bs);
 }
 
 // ---- after the factorization -----------------------------------------------
@@ -357,12 +566,12 @@ constexpr int kSolveThreads = 256;
 
 template <typename T>
 __global__ void gather_rows_kernel(const double* b, const int32_t* row_perm, T* y, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = (T)b[row_perm[i]];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = load_value<T>(b, row_perm[i]);
 }
 
 template <typename T>
 __global__ void scatter_cols_kernel(const T* x, const int32_t* col_perm, double* b, int n) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) b[col_perm[j]] = (double)x[j];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) store_value(b, col_perm[j], x[j]);
 }
 
 constexpr int kRowChunk = 256;  // rows of L21 / U12 per CTA (one per thread)
@@ -395,7 +604,7 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_diag_kernel(const FrontDesc
       T v = lane < w ? ys[kb + lane] : T(0);
 #pragma unroll
       for (int k = 0; k < 32; ++k) {
-        const T yk = __shfl_sync(0xffffffffu, v, k);
+        const T yk = shfl_t(v, k);
         v -= tri[k][lane] * yk;  // zero on and above the diagonal and outside the block
       }
       if (lane < w) ys[kb + lane] = v;
@@ -531,8 +740,8 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_diag_kernel(const FrontDesc
     if (warp == 0) {
       T v = lane < w ? xs[j0 + lane] : T(0);
       for (int j = w - 1; j >= 0; --j) {
-        if (lane == j) v = v * (T(1) / tri[j][j]);
-        const T xj = __shfl_sync(0xffffffffu, v, j);
+        if (lane == j) v = v * recip_t(tri[j][j]);
+        const T xj = shfl_t(v, j);
         if (lane < j) v -= tri[j][lane] * xj;
       }
       if (lane < w) xs[j0 + lane] = v;
@@ -636,12 +845,42 @@ int grid_for(alg_ctx* ctx, int64_t work, int threads) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((work + threads - 1) / threads, 8LL * ctx->sm_count));
 }
 
+// The complex front's partial LU (kernels above) on lane context lc.
+// Stream-ordered; a zero pivot lands in lc's status (singular_col).
+int zfront_lu(alg_ctx* lc, zc* f, int rows, int size, int cols, int* ipiv, int* perm) {
+  cudaStream_t st = lc->stream;
+  for (int k0 = 0; k0 < size; k0 += kZnb) {
+    const int k1 = std::min(size, k0 + kZnb);
+    zfront_panel_kernel<<<1, kZPanelThreads, 0, st>>>(f, rows, k0, k1, ipiv, perm, lc->d_status);
+    count_launches();
+    if (cols > k1 - k0) {
+      zfront_swap_kernel<<<grid_for(lc, cols - (k1 - k0), 256), 256, 0, st>>>(f, rows, cols, k0, k1, ipiv,
+                                                                                 lc->d_status);
+      count_launches();
+    }
+    if (cols > k1) {
+      zfront_trsm_kernel<<<grid_for(lc, cols - k1, 256), 256, 0, st>>>(f, rows, cols, k0, k1, lc->d_status);
+      count_launches();
+      if (rows > k1) {
+        const dim3 grid((rows - k1 + 63) / 64, (cols - k1 + 63) / 64);
+        zfront_gemm_kernel<<<grid, kSmallThreads, 0, st>>>(f + k1 + (int64_t)k1 * rows, f + k1 + (int64_t)k0 * rows,
+                                                           f + k0 + (int64_t)k1 * rows, rows, rows - k1, cols - k1,
+                                                           k1 - k0, lc->d_status);
+        count_launches();
+      }
+    }
+    ALG_CUDA_TRY(cudaGetLastError());
+  }
+  return ALG_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
-int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
+int DeviceLu::init(alg_ctx* c, const FrontPlan* p, int w) {
   ctx = c;
   plan = p;
+  words = w;
   const FrontPlan& F = *p;
   ALG_TRY(upload(F.fronts, &d_fronts));
   ALG_TRY(upload(F.child_idx, &d_child_idx));
@@ -655,9 +894,9 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
   ALG_TRY(upload(F.small_level_fronts, &d_small_levels));
   ALG_TRY(upload(F.col_perm, &d_col_perm));
   const size_t n = (size_t)std::max<idx>(F.n, 1);
-  ALG_TRY(dmalloc((void**)&d_values, sizeof(double) * std::max<idx>(F.nnz, 1)));
-  ALG_TRY(dmalloc((void**)&d_block, sizeof(double) * F.block_total));
-  ALG_TRY(dmalloc((void**)&d_stack, sizeof(double) * F.stack_total));
+  ALG_TRY(dmalloc((void**)&d_values, sizeof(double) * words * std::max<idx>(F.nnz, 1)));
+  ALG_TRY(dmalloc((void**)&d_block, sizeof(double) * words * F.block_total));
+  ALG_TRY(dmalloc((void**)&d_stack, sizeof(double) * words * F.stack_total));
   n_lanes = std::max(1, std::min(F.n_lanes, kMaxLanes));
   lane_ctx[0] = ctx;
   int64_t max_rows = 1;
@@ -669,15 +908,15 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
       ALG_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
     }
     const int64_t fb = k < (int)F.lane_front_buf.size() ? F.lane_front_buf[k] : F.front_buf;
-    ALG_TRY(dmalloc((void**)&d_front[k], sizeof(double) * std::max<int64_t>(fb, 1)));
+    ALG_TRY(dmalloc((void**)&d_front[k], sizeof(double) * words * std::max<int64_t>(fb, 1)));
     ALG_TRY(dmalloc((void**)&d_ipiv[k], sizeof(int) * max_rows));
     ALG_TRY(dmalloc((void**)&d_perm[k], sizeof(int) * max_rows));
     ALG_TRY(dmalloc((void**)&d_rowtmp[k], sizeof(int32_t) * max_rows));
   }
   ALG_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   ALG_TRY(dmalloc((void**)&d_flag, sizeof(int) * 4));
-  ALG_TRY(dmalloc((void**)&d_y, sizeof(double) * n));
-  ALG_TRY(dmalloc((void**)&d_rhs, sizeof(double) * n));
+  ALG_TRY(dmalloc((void**)&d_y, sizeof(double) * words * n));
+  ALG_TRY(dmalloc((void**)&d_rhs, sizeof(double) * words * n));
   {
     // solve schedule and the partial-sum offsets of the column chunks
     std::vector<SolveItem> fwd, fin, bwd;
@@ -689,6 +928,7 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
     // (ALG_SPLU_SOLVE_BIG overrides, for tests of that path on small grids)
     int big_size = kSolveBigSize;
     if (const char* e = std::getenv("ALG_SPLU_SOLVE_BIG")) big_size = std::max(32, std::atoi(e));
+    if (words == 2) big_size = INT_MAX;  // complex: every diagonal block by the one-CTA kernels
     for (idx s = 0; s < F.ns; ++s) {
       const FrontDesc& d = F.fronts[s];
       poff[s] = ptot;
@@ -731,14 +971,14 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p) {
     ALG_TRY(upload(bwd, &d_bwd_items));
     ALG_TRY(upload(poff, &d_part_off));
     ALG_TRY(upload(fpoff, &d_fpart_off));
-    ALG_TRY(dmalloc((void**)&d_partial, sizeof(double) * std::max<int64_t>(ptot, 1)));
-    ALG_TRY(dmalloc((void**)&d_fpartial, sizeof(double) * std::max<int64_t>(fptot, 1)));
+    ALG_TRY(dmalloc((void**)&d_partial, sizeof(double) * words * std::max<int64_t>(ptot, 1)));
+    ALG_TRY(dmalloc((void**)&d_fpartial, sizeof(double) * words * std::max<int64_t>(fptot, 1)));
     tflag_count = max_big / 64 + 2;
     ALG_TRY(dmalloc((void**)&d_tflags, sizeof(int) * (tflag_count + 1)));
   }
   for (int b = 0; b < 2; ++b) {
-    ALG_TRY(dmalloc((void**)&fac[b].L, sizeof(double) * F.l_total));
-    ALG_TRY(dmalloc((void**)&fac[b].U, sizeof(double) * F.u_total));
+    ALG_TRY(dmalloc((void**)&fac[b].L, sizeof(double) * words * F.l_total));
+    ALG_TRY(dmalloc((void**)&fac[b].U, sizeof(double) * words * F.u_total));
     ALG_TRY(dmalloc((void**)&fac[b].rowid, sizeof(int32_t) * F.rowid_total));
     ALG_TRY(dmalloc((void**)&fac[b].pos_of_row, sizeof(int32_t) * n));
     ALG_TRY(dmalloc((void**)&fac[b].row_perm, sizeof(int32_t) * n));
@@ -786,6 +1026,7 @@ void DeviceLu::release() {
 }
 
 int DeviceLu::factor(int b) {
+  if (words == 2) return factor_t<zc>(b, d_values, -1);  // complex: FP64 only
   if (prec < 0) return factor_t<double>(b, d_values, -1);
   ALG_TRY(ensure_refine_buffers());
   const FrontPlan& F = *plan;
@@ -807,7 +1048,7 @@ template <typename T>
 int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   const FrontPlan& F = *plan;
   Factors& out = fac[b];
-  out.prec = std::is_same<T, double>::value ? -1 : (tc_prec < 0 ? ALG_PREC_FP32 : tc_prec);
+  out.prec = std::is_same<T, float>::value ? (tc_prec < 0 ? ALG_PREC_FP32 : tc_prec) : -1;
   cudaStream_t st = ctx->stream;
   T* block = reinterpret_cast<T*>(d_block);
   T* L = reinterpret_cast<T*>(out.L);
@@ -912,22 +1153,27 @@ int DeviceLu::factor_big(int b, int32_t s, int lane, const double* values, int t
   big_assemble_kernel<T><<<grid_for(lc, work, 256), 256, 0, st>>>(ba);
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
-  LuPlan lp;
-  // block width of a large front's LU (ALG_SPLU_NB: measurement switch)
-  static const int splu_nb = [] {
-    const char* e = std::getenv("ALG_SPLU_NB");
-    return e ? std::max(16, std::atoi(e)) : 64;
-  }();
-  lp.nb = splu_nb;
-  lp.nbl = 16;
-  lp.tc_prec = tc_prec;
-  if constexpr (std::is_same<T, float>::value) {
-    // the mixed form's FP32 fronts pivot by tournament (refinement restores
-    // the FP64 backward error); the FP64 form keeps the reference's pivots
-    lp.tslu = 1;
-    lp.nbl = 32;
+  if constexpr (std::is_same<T, zc>::value) {
+    ALG_TRY(zfront_lu(lc, front, d.rows, d.size, cols, d_ipiv[lane], d_perm[lane]));
+  } else {
+    LuPlan lp;
+    // block width of a large front's LU (ALG_SPLU_NB: measurement switch)
+    static const int splu_nb = [] {
+      const char* e = std::getenv("ALG_SPLU_NB");
+      return e ? std::max(16, std::atoi(e)) : 64;
+    }();
+    lp.nb = splu_nb;
+    lp.nbl = 16;
+    lp.tc_prec = tc_prec;
+    if constexpr (std::is_same<T, float>::value) {
+      // the mixed form's FP32 fronts pivot by tournament (refinement restores
+      // the FP64 backward error); the FP64 form keeps the reference's pivots
+      lp.tslu = 1;
+      lp.nbl = 32;
+    }
+    ALG_TRY((lu_factor_partial_dev<T, false>(lc, front, d.rows, d.size, cols, d.rows, d_ipiv[lane], d_perm[lane],
+                                             lp)));
   }
-  ALG_TRY((lu_factor_partial_dev<T, false>(lc, front, d.rows, d.size, cols, d.rows, d_ipiv[lane], d_perm[lane], lp)));
   T* L = reinterpret_cast<T*>(out.L);
   T* U = reinterpret_cast<T*>(out.U);
   ALG_CUDA_TRY(cudaMemcpyAsync(L + d.l_off, front, sizeof(T) * (size_t)d.rows * d.size, cudaMemcpyDeviceToDevice, st));
@@ -1014,9 +1260,11 @@ int DeviceLu::sweep_t(int b) {
       fwd_diag_kernel<T><<<cnt, kSolveThreads, 0, st>>>(d_fronts, d_solve_small + solve_small_ptr[h], L, y);
       count_launches();
     }
-    for (int32_t s : solve_big[h]) {
-      const FrontDesc& d = F.fronts[s];
-      ALG_TRY(tri_solve_dev<T>(ctx, L + d.l_off, d.rows, d.size, y + d.begin, false, d_tflags, abort_flag));
+    if constexpr (!std::is_same<T, zc>::value) {  // (none for complex factors)
+      for (int32_t s : solve_big[h]) {
+        const FrontDesc& d = F.fronts[s];
+        ALG_TRY(tri_solve_dev<T>(ctx, L + d.l_off, d.rows, d.size, y + d.begin, false, d_tflags, abort_flag));
+      }
     }
     const int ni = fwd_item_ptr[h + 1] - fwd_item_ptr[h];
     if (ni > 0) {
@@ -1044,14 +1292,16 @@ int DeviceLu::sweep_t(int b) {
                                                         d_part_off, partial, y);
       count_launches();
     }
-    for (int32_t s : solve_big[h]) {
-      const FrontDesc& d = F.fronts[s];
-      if (d.ncb > 0) {
-        bwd_partials_kernel<T><<<(d.size + kSolveThreads - 1) / kSolveThreads, kSolveThreads, 0, st>>>(
-            d_fronts, s, d_part_off, partial, y);
-        count_launches();
+    if constexpr (!std::is_same<T, zc>::value) {
+      for (int32_t s : solve_big[h]) {
+        const FrontDesc& d = F.fronts[s];
+        if (d.ncb > 0) {
+          bwd_partials_kernel<T><<<(d.size + kSolveThreads - 1) / kSolveThreads, kSolveThreads, 0, st>>>(
+              d_fronts, s, d_part_off, partial, y);
+          count_launches();
+        }
+        ALG_TRY(tri_solve_dev<T>(ctx, L + d.l_off, d.rows, d.size, y + d.begin, true, d_tflags, abort_flag));
       }
-      ALG_TRY(tri_solve_dev<T>(ctx, L + d.l_off, d.rows, d.size, y + d.begin, true, d_tflags, abort_flag));
     }
   }
   scatter_cols_kernel<T><<<grid_for(ctx, n, 256), 256, 0, st>>>(y, d_col_perm, d_rhs, n);
@@ -1068,6 +1318,7 @@ int DeviceLu::solve(int b) {
   if (F.n == 0) return ALG_OK;
   last = RefineReport();
   last.precision = fac[b].prec;
+  if (words == 2) return sweep_t<zc>(b);
   if (fac[b].prec < 0) return sweep_t<double>(b);
   return refine(b);
 }

@@ -8,6 +8,10 @@
 // and FP32 accumulation) and refines every solve in FP64 against A's values
 // (r = b - A x in FP64, x += LU32^-1 r) until the normwise backward error
 // meets the target; when it does not, the set is refactored in FP64.
+//
+// Scalar. A handle's values are real (words = 1) or complex (words = 2:
+// SparseLu<Complex64>, interleaved re, im); the arenas are sized in doubles
+// times words. Complex factors are FP64 only.
 #pragma once
 
 #include <cstdint>
@@ -39,6 +43,7 @@ struct RefineReport {
 struct DeviceLu {
   alg_ctx* ctx = nullptr;
   const FrontPlan* plan = nullptr;
+  int words = 1;            // doubles per value: 1 real, 2 complex
   int prec = -1;            // precision of the next factorization (-1: FP64)
   double tol = 0.0;         // backward-error target of the mixed solve (<= 0: 10 n 2^-53)
   int max_ir = 0;           // refinement steps before the FP64 refactorization (<= 0: 10)
@@ -48,7 +53,7 @@ struct DeviceLu {
   int32_t *d_anew_slot = nullptr, *d_anew_col = nullptr, *d_new_rows = nullptr;
   int32_t *d_small_levels = nullptr, *d_col_perm = nullptr;
   double* d_values = nullptr;  // A's values (CSC order) of the next factorization
-  // arenas sized in doubles; the FP32 form uses their first halves as floats
+  // arenas sized in doubles (times words); the FP32 form uses their first halves as floats
   double* d_block = nullptr;   // small fronts' blocks
   double* d_stack = nullptr;   // large fronts' contribution blocks
   // per lane (independent subtrees of large fronts run concurrently): a
@@ -96,7 +101,7 @@ struct DeviceLu {
     unsigned* ucount = nullptr;
   } fac[2];
 
-  int init(alg_ctx* ctx, const FrontPlan* plan);
+  int init(alg_ctx* ctx, const FrontPlan* plan, int words = 1);
   void release();
   int factor(int set);                 // d_values -> set, stream-ordered
   int finish(int set, Stats* stats);   // synchronises; SP_OK or SP_SINGULAR

@@ -377,7 +377,7 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, int 
 // merged columns stay contiguous) into it when the merged front's flops stay
 // within (1 + tol) of the two separate fronts', or, for two large fronts,
 // when the extra flops cost less than the child's contribution-block traffic
-// and launch chain: a merged step no longer copies the whole contribution
+// and launch chain (times traffic_scale; 0 turns that rule off): a merged step no longer copies the whole contribution
 // block into the next front. The merged front of a child c and its parent s
 // has size_c + size_s columns, rows_s + size_c rows and the parent's Struct
 // (c's Struct outside s's columns is contained in s's); the parent's other
@@ -391,7 +391,8 @@ int build_front_plan(const Pattern& p, const Supernodal& S, int small_rows, int 
 constexpr double kFlopsPerByte = 5.0;
 constexpr double kFrontOverheadFlops = 7.5e8;
 
-void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std::vector<idx>* ptr_out) {
+void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, double traffic_scale,
+                       std::vector<idx>* ptr_out) {
   const idx ns = F.ns;
   auto flops = [](double m, double k, double c) {
     return 2.0 * k * k * m - 2.0 / 3.0 * k * k * k + k * k * c + 2.0 * (m - k) * c * k;
@@ -413,7 +414,7 @@ void amalgamate_chains(const FrontPlan& F, const Supernodal& S, double tol, std:
       // (only between large fronts: a small front's columns stay in the
       // batched kernel, off the large fronts' column-serial panel chain)
       const double cb_bytes = 24.0 * (gm[s - 1] - gk[s - 1]) * gc[s - 1];
-      const double saved = kFlopsPerByte * cb_bytes + kFrontOverheadFlops;
+      const double saved = traffic_scale * (kFlopsPerByte * cb_bytes + kFrontOverheadFlops);
       const double merged = flops(m2, k2, c2);
       const bool both_large = !F.fronts[s - 1].small && !d.small;
       if (merged <= (1.0 + tol) * sep || (both_large && merged - sep <= saved)) {
@@ -441,6 +442,16 @@ void repartition(const Supernodal& S, const std::vector<idx>& ptr, Supernodal* o
     const idx last = ptr[s + 1] - 1;
     if (S.etree[last] >= 0) out->super_etree[s] = owner[S.etree[last]];
   }
+}
+
+void split_at_etree_breaks(const Supernodal& S, Supernodal* out) {
+  std::vector<idx> ptr(1, 0);
+  for (idx s = 0; s < S.n_supernodes(); ++s) {
+    for (idx j = S.supernode_ptr[s] + 1; j < S.supernode_ptr[s + 1]; ++j)
+      if (S.etree[j - 1] != j) ptr.push_back(j);
+    ptr.push_back(S.supernode_ptr[s + 1]);
+  }
+  repartition(S, ptr, out);
 }
 
 }  // namespace sp

@@ -6,7 +6,9 @@
     lu.effective_method(), lu.flop_ratio(), lu.stats()         sparse_lu.rs:137-155
 
 CSC arrays: col_ptr (n + 1) and row_idx (nnz) as integer numpy arrays,
-values (nnz) float64. Errors are raised as SparseError whose `kind` is the
+values (nnz) float64, or complex128 for SparseLu<Complex64> (lu.rs:61-82;
+then b is complex128 too; the first factorization fixes the handle's
+scalar). Errors are raised as SparseError whose `kind` is the
 reference's Error variant and whose message is its Display string. analyze
 runs on the host (COLAMD and the supernodal symbolic analysis); factorize and
 solve run on the GPU through libalgebra_linear_gpu.so.
@@ -123,15 +125,18 @@ class SparseLu:
 
     def factorize(self, col_ptr, row_idx, values) -> None:
         cp, ri = _idx(col_ptr), _idx(row_idx)
-        v = np.ascontiguousarray(values, dtype=np.float64)
-        _check(self._lib.alg_splu_factorize(self._h, cp.ctypes.data if cp.size else None, cp.size,
-                                            ri.ctypes.data if ri.size else None, ri.size,
-                                            v.ctypes.data if v.size else None, v.size))
+        cplx = np.iscomplexobj(values)
+        v = np.ascontiguousarray(values, dtype=np.complex128 if cplx else np.float64)
+        fn = self._lib.alg_zsplu_factorize if cplx else self._lib.alg_splu_factorize
+        _check(fn(self._h, cp.ctypes.data if cp.size else None, cp.size, ri.ctypes.data if ri.size else None,
+                  ri.size, v.ctypes.data if v.size else None, v.size))
 
     def solve(self, b: np.ndarray) -> None:
-        if not isinstance(b, np.ndarray) or b.dtype != np.float64 or b.ndim != 1 or not b.flags.c_contiguous:
-            raise TypeError("b must be a contiguous 1-D float64 numpy array")
-        _check(self._lib.alg_splu_solve(self._h, b.ctypes.data if b.size else None, b.size))
+        if (not isinstance(b, np.ndarray) or b.dtype not in (np.float64, np.complex128) or b.ndim != 1
+                or not b.flags.c_contiguous):
+            raise TypeError("b must be a contiguous 1-D float64 or complex128 numpy array")
+        fn = self._lib.alg_zsplu_solve if b.dtype == np.complex128 else self._lib.alg_splu_solve
+        _check(fn(self._h, b.ctypes.data if b.size else None, b.size))
 
     def effective_method(self) -> str:
         return "Supernodal" if self._lib.alg_splu_effective_method(self._h) == SUPERNODAL else "Simplicial"

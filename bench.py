@@ -67,6 +67,7 @@ def parse_args():
     ap.add_argument("--forms", default="")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="dense: skip the other orders and right-hand sides")
     ap.add_argument("--workload", choices=["dense", "sparse", "serve", "batched"], default="dense",
                     help="dense: dgesv (the headline); sparse: supernodal LU refactorize+solve rounds; "
                          "serve: Poisson stream of dense and sparse requests through the serving loop; "
@@ -954,6 +955,9 @@ def run_serve(args, world, rank, local, pg):
             }
             print(json.dumps({mode: rate, **results[f"{mode}@{rate:g}"]}), file=sys.stderr, flush=True)
     best = min(results.values(), key=lambda r: r["p99_ms"])
+    # bytes each request moves (inputs in, solution out), mean over the stream's mix
+    h2d = 0.7 * np.mean([8.0 * (a.size + b.size) for a, b in dense_pool]) + 0.3 * 8.0 * (len(ri) + nsp)
+    d2h = 0.7 * np.mean([8.0 * b.size for _, b in dense_pool]) + 0.3 * 8.0 * nsp
     line = {
         "metric": "serving p99 latency (ms) of a mixed dense/sparse Poisson stream; solves/s",
         "value": best["p99_ms"], "unit": "ms", "n_gpus": world, "steps": args.requests, "warmup": 0,
@@ -963,10 +967,63 @@ def run_serve(args, world, rank, local, pg):
                                "Poisson arrivals", "workers": args.workers, "budget_gb": args.budget_gb,
                    "rates": rates, "parallelism": f"replicas x{world}"},
         "results": results,
+        # every request already carries host buffers through the loop: the
+        # headline is end to end
+        "e2e": {"value": best["p99_ms"], "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "alg_server_submit / alg_server_wait with host buffers"},
+        "roofline": None,
+        "roofline_note": "a latency metric of a mixed request stream; the kernels' rooflines are those of the "
+                         "dense and sparse lines",
     }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        lu.factorize(cp, ri, sparse_pool[0])
+        line["cpu_baseline"] = serve_cpu_baseline(dense_pool, lu.stats())
     if rank == 0:
         print(json.dumps(line), flush=True)
     lu.close()
+
+
+def serve_cpu_baseline(dense_pool, sparse_stats):
+    """The mean service time of the stream's mix on one host core, from the
+    oracle (the reference's dgesv and supernodal LU restated): the pool's
+    dense systems of order <= 384 timed as they are, larger ones scaled by
+    n^3 from the largest of those; the 300 x 300 refactorize + solve scaled
+    by the reference's flop estimate from the oracle's rate on a 100 x 100
+    grid. A core serves at most 1000 / mean requests per second."""
+    import numpy as np
+
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+    from oracle import dense as od
+    from oracle import sparse as osp
+
+    with _OneCore() as pin:
+        timed = {}
+        for a, b in dense_pool:
+            n = b.size
+            if n <= 384 and n not in timed:
+                aa, bb = a.copy(), b.copy()
+                t0 = time.perf_counter()
+                od.dgesv(aa, bb, n)
+                timed[n] = time.perf_counter() - t0
+        n_ref = max(timed)
+        dense_ms = [1e3 * (timed[b.size] if b.size in timed else timed[n_ref] * (b.size / n_ref) ** 3)
+                    for _, b in dense_pool]
+        cp, ri, kind = grid_csc(100, 100, 1)
+        v, _ = osp.convection_diffusion_values(kind, SEEDY)
+        sym = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()
+        t0 = time.perf_counter()
+        f = osp.Factors(len(cp) - 1, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], sym["supernode_ptr"])
+        f.solve(np.ones(len(cp) - 1))
+        t = time.perf_counter() - t0
+    rate = (2.0 * f.flops_estimate() + 2.0 * (f.nnz_l + f.nnz_u)) / t
+    fl300 = 2.0 * sparse_stats["flops_estimate"] + 2.0 * (sparse_stats["nnz_l"] + sparse_stats["nnz_u"])
+    sparse_ms = 1e3 * fl300 / rate
+    mean_ms = 0.7 * float(np.mean(dense_ms)) + 0.3 * sparse_ms
+    return {"value": mean_ms, "unit": "ms mean service per request", "capacity_solves_per_s": 1e3 / mean_ms,
+            "cores": 1, "kind": "port",
+            "sample": f"oracle dgesv on the pool's {len(timed)} orders <= {n_ref} (n^3-scaled above), sparse "
+                      f"rate on a 100x100 grid ({t:.1f} s) scaled to the 300x300 pattern's flop estimate",
+            **pin.info()}
 
 # --------------------------------------------------------------------------- arms
 def dense_config(n: int, nrhs: int, world: int) -> dict:
@@ -1042,6 +1099,42 @@ def run_reference(args, world, rank, pg):
     print(json.dumps(line), flush=True)
 
 
+# the rest of the dense configuration besides the headline order: the other
+# orders, 64 right-hand sides at the headline order, BF16 past n = 4096
+SWEEP = ((4096, 1, ("fp64_fma", "mixed_tf32x3", "mixed_bf16")),
+         (8192, 1, ("fp64_fma", "mixed_tf32x3", "mixed_bf16")),
+         (16384, 64, ("fp64_fma", "mixed_tf32x3")))
+
+
+def c2_sweep(ctx, reg, A16, s1, steps, warmup, dev_index):
+    """Each SWEEP configuration on its own system from the same DLARNV stream
+    (the 16384 one reuses the headline matrix with 64 new solutions):
+    per form ms / solve, GFLOP/s, backward and forward error, refinement."""
+    import torch
+
+    out = {}
+    for n, nrhs, names in SWEEP:
+        if n == A16.numel() ** 0.5:
+            A0, s2 = A16, s1
+        elif n < A16.numel() ** 0.5:
+            A0, s2 = ctx.larnv(2, [SEEDY[0], SEEDY[1], SEEDY[2], SEEDY[3] + 100 + n % 97], n * n)
+        else:
+            continue
+        xt, _ = ctx.larnv(2, s2, n * nrhs)
+        b0 = (A0.view(n, n).t() @ xt.view(nrhs, n).t()).t().contiguous().view(-1)
+        torch.cuda.synchronize()
+        row = {}
+        for name in names:
+            if name not in reg:
+                continue
+            r = run_form(name, reg[name], ctx, A0, b0, xt, n, nrhs, steps, warmup, None, sample_clocks=False,
+                         dev_index=dev_index)
+            row[name] = {k: r[k] for k in ("ms_per_step", "gflops", "backward_error", "forward_error", "refinement")}
+        out[f"n={n},nrhs={nrhs}"] = row
+        del A0, xt, b0
+    return out
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
 
@@ -1100,6 +1193,8 @@ def run_ours(args, world, rank, local, pg):
     }
     if not args.no_e2e:
         line["e2e"] = e2e_run(head, A0, b0, n, nrhs, steps=max(2, min(args.steps, 3)))
+    if world == 1 and not args.no_sweep and not args.forms:
+        line["c2_sweep"] = c2_sweep(ctx, reg, A0, s1, steps=3, warmup=2, dev_index=local)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(n)
     if rank == 0:

@@ -383,6 +383,18 @@ int alg_splu_flop_ratio(const alg_splu* lu, double* ratio);
 int alg_splu_get_stats(const alg_splu* lu, alg_splu_stats* out);
 void alg_splu_free(alg_splu* lu);
 
+/* SparseLu<Complex64> (the handle is generic over SparseScalar, lu.rs:20-82;
+ * analyze is shared, the pattern alone): factorize and solve with complex
+ * values, values_len entries / b_len entries as interleaved (re, im)
+ * doubles. Pivots by the modulus, multipliers by Complex::inv, in FP64
+ * (the mixed-precision setting applies to real factorizations only). The
+ * first factorization fixes a handle's scalar: a real call on a complex
+ * handle, or the reverse, is ALG_INVALID_ARGUMENT. Same errors otherwise as
+ * the real calls; ALG_SP_NOT_FINITE when either part is not finite. */
+int alg_zsplu_factorize(alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx,
+                        size_t row_idx_len, const double* values, size_t values_len);
+int alg_zsplu_solve(const alg_splu* lu, double* b, size_t b_len);
+
 /* Inspection (no reference counterpart; for tests and tools): the symbolic
  * analysis (any pointer may be NULL; supernode_ptr holds n_supernodes + 1)
  * and the row permutation of the current factors (position -> row). */

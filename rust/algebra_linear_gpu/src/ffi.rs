@@ -207,6 +207,8 @@ unsafe extern "C" {
     pub fn alg_splu_flop_ratio(lu: *const alg_splu, ratio: *mut f64) -> c_int;
     pub fn alg_splu_get_stats(lu: *const alg_splu, out: *mut alg_splu_stats) -> c_int;
     pub fn alg_splu_free(lu: *mut alg_splu);
+    pub fn alg_zsplu_factorize(lu: *mut alg_splu, col_ptr: *const usize, col_ptr_len: usize, row_idx: *const usize, row_idx_len: usize, values: *const f64, values_len: usize) -> c_int;
+    pub fn alg_zsplu_solve(lu: *const alg_splu, b: *mut f64, b_len: usize) -> c_int;
     pub fn alg_splu_symbolic(lu: *const alg_splu, col_perm: *mut usize, col_perm_inv: *mut usize, col_counts: *mut usize, supernode_ptr: *mut usize, n_supernodes: *mut usize) -> c_int;
     pub fn alg_splu_row_perm(lu: *const alg_splu, row_perm: *mut usize) -> c_int;
     pub fn alg_splu_plan_info(lu: *const alg_splu, out: *mut alg_splu_plan) -> c_int;

@@ -10,7 +10,7 @@
 //! | `lapack::dgesv` (mod.rs:309) | [`lapack::dgesv`] |
 //! | `lapack::dgetri` (mod.rs:249) | [`lapack::dgetri`] |
 //! | `lapack::zgetrf` / `zgetrf_rect` / `zgesv` / `zgetri` (complex.rs:67, 169, 279, 217) | [`complex`] |
-//! | `sparse::faer::SparseLu<f64>` (sparse_lu.rs:45-156) | [`sparse::SparseLu`] |
+//! | `sparse::faer::SparseLu<f64>`, `SparseLu<Complex64>` (sparse_lu.rs:45-156, lu.rs:20-82) | [`sparse::SparseLu`] |
 //!
 //! Errors are the reference's enums ([`LapackError`], [`sparse::Error`]); a
 //! condition only a GPU has (no device, a CUDA error, out of device memory, a

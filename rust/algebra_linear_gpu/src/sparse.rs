@@ -1,14 +1,73 @@
 //! The sparse LU handle with the reference's API
-//! (`algebra_linear::sparse::faer::SparseLu<f64>`, src/sparse/faer/sparse_lu.rs:45-156).
+//! (`algebra_linear::sparse::faer::SparseLu<T>`, src/sparse/faer/sparse_lu.rs:45-156,
+//! for `T` = `f64` or `Complex64`, lu.rs:20-82).
 //! The symbolic analysis (COLAMD, elimination tree, column counts,
 //! supernodes) runs on the host as the reference's does; every numeric
 //! factorization and solve runs on the GPU. The caller owns the CSC arrays;
 //! they are borrowed per call and never retained.
 
 use core::ffi::c_int;
+use core::marker::PhantomData;
 use core::time::Duration;
 
+use num_complex::Complex64;
+
 use crate::ffi;
+
+mod sealed {
+    pub trait Sealed {}
+    impl Sealed for f64 {}
+    impl Sealed for num_complex::Complex64 {}
+}
+
+/// The scalars the sparse LU supports (the reference's `SparseScalar`,
+/// lu.rs:20-82): `f64` and `Complex64` (`#[repr(C)]` (re, im), passed to the
+/// library as interleaved doubles). Complex factors pivot by the modulus and
+/// take their multipliers by `Complex::inv`, in FP64.
+pub trait SparseScalar: Copy + sealed::Sealed {
+    #[doc(hidden)]
+    /// # Safety
+    /// `h` is a live handle; the slices are valid for their lengths.
+    unsafe fn factorize_raw(h: *mut ffi::alg_splu, col_ptr: &[usize], row_idx: &[usize], values: &[Self]) -> c_int;
+    #[doc(hidden)]
+    /// # Safety
+    /// `h` is a live handle; `b` is valid for its length.
+    unsafe fn solve_raw(h: *const ffi::alg_splu, b: &mut [Self]) -> c_int;
+}
+
+impl SparseScalar for f64 {
+    unsafe fn factorize_raw(h: *mut ffi::alg_splu, col_ptr: &[usize], row_idx: &[usize], values: &[Self]) -> c_int {
+        ffi::alg_splu_factorize(
+            h,
+            col_ptr.as_ptr(),
+            col_ptr.len(),
+            row_idx.as_ptr(),
+            row_idx.len(),
+            values.as_ptr(),
+            values.len(),
+        )
+    }
+    unsafe fn solve_raw(h: *const ffi::alg_splu, b: &mut [Self]) -> c_int {
+        ffi::alg_splu_solve(h, b.as_mut_ptr(), b.len())
+    }
+}
+
+impl SparseScalar for Complex64 {
+    unsafe fn factorize_raw(h: *mut ffi::alg_splu, col_ptr: &[usize], row_idx: &[usize], values: &[Self]) -> c_int {
+        ffi::alg_zsplu_factorize(
+            h,
+            col_ptr.as_ptr(),
+            col_ptr.len(),
+            row_idx.as_ptr(),
+            row_idx.len(),
+            values.as_ptr().cast::<f64>(),
+            values.len(),
+        )
+    }
+    unsafe fn solve_raw(h: *const ffi::alg_splu, b: &mut [Self]) -> c_int {
+        ffi::alg_zsplu_solve(h, b.as_mut_ptr().cast::<f64>(), b.len())
+    }
+}
 
 /// Errors reported by the sparse routines: the reference's `Error`
 /// (src/sparse/faer/error.rs:5-24) in declaration order, plus [`Error::Device`]
@@ -121,17 +180,18 @@ impl SparseLuStats {
 
 /// An opaque sparse LU factorization whose factors live on the GPU.
 #[derive(Debug)]
-pub struct SparseLu {
+pub struct SparseLu<T: SparseScalar = f64> {
     h: *mut ffi::alg_splu,
     n: usize,
     stats: Option<SparseLuStats>,
+    _scalar: PhantomData<T>,
 }
 
 // The handle is used by one thread at a time (`&mut` for factorize), as the
 // reference's is; moving it to another thread is fine.
-unsafe impl Send for SparseLu {}
+unsafe impl<T: SparseScalar> Send for SparseLu<T> {}
 
-impl SparseLu {
+impl<T: SparseScalar> SparseLu<T> {
     /// Analyzes the CSC pattern of a square matrix (sparse_lu.rs:64-78):
     /// `n = col_ptr.len() - 1`.
     ///
@@ -151,7 +211,7 @@ impl SparseLu {
         map(unsafe {
             ffi::alg_splu_analyze(col_ptr.as_ptr(), col_ptr.len(), row_idx.as_ptr(), row_idx.len(), m, thr, &mut h)
         })?;
-        Ok(Self { h, n, stats: None })
+        Ok(Self { h, n, stats: None, _scalar: PhantomData })
     }
 
     /// Factorizes new values on the analyzed pattern (sparse_lu.rs:91-121).
@@ -161,20 +221,10 @@ impl SparseLu {
     /// # Errors
     ///
     /// The CSC view errors, then [`Error::StructureMismatch`],
-    /// [`Error::NotFinite`], [`Error::Singular`].
-    pub fn factorize(&mut self, col_ptr: &[usize], row_idx: &[usize], values: &[f64]) -> Result<(), Error> {
-        // SAFETY: the slices are valid for their lengths for the call.
-        map(unsafe {
-            ffi::alg_splu_factorize(
-                self.h,
-                col_ptr.as_ptr(),
-                col_ptr.len(),
-                row_idx.as_ptr(),
-                row_idx.len(),
-                values.as_ptr(),
-                values.len(),
-            )
-        })?;
+    /// [`Error::NotFinite`] (either part, for complex values), [`Error::Singular`].
+    pub fn factorize(&mut self, col_ptr: &[usize], row_idx: &[usize], values: &[T]) -> Result<(), Error> {
+        // SAFETY: the handle is live and the slices are valid for their lengths for the call.
+        map(unsafe { T::factorize_raw(self.h, col_ptr, row_idx, values) })?;
         // SAFETY: a plain C struct, filled by the library.
         let mut s: ffi::alg_splu_stats = unsafe { core::mem::zeroed() };
         map(unsafe { ffi::alg_splu_get_stats(self.h, &mut s) })?;
@@ -203,9 +253,9 @@ impl SparseLu {
     ///
     /// [`Error::NotFactorized`] before a successful factorization,
     /// [`Error::BadShape`] if `b.len() != n`.
-    pub fn solve(&self, b: &mut [f64]) -> Result<(), Error> {
-        // SAFETY: b is valid for its length for the call.
-        map(unsafe { ffi::alg_splu_solve(self.h, b.as_mut_ptr(), b.len()) })
+    pub fn solve(&self, b: &mut [T]) -> Result<(), Error> {
+        // SAFETY: the handle is live and b is valid for its length for the call.
+        map(unsafe { T::solve_raw(self.h, b) })
     }
 
     /// The method selected during analysis (sparse_lu.rs:137-140).
@@ -240,7 +290,7 @@ impl SparseLu {
     }
 }
 
-impl Drop for SparseLu {
+impl<T: SparseScalar> Drop for SparseLu<T> {
     fn drop(&mut self) {
         // SAFETY: the handle came from alg_splu_analyze and is freed once.
         unsafe { ffi::alg_splu_free(self.h) };

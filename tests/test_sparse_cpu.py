@@ -145,6 +145,26 @@ def test_large_fronts_split_into_lanes(monkeypatch):
             assert plan["n_fronts"] == one["n_fronts"] and plan["plan_flops"] == one["plan_flops"]
 
 
+def test_plan_fronts_follow_the_column_etree(monkeypatch):
+    """The GPU plan cuts the reference's relaxed supernodes where the next
+    column is not the etree parent of the one before: a front then passes up
+    the unpivoted rows of its own subtree only, so the plan's flops stay
+    below the cost of the chol(A^T A) columns, sum 2 cc_j^2 (the glued
+    partition is several times above it on 3-D grids)."""
+    from oracle import sparse as osp
+
+    cp, ri, _ = osp.grid_pattern(24, 24, 24)
+    lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+    cc = lu.symbolic()["col_counts"].astype(float)
+    bound = 2.0 * (cc ** 2).sum()
+    split = lu.plan()
+    assert split["plan_flops"] <= bound
+    monkeypatch.setenv("ALG_SPLU_KEEP_GLUED", "1")
+    glued = SparseLu.analyze(cp, ri, LuMethod.supernodal()).plan()
+    assert glued["plan_flops"] > 1.5 * split["plan_flops"]
+    assert glued["factor_bytes"] > split["factor_bytes"]
+
+
 def _tridiag(n, dense=False):
     cp, ri, v = [0], [], []
     for j in range(n):
