@@ -59,22 +59,36 @@ __global__ void abs_rowsum_kernel(const double* __restrict__ a, int lda, int n, 
   partial[(size_t)blockIdx.y * n + i] = s;
 }
 
-// r = b - A x for nrhs columns (FP64). Partial products per column chunk,
-// summed in a fixed order by residual_finish_kernel (deterministic).
+// r = b - A x for nrhs columns (FP64). Partial products per chunk of `cols`
+// columns (<= kResCols), summed in a fixed order by residual_finish_kernel
+// (deterministic). A thread per row streams its chunk with eight loads in
+// flight.
 __global__ void residual_partial_kernel(const double* __restrict__ a, int lda, int n,
-                                        const double* __restrict__ x, int ldx, int nrhs,
+                                        const double* __restrict__ x, int ldx, int nrhs, int cols,
                                         double* __restrict__ partial) {
   const int i = blockIdx.x * kResRows + threadIdx.x;
-  const int j0 = blockIdx.y * kResCols;
-  const int j1 = min(n, j0 + kResCols);
+  const int j0 = blockIdx.y * cols;
+  const int j1 = min(n, j0 + cols);
   const int r = blockIdx.z;
   __shared__ double xs[kResCols];
   for (int j = j0 + threadIdx.x; j < j1; j += kResRows) xs[j - j0] = x[(size_t)r * ldx + j];
   __syncthreads();
   if (i >= n) return;
   double s = 0.0;
-  for (int j = j0; j < j1; ++j) s = __fma_rn(a[(size_t)i + (size_t)j * lda], xs[j - j0], s);
+  const double* ai = a + i;
+#pragma unroll 8
+  for (int j = j0; j < j1; ++j) s = __fma_rn(ai[(size_t)j * lda], xs[j - j0], s);
   partial[((size_t)r * gridDim.y + blockIdx.y) * n + i] = s;
+}
+
+// Chunk width of the residual: kResCols, narrower when the grid would give
+// fewer than four CTAs per SM (the row blocks alone do not fill the GPU
+// below n ~ 16k); a multiple of 32.
+int res_cols(int n, int sms) {
+  const long long rows = (n + kResRows - 1) / kResRows;
+  int cols = kResCols;
+  while (cols > 32 && rows * ((n + cols - 1) / cols) < 4LL * sms) cols /= 2;
+  return cols;
 }
 
 // max that keeps a NaN (fmax would drop it and hide a diverged solve)
@@ -196,12 +210,13 @@ int inf_norm_dev(alg_ctx* ctx, const double* a, int n, int lda, double* out_host
 }
 
 int gemv_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x, double* y) {
-  const int nchunks = (n + kResCols - 1) / kResCols;
+  const int cols = res_cols(n, ctx->sm_count);
+  const int nchunks = (n + cols - 1) / cols;
   double* partial = nullptr;
   ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n, reinterpret_cast<void**>(&partial)));
   const int tok = prof_begin(ctx, ALG_K_RESID);
   residual_partial_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks, 1), kResRows, 0, ctx->stream>>>(
-      a, lda, n, x, n, 1, partial);
+      a, lda, n, x, n, 1, cols, partial);
   gemv_finish_kernel<<<grid_for(n, ctx->sm_count), kVecThreads, 0, ctx->stream>>>(partial, nchunks, n, y);
   count_launches(2);
   prof_end(ctx, tok, 2.0 * n * n, 8.0 * n * n + 16.0 * n);
@@ -211,7 +226,8 @@ int gemv_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x, dou
 
 int residual_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x, int ldx, const double* b,
                  int ldb, double* r, int ldr, int nrhs, double* rmax, double* xmax, double* bmax) {
-  const int nchunks = (n + kResCols - 1) / kResCols;
+  const int cols = res_cols(n, ctx->sm_count);
+  const int nchunks = (n + cols - 1) / cols;
   double* partial = nullptr;
   unsigned long long* st = nullptr;
   ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n * nrhs, reinterpret_cast<void**>(&partial)));
@@ -219,7 +235,7 @@ int residual_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x,
   ALG_CUDA_TRY(cudaMemsetAsync(st, 0, 32 * (size_t)nrhs, ctx->stream));
   const int tok = prof_begin(ctx, ALG_K_RESID);
   residual_partial_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks, nrhs), kResRows, 0, ctx->stream>>>(
-      a, lda, n, x, ldx, nrhs, partial);
+      a, lda, n, x, ldx, nrhs, cols, partial);
   residual_finish_kernel<<<dim3(std::max(1, std::min(4 * ctx->sm_count, (n + 255) / 256)), nrhs), 256, 0,
                            ctx->stream>>>(partial, nchunks, n, b, ldb, x, ldx, r, ldr, nrhs, st);
   count_launches(2);

@@ -521,6 +521,10 @@ __global__ void __launch_bounds__(kSmallThreads) zfront_gemm_kernel(zc* C, const
 // ---- after the factorization -----------------------------------------------
 // Final position of every row, the row permutation, and the nonzero counts
 // of each column of L and U (exact zeros are not stored, as in the reference).
+// Grid: fronts x kCountSplit; CTA (s, y) takes every kCountSplit-th group of
+// a front's columns, a warp per column.
+constexpr int kCountSplit = 16;
+
 template <typename T>
 __global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const int32_t* rowid, const T* L,
                                         const T* U, const int32_t* struct_cols, int32_t* pos_of_row,
@@ -529,14 +533,17 @@ __global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const i
   if (s >= ns) return;
   const FrontDesc d = fronts[s];
   const int rows = d.rows, size = d.size;
-  for (int k = threadIdx.x; k < size; k += blockDim.x) {
-    const int32_t r = rowid[d.rowid_off + k];
-    pos_of_row[r] = d.begin + k;
-    row_perm[d.begin + k] = r;
-  }
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int warp = (threadIdx.x >> 5) + (int)blockIdx.y * nw, nwt = nw * (int)gridDim.y;
+  if ((int)blockIdx.y * nw >= max(size, d.ncb)) return;  // no column for this CTA
+  if (blockIdx.y == 0)
+    for (int k = threadIdx.x; k < size; k += blockDim.x) {
+      const int32_t r = rowid[d.rowid_off + k];
+      pos_of_row[r] = d.begin + k;
+      row_perm[d.begin + k] = r;
+    }
   const T* lp = L + d.l_off;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int jj = warp; jj < size; jj += nw) {
+  for (int jj = warp; jj < size; jj += nwt) {
     int cl = 0, cu = 0;
     for (int i = lane; i < rows; i += 32) {
       const T v = lp[i + (int64_t)jj * rows];
@@ -553,7 +560,7 @@ __global__ void positions_counts_kernel(const FrontDesc* fronts, int ns, const i
     }
   }
   const T* up = U + d.u_off;
-  for (int t = warp; t < d.ncb; t += nw) {
+  for (int t = warp; t < d.ncb; t += nwt) {
     int cu = 0;
     for (int kk = lane; kk < size; kk += 32) cu += up[kk + (int64_t)t * size] != T(0);
     for (int off = 16; off > 0; off >>= 1) cu += __shfl_xor_sync(0xffffffffu, cu, off);
@@ -1108,8 +1115,8 @@ int DeviceLu::factor_t(int b, const double* values, int tc_prec) {
   for (int32_t s : F.top_fronts) ALG_TRY(factor_big<T>(b, s, 0, values, tc_prec));
   ALG_CUDA_TRY(cudaMemsetAsync(out.ucount, 0, sizeof(unsigned) * std::max<idx>(F.n, 1), st));
   if (F.ns > 0) {
-    positions_counts_kernel<T><<<(int)F.ns, 256, 0, st>>>(d_fronts, (int)F.ns, out.rowid, L, U, d_struct_cols,
-                                                           out.pos_of_row, out.row_perm, out.lcount, out.ucount);
+    positions_counts_kernel<T><<<dim3((unsigned)F.ns, kCountSplit), 256, 0, st>>>(
+        d_fronts, (int)F.ns, out.rowid, L, U, d_struct_cols, out.pos_of_row, out.row_perm, out.lcount, out.ucount);
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
@@ -1162,8 +1169,13 @@ int DeviceLu::factor_big(int b, int32_t s, int lane, const double* values, int t
       const char* e = std::getenv("ALG_SPLU_NB");
       return e ? std::max(16, std::atoi(e)) : 64;
     }();
+    // leaf-panel width (ALG_SPLU_NBL: measurement switch)
+    static const int splu_nbl = [] {
+      const char* e = std::getenv("ALG_SPLU_NBL");
+      return e ? std::max(1, std::min(32, std::atoi(e))) : 16;
+    }();
     lp.nb = splu_nb;
-    lp.nbl = 16;
+    lp.nbl = splu_nbl;
     lp.tc_prec = tc_prec;
     if constexpr (std::is_same<T, float>::value) {
       // the mixed form's FP32 fronts pivot by tournament (refinement restores
