@@ -86,11 +86,27 @@ def test_admission_respects_the_budget(gpu, oracle):
     assert all(r.status == 0 for r in reqs)
 
 
+def _eta_extended(a, x, b, n):
+    """The normwise backward error of x with the residual in x87 extended
+    precision (64-bit significand), so the reference value carries none of
+    the FP64 residual's own rounding."""
+    import numpy as np
+
+    A = a.reshape(n, n).T.astype(np.longdouble)
+    xl, bl = x.astype(np.longdouble), b.astype(np.longdouble)
+    r = bl - A @ xl
+    return float(np.abs(r).max() / (np.abs(A).sum(axis=1).max() * np.abs(xl).max() + np.abs(bl).max()))
+
+
 def test_reported_backward_error_matches_the_host(gpu, oracle):
     """A mixed dense request reports the refinement's final normwise
     backward error; it must agree with the error of the returned x computed
-    on the host (within a factor of 4: the residual is summed in another
-    order) and be within 10 n 2^-53. Plain FP64 requests report -1."""
+    on the host with an extended-precision residual, to a factor of 4 plus
+    the FP64 residual's own rounding (about sqrt(n) 2^-53 of the
+    normalisation), and be within 10 n 2^-53. Plain FP64 requests report
+    -1."""
+    import numpy as np
+
     from algebra_linear_b200.serve import Request, Server
 
     reqs, systems = [], []
@@ -106,10 +122,10 @@ def test_reported_backward_error_matches_the_host(gpu, oracle):
     assert all(r.status == 0 for r in reqs)
     assert reqs[-1].backward_error == -1.0
     for r, (a, b, n) in zip(reqs, systems):
-        host = oracle.backward_error(a, r.solution, b, n)
+        host = _eta_extended(a, r.solution, b, n)
         rep = r.backward_error
+        slack = 4 * np.sqrt(n) * 2.0**-53
         print(f"n={n}: reported eta {rep:.3e}, host eta {host:.3e}")
         assert host <= 10 * n * 2.0**-53, (n, host)
-        assert rep <= 10 * n * 2.0**-53, (n, rep)
-        if host > 0:
-            assert host / 4 <= rep <= 4 * host, (n, rep, host)
+        assert 0 < rep <= 10 * n * 2.0**-53, (n, rep)
+        assert host / 4 - slack <= rep <= 4 * host + slack, (n, rep, host)
