@@ -461,10 +461,73 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
   return rc;
 }
 
+// Right-hand sides from which the fused forms solve blocked (the dataflow
+// sweeps take four right-hand sides per pass).
+constexpr int kBlockedSolveRhs = 16;
+constexpr int kSolveBlock = 128;
+
+// b (n x nrhs, ldb) <- (LU)^{-1} P b for many right-hand sides (fused
+// arithmetic): the rows gathered by perm into the workspace, then each sweep
+// in blocks of kSolveBlock rows: the block's triangle solved in registers
+// (K3s), the right-hand sides of the rows not yet solved updated by one GEMM
+// (X_below -= L21 X_block, X_above -= U12 X_block; on the FP64 tensor cores
+// for FP64).
+template <typename T>
+int lu_solve_blocked_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs, int ldb) {
+  if (n == 0 || nrhs == 0) return ALG_OK;
+  T* x = nullptr;
+  ALG_TRY(ws_get(ctx, WS_X, sizeof(T) * (size_t)n * nrhs, reinterpret_cast<void**>(&x)));
+  constexpr size_t kSmem = sizeof(T) * kSolveBlock * kSolveBlock;
+  static const cudaError_t configured = [] {
+    cudaError_t e = cudaFuncSetAttribute(trsm_block_solve_kernel<T, false, 4, 2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(trsm_block_solve_kernel<T, true, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSmem);
+    return e;
+  }();
+  ALG_CUDA_TRY(configured);
+  const int tok = prof_begin(ctx, ALG_K_SOLVE);
+  {
+    const size_t cnt = (size_t)n * nrhs;
+    const int g = (int)std::max<size_t>(1, std::min<size_t>((cnt + 255) / 256, (size_t)ctx->sm_count * 8));
+    gather_perm_rows_kernel<T><<<g, 256, 0, ctx->stream>>>(b, ldb, perm, n, nrhs, x, n);
+    count_launches();
+  }
+  const int cta_cols = 2 * (kTrsmThreads / 32);
+  const int grid = (nrhs + cta_cols - 1) / cta_cols;
+  for (int k0 = 0; k0 < n; k0 += kSolveBlock) {  // L y = P b
+    const int kb = std::min(kSolveBlock, n - k0), k1 = k0 + kb;
+    trsm_block_solve_kernel<T, false, 4, 2><<<grid, kTrsmThreads, sizeof(T) * kb * kb, ctx->stream>>>(
+        lu, lda, k0, kb, x, n, nrhs);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+    if (k1 < n)
+      ALG_TRY((gemm_sub_dev<T, false>(ctx, n - k1, nrhs, kb, lu + (size_t)k1 + (size_t)k0 * lda, lda, x + k0, n,
+                                      x + k1, n)));
+  }
+  for (int k1 = n; k1 > 0; k1 -= kSolveBlock) {  // U x = y
+    const int kb = std::min(kSolveBlock, k1), k0 = k1 - kb;
+    trsm_block_solve_kernel<T, true, 4, 2><<<grid, kTrsmThreads, sizeof(T) * kb * kb, ctx->stream>>>(
+        lu, lda, k0, kb, x, n, nrhs);
+    count_launches();
+    ALG_CUDA_TRY(cudaGetLastError());
+    if (k0 > 0)
+      ALG_TRY((gemm_sub_dev<T, false>(ctx, k0, nrhs, kb, lu + (size_t)k0 * lda, lda, x + k0, n, x, n)));
+  }
+  ALG_CUDA_TRY(cudaMemcpy2DAsync(b, sizeof(T) * (size_t)ldb, x, sizeof(T) * (size_t)n, sizeof(T) * (size_t)n, nrhs,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+  prof_end(ctx, tok, 2.0 * n * n * nrhs, sizeof(T) * (double(n) * n + 4.0 * n * nrhs));
+  return ALG_OK;
+}
+
 template <typename T, bool EXACT>
 int lu_solve_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs,
                  int ldb) {
   if (nrhs > 65535) return ALG_BAD_SHAPE;
+  // the exact form keeps the reference's per-entry order (the dataflow
+  // sweeps); the fused forms solve many right-hand sides blocked
+  if (!EXACT && nrhs >= kBlockedSolveRhs) return lu_solve_blocked_dev<T>(ctx, lu, n, lda, perm, b, nrhs, ldb);
   return lu_solve_dataflow_dev<T, EXACT>(ctx, lu, n, lda, perm, b, nrhs, ldb);
 }
 

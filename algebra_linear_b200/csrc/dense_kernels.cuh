@@ -623,8 +623,10 @@ __global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<
         cand_idx[par][warp] = INT_MAX;
       }
       __syncthreads();
-      // ---- 2. warp 0 sends the CTA record (and row j) to every mailbox -------
-      if (warp == 0) {
+      // ---- 2. the CTA record (and row j) to every mailbox: each of the first
+      // min(NW, C) warps forms the record and sends it to the CTAs t with
+      // t % NW == warp (C == 1: warp 0 into the own mailbox) -------------------
+      if (warp < (C > 1 ? min(NW, C) : 1)) {
         double ck = -CUDART_INF;
         int ci = INT_MAX, cw = 0;
         if (lane < NW) { ck = cand_key[par][lane]; ci = cand_idx[par][lane]; cw = lane; }
@@ -639,7 +641,7 @@ __global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<
         const T* crow = &stage[par][cw][0];
         const bool own_j = j >= rb && j < re;
         // lane kw builds word kw of the record in a register and stores it
-        // into slot q of every CTA's mailbox with st.async (each 8-byte store
+        // into slot q of its CTAs' mailboxes with st.async (each 8-byte store
         // completes on that CTA's mbarrier); C == 1: straight into the own
         // mailbox. No staging in shared memory, no proxy fence, no bulk copy.
         const uint32_t bar_par = bar_base + 8u * par;
@@ -651,7 +653,7 @@ __global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<
           else if (kw < 3 + Rec::kRowWords) val = row_word<T, W>(crow, kw - 3);
           if (C > 1) {
             const uint32_t la = rec_base + 8u * (uint32_t)((par * kPanelMaxC + q) * Rec::kWords + kw);
-            for (int t = 0; t < C; ++t) st_async_b64(mapa_u32(la, t), val, mapa_u32(bar_par, t));
+            for (int t = warp; t < C; t += NW) st_async_b64(mapa_u32(la, t), val, mapa_u32(bar_par, t));
           } else {
             rec[par][0][kw] = val;
           }
@@ -663,7 +665,7 @@ __global__ void __launch_bounds__(kPanelRThreads, 1) panel_reg_kernel(PanelArgs<
             else if (kw < 1 + Rec::kRowWords) val = row_word<T, W>(&dstage[par][0], kw - 1);
             if (C > 1) {
               const uint32_t ld = diag_base + 8u * (uint32_t)(par * Rec::kDiagWords + kw);
-              for (int t = 0; t < C; ++t) st_async_b64(mapa_u32(ld, t), val, mapa_u32(bar_par, t));
+              for (int t = warp; t < C; t += NW) st_async_b64(mapa_u32(ld, t), val, mapa_u32(bar_par, t));
             } else {
               diag[par][kw] = val;
             }
@@ -950,6 +952,115 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T*
       const int i = lane + 32 * r;
       if (cc < ncol && i < kb) a[(size_t)(r0 + i) + (size_t)(c_first + cc) * lda] = x[c][r];
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3s: one block of the blocked many-right-hand-side solve (fused
+// arithmetic): X[r0:r0+kb, 0:ncols] <- T11^{-1} X[r0:r0+kb, :] with T11 =
+// lu[r0:r0+kb, r0:r0+kb], unit lower (UPPER false) or upper (UPPER true,
+// x_k = x_k / u_kk from the last row up). The K3 layout: T11 (kb <= 128) in
+// shared memory, each warp owns CPW columns of X with lane l holding rows
+// l, l + 32, ... in registers; step k broadcasts x_k from its owner lane.
+// ---------------------------------------------------------------------------
+template <typename T, bool UPPER, int RPT, int CPW>
+__global__ void __launch_bounds__(kTrsmThreads, 1) trsm_block_solve_kernel(const T* lu, int lda, int r0, int kb, T* x,
+                                                                        int ldx, int ncols) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* M = reinterpret_cast<T*>(smem_raw);  // kb x kb, column-major
+  constexpr int kCtaCols = CPW * (kTrsmThreads / 32);
+  const int c_first = blockIdx.x * kCtaCols;
+  const int ncol = min(kCtaCols, ncols - c_first);
+  if (ncol <= 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T v[CPW][RPT];
+#pragma unroll
+  for (int c = 0; c < CPW; ++c) {
+    const int cc = warp * CPW + c;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int i = lane + 32 * r;
+      v[c][r] = (cc < ncol && i < kb) ? x[(size_t)(r0 + i) + (size_t)(c_first + cc) * ldx] : T(0);
+    }
+  }
+  const int total = kb * kb;
+  for (int idx = threadIdx.x; idx < total; idx += kTrsmThreads) {
+    const int i = idx % kb, k = idx / kb;
+    const bool keep = UPPER ? i <= k : i > k;
+    M[idx] = keep ? lu[(size_t)(r0 + i) + (size_t)(r0 + k) * lda] : T(0);
+  }
+  __syncthreads();
+  if constexpr (!UPPER) {
+    for (int k = 0; k + 1 < kb; ++k) {
+      const int owner = k & 31, rk = k >> 5;
+      T u[CPW];
+#pragma unroll
+      for (int c = 0; c < CPW; ++c) {
+        T xv = v[c][0];
+#pragma unroll
+        for (int r = 1; r < RPT; ++r)
+          if (r == rk) xv = v[c][r];
+        u[c] = __shfl_sync(0xffffffffu, xv, owner);
+      }
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        const int i = lane + 32 * r;
+        if (i > k && i < kb) {
+          const T l = M[i + (size_t)k * kb];
+#pragma unroll
+          for (int c = 0; c < CPW; ++c) v[c][r] = msub<false>(v[c][r], l, u[c]);
+        }
+      }
+    }
+  } else {
+    for (int k = kb - 1; k >= 0; --k) {
+      const int owner = k & 31, rk = k >> 5;
+      const T d = M[k + (size_t)k * kb];
+      T u[CPW];
+#pragma unroll
+      for (int c = 0; c < CPW; ++c) {
+        T xv = v[c][0];
+#pragma unroll
+        for (int r = 1; r < RPT; ++r)
+          if (r == rk) xv = v[c][r];
+        if (lane == owner) {
+          xv = xv / d;
+#pragma unroll
+          for (int r = 0; r < RPT; ++r)
+            if (r == rk) v[c][r] = xv;
+        }
+        u[c] = __shfl_sync(0xffffffffu, xv, owner);
+      }
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        const int i = lane + 32 * r;
+        if (i < k) {
+          const T m = M[i + (size_t)k * kb];
+#pragma unroll
+          for (int c = 0; c < CPW; ++c) v[c][r] = msub<false>(v[c][r], m, u[c]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < CPW; ++c) {
+    const int cc = warp * CPW + c;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int i = lane + 32 * r;
+      if (cc < ncol && i < kb) x[(size_t)(r0 + i) + (size_t)(c_first + cc) * ldx] = v[c][r];
+    }
+  }
+}
+
+// x[i, c] = b[perm[i], c] (the row interchanges of P, n x ncols)
+template <typename T>
+__global__ void gather_perm_rows_kernel(const T* __restrict__ b, int ldb, const int* __restrict__ perm, int n,
+                                        int ncols, T* __restrict__ x, int ldx) {
+  const size_t cnt = (size_t)n * ncols;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    x[(size_t)i + (size_t)c * ldx] = b[(size_t)perm[i] + (size_t)c * ldb];
   }
 }
 

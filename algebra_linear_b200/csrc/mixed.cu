@@ -48,6 +48,9 @@ __global__ void cast_f64_f32_kernel(const double* __restrict__ a, int lda, float
 // chunks; partial[chunk][row].
 constexpr int kResRows = 256;
 constexpr int kResCols = 512;
+// right-hand sides from which the residual is one GEMM (the row kernel reads
+// A once per right-hand side)
+constexpr int kGemmResidualRhs = 4;
 
 __global__ void abs_rowsum_kernel(const double* __restrict__ a, int lda, int n, double* __restrict__ partial) {
   const int i = blockIdx.x * kResRows + threadIdx.x;
@@ -112,6 +115,29 @@ __global__ void residual_finish_kernel(const double* __restrict__ partial, int n
     mr = nanmax(mr, fabs(ri));
     mx = nanmax(mx, fabs(x[(size_t)r * ldx + i]));
     mb = nanmax(mb, fabs(bi));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    mr = nanmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
+    mx = nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    mb = nanmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&stats[r * 4 + 0], (unsigned long long)__double_as_longlong(mr));
+    atomicMax(&stats[r * 4 + 1], (unsigned long long)__double_as_longlong(mx));
+    atomicMax(&stats[r * 4 + 2], (unsigned long long)__double_as_longlong(mb));
+  }
+}
+
+// The norms of residual_finish_kernel for a residual already formed in res.
+__global__ void residual_norms_kernel(const double* __restrict__ res, int ldr, const double* __restrict__ x, int ldx,
+                                      const double* __restrict__ b, int ldb, int n,
+                                      unsigned long long* __restrict__ stats) {
+  const int r = blockIdx.y;
+  double mr = 0.0, mx = 0.0, mb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    mr = nanmax(mr, fabs(res[(size_t)r * ldr + i]));
+    mx = nanmax(mx, fabs(x[(size_t)r * ldx + i]));
+    mb = nanmax(mb, fabs(b[(size_t)r * ldb + i]));
   }
   for (int off = 16; off > 0; off >>= 1) {
     mr = nanmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
@@ -230,16 +256,29 @@ int residual_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* x,
   const int nchunks = (n + cols - 1) / cols;
   double* partial = nullptr;
   unsigned long long* st = nullptr;
-  ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n * nrhs, reinterpret_cast<void**>(&partial)));
+  if (nrhs < kGemmResidualRhs)
+    ALG_TRY(ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * n * nrhs, reinterpret_cast<void**>(&partial)));
   ALG_TRY(ws_get(ctx, WS_MISC, 4096 + 32 * (size_t)nrhs, reinterpret_cast<void**>(&st)));
   ALG_CUDA_TRY(cudaMemsetAsync(st, 0, 32 * (size_t)nrhs, ctx->stream));
-  const int tok = prof_begin(ctx, ALG_K_RESID);
-  residual_partial_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks, nrhs), kResRows, 0, ctx->stream>>>(
-      a, lda, n, x, ldx, nrhs, cols, partial);
-  residual_finish_kernel<<<dim3(std::max(1, std::min(4 * ctx->sm_count, (n + 255) / 256)), nrhs), 256, 0,
-                           ctx->stream>>>(partial, nchunks, n, b, ldb, x, ldx, r, ldr, nrhs, st);
-  count_launches(2);
-  prof_end(ctx, tok, 2.0 * n * n * nrhs, 8.0 * n * n + 24.0 * n * nrhs);
+  const dim3 fin(std::max(1, std::min(4 * ctx->sm_count, (n + 255) / 256)), nrhs);
+  if (nrhs >= kGemmResidualRhs) {
+    // R = B, then R -= A X as one FP64 tensor-core GEMM (A read once for
+    // all right-hand sides), then the norms
+    ALG_CUDA_TRY(cudaMemcpy2DAsync(r, sizeof(double) * ldr, b, sizeof(double) * ldb, sizeof(double) * n, nrhs,
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
+    ALG_TRY(gemm_dmma_sub_dev(ctx, n, nrhs, n, a, lda, x, ldx, r, ldr));
+    const int tok = prof_begin(ctx, ALG_K_RESID);
+    residual_norms_kernel<<<fin, 256, 0, ctx->stream>>>(r, ldr, x, ldx, b, ldb, n, st);
+    count_launches();
+    prof_end(ctx, tok, 0.0, 24.0 * n * nrhs);
+  } else {
+    const int tok = prof_begin(ctx, ALG_K_RESID);
+    residual_partial_kernel<<<dim3((n + kResRows - 1) / kResRows, nchunks, nrhs), kResRows, 0, ctx->stream>>>(
+        a, lda, n, x, ldx, nrhs, cols, partial);
+    residual_finish_kernel<<<fin, 256, 0, ctx->stream>>>(partial, nchunks, n, b, ldb, x, ldx, r, ldr, nrhs, st);
+    count_launches(2);
+    prof_end(ctx, tok, 2.0 * n * n * nrhs, 8.0 * n * n + 24.0 * n * nrhs);
+  }
   ALG_CUDA_TRY(cudaGetLastError());
   std::vector<unsigned long long> h(4 * (size_t)nrhs);
   ALG_CUDA_TRY(cudaMemcpyAsync(h.data(), st, 32 * (size_t)nrhs, cudaMemcpyDeviceToHost, ctx->stream));
@@ -316,7 +355,9 @@ int dgesv_mixed_dev(alg_ctx* ctx, const alg_mixed_opts& o, double* d_a, int n, i
   if (n == 0 || nrhs == 0) return ALG_OK;
   const double tol = o.tol > 0 ? o.tol : 10.0 * n * std::ldexp(1.0, -53);
   const int max_ir = o.max_ir > 0 ? o.max_ir : 30;
-  const int kmax = std::min(nrhs, 8);
+  // right-hand sides per preconditioner application: all of them up to 256
+  // (from 16 the FP32 solve is blocked, GEMM-rich)
+  const int kmax = std::min(nrhs, 256);
 
   LowpFactor F;
   F.ctx = ctx;

@@ -153,6 +153,28 @@ def test_dgesv_64_rhs_matches_dgetrs_per_column(gpu, oracle):
     assert rel_err(gb, rb) <= REL_TOL
 
 
+@pytest.mark.parametrize("n,nrhs", [(300, 64), (777, 16), (129, 200), (1000, 33)])
+def test_fused_many_rhs_blocked_solve(gpu, oracle, n, nrhs):
+    """From 16 right-hand sides the fused form solves blocked (128-row
+    triangles in registers, the rest by GEMMs): same pivots as the
+    reference, each column's backward error within 10 n 2^-53 and x within
+    1e-10 of the oracle's per-column dgetrs (another summation order)."""
+    from algebra_linear_b200.lapack import dgesv_nrhs
+
+    a0, s = oracle.larnv("Symmetric", [5, 6, 7, 2 * n + 1], n * n)
+    b0, _ = oracle.larnv("Symmetric", s, n * nrhs)
+    ra, rb = a0.copy(), b0.copy()
+    rc, ripiv = oracle.dgesv(ra, rb, n, nrhs)
+    assert rc == 0
+    ga, gb = a0.copy(), b0.copy()
+    ipiv = dgesv_nrhs(ga, gb, n, nrhs, update=1)
+    assert ipiv == ripiv
+    assert rel_err(gb, rb) <= 1e-10
+    for c in range(0, nrhs, max(1, nrhs // 4)):
+        col = slice(c * n, (c + 1) * n)
+        assert oracle.backward_error(a0, gb[col].copy(), b0[col].copy(), n) < 10 * n * 2.0**-53
+
+
 def test_forward_sweep_is_exact_and_solution_close(gpu, oracle):
     """Odd sizes across several solve blocks (64 rows each)."""
     from algebra_linear_b200.lapack import dgesv
