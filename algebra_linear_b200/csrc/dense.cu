@@ -464,58 +464,72 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
 // Right-hand sides from which the fused forms solve blocked (the dataflow
 // sweeps take four right-hand sides per pass).
 constexpr int kBlockedSolveRhs = 16;
-constexpr int kSolveBlock = 128;
 
 // b (n x nrhs, ldb) <- (LU)^{-1} P b for many right-hand sides (fused
-// arithmetic): the rows gathered by perm into the workspace, then each sweep
-// in blocks of kSolveBlock rows: the block's triangle solved in registers
-// (K3s), the right-hand sides of the rows not yet solved updated by one GEMM
-// (X_below -= L21 X_block, X_above -= U12 X_block; on the FP64 tensor cores
-// for FP64).
+// arithmetic): the inverses of the 128 x 128 diagonal blocks of L and U
+// (K3i, two launches), the rows gathered by perm, then per block one K3b
+// launch per sweep: X_block <- T_bb^{-1} X_block by every CTA, the rows not
+// yet solved updated by the block's column of the factor. The forward sweep
+// reads x1 and writes y into x2; the backward sweep reads x2 and writes x
+// into x1.
 template <typename T>
 int lu_solve_blocked_dev(alg_ctx* ctx, const T* lu, int n, int lda, const int* perm, T* b, int nrhs, int ldb) {
   if (n == 0 || nrhs == 0) return ALG_OK;
-  T* x = nullptr;
-  ALG_TRY(ws_get(ctx, WS_X, sizeof(T) * (size_t)n * nrhs, reinterpret_cast<void**>(&x)));
-  constexpr size_t kSmem = sizeof(T) * kSolveBlock * kSolveBlock;
+  constexpr int kb = kSolveKb;
+  const int nblk = (n + kb - 1) / kb;
+  T* x1 = nullptr;
+  ALG_TRY(ws_get(ctx, WS_X, sizeof(T) * (2 * (size_t)n * nrhs + 2 * (size_t)nblk * kb * kb),
+                 reinterpret_cast<void**>(&x1)));
+  T* x2 = x1 + (size_t)n * nrhs;
+  T* linv = x2 + (size_t)n * nrhs;
+  T* uinv = linv + (size_t)nblk * kb * kb;
+  constexpr size_t kInvSmem = sizeof(T) * kb * kb;
+  constexpr int kSolveCols = solve_cols<T>();
+  constexpr size_t kStepSmem = sizeof(T) * (kSolveKb * kSolveKb + kSolveKb * kSolveCols);
   static const cudaError_t configured = [] {
-    cudaError_t e = cudaFuncSetAttribute(trsm_block_solve_kernel<T, false, 4, 2>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    cudaError_t e = cudaFuncSetAttribute(tri_block_inverse_kernel<T, false, 4, 2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(trsm_block_solve_kernel<T, true, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSmem);
+      e = cudaFuncSetAttribute(tri_block_inverse_kernel<T, true, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kInvSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(block_solve_step_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kStepSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(block_solve_step_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kStepSmem);
     return e;
   }();
   ALG_CUDA_TRY(configured);
   const int tok = prof_begin(ctx, ALG_K_SOLVE);
   {
+    const dim3 ig(kb / (2 * (kTrsmThreads / 32)), nblk);
+    tri_block_inverse_kernel<T, false, 4, 2><<<ig, kTrsmThreads, kInvSmem, ctx->stream>>>(lu, lda, n, kb, linv);
+    tri_block_inverse_kernel<T, true, 4, 2><<<ig, kTrsmThreads, kInvSmem, ctx->stream>>>(lu, lda, n, kb, uinv);
     const size_t cnt = (size_t)n * nrhs;
     const int g = (int)std::max<size_t>(1, std::min<size_t>((cnt + 255) / 256, (size_t)ctx->sm_count * 8));
-    gather_perm_rows_kernel<T><<<g, 256, 0, ctx->stream>>>(b, ldb, perm, n, nrhs, x, n);
-    count_launches();
-  }
-  const int cta_cols = 2 * (kTrsmThreads / 32);
-  const int grid = (nrhs + cta_cols - 1) / cta_cols;
-  for (int k0 = 0; k0 < n; k0 += kSolveBlock) {  // L y = P b
-    const int kb = std::min(kSolveBlock, n - k0), k1 = k0 + kb;
-    trsm_block_solve_kernel<T, false, 4, 2><<<grid, kTrsmThreads, sizeof(T) * kb * kb, ctx->stream>>>(
-        lu, lda, k0, kb, x, n, nrhs);
-    count_launches();
+    gather_perm_rows_kernel<T><<<g, 256, 0, ctx->stream>>>(b, ldb, perm, n, nrhs, x1, n);
+    count_launches(3);
     ALG_CUDA_TRY(cudaGetLastError());
-    if (k1 < n)
-      ALG_TRY((gemm_sub_dev<T, false>(ctx, n - k1, nrhs, kb, lu + (size_t)k1 + (size_t)k0 * lda, lda, x + k0, n,
-                                      x + k1, n)));
   }
-  for (int k1 = n; k1 > 0; k1 -= kSolveBlock) {  // U x = y
-    const int kb = std::min(kSolveBlock, k1), k0 = k1 - kb;
-    trsm_block_solve_kernel<T, true, 4, 2><<<grid, kTrsmThreads, sizeof(T) * kb * kb, ctx->stream>>>(
-        lu, lda, k0, kb, x, n, nrhs);
+  const int ctiles = (nrhs + kSolveCols - 1) / kSolveCols;
+  for (int k0 = 0; k0 < n; k0 += kb) {  // L y = P b: x1 -> y in x2
+    const int kbe = std::min(kb, n - k0);
+    const int rows = n - (k0 + kbe);
+    const dim3 grid(std::max(1, (rows + kSolveKb - 1) / kSolveKb), ctiles);
+    block_solve_step_kernel<T, false><<<grid, 256, kStepSmem, ctx->stream>>>(
+        lu, lda, n, k0, kbe, linv + (size_t)(k0 / kb) * kb * kb, x1, x2, nrhs);
     count_launches();
-    ALG_CUDA_TRY(cudaGetLastError());
-    if (k0 > 0)
-      ALG_TRY((gemm_sub_dev<T, false>(ctx, k0, nrhs, kb, lu + (size_t)k0 * lda, lda, x + k0, n, x, n)));
   }
-  ALG_CUDA_TRY(cudaMemcpy2DAsync(b, sizeof(T) * (size_t)ldb, x, sizeof(T) * (size_t)n, sizeof(T) * (size_t)n, nrhs,
+  for (int blk = nblk - 1; blk >= 0; --blk) {  // U x = y: x2 -> x in x1
+    const int k0 = blk * kb, kbe = std::min(kb, n - k0);
+    const dim3 grid(std::max(1, (k0 + kSolveKb - 1) / kSolveKb), ctiles);
+    block_solve_step_kernel<T, true><<<grid, 256, kStepSmem, ctx->stream>>>(
+        lu, lda, n, k0, kbe, uinv + (size_t)blk * kb * kb, x2, x1, nrhs);
+    count_launches();
+  }
+  ALG_CUDA_TRY(cudaGetLastError());
+  ALG_CUDA_TRY(cudaMemcpy2DAsync(b, sizeof(T) * (size_t)ldb, x1, sizeof(T) * (size_t)n, sizeof(T) * (size_t)n, nrhs,
                                  cudaMemcpyDeviceToDevice, ctx->stream));
   prof_end(ctx, tok, 2.0 * n * n * nrhs, sizeof(T) * (double(n) * n + 4.0 * n * nrhs));
   return ALG_OK;

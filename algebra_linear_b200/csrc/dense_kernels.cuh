@@ -956,42 +956,45 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_lower_unit_reg_kernel(T*
 }
 
 // ---------------------------------------------------------------------------
-// K3s: one block of the blocked many-right-hand-side solve (fused
-// arithmetic): X[r0:r0+kb, 0:ncols] <- T11^{-1} X[r0:r0+kb, :] with T11 =
-// lu[r0:r0+kb, r0:r0+kb], unit lower (UPPER false) or upper (UPPER true,
-// x_k = x_k / u_kk from the last row up). The K3 layout: T11 (kb <= 128) in
-// shared memory, each warp owns CPW columns of X with lane l holding rows
-// l, l + 32, ... in registers; step k broadcasts x_k from its owner lane.
+// K3i: the inverses of the diagonal blocks of packed LU factors, for the
+// blocked many-right-hand-side solve (fused arithmetic). Block b = rows and
+// columns [b kb, b kb + kb) (the last one may be short; its inverse is
+// zero-padded to kb x kb): inv + b kb^2 <- T_bb^{-1}, column-major with
+// leading dimension kb, T_bb unit lower (UPPER false) or upper. Grid: column
+// groups x blocks. The K3 layout: T_bb (kb <= 128) in shared memory, each
+// warp owns CPW columns of the identity with lane l holding rows l, l + 32,
+// ... in registers; step k broadcasts row k from its owner lane (upper:
+// x_k / u_kk, from the last row up).
 // ---------------------------------------------------------------------------
 template <typename T, bool UPPER, int RPT, int CPW>
-__global__ void __launch_bounds__(kTrsmThreads, 1) trsm_block_solve_kernel(const T* lu, int lda, int r0, int kb, T* x,
-                                                                        int ldx, int ncols) {
+__global__ void __launch_bounds__(kTrsmThreads, 1) tri_block_inverse_kernel(const T* lu, int lda, int n, int kb,
+                                                                         T* inv) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* M = reinterpret_cast<T*>(smem_raw);  // kb x kb, column-major
   constexpr int kCtaCols = CPW * (kTrsmThreads / 32);
+  const int r0 = blockIdx.y * kb;
+  const int bk = min(kb, n - r0);
   const int c_first = blockIdx.x * kCtaCols;
-  const int ncol = min(kCtaCols, ncols - c_first);
-  if (ncol <= 0) return;
+  if (c_first >= kb) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   T v[CPW][RPT];
 #pragma unroll
   for (int c = 0; c < CPW; ++c) {
-    const int cc = warp * CPW + c;
+    const int col = c_first + warp * CPW + c;
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
       const int i = lane + 32 * r;
-      v[c][r] = (cc < ncol && i < kb) ? x[(size_t)(r0 + i) + (size_t)(c_first + cc) * ldx] : T(0);
+      v[c][r] = (i == col && col < bk) ? T(1) : T(0);
     }
   }
-  const int total = kb * kb;
-  for (int idx = threadIdx.x; idx < total; idx += kTrsmThreads) {
+  for (int idx = threadIdx.x; idx < kb * kb; idx += kTrsmThreads) {
     const int i = idx % kb, k = idx / kb;
-    const bool keep = UPPER ? i <= k : i > k;
+    const bool keep = (i < bk && k < bk) && (UPPER ? i <= k : i > k);
     M[idx] = keep ? lu[(size_t)(r0 + i) + (size_t)(r0 + k) * lda] : T(0);
   }
   __syncthreads();
   if constexpr (!UPPER) {
-    for (int k = 0; k + 1 < kb; ++k) {
+    for (int k = 0; k + 1 < bk; ++k) {
       const int owner = k & 31, rk = k >> 5;
       T u[CPW];
 #pragma unroll
@@ -1005,7 +1008,7 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_block_solve_kernel(const
 #pragma unroll
       for (int r = 0; r < RPT; ++r) {
         const int i = lane + 32 * r;
-        if (i > k && i < kb) {
+        if (i > k && i < bk) {
           const T l = M[i + (size_t)k * kb];
 #pragma unroll
           for (int c = 0; c < CPW; ++c) v[c][r] = msub<false>(v[c][r], l, u[c]);
@@ -1013,7 +1016,7 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_block_solve_kernel(const
       }
     }
   } else {
-    for (int k = kb - 1; k >= 0; --k) {
+    for (int k = bk - 1; k >= 0; --k) {
       const int owner = k & 31, rk = k >> 5;
       const T d = M[k + (size_t)k * kb];
       T u[CPW];
@@ -1042,15 +1045,113 @@ __global__ void __launch_bounds__(kTrsmThreads, 1) trsm_block_solve_kernel(const
       }
     }
   }
+  T* out = inv + (size_t)blockIdx.y * kb * kb;
 #pragma unroll
   for (int c = 0; c < CPW; ++c) {
-    const int cc = warp * CPW + c;
+    const int col = c_first + warp * CPW + c;
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
       const int i = lane + 32 * r;
-      if (cc < ncol && i < kb) x[(size_t)(r0 + i) + (size_t)(c_first + cc) * ldx] = v[c][r];
+      if (col < kb && i < kb) out[i + (size_t)col * kb] = v[c][r];
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// K3b: one step of the blocked many-right-hand-side solve, for the block of
+// rows [k0, k0 + kbe): every CTA forms X_new = T_bb^{-1} X[k0:k0+kbe, tile]
+// (the block's inverse from K3i; CTA x = 0 stores it in Y), then updates its
+// 128 rows of the rows not yet solved, X[rows, tile] -= T[rows, k0:k0+kbe]
+// X_new (lower: the rows below the block; upper: the rows above). A tile of
+// 128 rows x solve_cols<T>() right-hand sides per CTA, the operands in
+// shared memory (kSolveKb x kSolveKb of the factor, the block rows of X).
+// Rows of X outside [k0, k0 + kbe) are touched only by the CTA that owns
+// them, and X[k0:k0+kbe] is only read in a step, so the CTAs need no sync.
+// ---------------------------------------------------------------------------
+constexpr int kSolveKb = 128;
+// right-hand sides per CTA: 32 in FP32 (two CTAs per SM), 64 in FP64 (one);
+// a thread takes 8 rows x kSolveCols / 16 of them
+template <typename T>
+constexpr int solve_cols() { return sizeof(T) == 4 ? 32 : 64; }
+
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256) block_solve_step_kernel(const T* __restrict__ lu, int lda, int n, int k0,
+                                                               int kbe, const T* __restrict__ inv, T* x,
+                                                               T* __restrict__ y, int nrhs) {
+  constexpr int kSolveCols = solve_cols<T>(), kSolveTc = kSolveCols / 16;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);  // [k][i], kSolveKb x kSolveKb
+  T* Xs = As + kSolveKb * kSolveKb;        // [k][c], kSolveKb x kSolveCols
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int c0 = blockIdx.y * kSolveCols;
+  const int nc = min(kSolveCols, nrhs - c0);
+  const int ur0 = UPPER ? 0 : k0 + kbe, ur1 = UPPER ? k0 : n;
+  const int rt = ur0 + blockIdx.x * kSolveKb;  // this CTA's first update row
+  for (int e = tid; e < kSolveKb * kSolveKb; e += 256) {
+    const int i = e % kSolveKb, k = e / kSolveKb;
+    As[e] = (i < kbe && k < kbe) ? inv[i + (size_t)k * kSolveKb] : T(0);
+  }
+  for (int e = tid; e < kSolveKb * kSolveCols; e += 256) {
+    const int c = e % kSolveCols, k = e / kSolveCols;
+    Xs[e] = (k < kbe && c < nc) ? x[(size_t)(k0 + k) + (size_t)(c0 + c) * n] : T(0);
+  }
+  __syncthreads();
+  T acc[8][kSolveTc];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < kSolveTc; ++c) acc[r][c] = T(0);
+  for (int k = 0; k < kbe; ++k) {
+    T av[8], bv[kSolveTc];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) av[r] = As[k * kSolveKb + tx + 16 * r];
+#pragma unroll
+    for (int c = 0; c < kSolveTc; ++c) bv[c] = Xs[k * kSolveCols + ty * kSolveTc + c];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < kSolveTc; ++c) acc[r][c] = fma_rn(av[r], bv[c], acc[r][c]);
+  }
+  __syncthreads();  // every thread is done with X_old
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < kSolveTc; ++c) {
+      const int i = tx + 16 * r, cc = ty * kSolveTc + c;
+      Xs[i * kSolveCols + cc] = acc[r][c];
+      if (blockIdx.x == 0 && i < kbe && cc < nc) y[(size_t)(k0 + i) + (size_t)(c0 + cc) * n] = acc[r][c];
+    }
+  if (rt >= ur1) return;  // no rows left to update (uniform over the CTA)
+  for (int e = tid; e < kSolveKb * kSolveKb; e += 256) {
+    const int i = e % kSolveKb, k = e / kSolveKb;
+    As[e] = (rt + i < ur1 && k < kbe) ? lu[(size_t)(rt + i) + (size_t)(k0 + k) * lda] : T(0);
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < kSolveTc; ++c) {
+      const int i = rt + tx + 16 * r, cc = ty * kSolveTc + c;
+      acc[r][c] = (i < ur1 && cc < nc) ? x[(size_t)i + (size_t)(c0 + cc) * n] : T(0);
+    }
+  __syncthreads();
+  for (int k = 0; k < kbe; ++k) {
+    T av[8], bv[kSolveTc];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) av[r] = As[k * kSolveKb + tx + 16 * r];
+#pragma unroll
+    for (int c = 0; c < kSolveTc; ++c) bv[c] = Xs[k * kSolveCols + ty * kSolveTc + c];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < kSolveTc; ++c) acc[r][c] = msub<false>(acc[r][c], av[r], bv[c]);
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < kSolveTc; ++c) {
+      const int i = rt + tx + 16 * r, cc = ty * kSolveTc + c;
+      if (i < ur1 && cc < nc) x[(size_t)i + (size_t)(c0 + cc) * n] = acc[r][c];
+    }
 }
 
 // x[i, c] = b[perm[i], c] (the row interchanges of P, n x ncols)
