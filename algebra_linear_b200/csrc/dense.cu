@@ -316,7 +316,9 @@ int lu_factor_partial_dev(alg_ctx* ctx, T* a, int m, int nc, int ntot, int lda, 
     count_launches();
     ALG_CUDA_TRY(cudaGetLastError());
   }
-  const int nb = std::max(1, plan.nb);
+  // a block's interchanges move at most 2 nb rows, and the deferred-swap
+  // kernel holds kSwapMaxMoves of them: wider blocks are cut to that
+  const int nb = std::min(std::max(1, plan.nb), kSwapMaxMoves / 2);
   const int nbl = std::max(1, std::min(plan.nbl, kPanelMaxW));
   // persistent tensor-core grids: the wide update's cap (0: every SM) and the
   // look-ahead chain's (its launches must fit on the SMs the wide update

@@ -103,6 +103,8 @@ int gmres_ir_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* b,
   if ((size_t)nchunks * (m + 1) > 2048) return ALG_BAD_SHAPE;
   double rmax = 0, xmax = 0, bmax = 0;
   res->outer = res->inner = 0;
+  double prev_eta = INFINITY;
+  int stalled = 0;
   for (int outer = 0; outer < go.max_outer; ++outer) {
     ALG_TRY(residual_dev(ctx, a, n, lda, x, n, b, n, r, n, 1, &rmax, &xmax, &bmax));
     const double den = anorm * xmax + bmax;
@@ -112,6 +114,15 @@ int gmres_ir_dev(alg_ctx* ctx, const double* a, int n, int lda, const double* b,
       res->converged = true;
       return ALG_OK;
     }
+    // two restart cycles in a row that do not halve the backward error: the
+    // preconditioner is too weak for this matrix; give up (the caller falls
+    // back to the FP64 LU) instead of running out the cycle limit
+    if (res->backward_error > 0.5 * prev_eta) {
+      if (++stalled >= 2) return ALG_CONVERGENCE;
+    } else {
+      stalled = 0;
+    }
+    prev_eta = res->backward_error;
     // z0 = M^{-1} r, beta = ||z0||
     ALG_TRY(M(ctx, r, t));
     double beta = 0.0;

@@ -175,6 +175,35 @@ def test_tournament_pivoting_panels(gpu, oracle, n, prec):
     assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53
 
 
+def test_block_widths_past_the_swap_limit_are_cut(gpu, oracle, monkeypatch):
+    """A block's interchanges move up to 2 nb rows and the deferred-swap
+    kernel holds 512, so a requested block width over 256 (ALG_NB,
+    ALG_NB_TC) is cut to 256: the exact form stays bit-identical to the
+    oracle and the mixed form converges by plain refinement."""
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+    from algebra_linear_b200.lapack import dgetrf
+
+    n = 2048
+    a, _, b = oracle.c1_system(n, seed=[4, 4, 2, 7])
+    monkeypatch.setenv("ALG_NB", "384")
+    g = a.copy()
+    ipiv, _ = dgetrf(g, n)
+    ref = a.copy()
+    rc, ripiv, _, _ = oracle.dgetrf(ref, n)
+    assert rc == 0 and ipiv == ripiv and np.array_equal(g.view(np.uint64), ref.view(np.uint64))
+    monkeypatch.setenv("ALG_NB_TC", "320")
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        B = torch.from_numpy(b.copy()).cuda()
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, 1, precision="tf32x3", pivoting="tournament", no_gmres=True,
+                                    no_fallback=True)
+        x = B.cpu().numpy()
+    assert rep["path"] == "ir", rep
+    assert oracle.backward_error(a, x, b, n) <= 10 * n * 2.0**-53
+
+
 def test_tournament_single_launch_matches_level_launches(gpu, oracle, monkeypatch):
     """The single cooperative launch per leaf and the one-launch-per-level
     form run the same arithmetic: bit-identical solutions."""
