@@ -130,6 +130,28 @@ def test_mixed_64_rhs(gpu, oracle):
         assert eta <= 10 * n * 2.0**-53, (k, eta)
 
 
+@pytest.mark.parametrize("n,nrhs", [(3001, 17), (1300, 100)])
+def test_mixed_many_rhs_odd_orders(gpu, oracle, n, nrhs):
+    """From 16 right-hand sides the FP32 solves are blocked (a short last
+    128-row block here) and the refinement's residual is one FP64
+    tensor-core GEMM: every column reaches the FP64 backward error."""
+    import torch
+
+    from algebra_linear_b200 import device, mixed
+
+    a, s = oracle.larnv("Symmetric", [6, 1, 8, 2 * n + 1], n * n)
+    b, _ = oracle.larnv("Symmetric", s, n * nrhs)
+    with device.Context() as ctx:
+        A = torch.from_numpy(a.copy()).cuda()
+        B = torch.from_numpy(b.copy()).cuda()
+        rep = mixed.dgesv_mixed_dev(ctx, A, B, n, nrhs, precision="tf32x3", no_fallback=True)
+        x = B.cpu().numpy()
+    assert rep["path"] in ("ir", "gmres"), rep
+    for k in range(nrhs):
+        eta = oracle.backward_error(a, x[k * n:(k + 1) * n], b[k * n:(k + 1) * n], n)
+        assert eta <= 10 * n * 2.0**-53, (k, eta)
+
+
 def test_butterfly_form_on_a_diagonally_dominant_system(gpu, oracle):
     """The butterfly + no-pivoting form on A + n I (where LU without pivoting
     is stable), refined to the FP64 backward error; A is left unchanged."""
