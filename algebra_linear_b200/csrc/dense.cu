@@ -233,9 +233,21 @@ int gemm_sub_dev(alg_ctx* ctx, int M, int N, int K, const T* A, int lda, const T
     if (!dmma_disabled()) return gemm_dmma_sub_dev(ctx, M, N, K, A, lda, B, ldb, C, ldc);
   }
   const int tok = prof_begin(ctx, ALG_K_GEMM);
+  // FP64 (the exact form's update) stages its operands by cp.async:
+  // fp64_exact 296.2 ms against 308.7 ms at n = 16384; FP32 keeps the
+  // register-prefetch form (mixed_fp32 133.8 ms against 138.3 ms).
+  // ALG_GEMM_SYNC=1: the register-prefetch form for FP64 too (measurement switch)
+  static const bool sync_env = [] {
+    const char* e = std::getenv("ALG_GEMM_SYNC");
+    return e != nullptr && e[0] == '1';
+  }();
+  const bool sync_form = sizeof(T) == 4 || sync_env;
   if (gemm_wide_tiles()) {
     dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + 127) / 128);
     gemm_sub_kernel<T, EXACT, 128><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  } else if (!sync_form) {
+    dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + 63) / 64);
+    gemm_sub_async_kernel<T, EXACT><<<grid, 128, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
   } else {
     dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + 63) / 64);
     gemm_sub_kernel<T, EXACT, 64><<<grid, 128, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);

@@ -1270,6 +1270,112 @@ __global__ void __launch_bounds__(2 * BN, BN == 64 ? 2 : 1) gemm_sub_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// K4a: the same update (128 x 64 tile, 128 threads, 8 x 8 per thread, each
+// entry's terms in increasing k) with A and B staged by cp.async through a
+// three-stage shared-memory ring instead of registers: no prefetch registers,
+// and the loads of chunk c + 2 run while chunk c is multiplied. Element-wise
+// copies (any leading dimension and offset); out-of-range elements are
+// zero-filled, which leaves every in-range entry unchanged bit for bit.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void cp_async_elem_zfill(T* dst, const T* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+  }
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr int kGemmAsyncStages = 3;
+
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(128, 2) gemm_sub_async_kernel(int M, int N, int K, const T* __restrict__ A, int lda,
+                                                                const T* __restrict__ B, int ldb, T* __restrict__ Cm,
+                                                                int ldc) {
+  constexpr int kBN = 64, kHalf = kBN / 2, kThreads = 128, kBS = kBN + 2;
+  constexpr int kStage = kGemmBK * kGemmBM + kGemmBK * kBS;
+  __shared__ __align__(16) T smem[kGemmAsyncStages * kStage];
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * kBN;
+
+  auto load_stage = [&](int stage, int k0) {
+    T* As = smem + stage * kStage;  // [k][m]
+    T* Bs = As + kGemmBK * kGemmBM;  // [k][n], padded rows
+#pragma unroll
+    for (int r = 0; r < kGemmBK * kGemmBM / kThreads; ++r) {
+      const int e = tid + r * kThreads;
+      const int mm = e & (kGemmBM - 1), kk = e / kGemmBM;
+      const int gm = m0 + mm, gk = k0 + kk;
+      const bool ok = gm < M && gk < K;
+      cp_async_elem_zfill(As + kk * kGemmBM + mm, ok ? A + (size_t)gm + (size_t)gk * lda : A, ok);
+    }
+#pragma unroll
+    for (int r = 0; r < kGemmBK * kBN / kThreads; ++r) {
+      const int e = tid + r * kThreads;
+      const int kk = e % kGemmBK, nn = e / kGemmBK;
+      const int gn = n0 + nn, gk = k0 + kk;
+      const bool ok = gn < N && gk < K;
+      cp_async_elem_zfill(Bs + kk * kBS + nn, ok ? B + (size_t)gk + (size_t)gn * ldb : B, ok);
+    }
+  };
+
+  const int nch = (K + kGemmBK - 1) / kGemmBK;
+#pragma unroll
+  for (int st = 0; st < kGemmAsyncStages - 1; ++st) {
+    if (st < nch) load_stage(st, st * kGemmBK);
+    cp_async_commit_group();
+  }
+  T acc[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int mi = m0 + (r >> 2) * 64 + tx * 4 + (r & 3);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int nj = n0 + (c >> 2) * kHalf + ty * 4 + (c & 3);
+      acc[r][c] = (mi < M && nj < N) ? Cm[(size_t)mi + (size_t)nj * ldc] : T(0);
+    }
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_async_wait_group<kGemmAsyncStages - 2>();  // chunk ch has landed
+    __syncthreads();  // ... for every thread, and chunk ch - 1's stage is free
+    if (ch + kGemmAsyncStages - 1 < nch)
+      load_stage((ch + kGemmAsyncStages - 1) % kGemmAsyncStages, (ch + kGemmAsyncStages - 1) * kGemmBK);
+    cp_async_commit_group();
+    const T* As = smem + (ch % kGemmAsyncStages) * kStage;
+    const T* Bs = As + kGemmBK * kGemmBM;
+#pragma unroll
+    for (int kk = 0; kk < kGemmBK; ++kk) {
+      T af[8], bf[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) af[r] = As[kk * kGemmBM + (r >> 2) * 64 + tx * 4 + (r & 3)];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) bf[c] = Bs[kk * kBS + (c >> 2) * kHalf + ty * 4 + (c & 3)];
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[r][c] = msub<EXACT>(acc[r][c], af[r], bf[c]);
+    }
+  }
+  cp_async_wait_group<0>();
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int mi = m0 + (r >> 2) * 64 + tx * 4 + (r & 3);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int nj = n0 + (c >> 2) * kHalf + ty * 4 + (c & 3);
+      if (mi < M && nj < N) Cm[(size_t)mi + (size_t)nj * ldc] = acc[r][c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K5: triangular solves with the packed factors (getrs), blocked by kSolveB
 // rows. The forward sweep gives x_i the terms l_ij x_j in increasing j with
 // rounded product and difference — the reference's row-dot sequence
