@@ -260,6 +260,7 @@ def run_form(name, spec, ctx, A0, b0, xt, n, nrhs, steps, warmup, pg, sample_clo
         pg.barrier()
     eta = backward_error(A0, b, b0, n, nrhs)
     fwd = float((b - xt).abs().max() / xt.abs().max())
+    x_last = b.clone()
     # the per-kernel-class breakdown (CUDA events around every launch, on the
     # launching streams) comes from separate profiled steps, so the events
     # cost nothing in the timed ones; per step
@@ -289,7 +290,18 @@ def run_form(name, spec, ctx, A0, b0, xt, n, nrhs, steps, warmup, pg, sample_clo
         "gpu_launches": int(launches),
         "profile": prof,
         "clocks": sampler.summary() if sampler else None,
+        "_x": x_last,  # the last timed step's solution (dropped before printing)
     }
+
+
+def forward_vs(results, ref_name):
+    """Each form's max-norm forward error against another form's solution
+    (the FP64 form's x, as C2 asks), then the solutions are dropped."""
+    ref = results.get(ref_name, {}).get("_x")
+    for r in results.values():
+        x = r.pop("_x", None)
+        if ref is not None and x is not None:
+            r[f"forward_error_vs_{ref_name}"] = float((x - ref).abs().max() / ref.abs().max())
 
 
 def gemm_peaks_tflops():
@@ -1146,7 +1158,9 @@ def c2_sweep(ctx, reg, A16, s1, steps, warmup, dev_index):
                 continue
             r = run_form(name, reg[name], ctx, A0, b0, xt, n, nrhs, steps, warmup, None, sample_clocks=False,
                          dev_index=dev_index)
-            row[name] = {k: r[k] for k in ("ms_per_step", "gflops", "backward_error", "forward_error", "refinement")}
+            row[name] = {k: r[k] for k in ("ms_per_step", "gflops", "backward_error", "forward_error", "refinement",
+                                           "_x")}
+        forward_vs(row, "fp64_fma")
         out[f"n={n},nrhs={nrhs}"] = row
         del A0, xt, b0
     return out
@@ -1195,6 +1209,9 @@ def run_ours(args, world, rank, local, pg):
     for name in names:
         results[name] = run_form(name, reg[name], ctx, A0, b0, xt, n, nrhs, args.steps, args.warmup, pg,
                                  sample_clocks=True, dev_index=local)
+    # forward error of every form against the bit-exact FP64 form's solution
+    # (the reference's LU bit for bit), as C2 asks
+    forward_vs(results, "fp64_exact")
     tol = 10 * n * 2.0**-53
     ok = {k: v for k, v in results.items() if v["backward_error"] <= tol}
     head = max(ok or results, key=lambda k: (ok or results)[k]["gflops"])
