@@ -1,0 +1,67 @@
+"""Host-side pieces of bench.py, on the CPU: the workload generators match
+the configurations they name (C3 orders, C4 and C5 stencil sizes), the
+forward-error comparison between forms, and a failing sub-workload is
+recorded instead of ending the benchmark line."""
+
+import pathlib
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+import bench  # noqa: E402
+
+
+def test_c3_orders_are_log_uniform_in_8_512():
+    n = bench.batched_orders(20000, 1991)
+    assert n.size == 20000 and n.min() >= 8 and n.max() <= 512
+    # log-uniform: about a sixth of the systems in each factor-2 band
+    frac = np.mean((n > 256) & (n <= 512))
+    assert 0.13 < frac < 0.20, frac
+    assert np.array_equal(n, bench.batched_orders(20000, 1991))  # seeded
+
+
+@pytest.mark.parametrize("dims,n,nnz", [((48, 48, 48), 110592, 760320), ((300, 300, 1), 90000, 448800)])
+def test_stencil_sizes_of_c4_and_c5(dims, n, nnz):
+    cp, ri, kind = bench.grid_csc(*dims)
+    assert cp.size == n + 1 and int(cp[-1]) == nnz and ri.size == nnz and kind.size == nnz
+    # rows sorted within every column, one diagonal entry per column
+    cpi = cp.astype(np.int64)
+    ends = cpi[1:]
+    assert np.all(np.diff(ri.astype(np.int64))[np.setdiff1d(np.arange(nnz - 1), ends[:-1] - 1)] > 0)
+    assert int((kind == 0).sum()) == n
+
+
+def test_forward_error_against_a_reference_form():
+    torch = pytest.importorskip("torch")
+    x = torch.tensor([1.0, -2.0, 4.0], dtype=torch.float64)
+    dx = torch.tensor([0.0, 0.0, 4e-6], dtype=torch.float64)
+    res = {"fp64_exact": {"_x": x.clone()}, "mixed": {"_x": x + dx}, "other": {"backward_error": 1.0}}
+    bench.forward_vs(res, "fp64_exact")
+    assert res["fp64_exact"]["forward_error_vs_fp64_exact"] == 0.0
+    assert abs(res["mixed"]["forward_error_vs_fp64_exact"] - 1e-6) < 1e-12
+    assert all("_x" not in r for r in res.values())
+    res = {"mixed": {"_x": x}}
+    bench.forward_vs(res, "fp64_exact")  # no reference form: nothing computed, solutions dropped
+    assert res == {"mixed": {}}
+
+
+def test_a_failing_sub_workload_is_recorded():
+    class Args:
+        pass
+
+    def boom(args, world, rank, local, pg):
+        assert args.steps == 3 and args.warmup == 2 and args.no_cpu and not args.emit
+        raise RuntimeError("no device")
+
+    out = bench.sub_arm(boom, Args(), 1, 0, 0, None)
+    assert out == {"error": "RuntimeError('no device')"}
+
+    def ok(args, world, rank, local, pg):
+        return {"metric": "m", "value": 1.0, "n_gpus": 1, "data": "d", "e2e": {"value": 2.0}}
+
+    assert bench.sub_arm(ok, Args(), 1, 0, 0, None) == {"metric": "m", "value": 1.0, "e2e": {"value": 2.0}}
