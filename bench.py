@@ -77,8 +77,9 @@ def parse_args():
     ap.add_argument("--grid", type=int, default=48, help="sparse: grid points per side")
     ap.add_argument("--grid-nz", type=int, default=0, help="sparse: points along z (0: = grid; 1: 2-D)")
     ap.add_argument("--cpu-grid", type=int, default=16, help="sparse: grid side of the CPU-baseline sample")
-    ap.add_argument("--sparse-precision", choices=["fp64", "fp32", "tf32", "tf32x3", "bf16"], default="fp64",
-                    help="sparse: front precision (fp64 = the reference's arithmetic; others refine in FP64)")
+    ap.add_argument("--sparse-precision", choices=["fp64", "fp32", "tf32", "tf32x3", "bf16", "complex"],
+                    default="fp64", help="sparse: front precision (fp64 = the reference's arithmetic; others refine "
+                                         "in FP64; complex = SparseLu<Complex64>)")
     ap.add_argument("--requests", type=int, default=10000, help="serve: requests per rate")
     ap.add_argument("--rates", default="20,40,55",
                     help="serve: Poisson arrival rates (requests/s), below the loop's capacity")
@@ -532,6 +533,68 @@ def sparse_cpu_baseline(side: int):
     return {"value": fl / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
             "sample": f"one factorize+solve of the {side}^3 grid ({t:.1f} s); the reference path is single-threaded",
             **pin.info()}
+
+
+def run_sparse_complex(args, world, rank, local, pg):
+    """SparseLu<Complex64> on the sparse workload: the convection-diffusion
+    values plus imaginary parts 0.5 U(0,1) - 0.25, analyze once, then per
+    round both parts x (1 + 0.01 U(-1,1)), factorize and solve through the
+    host API (values and b copied in, x out: end to end, wall-clock around
+    each synchronous call). GFLOP/s counts the reference's flop estimate in
+    complex multiply-adds x 8 real flops."""
+    import numpy as np
+    import torch
+
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+
+    torch.cuda.set_device(local)
+    nx = args.grid
+    nz = args.grid_nz if args.grid_nz > 0 else nx
+    cp, ri, kind = grid_csc(nx, nx, nz)
+    n, nnz = len(cp) - 1, len(ri)
+    rng = np.random.default_rng(1991 + 2 * rank)
+    u, w = rng.uniform(0.0, 1.0, nnz), rng.uniform(0.0, 1.0, nnz)
+    re = np.where(kind == 0, 6.0 + 0.1 * u, np.where(kind == 2, -1.0 + 0.3 * u,
+                                                     np.where(kind == 1, -1.0 - 0.3 * u, -1.0)))
+    v0 = re + 1j * (0.5 * w - 0.25)
+    t0 = time.perf_counter()
+    lu = SparseLu.analyze(cp, ri, LuMethod.supernodal())
+    analyze_s = time.perf_counter() - t0
+    b0 = np.ones(n, dtype=np.complex128) * (1 - 2j)
+    times, x, v = [], None, v0
+    for it in range(args.warmup + args.steps):
+        v = v0 * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, nnz)) + 1j * v0.imag * 0.01 * rng.uniform(-1.0, 1.0, nnz)
+        x = b0.copy()
+        t0 = time.perf_counter()
+        lu.factorize(cp, ri, v)
+        lu.solve(x)
+        if it >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    st = lu.stats()
+    import scipy.sparse as sps
+
+    A = sps.csc_matrix((v, ri.astype(np.int64), cp.astype(np.int64)), shape=(n, n))
+    eta = float(np.abs(b0 - A @ x).max() / (abs(A).sum(axis=1).max() * np.abs(x).max() + np.abs(b0).max()))
+    per = statistics.median(times)
+    fl = 8.0 * st["flops_estimate"] + 8.0 * (st["nnz_l"] + st["nnz_u"])
+    line = {
+        "metric": "complex sparse LU refactorize+solve GFLOP/s (reference flop estimate, 8 flops per complex "
+                  "multiply-add)", "value": fl * world / per / 1e9, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic: convection-diffusion stencil + i (0.5 U(0,1) - 0.25), numpy-seeded",
+        "config": {"workload": f"{nx}x{nx}x{nz} grid, complex values, n={n}, nnz={nnz}; analyze once, then per "
+                               "round: values x (1 + 0.01 U(-1,1)), factorize, solve (host API, end to end)",
+                   "n": n, "nnz": nnz, "parallelism": f"replicas x{world}"},
+        "analyze_s": analyze_s, "backward_error": eta,
+        "stats": {k: st[k] for k in ("nnz_l", "nnz_u", "fill_ratio", "flops_estimate")},
+        "e2e": {"value": fl * world / per / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": 16 * nnz + 16 * n,
+                "d2h_bytes_per_step": 16 * n, "ms_per_step": 1e3 * per,
+                "api": "alg_zsplu_factorize + alg_zsplu_solve"},
+    }
+    lu.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_sparse(args, world, rank, local, pg):
@@ -1264,6 +1327,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, pg)
+        elif args.workload == "sparse" and args.sparse_precision == "complex":
+            run_sparse_complex(args, world, rank, local, pg)
         elif args.workload == "sparse":
             run_sparse(args, world, rank, local, pg)
         elif args.workload == "serve":
