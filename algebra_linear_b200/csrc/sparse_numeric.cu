@@ -378,12 +378,12 @@ __global__ void big_finalize_kernel(FrontDesc d, const T* front, const int* perm
 // ---- large complex fronts ----------------------------------------------------
 // The partial LU of a complex front (the contract of lu_factor_partial_dev:
 // the first `size` columns over all rows, interchanges across every column,
-// U12 and the Schur complement), blocked by kZnb columns, four launches per
+// U12 and the Schur complement), blocked by kZnb columns, five launches per
 // block: the block's columns over all rows by one CTA (the reference's pivot
 // rule, lu_front supernodal_lu.rs:490-533: the first row of largest modulus,
 // multipliers by the reciprocal, the rank-1 updates inside the block); its
 // interchanges on the other columns; its rows of U12 by a unit-lower solve;
-// the trailing block by the tiled GEMM, one CTA per 64 x 64 tile.
+// the trailing block as one real FP64 tensor-core GEMM (below).
 constexpr int kZnb = 32;
 constexpr int kZPanelThreads = 1024;
 
@@ -510,12 +510,27 @@ __global__ void __launch_bounds__(256) zfront_trsm_kernel(zc* f, int rows, int c
   }
 }
 
-// Trailing block: C -= L21 U12, one 64 x 64 tile per CTA.
-__global__ void __launch_bounds__(kSmallThreads) zfront_gemm_kernel(zc* C, const zc* A, const zc* B, int ld, int mr,
-                                                                    int nc, int kd, const DevStatus* st) {
-  __shared__ zc As[64 * 16], Bs[16 * 64];
+// L21 of a block (mr x w complex, rows k1.. of columns k0..k1) written as the
+// real 2mr x 2w matrix whose complex entry a occupies the 2 x 2 block
+// [re -im; im re]: then, with B and C viewed as real matrices of twice the
+// rows (the interleaved (re, im) layout), C -= L21 U12 is one real GEMM
+// (the FP64 tensor cores), the complex products' four real terms summed in
+// another order than num-complex's (values to rounding, as the real path).
+__global__ void zblock_expand_kernel(const zc* __restrict__ f, int rows, int k0, int w, int k1, int mr,
+                                     double* __restrict__ ah, const DevStatus* st) {
   if (front_stopped(st)) return;
-  cta_gemm_tile(C, A, B, ld, mr, nc, kd, (int)blockIdx.x * 64, (int)blockIdx.y * 64, As, Bs);
+  const int ld = 2 * mr;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)mr * w;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % mr), l = (int)(e / mr);
+    const zc a = f[(k1 + i) + (int64_t)(k0 + l) * rows];
+    double* c0 = ah + (int64_t)(2 * l) * ld + 2 * i;
+    double* c1 = c0 + ld;
+    c0[0] = a.re;
+    c0[1] = a.im;
+    c1[0] = -a.im;
+    c1[1] = a.re;
+  }
 }
 
 // ---- after the factorization -----------------------------------------------
@@ -854,7 +869,7 @@ int grid_for(alg_ctx* ctx, int64_t work, int threads) {
 
 // The complex front's partial LU (kernels above) on lane context lc.
 // Stream-ordered; a zero pivot lands in lc's status (singular_col).
-int zfront_lu(alg_ctx* lc, zc* f, int rows, int size, int cols, int* ipiv, int* perm) {
+int zfront_lu(alg_ctx* lc, zc* f, int rows, int size, int cols, int* ipiv, int* perm, double* ah) {
   cudaStream_t st = lc->stream;
   for (int k0 = 0; k0 < size; k0 += kZnb) {
     const int k1 = std::min(size, k0 + kZnb);
@@ -869,11 +884,15 @@ int zfront_lu(alg_ctx* lc, zc* f, int rows, int size, int cols, int* ipiv, int* 
       zfront_trsm_kernel<<<grid_for(lc, cols - k1, 256), 256, 0, st>>>(f, rows, cols, k0, k1, lc->d_status);
       count_launches();
       if (rows > k1) {
-        const dim3 grid((rows - k1 + 63) / 64, (cols - k1 + 63) / 64);
-        zfront_gemm_kernel<<<grid, kSmallThreads, 0, st>>>(f + k1 + (int64_t)k1 * rows, f + k1 + (int64_t)k0 * rows,
-                                                           f + k0 + (int64_t)k1 * rows, rows, rows - k1, cols - k1,
-                                                           k1 - k0, lc->d_status);
+        // trailing block: C -= L21 U12 as one real FP64 tensor-core GEMM of
+        // the 2 x 2 real form of L21 and the real views of U12 and C
+        const int mr = rows - k1, w = k1 - k0;
+        zblock_expand_kernel<<<grid_for(lc, (int64_t)mr * w, 256), 256, 0, st>>>(f, rows, k0, w, k1, mr, ah,
+                                                                                  lc->d_status);
         count_launches();
+        ALG_TRY(gemm_dmma_sub_dev(lc, 2 * mr, cols - k1, 2 * w, ah, 2 * mr,
+                                  reinterpret_cast<const double*>(f + k0 + (int64_t)k1 * rows), 2 * rows,
+                                  reinterpret_cast<double*>(f + k1 + (int64_t)k1 * rows), 2 * rows));
       }
     }
     ALG_CUDA_TRY(cudaGetLastError());
@@ -919,6 +938,8 @@ int DeviceLu::init(alg_ctx* c, const FrontPlan* p, int w) {
     ALG_TRY(dmalloc((void**)&d_ipiv[k], sizeof(int) * max_rows));
     ALG_TRY(dmalloc((void**)&d_perm[k], sizeof(int) * max_rows));
     ALG_TRY(dmalloc((void**)&d_rowtmp[k], sizeof(int32_t) * max_rows));
+    if (words == 2)  // 2 rows x 2 kZnb columns of doubles per complex row
+      ALG_TRY(dmalloc((void**)&d_zblock[k], sizeof(double) * 4 * kZnb * max_rows));
   }
   ALG_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   ALG_TRY(dmalloc((void**)&d_flag, sizeof(int) * 4));
@@ -1011,7 +1032,7 @@ int DeviceLu::ensure_refine_buffers() {
 
 void DeviceLu::release() {
   for (int k = 0; k < kMaxLanes; ++k) {
-    for (void* q : {(void*)d_front[k], (void*)d_ipiv[k], (void*)d_perm[k], (void*)d_rowtmp[k]})
+    for (void* q : {(void*)d_front[k], (void*)d_ipiv[k], (void*)d_perm[k], (void*)d_rowtmp[k], (void*)d_zblock[k]})
       if (q) cudaFree(q);
     if (k > 0 && lane_ctx[k]) alg_ctx_destroy(lane_ctx[k]);
     if (ev_join[k]) cudaEventDestroy(ev_join[k]);
@@ -1161,7 +1182,7 @@ int DeviceLu::factor_big(int b, int32_t s, int lane, const double* values, int t
   count_launches();
   ALG_CUDA_TRY(cudaGetLastError());
   if constexpr (std::is_same<T, zc>::value) {
-    ALG_TRY(zfront_lu(lc, front, d.rows, d.size, cols, d_ipiv[lane], d_perm[lane]));
+    ALG_TRY(zfront_lu(lc, front, d.rows, d.size, cols, d_ipiv[lane], d_perm[lane], d_zblock[lane]));
   } else {
     LuPlan lp;
     // block width of a large front's LU (ALG_SPLU_NB: measurement switch)

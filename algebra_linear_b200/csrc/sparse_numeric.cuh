@@ -67,6 +67,7 @@ struct DeviceLu {
   int* d_ipiv[kMaxLanes] = {};
   int* d_perm[kMaxLanes] = {};
   int32_t* d_rowtmp[kMaxLanes] = {};
+  double* d_zblock[kMaxLanes] = {};  // complex: a block column of L21 in its real 2x2 form
   int* d_flag = nullptr;       // [0]: a small front met a zero pivot
   double *d_y = nullptr, *d_rhs = nullptr;
   // solve schedule: per level the fronts solved by the one-CTA diagonal
