@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstddef>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -67,21 +68,19 @@ __device__ __forceinline__ bool stopped(const DevStatus* st) {
 
 constexpr int kPivThreads = 1024;
 
-// Step j of the factorization of an m x nc matrix (m >= nc): pivot, swap of
-// the whole rows (all nc columns), scaling of column j below the diagonal.
-__global__ void __launch_bounds__(kPivThreads) zpivot_kernel(double2* __restrict__ a, int lda, int m, int nc, int j,
-                                                             int* __restrict__ ipiv, DevStatus* st) {
-  __shared__ double sb[kPivThreads / 32];
-  __shared__ int si[kPivThreads / 32];
-  __shared__ int piv_s;
-  if (stopped(st)) return;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  double2* col = a + (size_t)j * lda;
-  // first maximum over this thread's rows below the diagonal (a NaN is never
-  // greater, as in the reference's scan); -1 means none
+// The pivot row of column j (rows j..m-1) by the reference's scan, computed
+// by every thread of the CTA: the diagonal comes first, a row below replaces
+// it only when strictly greater in |Re| + |Im| (a NaN never is), and among
+// equal rows the first. ipiv[j] is written; a zero (or empty) pivot is
+// recorded in the status block and -1 returned instead. sb and si hold one
+// entry per warp.
+__device__ int zpick_pivot(const double2* __restrict__ col, int m, int j, int* __restrict__ ipiv, DevStatus* st,
+                           double* sb, int* si, int* piv_s) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nt = blockDim.x;
+  // first maximum over this thread's rows below the diagonal; -1 means none
   double best = -1.0;
   int bi = INT_MAX;
-  for (int i = j + 1 + t; i < m; i += kPivThreads) {
+  for (int i = j + 1 + t; i < m; i += nt) {
     const double c = zabs1(col[i]);
     if (c > best) {
       best = c;
@@ -106,13 +105,11 @@ __global__ void __launch_bounds__(kPivThreads) zpivot_kernel(double2* __restrict
   if (t == 0) {
     double gb = sb[0];
     int gi = si[0];
-    for (int w = 1; w < kPivThreads / 32; ++w)
+    for (int w = 1; w < nt / 32; ++w)
       if (sb[w] > gb || (sb[w] == gb && si[w] < gi)) {
         gb = sb[w];
         gi = si[w];
       }
-    // the diagonal entry comes first in the reference's scan: a row below
-    // replaces it only when strictly greater (never when it is NaN)
     const double vj = zabs1(col[j]);
     int jp = j;
     double pbest = vj;
@@ -126,10 +123,23 @@ __global__ void __launch_bounds__(kPivThreads) zpivot_kernel(double2* __restrict
     } else {
       ipiv[j] = jp;
     }
-    piv_s = jp;
+    *piv_s = jp;
   }
   __syncthreads();
-  const int jp = piv_s;
+  return *piv_s;
+}
+
+// Step j of the factorization of an m x nc matrix (m >= nc): pivot, swap of
+// the whole rows (all nc columns), scaling of column j below the diagonal.
+__global__ void __launch_bounds__(kPivThreads) zpivot_kernel(double2* __restrict__ a, int lda, int m, int nc, int j,
+                                                             int* __restrict__ ipiv, DevStatus* st) {
+  __shared__ double sb[kPivThreads / 32];
+  __shared__ int si[kPivThreads / 32];
+  __shared__ int piv_s;
+  if (stopped(st)) return;
+  const int t = threadIdx.x;
+  double2* col = a + (size_t)j * lda;
+  const int jp = zpick_pivot(col, m, j, ipiv, st, sb, si, &piv_s);
   if (jp < 0) return;
   if (jp != j) {
     for (int k = t; k < nc; k += kPivThreads) {
@@ -156,6 +166,205 @@ __global__ void __launch_bounds__(256) zupdate_kernel(double2* __restrict__ a, i
     double2* c = a + (size_t)k * lda;
     c[i] = zsub(c[i], zmul(l, c[j]));
   }
+}
+
+// ---- Blocked form: the same operations on every entry, in the same order ----
+//
+// Columns are taken kZpw at a time. For the block [k0, k0 + w):
+//   zpanel_kernel      one CTA runs the reference's steps k0..k0+w-1 on the
+//                      block's own columns over all rows (pivot, swap within
+//                      the block, division, rank-1 updates of the block's
+//                      later columns);
+//   zswap_trsm_kernel  a thread per column outside the block applies the
+//                      block's interchanges in order; right of the block it
+//                      then forms the block's rows of U by the unit-lower
+//                      solve, row r taking l_rk u_k for k = k0, k0 + 1, ...;
+//   zgemm_exact_kernel the trailing block a_ic -= l_ik u_kc, k increasing
+//                      over the block, a CTA per 64 x 64 tile.
+// Every entry right of the block therefore receives the terms of steps
+// k0, k0 + 1, ... in that order, each product and difference rounded on its
+// own, as in the reference's loop, and the interchanges move whole rows
+// (factors and all) before any of the block's terms reach them, which is
+// where the reference's row swap leaves them. A zero pivot at column s of
+// the block stops the panel there; the other two kernels then apply only
+// the steps k0..s-1 (the valid width), which is the state the reference's
+// loop leaves on its early return.
+constexpr int kZpw = 16;
+constexpr int kZpanelThreads = 384;
+constexpr int kZtile = 64;
+
+// Steps of the block [k0, k0 + w) that ran: w, fewer when the panel stopped
+// at a zero pivot inside the block, 0 or less after one before it.
+__device__ __forceinline__ int valid_width(const DevStatus* st, int k0, int w) {
+  const int s = *reinterpret_cast<const volatile int*>(&st->singular_col);
+  return s == INT_MAX ? w : min(w, s - k0);
+}
+
+__global__ void __launch_bounds__(kZpanelThreads) zpanel_kernel(double2* __restrict__ a, int lda, int m, int k0, int w,
+                                                                int* __restrict__ ipiv, DevStatus* st) {
+  __shared__ double sb[kZpanelThreads / 32];
+  __shared__ int si[kZpanelThreads / 32];
+  __shared__ int piv_s;
+  __shared__ double2 urow[kZpw];
+  if (stopped(st)) return;
+  const int t = threadIdx.x;
+  for (int j = k0; j < k0 + w; ++j) {
+    double2* col = a + (size_t)j * lda;
+    const int jp = zpick_pivot(col, m, j, ipiv, st, sb, si, &piv_s);
+    if (jp < 0) return;
+    // the interchange within the block's columns; row j (the pivot row
+    // after it) kept for the updates
+    if (t < w) {
+      double2* c = a + (size_t)(k0 + t) * lda;
+      const double2 x = c[j];
+      if (jp != j) {
+        const double2 y = c[jp];
+        c[j] = y;
+        c[jp] = x;
+        urow[t] = y;
+      } else {
+        urow[t] = x;
+      }
+    }
+    __syncthreads();
+    const int jj = j - k0;
+    const double2 d = urow[jj];
+    for (int i = j + 1 + t; i < m; i += kZpanelThreads) {
+      // the multiplier first (the division is a call, and nothing may stay
+      // live across it), then the row's entries in the block's later
+      // columns loaded together before any store, so that their latencies
+      // overlap
+      const double2 l = zdiv(col[i], d);
+      col[i] = l;
+      double2* row = a + i + (size_t)k0 * lda;
+      double2 v[kZpw];
+#pragma unroll
+      for (int c = 1; c < kZpw; ++c)
+        if (c > jj && c < w) v[c] = row[(size_t)c * lda];
+#pragma unroll
+      for (int c = 1; c < kZpw; ++c)
+        if (c > jj && c < w) row[(size_t)c * lda] = zsub(v[c], zmul(l, urow[c]));
+    }
+    __syncthreads();  // column j + 1 is final below row j before its pivot search
+  }
+}
+
+// A thread per column outside the block (nc - w of them): the block's valid
+// interchanges; right of the block, then the block's rows of U:
+// u_r = a_r - sum over k < r of l_rk u_k, the terms in increasing k, with
+// the block's unit-lower factor staged in shared memory. The interchanges
+// (row j with row ipiv[j], j = k0, k0 + 1, ... in order) are composed once
+// per CTA into a gather over the rows they touch: the block's own rows
+// first, then the rows below the block that a pivot came from, at most
+// 2 kZpw in all. Each thread then loads those entries of its column together
+// and stores them permuted: the same final rows as the swaps one by one.
+__global__ void __launch_bounds__(256) zswap_trsm_kernel(double2* __restrict__ a, int lda, int nc, int k0, int w,
+                                                         const int* __restrict__ ipiv, const DevStatus* st) {
+  constexpr int kRows = 2 * kZpw;
+  __shared__ double2 Ls[kZpw * kZpw];  // Ls[r + k * kZpw] = l(k0 + r, k0 + k)
+  __shared__ int pos_s[kRows];         // the touched rows
+  __shared__ int src_s[kRows];         // the row whose entry ends at pos_s[q]
+  __shared__ int ns_s;
+  const int wv = valid_width(st, k0, w);
+  if (wv <= 0) return;
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    const int r = e % w, k = e / w;
+    Ls[r + k * kZpw] = a[k0 + r + (size_t)(k0 + k) * lda];
+  }
+  if (threadIdx.x == 0) {
+    int ns = w;
+    for (int q = 0; q < w; ++q) pos_s[q] = src_s[q] = k0 + q;
+    for (int j = k0; j < k0 + wv; ++j) {
+      const int jp = ipiv[j];  // jp >= j
+      if (jp == j) continue;
+      int qb = jp - k0;
+      if (jp >= k0 + w) {
+        qb = w;
+        while (qb < ns && pos_s[qb] != jp) ++qb;
+        if (qb == ns) {
+          pos_s[ns] = src_s[ns] = jp;
+          ++ns;
+        }
+      }
+      const int qa = j - k0, x = src_s[qa];
+      src_s[qa] = src_s[qb];
+      src_s[qb] = x;
+    }
+    ns_s = ns;
+  }
+  __syncthreads();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc - w) return;
+  const bool right = c >= k0;
+  if (right) c += w;  // past the block's own columns
+  double2* col = a + (size_t)c * lda;
+  const int ns = ns_s;
+  double2 v[kRows];
+#pragma unroll
+  for (int q = 0; q < kRows; ++q)
+    if (q < ns) v[q] = col[src_s[q]];
+  if (right) {
+#pragma unroll
+    for (int r = 1; r < kZpw; ++r) {
+      const int kend = min(r, wv);
+#pragma unroll
+      for (int k = 0; k < kZpw - 1; ++k)
+        if (r < w && k < kend) v[r] = zsub(v[r], zmul(Ls[r + k * kZpw], v[k]));
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kRows; ++q)
+    if (q < ns && (src_s[q] != pos_s[q] || (right && q > 0 && q < w))) col[pos_s[q]] = v[q];
+}
+
+// The trailing block, rows and columns from k0 + w: a CTA per 64 x 64 tile,
+// 256 threads with 4 x 4 entries each (rows tx + 16 i, columns ty + 16 j);
+// the block's 64 x wv slice of L and wv x 64 slice of U staged in shared
+// memory, each entry's terms taken in increasing k.
+__global__ void __launch_bounds__(256) zgemm_exact_kernel(double2* __restrict__ a, int lda, int m, int nc, int k0,
+                                                          int w, const DevStatus* st) {
+  __shared__ double2 As[kZpw][kZtile];  // As[k][r] = l(r0 + r, k0 + k)
+  __shared__ double2 Bs[kZpw][kZtile];  // Bs[k][c] = u(k0 + k, c0 + c)
+  const int wv = valid_width(st, k0, w);
+  if (wv <= 0) return;
+  const int r0 = k0 + w + blockIdx.x * kZtile, c0 = k0 + w + blockIdx.y * kZtile;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  const double2 zero = make_double2(0.0, 0.0);
+  for (int e = t; e < wv * kZtile; e += blockDim.x) {
+    const int r = e % kZtile, k = e / kZtile;  // rows fastest: contiguous in a column
+    As[k][r] = r0 + r < m ? a[r0 + r + (size_t)(k0 + k) * lda] : zero;
+  }
+  for (int e = t; e < wv * kZtile; e += blockDim.x) {
+    const int k = e % wv, cc = e / wv;  // the block's rows fastest: contiguous in a column
+    Bs[k][cc] = c0 + cc < nc ? a[k0 + k + (size_t)(c0 + cc) * lda] : zero;
+  }
+  __syncthreads();
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + tx + 16 * i, cc = c0 + ty + 16 * j;
+      acc[i][j] = (r < m && cc < nc) ? a[r + (size_t)cc * lda] : zero;
+    }
+  for (int k = 0; k < wv; ++k) {
+    double2 l[4], u[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) l[i] = As[k][tx + 16 * i];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) u[j] = Bs[k][ty + 16 * j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = zsub(acc[i][j], zmul(l[i], u[j]));
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + tx + 16 * i, cc = c0 + ty + 16 * j;
+      if (r < m && cc < nc) a[r + (size_t)cc * lda] = acc[i][j];
+    }
 }
 
 constexpr int kSolveThreads = 1024;
@@ -279,6 +488,29 @@ __global__ void __launch_bounds__(256) zgetri_swap_kernel(double2* __restrict__ 
 // Factorization of the m x nc device matrix (m >= nc), stream-ordered; a zero
 // pivot lands in the status block's singular_col.
 int zlu_factor_dev(alg_ctx* ctx, double2* d_a, int m, int nc, int lda, int* d_ipiv) {
+  // ALG_ZLU_UNBLOCKED=1 (measurement switch): one pivot and one rank-1
+  // launch per column instead of the blocked form; both give the same bits
+  static const bool unblocked = std::getenv("ALG_ZLU_UNBLOCKED") != nullptr;
+  if (!unblocked) {
+    for (int k0 = 0; k0 < nc; k0 += kZpw) {
+      const int w = std::min(kZpw, nc - k0);
+      zpanel_kernel<<<1, kZpanelThreads, 0, ctx->stream>>>(d_a, lda, m, k0, w, d_ipiv, ctx->d_status);
+      int launches = 1;
+      if (nc > w) {
+        zswap_trsm_kernel<<<(nc - w + 255) / 256, 256, 0, ctx->stream>>>(d_a, lda, nc, k0, w, d_ipiv, ctx->d_status);
+        ++launches;
+      }
+      const int rows = m - k0 - w, cols = nc - k0 - w;
+      if (rows > 0 && cols > 0) {
+        dim3 grid((rows + kZtile - 1) / kZtile, (cols + kZtile - 1) / kZtile);
+        zgemm_exact_kernel<<<grid, 256, 0, ctx->stream>>>(d_a, lda, m, nc, k0, w, ctx->d_status);
+        ++launches;
+      }
+      count_launches(launches);
+    }
+    ALG_CUDA_TRY(cudaGetLastError());
+    return ALG_OK;
+  }
   for (int j = 0; j < nc; ++j) {
     zpivot_kernel<<<1, kPivThreads, 0, ctx->stream>>>(d_a, lda, m, nc, j, d_ipiv, ctx->d_status);
     const int rows = m - j - 1, cols = nc - j - 1;

@@ -2,8 +2,9 @@
 zgetrf_rect, zgesv, zgetri) against the complex oracle: identical pivots and
 bit-identical factors and solutions (both run the reference's operations in
 the reference's order), on the reference's own test matrices, on sizes whose
-rows and columns exceed one CTA's threads, on pivot ties, on NaN entries, and
-on the partial state a zero pivot leaves."""
+rows and columns exceed one CTA's threads and span many 16-column blocks, on
+pivot ties, on NaN entries, and on the partial state a zero pivot leaves,
+inside a block and at its edges."""
 
 import numpy as np
 import pytest
@@ -126,6 +127,21 @@ def test_zero_pivot_leaves_the_reference_partial_state(gpu, oz):
     M[:2, :2] = [[2 + 1j, 0.5j], [1 - 1j, 3 + 0j]]
     M[:, 2] = M[:, 0] + M[:, 1]
     M[2:, 3:] = rng.standard_normal((3, 2)) + 1j * rng.standard_normal((3, 2))
+    assert _agrees(oz, M.T.ravel().copy(), n) == oz.SINGULAR
+
+
+@pytest.mark.parametrize("s", [15, 16, 17, 40, 250])
+def test_zero_pivot_at_and_past_block_edges(gpu, oz, s):
+    # rows s.. of columns 0..s zero: the pivots of the first s columns come
+    # from the rows above, and column s meets an exactly zero pivot. The
+    # factorization runs in 16-column blocks, so s = 15, 16, 17 stop at the
+    # last column of a block, the first of the next and the second; the
+    # columns right of the stopping block must hold exactly the updates of
+    # the steps before s, as the reference's early return leaves them.
+    n = 300
+    rng = np.random.default_rng(s)
+    M = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    M[s:, : s + 1] = 0
     assert _agrees(oz, M.T.ravel().copy(), n) == oz.SINGULAR
 
 
