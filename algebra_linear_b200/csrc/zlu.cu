@@ -13,16 +13,16 @@
 // Layout: a complex entry is a double2 (re, im), the interleaved layout of
 // the host's complex arrays; matrices column-major, a[i + j * lda].
 //
-// Factorization (complex.rs:67-124 zgetf2, 169-208 zgetrf_rect): one step per
-// column, as the reference's loop:
-//   zpivot_kernel   one CTA: the first row with the largest |Re| + |Im| at or
-//                   below the diagonal (the reference's strict-greater scan,
-//                   NaN included), the zero-pivot test, the whole-row swap,
-//                   the column below the pivot divided by it;
-//   zupdate_kernel  the rank-1 update a_ik -= l_i u_k of the trailing block.
-// Every entry therefore takes its terms in increasing column order, exactly
-// as in the reference. After a zero pivot both kernels do nothing, so the
-// matrix is left as the reference leaves it.
+// Factorization (complex.rs:67-124 zgetf2, 169-208 zgetrf_rect): blocked by
+// 16 columns (zpanel_kernel, zswap_trsm_kernel, zgemm_exact_kernel below),
+// every entry still taking its terms in increasing column order with each
+// operation rounded on its own, so the factors are the reference's bit for
+// bit. The pivot is the first row with the largest |Re| + |Im| at or below
+// the diagonal (the reference's strict-greater scan, NaN included); a zero
+// pivot stops the factorization with exactly the steps before it applied,
+// as the reference's early return leaves the matrix. The unblocked form
+// (zpivot_kernel + zupdate_kernel, one step per column) stays as a
+// measurement switch.
 //
 // Solve (complex.rs:279-312): the interchanges applied to b in order; the
 // unit-lower sweep as a column pipeline (one CTA; row i takes its term for
@@ -77,6 +77,8 @@ constexpr int kPivThreads = 1024;
 __device__ int zpick_pivot(const double2* __restrict__ col, int m, int j, int* __restrict__ ipiv, DevStatus* st,
                            double* sb, int* si, int* piv_s) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nt = blockDim.x;
+  // the diagonal's measure, loaded early by the thread that decides
+  const double vj = t == 0 ? zabs1(col[j]) : 0.0;
   // first maximum over this thread's rows below the diagonal; -1 means none
   double best = -1.0;
   int bi = INT_MAX;
@@ -110,7 +112,6 @@ __device__ int zpick_pivot(const double2* __restrict__ col, int m, int j, int* _
         gb = sb[w];
         gi = si[w];
       }
-    const double vj = zabs1(col[j]);
     int jp = j;
     double pbest = vj;
     if (gi != INT_MAX && gb > vj) {
@@ -200,52 +201,126 @@ __device__ __forceinline__ int valid_width(const DevStatus* st, int k0, int w) {
   return s == INT_MAX ? w : min(w, s - k0);
 }
 
+// The panel runs in sub-panels of kZsub columns, so that each step's rank-1
+// update touches at most kZsub - 1 columns: after a sub-panel's steps, the
+// block's columns right of it take that sub-panel's terms at once (its rows
+// of U by a unit-lower solve, a thread per column; the rows below by a rank
+// kZsub update, a thread per row, each entry's terms in increasing k), which
+// reads and writes the block about a third as often as a rank-1 update per
+// step. A zero pivot inside a sub-panel still lets the steps before it reach
+// the columns right of it, as the reference's loop has applied them.
+constexpr int kZsub = 4;
+
+// A shared-memory load the compiler keeps where it is written: the rank
+// update reads the same kZsub x 12 values of U for every row, and hoisted
+// out of the row loop they would not fit in registers.
+__device__ __forceinline__ double2 lds_f64x2(const double2* p) {
+  double2 r;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+               : "=d"(r.x), "=d"(r.y)
+               : "r"(static_cast<unsigned>(__cvta_generic_to_shared(p))));
+  return r;
+}
+
 __global__ void __launch_bounds__(kZpanelThreads) zpanel_kernel(double2* __restrict__ a, int lda, int m, int k0, int w,
                                                                 int* __restrict__ ipiv, DevStatus* st) {
   __shared__ double sb[kZpanelThreads / 32];
   __shared__ int si[kZpanelThreads / 32];
   __shared__ int piv_s;
   __shared__ double2 urow[kZpw];
+  __shared__ double2 usub[kZsub][kZpw];  // the sub-panel's rows of U right of it
   if (stopped(st)) return;
-  const int t = threadIdx.x;
-  for (int j = k0; j < k0 + w; ++j) {
-    double2* col = a + (size_t)j * lda;
-    const int jp = zpick_pivot(col, m, j, ipiv, st, sb, si, &piv_s);
-    if (jp < 0) return;
-    // the interchange within the block's columns; row j (the pivot row
-    // after it) kept for the updates
-    if (t < w) {
-      double2* c = a + (size_t)(k0 + t) * lda;
-      const double2 x = c[j];
-      if (jp != j) {
-        const double2 y = c[jp];
-        c[j] = y;
-        c[jp] = x;
-        urow[t] = y;
-      } else {
-        urow[t] = x;
+  const int t = threadIdx.x, kend = k0 + w;
+  for (int s0 = k0; s0 < kend; s0 += kZsub) {
+    const int s1 = min(s0 + kZsub, kend);
+    int jv = s1 - s0;  // the sub-panel's steps that ran
+#pragma unroll 1
+    for (int j = s0; j < s1; ++j) {
+      double2* col = a + (size_t)j * lda;
+      const int jp = zpick_pivot(col, m, j, ipiv, st, sb, si, &piv_s);
+      if (jp < 0) {  // the same for every thread (read from shared memory)
+        jv = j - s0;
+        break;
       }
-    }
-    __syncthreads();
-    const int jj = j - k0;
-    const double2 d = urow[jj];
-    for (int i = j + 1 + t; i < m; i += kZpanelThreads) {
-      // the multiplier first (the division is a call, and nothing may stay
-      // live across it), then the row's entries in the block's later
-      // columns loaded together before any store, so that their latencies
-      // overlap
-      const double2 l = zdiv(col[i], d);
-      col[i] = l;
-      double2* row = a + i + (size_t)k0 * lda;
-      double2 v[kZpw];
+      // the interchange within the block's columns; row j (the pivot row
+      // after it) kept for the updates
+      if (t < w) {
+        double2* c = a + (size_t)(k0 + t) * lda;
+        const double2 x = c[j];
+        if (jp != j) {
+          const double2 y = c[jp];
+          c[j] = y;
+          c[jp] = x;
+          urow[t] = y;
+        } else {
+          urow[t] = x;
+        }
+      }
+      __syncthreads();
+      const int jj = j - s0;
+      const double2 d = urow[j - k0];
+#pragma unroll 1
+      for (int i = j + 1 + t; i < m; i += kZpanelThreads) {
+        // the row's entries in the sub-panel's later columns loaded together
+        // with the one below the pivot, before any store
+        double2* row = a + i + (size_t)s0 * lda;
+        const double2 x = col[i];
+        double2 v[kZsub];
 #pragma unroll
-      for (int c = 1; c < kZpw; ++c)
-        if (c > jj && c < w) v[c] = row[(size_t)c * lda];
+        for (int c = 1; c < kZsub; ++c)
+          if (c > jj && s0 + c < s1) v[c] = row[(size_t)c * lda];
+        const double2 l = zdiv(x, d);
+        col[i] = l;
 #pragma unroll
-      for (int c = 1; c < kZpw; ++c)
-        if (c > jj && c < w) row[(size_t)c * lda] = zsub(v[c], zmul(l, urow[c]));
+        for (int c = 1; c < kZsub; ++c)
+          if (c > jj && s0 + c < s1) row[(size_t)c * lda] = zsub(v[c], zmul(l, urow[s0 - k0 + c]));
+      }
+      __syncthreads();  // column j + 1 is final below row j before its pivot search
     }
-    __syncthreads();  // column j + 1 is final below row j before its pivot search
+    const int nr = kend - s1;  // the block's columns right of the sub-panel
+    if (nr > 0 && jv > 0) {
+      if (t < nr) {
+        double2* c = a + (size_t)(s1 + t) * lda;
+        double2 v[kZsub];
+#pragma unroll
+        for (int r = 0; r < kZsub; ++r)
+          if (s0 + r < s1) v[r] = c[s0 + r];
+#pragma unroll
+        for (int r = 1; r < kZsub; ++r)
+#pragma unroll
+          for (int k = 0; k < kZsub - 1; ++k)
+            if (s0 + r < s1 && k < r && k < jv) v[r] = zsub(v[r], zmul(a[s0 + r + (size_t)(s0 + k) * lda], v[k]));
+#pragma unroll
+        for (int r = 0; r < kZsub; ++r)
+          if (s0 + r < s1) {
+            if (r > 0) c[s0 + r] = v[r];
+            usub[r][t] = v[r];
+          }
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int i = s1 + t; i < m; i += kZpanelThreads) {
+        double2 l[kZsub];
+#pragma unroll
+        for (int k = 0; k < kZsub; ++k)
+          if (k < jv) l[k] = a[i + (size_t)(s0 + k) * lda];
+        double2* row = a + i + (size_t)s1 * lda;
+        double2 v[kZpw - kZsub];
+#pragma unroll
+        for (int c = 0; c < kZpw - kZsub; ++c)
+          if (c < nr) v[c] = row[(size_t)c * lda];
+#pragma unroll
+        for (int c = 0; c < kZpw - kZsub; ++c)
+          if (c < nr) {
+#pragma unroll
+            for (int k = 0; k < kZsub; ++k)
+              if (k < jv) v[c] = zsub(v[c], zmul(l[k], lds_f64x2(&usub[k][c])));
+            row[(size_t)c * lda] = v[c];
+          }
+      }
+      __syncthreads();
+    }
+    if (jv < s1 - s0) return;  // stopped at a zero pivot
   }
 }
 
@@ -258,7 +333,9 @@ __global__ void __launch_bounds__(kZpanelThreads) zpanel_kernel(double2* __restr
 // first, then the rows below the block that a pivot came from, at most
 // 2 kZpw in all. Each thread then loads those entries of its column together
 // and stores them permuted: the same final rows as the swaps one by one.
-__global__ void __launch_bounds__(256) zswap_trsm_kernel(double2* __restrict__ a, int lda, int nc, int k0, int w,
+constexpr int kZswapThreads = 128;
+
+__global__ void __launch_bounds__(kZswapThreads) zswap_trsm_kernel(double2* __restrict__ a, int lda, int nc, int k0, int w,
                                                          const int* __restrict__ ipiv, const DevStatus* st) {
   constexpr int kRows = 2 * kZpw;
   __shared__ double2 Ls[kZpw * kZpw];  // Ls[r + k * kZpw] = l(k0 + r, k0 + k)
@@ -271,11 +348,14 @@ __global__ void __launch_bounds__(256) zswap_trsm_kernel(double2* __restrict__ a
     const int r = e % w, k = e / w;
     Ls[r + k * kZpw] = a[k0 + r + (size_t)(k0 + k) * lda];
   }
+  __shared__ int piv_s[kZpw];
+  if (threadIdx.x < wv) piv_s[threadIdx.x] = ipiv[k0 + threadIdx.x];
+  __syncthreads();
   if (threadIdx.x == 0) {
     int ns = w;
     for (int q = 0; q < w; ++q) pos_s[q] = src_s[q] = k0 + q;
     for (int j = k0; j < k0 + wv; ++j) {
-      const int jp = ipiv[j];  // jp >= j
+      const int jp = piv_s[j - k0];  // jp >= j
       if (jp == j) continue;
       int qb = jp - k0;
       if (jp >= k0 + w) {
@@ -497,7 +577,7 @@ int zlu_factor_dev(alg_ctx* ctx, double2* d_a, int m, int nc, int lda, int* d_ip
       zpanel_kernel<<<1, kZpanelThreads, 0, ctx->stream>>>(d_a, lda, m, k0, w, d_ipiv, ctx->d_status);
       int launches = 1;
       if (nc > w) {
-        zswap_trsm_kernel<<<(nc - w + 255) / 256, 256, 0, ctx->stream>>>(d_a, lda, nc, k0, w, d_ipiv, ctx->d_status);
+        zswap_trsm_kernel<<<(nc - w + kZswapThreads - 1) / kZswapThreads, kZswapThreads, 0, ctx->stream>>>(d_a, lda, nc, k0, w, d_ipiv, ctx->d_status);
         ++launches;
       }
       const int rows = m - k0 - w, cols = nc - k0 - w;

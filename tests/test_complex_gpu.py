@@ -145,6 +145,29 @@ def test_zero_pivot_at_and_past_block_edges(gpu, oz, s):
     assert _agrees(oz, M.T.ravel().copy(), n) == oz.SINGULAR
 
 
+def _exact_singular(n, s, seed):
+    """A = L U in exact dyadic arithmetic: unit-lower L whose entries have
+    |Re| + |Im| <= 1 (the diagonal pivot always wins, so no interchange), U
+    with a real power-of-two diagonal except u_ss = 0. Elimination then
+    reproduces L and U exactly and meets an exactly zero pivot at column s
+    after nonzero multipliers, so every column right of s must hold exactly
+    the terms of steps 0..s-1."""
+    rng = np.random.default_rng(seed)
+    entries = np.array([0, 0.5, -0.5, 0.5j, -0.5j, 0.25 + 0.25j, -0.25 + 0.5j, 0.75, -0.25j, 0.5 - 0.25j])
+    L = np.tril(rng.choice(entries, (n, n)), -1) + np.eye(n)
+    U = np.triu(rng.integers(-3, 4, (n, n)) + 1j * rng.integers(-3, 4, (n, n)), 1).astype(np.complex128)
+    U[np.arange(n), np.arange(n)] = rng.choice([1.0, 2.0, 4.0], n)
+    U[s, s] = 0
+    return (L @ U).T.ravel().copy()
+
+
+@pytest.mark.parametrize("s", [1, 2, 3, 5, 6, 13, 17, 21, 45, 130])
+def test_zero_pivot_after_nonzero_multipliers(gpu, oz, s):
+    # the blocked form runs 16-column blocks of 4-column sub-panels: s falls
+    # inside a sub-panel, at its edges, and in later blocks
+    assert _agrees(oz, _exact_singular(300, s, s), 300) == oz.SINGULAR
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 8, 100, 1030])
 def test_zgetri_is_bit_identical(gpu, oz, n):
     # complex.rs:463-486 / parity.rs:463-510: zgetrf then zgetri
