@@ -1229,6 +1229,46 @@ def c2_sweep(ctx, reg, A16, s1, steps, warmup, dev_index):
     return out
 
 
+def torch_lu_solve(A0, b0, n, nrhs):
+    """x (flat, column-major like b0) of A x = b through torch.linalg's LU
+    (cuSOLVER on a GPU tensor, LAPACK on a CPU one); A0 and b0 hold A and b
+    column-major, as the library's entry points take them."""
+    import torch
+
+    LU, piv = torch.linalg.lu_factor(A0.view(n, n).t())  # the .t() view is A, column-major
+    X = torch.linalg.lu_solve(LU, piv, b0.view(nrhs, n).t())
+    return X.t().contiguous().view(-1)
+
+
+def cusolver_context(A0, b0, n, nrhs, steps=2, warmup=1):
+    """cuSOLVER's getrf + getrs (through torch.linalg.lu_factor / lu_solve) on
+    the same A and b, device-timed: a library ceiling reported beside the
+    line for context, never part of this library's path. A failure is
+    recorded instead of ending the line."""
+    import torch
+
+    try:
+        torch.backends.cuda.preferred_linalg_library("cusolver")
+        times = []
+        for it in range(warmup + steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            x = torch_lu_solve(A0, b0, n, nrhs)
+            e1.record()
+            torch.cuda.synchronize()
+            if it >= warmup:
+                times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        eta = backward_error(A0, x, b0, n, nrhs)
+        del x
+        return {"library": "cuSOLVER getrf + getrs via torch.linalg.lu_factor / lu_solve (FP64)",
+                "ms_per_solve": ms, "gflops": flops_dgesv(n, nrhs) / (ms * 1e6), "backward_error": eta,
+                "steps": steps, "note": "context only: not this library's code"}
+    except Exception as e:  # noqa: BLE001 - the line must still print
+        return {"error": repr(e)[:200]}
+
+
 def sub_arm(fn, args, world, rank, local, pg):
     """Another workload's arm with its defaults, 3 timed steps after 2
     warm-ups and no CPU baseline, returned as a dict (without the fields the
@@ -1309,6 +1349,7 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_e2e:
         line["e2e"] = e2e_run(head, A0, b0, n, nrhs, steps=max(2, min(args.steps, 3)))
     if world == 1 and not args.no_sweep and not args.forms:
+        line["context_cusolver"] = cusolver_context(A0, b0, n, nrhs)
         line["c2_sweep"] = c2_sweep(ctx, reg, A0, s1, steps=3, warmup=2, dev_index=local)
         # the batched (20 000 systems) and sparse (48^3 grid, FP64) workloads,
         # each its own short run with its own e2e, in the same record

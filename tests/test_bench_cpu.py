@@ -1,7 +1,8 @@
 """Host-side pieces of bench.py, on the CPU: the workload generators match
 the configurations they name (C3 orders, C4 and C5 stencil sizes), the
-forward-error comparison between forms, and a failing sub-workload is
-recorded instead of ending the benchmark line."""
+forward-error comparison between forms, the library-context solve's
+reading of the column-major layout, and a failing sub-workload is recorded
+instead of ending the benchmark line."""
 
 import pathlib
 import sys
@@ -65,3 +66,20 @@ def test_a_failing_sub_workload_is_recorded():
         return {"metric": "m", "value": 1.0, "n_gpus": 1, "data": "d", "e2e": {"value": 2.0}}
 
     assert bench.sub_arm(ok, Args(), 1, 0, 0, None) == {"metric": "m", "value": 1.0, "e2e": {"value": 2.0}}
+
+
+def test_library_context_solve_reads_the_column_major_layout():
+    torch = pytest.importorskip("torch")
+    n, nrhs = 37, 3
+    g = torch.Generator().manual_seed(3)
+    A = torch.rand(n, n, generator=g, dtype=torch.float64) - 0.5  # A[i, j]
+    X = torch.rand(n, nrhs, generator=g, dtype=torch.float64)
+    B = A @ X
+    A0 = A.t().contiguous().view(-1)  # column-major: A0[i + j n] = A[i, j]
+    b0 = B.t().contiguous().view(-1)
+    x = bench.torch_lu_solve(A0, b0, n, nrhs)
+    assert bench.backward_error(A0, x, b0, n, nrhs) < 1e-14
+    assert torch.allclose(x.view(nrhs, n).t(), X, atol=1e-10)
+    # without a GPU the device-timed context records the failure instead of raising
+    if not torch.cuda.is_available():
+        assert "error" in bench.cusolver_context(A0, b0, n, nrhs)
