@@ -101,9 +101,26 @@ def dist_init(args):
         import torch.distributed as dist
 
         backend = "nccl" if args.impl == "ours" else "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        # the longest gap between two collectives of a replica is one form's
+        # warm-up or profiled steps (seconds); a rank that never arrives ends
+        # the others' wait with an error after this
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
         pg = dist
     return world, rank, local, pg
+
+
+def max_over_ranks(pg, x: float) -> float:
+    """The largest of every replica's x (a time: the whole job ends with its
+    slowest replica). A CUDA tensor on the current device under NCCL, a CPU
+    tensor under gloo; x itself with one process."""
+    if not pg:
+        return x
+    import torch
+
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
 
 
 # --------------------------------------------------------------------------- clocks
@@ -254,10 +271,8 @@ def run_form(name, spec, ctx, A0, b0, xt, n, nrhs, steps, warmup, pg, sample_clo
         sampler.__exit__()
     ms = e0.elapsed_time(e1)
     launches = lib.alg_kernel_launch_count() - launches0
+    ms = max_over_ranks(pg, ms)
     if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
         pg.barrier()
     eta = backward_error(A0, b, b0, n, nrhs)
     fwd = float((b - xt).abs().max() / xt.abs().max())
@@ -396,7 +411,10 @@ def roofline(res, form, peaks, gemm_peaks, cls=None):
     return out
 
 
-def e2e_run(form, A0, b0, n, nrhs, steps):
+def e2e_run(form, A0, b0, n, nrhs, steps, pg=None, world=1):
+    """The headline form through the host API, copies included, every
+    replica at once: the slowest replica's median step sets the whole job's
+    rate."""
     import numpy as np
     import torch
 
@@ -408,6 +426,8 @@ def e2e_run(form, A0, b0, n, nrhs, steps):
     hA = torch.empty_like(hA0).pin_memory()
     hb = torch.empty_like(hb0).pin_memory()
     times = []
+    if pg:
+        pg.barrier()
     for it in range(steps + 1):
         hA.copy_(hA0)
         hb.copy_(hb0)
@@ -424,10 +444,10 @@ def e2e_run(form, A0, b0, n, nrhs, steps):
             raise RuntimeError(f"e2e solve failed: {_lib.status_string(rc)}")
         if it > 0:
             times.append(dt)
-    t = statistics.median(times)
+    t = max_over_ranks(pg, statistics.median(times))
     h2d = 8 * n * n + 8 * n * nrhs
     d2h = 8 * n * nrhs + (0 if form.startswith("mixed") else 8 * n * n)
-    return {"value": flops_dgesv(n, nrhs) / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+    return {"value": flops_dgesv(n, nrhs) * world / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * t, "form": form, "steps": steps,
             "api": "alg_dgesv_ex" if not form.startswith("mixed") else "alg_dgesv_mixed"}
 
@@ -562,6 +582,8 @@ def run_sparse_complex(args, world, rank, local, pg):
     analyze_s = time.perf_counter() - t0
     b0 = np.ones(n, dtype=np.complex128) * (1 - 2j)
     times, x, v = [], None, v0
+    if pg:
+        pg.barrier()
     for it in range(args.warmup + args.steps):
         v = v0 * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, nnz)) + 1j * v0.imag * 0.01 * rng.uniform(-1.0, 1.0, nnz)
         x = b0.copy()
@@ -575,7 +597,7 @@ def run_sparse_complex(args, world, rank, local, pg):
 
     A = sps.csc_matrix((v, ri.astype(np.int64), cp.astype(np.int64)), shape=(n, n))
     eta = float(np.abs(b0 - A @ x).max() / (abs(A).sum(axis=1).max() * np.abs(x).max() + np.abs(b0).max()))
-    per = statistics.median(times)
+    per = max_over_ranks(pg, statistics.median(times))
     fl = 8.0 * st["flops_estimate"] + 8.0 * (st["nnz_l"] + st["nnz_u"])
     line = {
         "metric": "complex sparse LU refactorize+solve GFLOP/s (reference flop estimate, 8 flops per complex "
@@ -652,10 +674,7 @@ def run_sparse(args, world, rank, local, pg):
     ms = e0.elapsed_time(e1)
     launches = lib.alg_kernel_launch_count() - launches0
     x_last = b.clone()
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(pg, ms)
     # the per-kernel-class breakdown: separate profiled rounds (the events
     # around every launch stay out of the timed ones), per round
     psteps = max(1, min(args.steps, 2))
@@ -715,20 +734,22 @@ def run_sparse(args, world, rank, local, pg):
         "gpu_launches": int(launches), "clocks": sampler.summary(), "roofline": roof,
         "cublas_gemm_peaks_tflops": gemm_peaks,
     }
-    if not args.no_e2e and rank == 0:
+    if not args.no_e2e:
         lu_h = SparseLu.analyze(cp, ri, LuMethod.supernodal())
         lu_h.set_precision(args.sparse_precision)
         hv = [r.cpu().numpy() for r in rounds[-3:]]
         lu_h.factorize(cp, ri, hv[0])
         ts = []
+        if pg:
+            pg.barrier()
         for vv in hv:
             bh = np.ones(n)
             t0 = time.perf_counter()
             lu_h.factorize(cp, ri, vv)
             lu_h.solve(bh)
             ts.append(time.perf_counter() - t0)
-        t = statistics.median(ts)
-        line["e2e"] = {"value": fl_round / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * nnz + 8 * n,
+        t = max_over_ranks(pg, statistics.median(ts))
+        line["e2e"] = {"value": fl_round * world / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * nnz + 8 * n,
                        "d2h_bytes_per_step": 8 * n, "ms_per_step": 1e3 * t, "api": "alg_splu_factorize + alg_splu_solve"}
         lu_h.close()
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -877,10 +898,7 @@ def run_batched(args, world, rank, local, pg):
         ms = e0.elapsed_time(e1)
         kern_ms = sum(a.elapsed_time(b) for a, b in ek) / args.steps
         launches = lib.alg_kernel_launch_count() - launches0
-        if pg:
-            t = torch.tensor([ms], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(pg, ms)
         bad = int((info != 0).sum())
         eta = _batched_eta(A0, B, b0, groups)
         fwd = float(((B - xt).abs().max() / xt.abs().max()))
@@ -930,6 +948,8 @@ def run_batched(args, world, rank, local, pg):
         info = torch.zeros(plan64.count, dtype=torch.int32, device="cuda")
         pe = plan64 if head == "fp64" else batched.BatchPlan(ctx, orders, mixed=True)
         times = []
+        if pg:
+            pg.barrier()
         for it in range(4):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -940,7 +960,7 @@ def run_batched(args, world, rank, local, pg):
             torch.cuda.synchronize()
             if it > 0:
                 times.append(time.perf_counter() - t0)
-        t = statistics.median(times)
+        t = max_over_ranks(pg, statistics.median(times))
         line["e2e"] = {"value": plan64.count / t * world, "unit": "solves/s",
                        "h2d_bytes_per_step": 8 * (plan64.a_total + plan64.b_total),
                        "d2h_bytes_per_step": 8 * plan64.b_total, "ms_per_step": 1e3 * t,
@@ -1033,9 +1053,23 @@ def run_serve(args, world, rank, local, pg):
                 host_eta = max(host_eta, float(res / (np.abs(A_r).sum(axis=1).max() * np.abs(x_r).max()
                                                       + np.abs(r.b).max())))
             svc = np.array([r.service_ms for r in reqs])
+            if pg:
+                # replicas: every replica's requests in one distribution, the
+                # job's span from the first submission to the last completion
+                # (one host clock), the worst error of any replica
+                parts = [None] * world
+                pg.all_gather_object(parts, {"lat": lat, "kinds": kinds, "t0": t_first, "t1": t_last, "bad": bad,
+                                             "etas": etas, "host_eta": host_eta})
+                lat = np.concatenate([q["lat"] for q in parts])
+                all_kinds = np.concatenate([q["kinds"] for q in parts])
+                dense_lat, sparse_lat = lat[~all_kinds], lat[all_kinds]
+                span = (max(q["t1"] for q in parts) - min(q["t0"] for q in parts)) / 1e9
+                bad = sum(q["bad"] for q in parts)
+                etas = [e for q in parts for e in q["etas"]]
+                host_eta = max(q["host_eta"] for q in parts)
             results[f"{mode}@{rate:g}"] = {
-                "rate_offered": rate, "requests": args.requests, "failed": bad,
-                "solves_per_s": args.requests / span, "p50_ms": float(np.percentile(lat, 50)),
+                "rate_offered": rate * world, "requests": args.requests * world, "failed": bad,
+                "solves_per_s": args.requests * world / span, "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)),
                 "dense_p50_ms": float(np.percentile(dense_lat, 50)), "dense_p99_ms": float(np.percentile(dense_lat, 99)),
                 "sparse_p50_ms": float(np.percentile(sparse_lat, 50)) if sparse_lat.size else None,
@@ -1347,7 +1381,7 @@ def run_ours(args, world, rank, local, pg):
         "cublas_gemm_peaks_tflops": gemm_peaks,
     }
     if not args.no_e2e:
-        line["e2e"] = e2e_run(head, A0, b0, n, nrhs, steps=max(2, min(args.steps, 3)))
+        line["e2e"] = e2e_run(head, A0, b0, n, nrhs, steps=max(2, min(args.steps, 3)), pg=pg, world=world)
     if world == 1 and not args.no_sweep and not args.forms:
         line["context_cusolver"] = cusolver_context(A0, b0, n, nrhs)
         line["c2_sweep"] = c2_sweep(ctx, reg, A0, s1, steps=3, warmup=2, dev_index=local)
