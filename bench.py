@@ -406,7 +406,7 @@ def roofline(res, form, peaks, gemm_peaks, cls=None):
         out["traffic"] = ratio * rec["bytes"] / max(rec["launches"], 1)
     if cls == "panel":
         out["note"] = "latency-bound column chain (pivot search per column); bytes = the panel read and written once"
-        # per column of the leaf chain: what a latency-bound panel is judged by
+        # per column of the leaf chain: the measure of a latency-bound panel (HBM bytes say little)
         out["ns_per_column"] = 1e6 * rec["ms"] / max(rec["launches"], 1) / (32 if form.startswith("mixed") else 16)
     return out
 
