@@ -532,6 +532,108 @@ def grid_csc(nx: int, ny: int, nz: int):
     return np.cumsum(col_ptr).astype(np.uint64), r.astype(np.uint64), k
 
 
+def lattice_csc(m: int = 4):
+    """The matrix of the reference's own sparse benchmark (`bench_sparse_lu`,
+    src/sparse/faer/sparse_lu.rs:167-250): an m x m x m node lattice with
+    three dofs per node (node (i, j, k) owns columns 3 (i + m (j + m k)) + d),
+    every node coupled to itself and each node around it (up to 26) through a
+    full 3 x 3 block; rows sorted per column; off-diagonal values -1, the
+    diagonal 10 + the column's number of off-diagonals. m = 4: 192 dofs."""
+    import numpy as np
+
+    cp, ri = [0], []
+    for node in range(m**3):
+        i, j, k = node % m, (node // m) % m, node // (m * m)
+        near = sorted(ii + m * (jj + m * kk) for kk in range(k - 1, k + 2) for jj in range(j - 1, j + 2)
+                      for ii in range(i - 1, i + 2) if 0 <= ii < m and 0 <= jj < m and 0 <= kk < m)
+        rows = [3 * q + d for q in near for d in range(3)]
+        for _ in range(3):
+            ri.extend(rows)
+            cp.append(len(ri))
+    cp, ri = np.array(cp, np.uint64), np.array(ri, np.uint64)
+    n = len(cp) - 1
+    cols = np.repeat(np.arange(n), np.diff(cp).astype(np.int64))
+    diag = ri.astype(np.int64) == cols
+    off = np.bincount(cols[~diag], minlength=n).astype(np.float64)
+    v = np.where(diag, 10.0 + off[cols], -1.0)
+    return cp, ri, v
+
+
+def lattice_run(reps: int = 160):
+    """The reference's own sparse benchmark, timed as `bench_sparse_lu` times
+    it: the 192-dof lattice (lattice_csc(4)) analyzed once per method, then
+    `reps` factorizations and 10 reps solves of the same values through the
+    host API (values and b copied in, the solution out; wall clock around the
+    loop of synchronous calls), with the reference's published times on its
+    own machine and the oracle's restatement of the supernodal and simplicial
+    factorizations timed on one host core (the CPU baseline). A failure is
+    recorded instead of ending the line."""
+    import numpy as np
+
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+
+    try:
+        cp, ri, v = lattice_csc(4)
+        n, nnz = len(cp) - 1, len(ri)
+        cols = np.repeat(np.arange(n), np.diff(cp).astype(np.int64))
+        out = {"workload": "bench_sparse_lu (sparse_lu.rs:167-250): 4x4x4 lattice, 3 dofs per node, full 3x3 "
+                           "coupling blocks; analyze once, then factorize and solve the same values repeatedly",
+               "n": n, "nnz": nnz, "reps": reps}
+        syms = {}
+        for label, method in (("simplicial", LuMethod.simplicial()), ("auto", LuMethod.auto())):
+            lu = SparseLu.analyze(cp, ri, method)
+            lu.factorize(cp, ri, v)
+            st = lu.stats()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                lu.factorize(cp, ri, v)
+            per_f = (time.perf_counter() - t0) / reps
+            b = np.ones(n)
+            lu.solve(b)
+            t0 = time.perf_counter()
+            for _ in range(10 * reps):
+                b.fill(1.0)
+                lu.solve(b)
+            per_s = (time.perf_counter() - t0) / (10 * reps)
+            ax = np.bincount(ri.astype(np.int64), weights=v * b[cols], minlength=n)
+            anorm = np.bincount(ri.astype(np.int64), weights=np.abs(v), minlength=n).max()
+            eta = float(np.abs(1.0 - ax).max() / (anorm * np.abs(b).max() + 1.0))
+            out[label] = {"method": lu.effective_method(), "factorize_ms": 1e3 * per_f, "solve_us": 1e6 * per_s,
+                          "fill_ratio": st["fill_ratio"], "nnz_l": st["nnz_l"], "nnz_u": st["nnz_u"],
+                          "backward_error": eta}
+            syms[label] = lu.symbolic()
+            lu.close()
+        out["reference_published"] = {
+            "simplicial_factorize_ms": 1.248, "supernodal_factorize_ms": 0.604, "fill_ratio": 2.96,
+            "machine": "Intel i9-13900KF, one core", "source": "README.md:119-120, src/sparse/faer/solver.rs:21-25"}
+        out["cpu_baseline"] = lattice_cpu_baseline(cp, ri, v, syms, reps)
+        return out
+    except Exception as e:  # noqa: BLE001 - the line must still print
+        return {"error": repr(e)[:200]}
+
+
+def lattice_cpu_baseline(cp, ri, v, syms, reps):
+    """The oracle's simplicial and supernodal factorizations of the lattice
+    (restatements of lu.rs:209-327 and supernodal_lu.rs:145-480) on one host
+    core, reps times each: ms per factorization."""
+    from oracle import sparse as osp
+
+    n = len(cp) - 1
+    out = {"unit": "ms per factorize", "cores": 1, "kind": "port"}
+    with _OneCore() as pin:
+        for label, snp in (("simplicial", None), ("auto", syms["auto"]["supernode_ptr"])):
+            sym = syms[label]
+            osp.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], snp)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                osp.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], snp)
+            out[f"{label}_factorize_ms"] = 1e3 * (time.perf_counter() - t0) / reps
+    out["sample"] = (f"{reps} factorizations of the lattice per method by the oracle's C++ restatement (the "
+                     "reference crate cannot be built here)")
+    out.update(pin.info())
+    return out
+
+
 def sparse_cpu_baseline(side: int):
     """The oracle (C++ restatement of the reference's supernodal LU,
     supernodal_lu.rs) on one host core: one factorize + solve of the
@@ -1389,6 +1491,8 @@ def run_ours(args, world, rank, local, pg):
         # each its own short run with its own e2e, in the same record
         line["c3_batched"] = sub_arm(run_batched, args, world, rank, local, pg)
         line["c4_sparse"] = sub_arm(run_sparse, args, world, rank, local, pg)
+        # the reference's own sparse benchmark matrix (192 dofs), beside its published times
+        line["bench_sparse_lu"] = lattice_run()
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(n)
     if rank == 0:

@@ -83,3 +83,73 @@ def test_library_context_solve_reads_the_column_major_layout():
     # without a GPU the device-timed context records the failure instead of raising
     if not torch.cuda.is_available():
         assert "error" in bench.cusolver_context(A0, b0, n, nrhs)
+
+
+def _reference_lattice(m):
+    """The loops of bench_sparse_lu (src/sparse/faer/sparse_lu.rs:176-218) as
+    they are written there: k outer, i inner, three columns per node, the
+    27 surrounding nodes' three rows each, sorted; values -1 off the diagonal
+    and 10 + (off-diagonal count) on it."""
+    node = lambda i, j, k: (k * m * m + j * m + i) * 3  # noqa: E731
+    cp, ri = [0], []
+    for k in range(m):
+        for j in range(m):
+            for i in range(m):
+                for _ in range(3):
+                    rows = []
+                    for dk in range(3):
+                        for dj in range(3):
+                            for di in range(3):
+                                ii, jj, kk = i + di - 1, j + dj - 1, k + dk - 1
+                                if min(ii, jj, kk) < 0 or max(ii, jj, kk) >= m:
+                                    continue
+                                base = node(ii, jj, kk)
+                                rows += [base, base + 1, base + 2]
+                    rows.sort()
+                    ri += rows
+                    cp.append(len(ri))
+    v = []
+    for c in range(len(cp) - 1):
+        off = sum(1 for p in range(cp[c], cp[c + 1]) if ri[p] != c)
+        v += [10.0 + off if ri[p] == c else -1.0 for p in range(cp[c], cp[c + 1])]
+    return cp, ri, v
+
+
+def test_lattice_is_the_reference_benchmark_matrix():
+    cp, ri, v = bench.lattice_csc(4)
+    rcp, rri, rv = _reference_lattice(4)
+    assert cp.tolist() == rcp and ri.tolist() == rri and v.tolist() == rv
+    assert len(cp) - 1 == 192
+
+
+def test_lattice_fill_is_the_published_one(oracle):
+    """README.md:119 and solver.rs:21-25 report fill 2.96 for this matrix:
+    the host analysis (COLAMD order, supernodes) and the oracle's simplicial
+    and supernodal factorizations over it reproduce it, and Auto picks the
+    supernodal method, as the README's second row has it."""
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+    from oracle import sparse as osp
+
+    cp, ri, v = bench.lattice_csc(4)
+    n = len(cp) - 1
+    auto = SparseLu.analyze(cp, ri, LuMethod.auto())
+    assert auto.effective_method() == "Supernodal" and auto.flop_ratio() > 40.0
+    for method in (LuMethod.simplicial(), LuMethod.supernodal()):
+        sym = SparseLu.analyze(cp, ri, method).symbolic()
+        snp = sym["supernode_ptr"] if method.kind == LuMethod.supernodal().kind else None
+        f = osp.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"], snp)
+        assert f.status == 0
+        assert round((f.nnz_l + f.nnz_u) / len(ri), 2) == 2.96
+        x = f.solve(np.ones(n))
+        A = np.zeros((n, n))
+        A[ri.astype(np.int64), np.repeat(np.arange(n), np.diff(cp).astype(np.int64))] = v
+        assert np.max(np.abs(A @ x - 1.0)) < 1e-13
+
+
+def test_lattice_run_records_a_failure_instead_of_raising():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the GPU run measures it")
+    out = bench.lattice_run(reps=2)
+    assert set(out) == {"error"} and "device" in out["error"].lower()
