@@ -449,3 +449,54 @@ def test_complex_oracle_on_real_values_follows_the_real_oracle(oracle_sparse):
         np.testing.assert_allclose(fz.l_val[:fz.nnz_l].real, fr.l_val[:fr.nnz_l], rtol=1e-12, atol=1e-15)
         np.testing.assert_allclose(fz.u_val[:fz.nnz_u].real, fr.u_val[:fr.nnz_u], rtol=1e-12, atol=1e-15)
         assert not np.any(fz.l_val[:fz.nnz_l].imag) and not np.any(fz.u_val[:fz.nnz_u].imag)
+
+
+def test_oracle_solves_the_reference_structured_patterns(oracle_sparse):
+    """supernodal_lu.rs:686-706 (solve_both, :671-684): the simplicial and
+    supernodal restatements agree to 1e-9 on the 2 x 2 example, tridiagonal,
+    arrow and grid patterns with 5 on the diagonal and 1 off it."""
+    import sparse_patterns as sp
+
+    cases = [(2, ([0, 2, 4], [0, 1, 0, 1]), np.array([4.0, 1.0, 1.0, 3.0]), np.array([1.0, 2.0]))]
+    for n, (cp, ri) in sp.STRUCTURED:
+        cases.append((n, (cp, ri), sp.diagonal_values(cp, ri, 5.0, 1.0), 1.0 + np.arange(n)))
+    for n, (cp, ri), v, b in cases:
+        fs, _ = _simplicial(oracle_sparse, cp, ri, v)
+        fn = _oracle_factors(oracle_sparse, cp, ri, v)
+        assert fs.status == 0 and fn.status == 0
+        assert sp.close(fn.solve(b), fs.solve(b), 1e-9), n
+
+
+def test_oracle_reconstructs_the_reference_patterns(oracle_sparse):
+    """supernodal_lu.rs:708-741: P A Q = L U within 1e-10 on tridiag(6),
+    arrow(7) and the 3 x 4 grid."""
+    import sparse_patterns as sp
+
+    for n, (cp, ri) in [(6, sp.tridiag(6)), (7, sp.arrow(7)), (12, sp.grid(3, 4))]:
+        v = sp.diagonal_values(cp, ri, 5.0, 1.0)
+        f = _oracle_factors(oracle_sparse, cp, ri, v)
+        assert f.status == 0
+        L, U = _lu_dense(f)
+        col_perm = SparseLu.analyze(cp, ri, LuMethod.supernodal()).symbolic()["col_perm"]
+        PAQ = sp.dense(cp, ri, v)[f.row_perm.astype(int)][:, col_perm]
+        assert np.max(np.abs(L @ U - PAQ)) < 1e-10, n
+
+
+def test_oracle_solves_the_reference_random_system(oracle_sparse):
+    """supernodal_lu.rs:744-763: the diagonally dominant system of the tests'
+    LCG (n = 16, seed 0x1234_5678), x = (i mod 7) - 3: both restatements
+    agree to 1e-9 and the supernodal one recovers x to 1e-9; and the 1 x 1
+    system [2] x = [6] gives 3 (supernodal_lu.rs:839-852)."""
+    import sparse_patterns as sp
+
+    n = 16
+    cp, ri, v = sp.diagonally_dominant(n, 0x1234_5678)
+    assert cp[-1] == len(ri) == len(v) and all(any(ri[k] == j for k in range(cp[j], cp[j + 1])) for j in range(n))
+    x = (np.arange(n) % 7) - 3.0
+    b = sp.dense(cp, ri, v) @ x
+    fs, _ = _simplicial(oracle_sparse, cp, ri, v)
+    fn = _oracle_factors(oracle_sparse, cp, ri, v)
+    xn = fn.solve(b)
+    assert sp.close(xn, fs.solve(b), 1e-9) and sp.close(xn, x, 1e-9)
+    f1 = _oracle_factors(oracle_sparse, [0, 1], [0], np.array([2.0]))
+    assert abs(f1.solve([6.0])[0] - 3.0) < 1e-14

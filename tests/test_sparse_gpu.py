@@ -273,3 +273,37 @@ def test_reference_benchmark_lattice_matches_the_oracle(gpu, osp, method):
     x2 = b.copy()
     lu.solve(x2)
     assert np.array_equal(x2, x)
+
+
+@pytest.mark.parametrize("method", ["simplicial", "supernodal"])
+def test_reference_structured_patterns_and_random_system(gpu, osp, method):
+    """The reference's own small supernodal tests through the GPU path:
+    solves_structured_patterns (supernodal_lu.rs:691-706: tridiagonal,
+    arrow and grid patterns, 5 on the diagonal and 1 off it, b = 1 + i),
+    solves_a_random_diagonally_dominant_system (:744-763: the tests' LCG,
+    n = 16, x = (i mod 7) - 3, recovered to 1e-9) and handles_zero_and_one
+    (:839-852: [2] x = [6] gives 3); every solution within 1e-12 relative of
+    the oracle's and the oracle's pivots, under both methods."""
+    import sparse_patterns as sp
+
+    m = LuMethod.simplicial() if method == "simplicial" else LuMethod.supernodal()
+    cases = [(cp, ri, sp.diagonal_values(cp, ri, 5.0, 1.0), 1.0 + np.arange(n), None) for n, (cp, ri) in sp.STRUCTURED]
+    cp, ri, v = sp.diagonally_dominant(16, 0x1234_5678)
+    x_true = (np.arange(16) % 7) - 3.0
+    cases.append((cp, ri, v, sp.dense(cp, ri, v) @ x_true, x_true))
+    cases.append(([0, 1], [0], np.array([2.0]), np.array([6.0]), np.array([3.0])))
+    for cp, ri, v, b, want in cases:
+        n = len(cp) - 1
+        lu = SparseLu.analyze(cp, ri, m)
+        lu.factorize(cp, ri, v)
+        sym = lu.symbolic()
+        ref = osp.Factors(n, cp, ri, v, sym["col_perm"], sym["col_perm_inv"],
+                          None if method == "simplicial" else sym["supernode_ptr"])
+        assert ref.status == 0
+        assert np.array_equal(lu.row_perm(), ref.row_perm.astype(np.int64)), n
+        x = b.copy()
+        lu.solve(x)
+        xr = ref.solve(b)
+        assert np.max(np.abs(x - xr) / np.maximum(np.abs(xr), 1.0)) <= 1e-12, n
+        if want is not None:
+            assert sp.close(x, want, 1e-9), n
