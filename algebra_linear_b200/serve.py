@@ -57,12 +57,24 @@ class Request:
 
     @classmethod
     def dense(cls, a, b, mixed=False) -> "Request":
+        """A x = b, a column-major n x n with n = len(b). The loop reads n^2
+        entries of a and n of b from these host arrays, so their lengths are
+        checked here (the C ABI cannot see them)."""
         b = _f64(b)
+        if np.size(a) != b.size * b.size:
+            raise ValueError(f"a holds {np.size(a)} entries, an n x n matrix with n = len(b) = {b.size} needs "
+                             f"{b.size * b.size}")
         return cls(DENSE, b.size, b, a=a, mixed=mixed)
 
     @classmethod
     def sparse(cls, pattern, values, b) -> "Request":
+        """Refactorize the analyzed `pattern` (a SparseLu) with `values` (one
+        per entry of its pattern) and solve for b (length n); both lengths
+        are checked here, as the loop reads that many entries."""
         b = _f64(b)
+        if b.size != pattern.n or np.size(values) != pattern.nnz:
+            raise ValueError(f"the pattern has n = {pattern.n} and {pattern.nnz} entries; got len(b) = {b.size} "
+                             f"and {np.size(values)} values")
         return cls(SPARSE, b.size, b, values=values, pattern=pattern)
 
     @property

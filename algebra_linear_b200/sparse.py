@@ -108,10 +108,11 @@ def _idx(a) -> np.ndarray:
 class SparseLu:
     """Opaque sparse LU handle (sparse_lu.rs:45-156)."""
 
-    def __init__(self, handle, n: int):
+    def __init__(self, handle, n: int, nnz: int):
         self._lib = _lib.load()
         self._h = handle
         self.n = n
+        self.nnz = nnz  # the analyzed pattern's entries: every values array has this length
 
     @classmethod
     def analyze(cls, col_ptr, row_idx, method: LuMethod = LuMethod()) -> "SparseLu":
@@ -121,7 +122,7 @@ class SparseLu:
         _check(lib.alg_splu_analyze(cp.ctypes.data if cp.size else None, cp.size,
                                     ri.ctypes.data if ri.size else None, ri.size, method.kind,
                                     method.flop_ratio_threshold, C.byref(h)))
-        return cls(h, cp.size - 1)
+        return cls(h, cp.size - 1, ri.size)
 
     def factorize(self, col_ptr, row_idx, values) -> None:
         cp, ri = _idx(col_ptr), _idx(row_idx)
