@@ -23,6 +23,12 @@ def _check(rc: int) -> None:
         raise LapackError(_KINDS.get(rc, _lib.status_string(rc)), rc)
 
 
+def _dev_tensor(t, dtype, numel: int, name: str) -> None:
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and t.is_contiguous()
+            and t.numel() >= numel):
+        raise TypeError(f"{name} must be a contiguous {dtype} CUDA tensor with >= {numel} entries")
+
+
 class BatchPlan:
     def __init__(self, ctx, orders, mixed: bool = False):
         self._lib = _lib.load()
@@ -40,6 +46,19 @@ class BatchPlan:
         ctx.adopt(self)
         self.a_total = int((self.orders.astype(np.int64) ** 2).sum())
         self.b_total = int(self.orders.sum())
+        # the packed arrays must reach the end of the last system at its offset
+        n64 = self.orders.astype(np.int64)
+        self._a_need = int((self.a_off[: self.count] + n64 * n64).max()) if self.count else 0
+        self._b_need = int((self.b_off[: self.count] + n64).max()) if self.count else 0
+
+    def _check_operands(self, a, b, info):
+        """The kernels read and write the packed systems through raw device
+        pointers: the tensors must be contiguous CUDA tensors of the right
+        type that reach every system, or the launch would touch memory past
+        them."""
+        _dev_tensor(a, torch.float64, self._a_need, "a")
+        _dev_tensor(b, torch.float64, self._b_need, "b")
+        _dev_tensor(info, torch.int32, self.count, "info")
 
     def close(self):
         if self.handle:
@@ -53,6 +72,7 @@ class BatchPlan:
             pass
 
     def solve(self, a: torch.Tensor, b: torch.Tensor, info: torch.Tensor, graph: bool = False):
+        self._check_operands(a, b, info)
         fn = self._lib.alg_batch_solve_graph if graph else self._lib.alg_batch_solve
         _check(fn(self.handle, a.data_ptr(), b.data_ptr(), info.data_ptr()))
 
@@ -78,6 +98,8 @@ class BatchPlan:
                 out = self.info()
                 out["tuned"] = "cache"
                 return out
+        self._check_operands(a, b, info)
+        self._check_operands(a_src, b_src, info)
         th = np.zeros(8, dtype=np.int32)
         _check(self._lib.alg_batch_autotune(self.handle, a.data_ptr(), b.data_ptr(), info.data_ptr(),
                                             a_src.data_ptr(), b_src.data_ptr(), th.ctypes.data))

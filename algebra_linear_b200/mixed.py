@@ -58,6 +58,10 @@ def _check(rc: int) -> None:
 
 def dgesv_mixed_dev(ctx, A, b, n: int, nrhs: int = 1, precision: str = "fp32", **kw) -> dict:
     """A (n*n float64 CUDA tensor, column-major) is read; b (n*nrhs) becomes x."""
+    from .device import _dev_f64
+
+    _dev_f64(A, n * n, "A")
+    _dev_f64(b, n * nrhs, "b")
     o = opts(precision, **kw)
     rep = Report()
     _check(_lib.load().alg_dgesv_mixed_dev(ctx.handle, C.byref(o), A.data_ptr(), n, n, b.data_ptr(), nrhs, n,
