@@ -105,6 +105,14 @@ def _idx(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint64)
 
 
+def _dev_f64(t, numel: int, name: str) -> None:
+    import torch
+
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+            and t.numel() >= numel):
+        raise TypeError(f"{name} must be a contiguous float64 CUDA tensor with >= {numel} entries")
+
+
 class SparseLu:
     """Opaque sparse LU handle (sparse_lu.rs:45-156)."""
 
@@ -202,9 +210,14 @@ class SparseLu:
         ctx.adopt(self)
 
     def factorize_dev(self, values) -> None:
+        """values: the pattern's nnz entries, a float64 CUDA tensor (read
+        through a raw device pointer, so its reach is checked here)."""
+        _dev_f64(values, self.nnz, "values")
         _check(self._lib.alg_splu_factorize_dev(self._h, _lib.ptr(values)))
 
     def solve_dev(self, b) -> None:
+        """b (n entries, a float64 CUDA tensor) becomes x."""
+        _dev_f64(b, self.n, "b")
         _check(self._lib.alg_splu_solve_dev(self._h, _lib.ptr(b)))
 
     def close(self) -> None:

@@ -41,3 +41,13 @@ def test_mixed_device_solve_checks_before_launching():
         mixed.dgesv_mixed_dev(ctx, torch.zeros(n * n, dtype=torch.float64), torch.zeros(n, dtype=torch.float64), n)
     with pytest.raises(TypeError, match="A must be"):
         mixed.dgesv_mixed_dev(ctx, torch.zeros(n * n, dtype=torch.float32), torch.zeros(n, dtype=torch.float64), n)
+
+
+def test_sparse_device_calls_check_before_launching():
+    from algebra_linear_b200.sparse import LuMethod, SparseLu
+
+    lu = SparseLu.analyze([0, 2, 4], [0, 1, 0, 1], LuMethod.supernodal())
+    with pytest.raises(TypeError, match="values must be"):
+        lu.factorize_dev(torch.tensor([4.0, 1.0, 1.0, 3.0], dtype=torch.float64))  # a host tensor
+    with pytest.raises(TypeError, match="b must be"):
+        lu.solve_dev(torch.ones(2, dtype=torch.float64))
