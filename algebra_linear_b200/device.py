@@ -78,6 +78,8 @@ class Context:
 
     def larnv(self, dist: int, seed, n: int, out: torch.Tensor | None = None):
         """The reference's DLARNV stream on the device; returns (x, seed_after)."""
+        if out is not None:
+            _dev_f64(out, n, "out")
         x = out if out is not None else torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
         s_in = (C.c_uint32 * 4)(*seed)
         s_out = (C.c_uint32 * 4)()
@@ -95,6 +97,8 @@ class Context:
     def dgetrs(self, lu: torch.Tensor, perm: torch.Tensor, b: torch.Tensor, n: int, nrhs: int = 1):
         _dev_f64(lu, n * n, "lu")
         _dev_f64(b, n * nrhs, "b")
+        if not (perm.is_cuda and perm.dtype == torch.int32 and perm.is_contiguous() and perm.numel() >= n):
+            raise TypeError(f"perm must be a contiguous int32 CUDA tensor with >= {n} entries")
         _check(self._lib.alg_dgetrs_dev(self.handle, lu.data_ptr(), n, n, perm.data_ptr(), b.data_ptr(), nrhs, n))
 
     def dgesv(self, a: torch.Tensor, b: torch.Tensor, n: int, nrhs: int = 1, update: int = _lib.UPDATE_EXACT):
