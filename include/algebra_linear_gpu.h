@@ -367,7 +367,10 @@ int alg_splu_analyze(const size_t* col_ptr, size_t col_ptr_len, const size_t* ro
 /* SparseLu::factorize (sparse_lu.rs:91-121): CSC view errors, then
  * ALG_SP_STRUCTURE_MISMATCH (order, nnz and FNV-1a fingerprint),
  * ALG_SP_NOT_FINITE, ALG_SP_SINGULAR. Synchronises. On failure the previous
- * factors and statistics stay in place. */
+ * factors and statistics stay in place. The first factorization places the
+ * handle's factors on the device current at that call (or on the device of
+ * the context given to alg_splu_set_ctx); later calls on the handle are made
+ * with that device current. */
 int alg_splu_factorize(alg_splu* lu, const size_t* col_ptr, size_t col_ptr_len, const size_t* row_idx,
                        size_t row_idx_len, const double* values, size_t values_len);
 /* SparseLu::solve (sparse_lu.rs:125-130): ALG_SP_NOT_FACTORIZED before a
